@@ -1,0 +1,89 @@
+"""The CPU oracle against the golden fixtures produced by the unmodified reference."""
+import numpy as np
+import pytest
+from scipy.interpolate import CubicSpline
+
+from oracle import pm3d_oracle as O
+from oracle.recipe_oracle import recipe_ic
+
+RTOL = 1e-11
+
+
+def rel(a, b):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def yoo_spline():
+    # The 'yoo' profile of pbhgr/pbhgr/profiles.py:52-53 with clamped ends (:60).
+    r = np.linspace(0.0, 40.0, 4001)
+    return CubicSpline(r, np.exp(-r ** 2 / 6), bc_type=((1, 0.0), (1, 0.0)))
+
+
+def test_mesh_ops_match_reference(golden):
+    g = golden("mesh_8")
+    m = g["meta"]
+    dx = m["L"] / m["N"]
+    assert rel(O.deposit(g["X"], m["N"], dx), g["rho"]) < 1e-14
+    assert rel(O.interp(g["F"], g["X"], m["N"], dx), g["Fi"]) < 1e-14
+    # mass: every particle deposits exactly unit weight
+    assert abs(g["rho"].sum() - len(g["X"])) < 1e-9
+
+
+@pytest.mark.parametrize("case", ["zeta_16", "zeta_16_np8_smooth"])
+def test_make_ic_forces_steps_match_reference(golden, case):
+    g = golden(case)
+    m = g["meta"]
+    mesh = O.Mesh(m["N"], m["L"], m["Np"], m["smooth"])
+    rng = np.random.default_rng(m["seed"])
+    ic = O.zeta_ic(mesh, rng, m["mu"], yoo_spline(), m["e"], m["p"], m["tail"], (2.0, 10.0))
+    assert rel(ic["x"], g["x0"]) < RTOL
+    assert rel(ic["p"], g["p0"]) < RTOL
+    assert rel(ic["delta_lin"], g["delta_lin"]) < RTOL
+    assert rel(ic["r_ell_q"], g["r_ell_q"]) < RTOL
+    assert abs(ic["tail_rms_grid"] - m["tail_rms_grid"]) <= 1e-12 * max(1.0, m["tail_rms_grid"])
+    acc, delta = O.accelerations(mesh, g["x0"], 1.0)
+    assert rel(acc, g["acc0"]) < RTOL
+    assert rel(delta, g["delta0"]) < RTOL
+    tr = O.Trajectory(mesh, g["x0"], g["p0"])
+    a = 1.0
+    for da in g["das"]:
+        a, delta = tr.step(a, da)
+    assert abs(a - m["a_end"]) < 1e-14
+    assert rel(tr.x, g["x_end"]) < RTOL
+    assert rel(tr.p, g["p_end"]) < RTOL
+    assert rel(delta, g["delta_end"]) < RTOL
+    assert rel(tr.acc, g["acc_end"]) < RTOL
+    d = O.analyse(mesh, tr.x, g["r_ell_q"], a, order=g["ref_order30"])
+    for k, v in m["analyse"].items():
+        assert np.allclose(d[k], v, rtol=1e-9, atol=1e-12), k
+
+
+def test_recipe_trajectory_matches_reference(golden):
+    g = golden("recipe_16")
+    m = g["meta"]
+    mesh = O.Mesh(m["N"], 1.0, m["Np"])
+    ic = recipe_ic(mesh, m["R"], m["delta0"], m["noise_frac"], m["seed"])
+    assert rel(ic["x"], g["x0"]) < 1e-14
+    tr = O.Trajectory(mesh, g["x0"], g["p0"])
+    a, fac = 1.0, 100.0 ** (1.0 / 100.0) - 1.0
+    for s in range(1, m["steps"] + 1):
+        a, delta = tr.step(a, a * fac)
+        if f"x_{s}" in g:
+            assert rel(tr.x, g[f"x_{s}"]) < RTOL
+            assert rel(tr.p, g[f"p_{s}"]) < RTOL
+            assert rel(delta, g[f"delta_{s}"]) < RTOL
+
+
+def test_momentum_and_mass_invariants(golden):
+    # pm3d conserves total momentum to round-off and deposits exactly Np^3.
+    g = golden("recipe_16")
+    m = g["meta"]
+    mesh = O.Mesh(m["N"], 1.0, m["Np"])
+    tr = O.Trajectory(mesh, g["x0"], g["p0"])
+    P0 = tr.p.sum(axis=0)
+    a = 1.0
+    for _ in range(5):
+        a, delta = tr.step(a, 0.05 * a)
+    assert np.all(np.abs(tr.p.sum(axis=0) - P0) < 1e-12 * np.abs(tr.p).sum())
+    assert abs(O.deposit(tr.x, m["N"], mesh.dx).sum() - m["Np"] ** 3) < 1e-8
