@@ -1,0 +1,152 @@
+/* pmb200 -- C ABI of the B200 particle-mesh engine for the pm3d hot path.
+ *
+ * The reference path (uniquehuman/pbh, pbhgr/pbhgr/pm3d.py) is a pure-numpy Python class with
+ * no FFI of its own; its plugin surface is the PM3D class (pm3d.py:26-129).  This header is
+ * the native boundary underneath the drop-in Python class pbh_b200.pm3d.PM3D, and follows the
+ * reference repository's own ctypes convention for native code (pbhgr/csrc/kernels.c:36,73
+ * loaded by pbhgr/pbhgr/spherical_ev.py:59-78): plain extern "C" functions, caller-owned
+ * contiguous buffers, an int return code.
+ *
+ * Conventions
+ *  - All array pointers are DEVICE pointers on the engine's device unless stated otherwise.
+ *  - Positions/momenta are (n, 3) float64 in lattice order: row i is the particle that
+ *    starts at lattice site i of PM3D's quiet start (pm3d.py:64-65), as PM3D.x / PM3D.p.
+ *  - Meshes are (N, N, N) C-order arrays, node (i, j, k) at ((i, j, k) + 1/2) dx (pm3d.py:42).
+ *  - Return value: 0 = OK; > 0 = number of flagged items (status words); < 0 = error:
+ *    -1..-999 = -(cudaError_t), -1000 - r = cuFFT result r, -2000 - k = invalid argument k.
+ *  - Calls are asynchronous on the engine's stream except those that return host data, which
+ *    synchronize it.  Use pm_engine_sync before reading device outputs from another stream.
+ *  - One host thread drives an engine at a time.
+ */
+#ifndef PMB200_H
+#define PMB200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct pm_engine pm_engine;
+
+/* One peak (one PM3D instance): PM3D(N, L, Np, seed, smooth) of pm3d.py:27. */
+typedef struct {
+  int N;          /* mesh side, power of two, 8..1024 */
+  int Np;         /* particles per side (n = Np^3) */
+  int tile;       /* deposit/push tile side, power of two <= N (0: automatic) */
+  int gradient;   /* 0: spectral -i k (the reference, pm3d.py:111-112); 1: 2-point; 2: 4-point FD */
+  double L;       /* box side */
+  double smooth;  /* Gaussian force smoothing in cells (pm3d.py:107-108) */
+  long long n;    /* particle count; 0 means Np^3 (any count is allowed, e.g. PM3D.deposit(X)) */
+} pm_peak_cfg;
+
+/* Step schedules (pm_set_particles). */
+#define PM_SCHED_RATIO 0    /* da = a*param for max_steps steps (uniform in ln a) */
+#define PM_SCHED_FRAC 1     /* da = min(param*a, a_end - a) until a >= a_end (pbhgr/scripts/pm3d_peak.py:26-27) */
+#define PM_SCHED_EXPLICIT 2 /* one step per pm_step_explicit call (PM3D.step, pm3d.py:117) */
+
+/* Peak states reported by pm_get_clock. */
+#define PM_STATE_IDLE 0
+#define PM_STATE_PRIME 1
+#define PM_STATE_RUN 2
+#define PM_STATE_FINALIZE 3
+#define PM_STATE_HOLD 4
+
+typedef struct {
+  double a;       /* expansion factor of the current positions */
+  double da;      /* next step */
+  double a_end;
+  double kpend;   /* pending closing-kick coefficient (0 when p is complete) */
+  double a_grid;  /* expansion factor the force grids were computed for */
+  int mode, state, nsteps, max_steps;
+} pm_clock_info;
+
+typedef struct {
+  double rho_max_over_mean;  /* max node count / n_mean of the last deposit (pm3d.py:158) */
+  double delta_max;          /* max delta of the last deposit (pbhgr/scripts/pm3d_peak.py:30) */
+  double mass_defect;        /* sum over nodes of (count - n_mean), exactly 0 unless corrupted */
+  unsigned status;           /* bit 0: non-finite momentum seen; bit 1: sort look-back gave up */
+} pm_stats_info;
+
+/* Create an engine holding npeaks independent peaks (a batched ensemble; npeaks = 1 is the
+ * plain single run).  Allocates all device memory and cuFFT plans up front; no later call
+ * allocates.  flags: bit 0 = sort only the bucket bits of the key each step (the full
+ * 64-bit key is sorted at priming); bit 1 = record the step as a CUDA graph. */
+int pm_engine_create(const pm_peak_cfg* cfg, int npeaks, int device, int flags, pm_engine** out);
+int pm_engine_destroy(pm_engine* e);
+int pm_engine_sync(pm_engine* e);
+/* Bytes of device memory the engine holds. */
+long long pm_engine_device_bytes(const pm_engine* e);
+
+/* Load particles (lattice order) for one peak at expansion factor a0 and choose its schedule.
+ * The peak primes (sort + deposit + forces at a0) on the next pm_run step.
+ * Replaces: assignment of PM3D.x / PM3D.p after make_ic (pm3d.py:67-68). */
+int pm_set_particles(pm_engine* e, int peak, const double* x, const double* p, double a0, int mode,
+                     double param, double a_end, int max_steps);
+
+/* Advance every peak that has work by nsteps engine steps (one batched step each).
+ * Replaces: the driver loop of pbhgr/scripts/pm3d_peak.py:26-28. */
+int pm_run(pm_engine* e, int nsteps);
+
+/* PM3D.step(a, da) for one peak (pm3d.py:117-129): a KDK step from a to a + da.  Forces at
+ * a are reused when the peak's current state is at a (pm3d.py:119), else recomputed. */
+int pm_step_explicit(pm_engine* e, int peak, double a, double da);
+
+/* Current particles, float64, lattice order; p includes the closing kick. (PM3D.x, PM3D.p) */
+int pm_get_particles(pm_engine* e, int peak, double* x, double* p);
+/* -grad Phi at the particles for expansion factor a, lattice order: the acc of
+ * PM3D.forces(a) (pm3d.py:101-114) at the current positions. */
+int pm_get_acc(pm_engine* e, int peak, double a, double* acc);
+/* delta of the last deposit (N^3 float32): the delta returned by PM3D.step/forces. */
+int pm_get_delta(pm_engine* e, int peak, float* delta);
+/* Float64 CIC counts of the current positions (N^3): PM3D.deposit(PM3D.x) (pm3d.py:81-89). */
+int pm_get_counts(pm_engine* e, int peak, double* counts);
+int pm_get_clock(pm_engine* e, int peak, pm_clock_info* out);   /* host struct */
+int pm_get_stats(pm_engine* e, int peak, pm_stats_info* out);   /* host struct */
+
+/* Initial particles on the GPU in float64 (setup call: allocates and frees its temporaries).
+ * kind 0 = PM3D.make_ic(mu, profile_spline, e, p, tail_rms, tail_k) (pm3d.py:40-73): amp = mu,
+ *   axes = zeldovich_axes(e, p), the spline as scipy PPoly breakpoints x[m+1] and
+ *   coefficients c[4][m] (HOST arrays), noise = rng.standard_normal((N,N,N)) when tail_rms > 0.
+ * kind 1 = Gaussian density peak delta0 exp(-sum x_i^2/2R_i^2) plus noise with P(k) ~ k^-2
+ *   scaled to rms noise_frac*delta0 (the benchmark recipe): amp = delta0, axes = R.
+ * Both continue with the reference's Zel'dovich tail (pm3d.py:59-72).  Outputs: x, p (n,3) in
+ * lattice order, optional delta_lin (N^3), and on the host the rms of the noise field on the
+ * grid (PM3D.tail_rms_grid for kind 0). */
+typedef struct {
+  int N, Np;
+  double L;
+  int kind;
+  double amp;
+  double axes[3];
+  const double* spline_x;  /* host, m + 1 breakpoints */
+  const double* spline_c;  /* host, 4*m coefficients, c[k*m + i] multiplies (r - x_i)^(3-k) */
+  int spline_m;
+  const double* noise;     /* device, N^3 standard normals, or NULL */
+  double tail_rms, k1, k2;
+  double noise_frac;
+} pm_ic_params;
+int pm_make_ic(const pm_ic_params* prm, double* x_out, double* p_out, double* delta_lin_out, double* noise_rms_out);
+
+/* Stateless helpers. */
+/* PM3D.interp(F, X) (pm3d.py:91-99) in float64: F (N^3), X (n,3) -> out (n). */
+int pm_interp64(const double* F, const double* X, long long n, int N, double L, double* out);
+/* Stable sort of n 64-bit keys over bits [lo, hi): keys_out, perm_out (original indices).
+ * tmp_keys/tmp_vals are caller scratch of n entries each. */
+int pm_sort_u64(const unsigned long long* keys, unsigned long long* keys_out, unsigned int* perm_out,
+                unsigned long long* tmp_keys, unsigned int* tmp_vals, long long n, int lo, int hi);
+/* Diagnostics of analyse (pm3d.py:132-159).  pm_rell_keys: the Lagrangian ellipsoidal radius
+ * r_ell_q of every lattice site (pm3d.py:71) as order-preserving uint64 keys, for picking the
+ * innermost sets with pm_sort_u64 (ties then fall to the lower lattice index).
+ * pm_analyse_partials: per-block float64 partial sums, 34 per block, over x (n,3, lattice
+ * order): for each of the 3 sets r_ell_q < set_radii[s] the count, sum of rel and the 6
+ * entries of sum rel rel^T, rel = periodic offset from centre (pm3d.py:142-147); then the 4
+ * counts of |rel| < radii[k] (pm3d.py:153-156).  A, centre, set_radii, radii are HOST arrays. */
+int pm_rell_keys(int Np, double L, const double* A, unsigned long long* keys);
+int pm_analyse_partials(const double* x, int Np, double L, const double* A, const double* centre,
+                        const double* set_radii, const double* radii, int nblocks, double* partials);
+/* Cell keys of split positions; used by tests to check the key layout. */
+int pm_cell_keys(const int* cells, long long n, int N, int tile, unsigned int* keys_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,131 @@
+// Shared definitions for the pm3d B200 engine (sm_100a).
+//
+// Particle state (one 16-byte vector each, so every access is a 128-bit load/store):
+//   pos  = int4 {cell, f_x, f_y, f_z}: `cell` is the linear index (ix*N + iy)*N + iz of the
+//          lower of the two mesh nodes bracketing the particle on each axis (mesh node i sits
+//          at (i + 1/2) dx, pbhgr/pbhgr/pm3d.py:76-79), and f_* in [0, 1) is the FP32 offset
+//          from that node in node units.  X = ((i + f + 1/2) dx) mod L.  CIC weights are then
+//          (1 - f, f) with no branch (pm3d.py:83-88).
+//   mom  = float4 {p_x, p_y, p_z, id}: canonical momentum p = a^2 dx/dt (pm3d.py:4) and the
+//          particle's lattice index (the row of PM3D.x) stored as int bits.
+#pragma once
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <stdint.h>
+
+typedef unsigned long long u64;
+typedef unsigned int u32;
+
+// Density is accumulated as unsigned 64-bit fixed point with 40 fractional bits: integer
+// sums are associative, so the deposit is bitwise deterministic in any order, and
+// delta = S/n_mean - 1 keeps full FP32 relative precision even where |delta| << 1.
+#define PM_FIX_BITS 40
+#define PM_FIX_ONE (1ULL << PM_FIX_BITS)
+
+#define PM_H_I 5.0
+
+// Per-peak lifecycle, read by the step kernels from device memory so that one captured
+// graph serves any mix of peaks.
+enum PeakState : int {
+  PS_IDLE = 0,      // nothing to do; state and grids are frozen
+  PS_PRIME = 1,     // new particles loaded: deposit + forces this step, no push
+  PS_RUN = 2,       // regular KDK step
+  PS_FINALIZE = 3,  // apply the pending closing kick, then go idle
+  PS_HOLD = 4       // stepped once on request; keeps its pending kick until told again
+};
+
+enum ScheduleMode : int {
+  SCHED_RATIO = 0,     // da = a*param for max_steps steps (uniform in ln a)
+  SCHED_FRAC = 1,      // da = min(param*a, a_end - a) until a >= a_end (pbhgr/scripts/pm3d_peak.py:26-27)
+  SCHED_EXPLICIT = 2   // one step of the da the host wrote, then hold
+};
+
+struct PeakDesc {
+  int N, log2N, T, log2T;
+  int log2NT;       // log2(N/T)
+  int ntiles;       // (N/T)^3
+  int nb;           // buckets = ntiles*8
+  int local_bits;   // 3*log2T
+  int key_bits;     // 3*log2N + 3
+  int gradient;     // 0 spectral (reference), 1 two-point finite difference, 2 four-point
+  double L, dx, smooth, n_mean, m_part;
+  long long n_mean_fix;    // round(n_mean * 2^40)
+  double inv_fix_nmean;    // 2^-40 / n_mean
+  long long p_off, n;      // particle range in the arena
+  long long tile_base;     // first global tile index of this peak
+  long long bucket_off;    // offset of this peak's bucket-start array (nb + 1 entries)
+  long long mode_base;     // first global mode-block of this peak (Green kernel)
+  long long nmodes;        // N*N*(N/2+1)
+  float* delta;            // N^3 FP32 density contrast (R2C input)
+  float2* spec;            // N*N*(N/2+1) complex spectrum (R2C output)
+  float2* gspec;           // 3 gradient spectra
+  float* force;            // 3 force grids of N^3 (C2R output)
+};
+
+struct PeakClock {
+  double a;        // expansion factor of the current positions
+  double da;       // size of the next step
+  double a_end;    // SCHED_FRAC end point
+  double kpend;    // pending closing-kick coefficient 0.5*da_prev/(a H(a)), 0 if none
+  double param;    // ratio (SCHED_RATIO) or da_frac (SCHED_FRAC)
+  double a_grid;   // expansion factor the force grids were computed at
+  int mode;        // ScheduleMode
+  int state;       // PeakState
+  int nsteps;      // steps taken
+  int max_steps;   // SCHED_RATIO length
+  int buf;         // which particle buffer holds the current state
+  int dep;         // 1 when this step re-deposits (set by the advance kernel)
+  int has_delta;   // delta/grids hold data
+  int pad;
+};
+
+// Per-peak device statistics.  Integer fields are reduced with integer atomics
+// (order-independent); FP64 sums are written per block and reduced in a fixed order.
+struct PeakStats {
+  u64 max_fix;            // max node count in fixed point
+  long long mass_defect;  // sum over nodes of (S - n_mean_fix): 0 when mass is exact
+  u32 status;             // bit 0: non-finite force/momentum, bit 1: fixed-point overflow
+  u32 pad;
+};
+
+#define PM_CHECK(x)                                  \
+  do {                                               \
+    cudaError_t e_ = (x);                            \
+    if (e_ != cudaSuccess) return -(int)e_;          \
+  } while (0)
+
+// ---------------------------------------------------------------------------- Morton
+__host__ __device__ __forceinline__ u32 pm_spread3(u32 v) {
+  v &= 0x3FF;
+  v = (v | (v << 16)) & 0x030000FFu;
+  v = (v | (v << 8)) & 0x0300F00Fu;
+  v = (v | (v << 4)) & 0x030C30C3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+__host__ __device__ __forceinline__ u32 pm_compact3(u32 v) {
+  v &= 0x09249249u;
+  v = (v | (v >> 2)) & 0x030C30C3u;
+  v = (v | (v >> 4)) & 0x0300F00Fu;
+  v = (v | (v >> 8)) & 0x030000FFu;
+  v = (v | (v >> 16)) & 0x3FFu;
+  return v;
+}
+// z occupies the lowest bit of each triple, so consecutive codes walk along z (the
+// contiguous axis of the mesh).
+__host__ __device__ __forceinline__ u32 pm_morton3(u32 x, u32 y, u32 z) {
+  return (pm_spread3(x) << 2) | (pm_spread3(y) << 1) | pm_spread3(z);
+}
+
+// Cell key of a node-lattice cell: [tile Morton | boundary mask (3) | in-tile Morton].
+// Bit b of the mask is set when the cell is the last layer of its tile along axis b
+// (x = bit 0, y = bit 1, z = bit 2); those cells also feed the next tile's nodes.
+__host__ __device__ __forceinline__ u32 pm_cell_key(const PeakDesc& P, int ix, int iy, int iz) {
+  const int m = P.T - 1;
+  u32 lx = ix & m, ly = iy & m, lz = iz & m;
+  u32 tx = ix >> P.log2T, ty = iy >> P.log2T, tz = iz >> P.log2T;
+  u32 mask = (lx == (u32)m ? 1u : 0u) | (ly == (u32)m ? 2u : 0u) | (lz == (u32)m ? 4u : 0u);
+  return (((pm_morton3(tx, ty, tz) << 3) | mask) << P.local_bits) | pm_morton3(lx, ly, lz);
+}
+
+__host__ __device__ __forceinline__ double pm_hubble(double a) { return PM_H_I / (a * sqrt(a)); }

@@ -1,0 +1,579 @@
+// Host side of the engine: memory layout, cuFFT plans, the step launch sequence and the
+// extern "C" API declared in include/pmb200.h.
+#include <cufft.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <new>
+#include <vector>
+
+#include "../../include/pmb200.h"
+#include "pm_kernels.cuh"
+#include "sort.cuh"
+
+namespace {
+
+int ilog2(int v) {
+  int r = 0;
+  while ((1 << r) < v) ++r;
+  return (1 << r) == v ? r : -1;
+}
+
+#define CU(x)                                         \
+  do {                                                \
+    cudaError_t e_ = (x);                             \
+    if (e_ != cudaSuccess) return -(int)e_;           \
+  } while (0)
+#define CF(x)                                         \
+  do {                                                \
+    cufftResult r_ = (x);                             \
+    if (r_ != CUFFT_SUCCESS) return -1000 - (int)r_;  \
+  } while (0)
+
+struct MeshClass {
+  int N = 0;
+  std::vector<int> peaks;
+  float* delta = nullptr;
+  float2* spec = nullptr;
+  float2* gspec = nullptr;
+  float* force = nullptr;
+  cufftHandle r2c = 0, c2r = 0;
+  bool plans = false;
+};
+
+}  // namespace
+
+struct pm_engine {
+  int device = 0;
+  int flags = 0;
+  cudaStream_t stream = nullptr;
+  int npeaks = 0;
+  std::vector<PeakDesc> peaks;
+  std::vector<MeshClass> classes;
+  long long ntot = 0, ntiles = 0, nmodeblk = 0, nbuckets = 0;
+  int Tmax = 0;
+  size_t smem_dep = 0, smem_push = 0;
+  // device arrays
+  PeakDesc* d_peaks = nullptr;
+  PeakClock* d_clocks = nullptr;
+  PeakStats* d_stats = nullptr;
+  long long* d_tile_base = nullptr;
+  long long* d_p_base = nullptr;
+  long long* d_mode_base = nullptr;
+  int4* pos[2] = {nullptr, nullptr};
+  float4* mom[2] = {nullptr, nullptr};
+  u64* keys[2] = {nullptr, nullptr};
+  u32* vals[2] = {nullptr, nullptr};
+  u32* bstart = nullptr;
+  SortPlan sort{};
+  int sort_result = 0;  // which (keys, vals) pair holds the sorted output
+  cudaGraphExec_t graph = nullptr;
+  long long bytes = 0;
+
+  StepArgs args() const {
+    StepArgs A{};
+    A.peaks = d_peaks;
+    A.clocks = d_clocks;
+    A.stats = d_stats;
+    A.sortseg = sort.seg;
+    A.tile_base = d_tile_base;
+    A.p_base = d_p_base;
+    A.mode_base = d_mode_base;
+    A.npeaks = npeaks;
+    A.pos[0] = pos[0];
+    A.pos[1] = pos[1];
+    A.mom[0] = mom[0];
+    A.mom[1] = mom[1];
+    A.keys_push = keys[0];
+    A.keys_sorted = keys[sort_result];
+    A.perm = vals[sort_result];
+    A.bstart = bstart;
+    return A;
+  }
+
+  template <class T>
+  int alloc(T** p, size_t count) {
+    const size_t b = sizeof(T) * (count ? count : 1);
+    cudaError_t e = cudaMalloc((void**)p, b);
+    if (e != cudaSuccess) return -(int)e;
+    bytes += (long long)b;
+    return 0;
+  }
+
+  int launch_step() {
+    const StepArgs A = args();
+    launch_push(A, ntiles, smem_push, stream);
+    launch_advance(A, stream);
+    int r = sort_run(&sort, keys[0], vals[0], keys[1], vals[1], true, true, stream);
+    if (r) return r;
+    launch_bucket_starts(A, ntot, stream);
+    launch_deposit(A, ntiles, smem_dep, nullptr, stream);
+    for (auto& c : classes) CF(cufftExecR2C(c.r2c, c.delta, (cufftComplex*)c.spec));
+    launch_green(A, nmodeblk, stream);
+    for (auto& c : classes) CF(cufftExecC2R(c.c2r, (cufftComplex*)c.gspec, c.force));
+    CU(cudaGetLastError());
+    return 0;
+  }
+
+  int step() {
+    if (flags & 2) {
+      if (!graph) {
+        cudaGraph_t g = nullptr;
+        CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        int r = launch_step();
+        cudaError_t ce = cudaStreamEndCapture(stream, &g);
+        if (r) return r;
+        CU(ce);
+        CU(cudaGraphInstantiate(&graph, g, 0));
+        cudaGraphDestroy(g);
+      }
+      CU(cudaGraphLaunch(graph, stream));
+      return 0;
+    }
+    return launch_step();
+  }
+
+  int read_clock(int pk, PeakClock* c) {
+    CU(cudaMemcpyAsync(c, d_clocks + pk, sizeof(PeakClock), cudaMemcpyDeviceToHost, stream));
+    CU(cudaStreamSynchronize(stream));
+    return 0;
+  }
+  int write_clock(int pk, const PeakClock& c) {
+    CU(cudaMemcpyAsync(d_clocks + pk, &c, sizeof(PeakClock), cudaMemcpyHostToDevice, stream));
+    CU(cudaStreamSynchronize(stream));
+    return 0;
+  }
+
+  ~pm_engine() {
+    if (graph) cudaGraphExecDestroy(graph);
+    for (auto& c : classes) {
+      if (c.plans) {
+        cufftDestroy(c.r2c);
+        cufftDestroy(c.c2r);
+      }
+      cudaFree(c.delta);
+      cudaFree(c.spec);
+      cudaFree(c.gspec);
+      cudaFree(c.force);
+    }
+    sort_plan_destroy(&sort);
+    cudaFree(d_peaks);
+    cudaFree(d_clocks);
+    cudaFree(d_stats);
+    cudaFree(d_tile_base);
+    cudaFree(d_p_base);
+    cudaFree(d_mode_base);
+    for (int b = 0; b < 2; ++b) {
+      cudaFree(pos[b]);
+      cudaFree(mom[b]);
+      cudaFree(keys[b]);
+      cudaFree(vals[b]);
+    }
+    cudaFree(bstart);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
+  E->npeaks = npeaks;
+  E->peaks.resize(npeaks);
+  std::map<int, int> class_of;
+  long long poff = 0, tb = 0, mb = 0, bo = 0;
+  int Tmax = 1;
+  int max_bits = 0, min_lo = 64;
+  std::vector<long long> tile_base(npeaks + 1), p_base(npeaks + 1), mode_base(npeaks + 1);
+  for (int i = 0; i < npeaks; ++i) {
+    const pm_peak_cfg& c = cfg[i];
+    const int l2 = ilog2(c.N);
+    if (l2 < 3 || l2 > 10) return -2001;
+    const long long npart = c.n > 0 ? c.n : (long long)c.Np * c.Np * c.Np;
+    if (c.Np < 1 || npart >= (1LL << 31)) return -2002;
+    if (!(c.L > 0)) return -2003;
+    int T = c.tile > 0 ? c.tile : std::min(16, c.N);
+    if (ilog2(T) < 1 || T > c.N) return -2004;
+    PeakDesc& P = E->peaks[i];
+    P = PeakDesc{};
+    P.N = c.N;
+    P.log2N = l2;
+    P.T = T;
+    P.log2T = ilog2(T);
+    P.log2NT = l2 - P.log2T;
+    P.ntiles = 1 << (3 * P.log2NT);
+    P.nb = P.ntiles * 8;
+    P.local_bits = 3 * P.log2T;
+    P.key_bits = 3 * l2 + 3;
+    P.gradient = c.gradient;
+    P.L = c.L;
+    P.dx = c.L / c.N;
+    P.smooth = c.smooth;
+    const double np3 = (double)c.Np * c.Np * c.Np;
+    P.n_mean = (double)npart / ((double)c.N * c.N * c.N);
+    P.m_part = 3.0 * PM_H_I * PM_H_I / (8.0 * M_PI) * c.L * c.L * c.L / np3;
+    P.n_mean_fix = (long long)llround(P.n_mean * (double)PM_FIX_ONE);
+    P.inv_fix_nmean = 1.0 / ((double)PM_FIX_ONE * P.n_mean);
+    P.p_off = poff;
+    P.n = npart;
+    P.tile_base = tb;
+    P.bucket_off = bo;
+    P.nmodes = (long long)c.N * c.N * (c.N / 2 + 1);
+    P.mode_base = mb;
+    tile_base[i] = tb;
+    p_base[i] = poff;
+    mode_base[i] = mb;
+    poff += P.n;
+    tb += P.ntiles;
+    bo += P.nb + 1;
+    mb += (P.nmodes + PM_THREADS - 1) / PM_THREADS;
+    Tmax = std::max(Tmax, T);
+    max_bits = std::max(max_bits, P.key_bits);
+    min_lo = std::min(min_lo, P.local_bits);
+    if (!class_of.count(c.N)) {
+      class_of[c.N] = (int)E->classes.size();
+      E->classes.push_back(MeshClass{});
+      E->classes.back().N = c.N;
+    }
+    E->classes[class_of[c.N]].peaks.push_back(i);
+  }
+  tile_base[npeaks] = tb;
+  p_base[npeaks] = poff;
+  mode_base[npeaks] = mb;
+  if (poff >= (1LL << 32)) return -2005;
+  E->ntot = poff;
+  E->ntiles = tb;
+  E->nmodeblk = mb;
+  E->nbuckets = bo;
+  E->Tmax = Tmax;
+  if (int rk = pm_kernels_init()) return rk;
+  E->smem_dep = pm_deposit_smem(Tmax);
+  E->smem_push = pm_push_smem(Tmax);
+
+  // Mesh arenas, one per mesh size, peaks of a class contiguous for batched cuFFT plans.
+  for (auto& mc : E->classes) {
+    const long long N = mc.N, N3 = N * N * N, M = N * N * (N / 2 + 1);
+    const int B = (int)mc.peaks.size();
+    int r;
+    if ((r = E->alloc(&mc.delta, (size_t)(B * N3)))) return r;
+    if ((r = E->alloc(&mc.spec, (size_t)(B * M)))) return r;
+    if ((r = E->alloc(&mc.gspec, (size_t)(3 * B * M)))) return r;
+    if ((r = E->alloc(&mc.force, (size_t)(3 * B * N3)))) return r;
+    CU(cudaMemsetAsync(mc.delta, 0, sizeof(float) * B * N3, E->stream));
+    CU(cudaMemsetAsync(mc.force, 0, sizeof(float) * 3 * B * N3, E->stream));
+    for (int k = 0; k < B; ++k) {
+      PeakDesc& P = E->peaks[mc.peaks[k]];
+      P.delta = mc.delta + k * N3;
+      P.spec = mc.spec + k * M;
+      P.gspec = mc.gspec + 3 * k * M;
+      P.force = mc.force + 3 * k * N3;
+    }
+    int n[3] = {(int)N, (int)N, (int)N};
+    CF(cufftPlanMany(&mc.r2c, 3, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_R2C, B));
+    CF(cufftPlanMany(&mc.c2r, 3, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2R, 3 * B));
+    mc.plans = true;
+    CF(cufftSetStream(mc.r2c, E->stream));
+    CF(cufftSetStream(mc.c2r, E->stream));
+    size_t ws = 0;
+    if (cufftGetSize(mc.r2c, &ws) == CUFFT_SUCCESS) E->bytes += (long long)ws;
+    if (cufftGetSize(mc.c2r, &ws) == CUFFT_SUCCESS) E->bytes += (long long)ws;
+  }
+
+  int r;
+  if ((r = E->alloc(&E->d_peaks, npeaks))) return r;
+  if ((r = E->alloc(&E->d_clocks, npeaks))) return r;
+  if ((r = E->alloc(&E->d_stats, npeaks))) return r;
+  if ((r = E->alloc(&E->d_tile_base, npeaks + 1))) return r;
+  if ((r = E->alloc(&E->d_p_base, npeaks + 1))) return r;
+  if ((r = E->alloc(&E->d_mode_base, npeaks + 1))) return r;
+  for (int b = 0; b < 2; ++b) {
+    if ((r = E->alloc(&E->pos[b], E->ntot))) return r;
+    if ((r = E->alloc(&E->mom[b], E->ntot))) return r;
+    if ((r = E->alloc(&E->keys[b], E->ntot))) return r;
+    if ((r = E->alloc(&E->vals[b], E->ntot))) return r;
+  }
+  if ((r = E->alloc(&E->bstart, E->nbuckets))) return r;
+  CU(cudaMemcpy(E->d_peaks, E->peaks.data(), sizeof(PeakDesc) * npeaks, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(E->d_tile_base, tile_base.data(), sizeof(long long) * (npeaks + 1), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(E->d_p_base, p_base.data(), sizeof(long long) * (npeaks + 1), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(E->d_mode_base, mode_base.data(), sizeof(long long) * (npeaks + 1), cudaMemcpyHostToDevice));
+  std::vector<PeakClock> clocks(npeaks);
+  for (auto& c : clocks) {
+    c = PeakClock{};
+    c.state = PS_IDLE;
+  }
+  CU(cudaMemcpy(E->d_clocks, clocks.data(), sizeof(PeakClock) * npeaks, cudaMemcpyHostToDevice));
+  CU(cudaMemset(E->d_stats, 0, sizeof(PeakStats) * npeaks));
+  CU(cudaMemset(E->bstart, 0, sizeof(u32) * E->nbuckets));
+
+  // Sort plan: one segment per peak.  The whole cell key is sorted every step (bits
+  // [0, key_bits)); with flag bit 0 only the bucket bits [local_bits, key_bits) are.
+  std::vector<SortSeg> segs(npeaks);
+  int max_span = 0;
+  for (int i = 0; i < npeaks; ++i) {
+    const PeakDesc& P = E->peaks[i];
+    segs[i].begin = P.p_off;
+    segs[i].end = P.p_off + P.n;
+    segs[i].lo = (E->flags & 1) ? P.local_bits : 0;
+    segs[i].hi = P.key_bits;
+    segs[i].active = 0;
+    max_span = std::max(max_span, P.key_bits - segs[i].lo);
+  }
+  const int npass = (max_span + 7) / 8;
+  if ((r = sort_plan_create(&E->sort, segs.data(), npeaks, npass))) return r;
+  E->bytes += (long long)E->sort.ntiles * SORT_RADIX * 8;
+  E->sort_result = npass & 1;
+  CU(cudaDeviceSynchronize());
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pm_engine_create(const pm_peak_cfg* cfg, int npeaks, int device, int flags, pm_engine** out) {
+  if (!cfg || npeaks < 1 || !out) return -2000;
+  *out = nullptr;
+  CU(cudaSetDevice(device));
+  pm_engine* E = new (std::nothrow) pm_engine();
+  if (!E) return -2;
+  E->device = device;
+  E->flags = flags;
+  cudaError_t ce = cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking);
+  if (ce != cudaSuccess) {
+    delete E;
+    return -(int)ce;
+  }
+  int r = engine_init(E, cfg, npeaks);
+  if (r) {
+    delete E;
+    return r;
+  }
+  *out = E;
+  return 0;
+}
+
+int pm_engine_destroy(pm_engine* e) {
+  if (!e) return -2000;
+  cudaSetDevice(e->device);
+  cudaStreamSynchronize(e->stream);
+  delete e;
+  return 0;
+}
+
+int pm_engine_sync(pm_engine* e) {
+  if (!e) return -2000;
+  CU(cudaStreamSynchronize(e->stream));
+  return 0;
+}
+
+long long pm_engine_device_bytes(const pm_engine* e) { return e ? e->bytes : 0; }
+
+int pm_set_particles(pm_engine* e, int peak, const double* x, const double* p, double a0, int mode, double param,
+                     double a_end, int max_steps) {
+  if (!e || peak < 0 || peak >= e->npeaks || !x || !p) return -2000;
+  if (!(a0 > 0) || mode < 0 || mode > 2) return -2001;
+  CU(cudaSetDevice(e->device));
+  const StepArgs A = e->args();
+  launch_reset_peak(A, peak, a0, mode, param, a_end, max_steps, e->stream);
+  launch_set_particles(A, peak, e->peaks[peak], x, p, e->stream);
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(e->stream));
+  return 0;
+}
+
+int pm_run(pm_engine* e, int nsteps) {
+  if (!e || nsteps < 0) return -2000;
+  CU(cudaSetDevice(e->device));
+  for (int s = 0; s < nsteps; ++s) {
+    int r = e->step();
+    if (r) return r;
+  }
+  return 0;
+}
+
+int pm_step_explicit(pm_engine* e, int peak, double a, double da) {
+  if (!e || peak < 0 || peak >= e->npeaks) return -2000;
+  if (!(a > 0) || !(da > 0)) return -2001;
+  CU(cudaSetDevice(e->device));
+  PeakClock c;
+  int r;
+  if ((r = e->read_clock(peak, &c))) return r;
+  // Bring the peak to "forces known at a" (pm3d.py:119-120).
+  if (c.state == PS_HOLD && c.a != a) {
+    c.state = PS_FINALIZE;  // apply the pending kick with the grids it belongs to
+    if ((r = e->write_clock(peak, c)) || (r = e->step()) || (r = e->read_clock(peak, &c))) return r;
+  }
+  if (c.state == PS_IDLE || c.state == PS_PRIME || (c.state == PS_HOLD && !c.has_delta)) {
+    c.a = a;
+    c.a_grid = a;
+    c.mode = SCHED_EXPLICIT;
+    c.state = PS_PRIME;
+    if ((r = e->write_clock(peak, c)) || (r = e->step()) || (r = e->read_clock(peak, &c))) return r;
+  }
+  if (c.state != PS_HOLD) return -2002;
+  c.mode = SCHED_EXPLICIT;
+  c.da = da;
+  c.state = PS_RUN;
+  if ((r = e->write_clock(peak, c)) || (r = e->step())) return r;
+  CU(cudaStreamSynchronize(e->stream));
+  return 0;
+}
+
+int pm_get_particles(pm_engine* e, int peak, double* x, double* p) {
+  if (!e || peak < 0 || peak >= e->npeaks) return -2000;
+  CU(cudaSetDevice(e->device));
+  launch_get_particles(e->args(), peak, e->peaks[peak], x, p, nullptr, 1.0, e->stream);
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(e->stream));
+  return 0;
+}
+
+int pm_get_acc(pm_engine* e, int peak, double a, double* acc) {
+  if (!e || peak < 0 || peak >= e->npeaks || !acc) return -2000;
+  if (!(a > 0)) return -2001;
+  CU(cudaSetDevice(e->device));
+  launch_get_particles(e->args(), peak, e->peaks[peak], nullptr, nullptr, acc, a, e->stream);
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(e->stream));
+  return 0;
+}
+
+int pm_get_delta(pm_engine* e, int peak, float* delta) {
+  if (!e || peak < 0 || peak >= e->npeaks || !delta) return -2000;
+  CU(cudaSetDevice(e->device));
+  const PeakDesc& P = e->peaks[peak];
+  CU(cudaMemcpyAsync(delta, P.delta, sizeof(float) * (size_t)P.N * P.N * P.N, cudaMemcpyDeviceToDevice, e->stream));
+  CU(cudaStreamSynchronize(e->stream));
+  return 0;
+}
+
+int pm_get_counts(pm_engine* e, int peak, double* counts) {
+  if (!e || peak < 0 || peak >= e->npeaks || !counts) return -2000;
+  CU(cudaSetDevice(e->device));
+  // Re-deposit the current positions of this peak only, writing float64 counts.
+  PeakClock c;
+  int r;
+  if ((r = e->read_clock(peak, &c))) return r;
+  if (!c.has_delta) return -2002;
+  std::vector<PeakClock> all(e->npeaks);
+  CU(cudaMemcpy(all.data(), e->d_clocks, sizeof(PeakClock) * e->npeaks, cudaMemcpyDeviceToHost));
+  std::vector<PeakClock> tmp = all;
+  for (int i = 0; i < e->npeaks; ++i) tmp[i].dep = i == peak ? 1 : 0;
+  CU(cudaMemcpy(e->d_clocks, tmp.data(), sizeof(PeakClock) * e->npeaks, cudaMemcpyHostToDevice));
+  PeakStats st;
+  CU(cudaMemcpy(&st, e->d_stats + peak, sizeof(PeakStats), cudaMemcpyDeviceToHost));
+  st.max_fix = 0;
+  st.mass_defect = 0;
+  CU(cudaMemcpy(e->d_stats + peak, &st, sizeof(PeakStats), cudaMemcpyHostToDevice));
+  // Same kernel with the extra float64 output; delta is rewritten with identical values.
+  launch_deposit(e->args(), e->ntiles, e->smem_dep, counts, e->stream);
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(e->stream));
+  CU(cudaMemcpy(e->d_clocks, all.data(), sizeof(PeakClock) * e->npeaks, cudaMemcpyHostToDevice));
+  return 0;
+}
+
+int pm_get_clock(pm_engine* e, int peak, pm_clock_info* out) {
+  if (!e || peak < 0 || peak >= e->npeaks || !out) return -2000;
+  CU(cudaSetDevice(e->device));
+  PeakClock c;
+  int r = e->read_clock(peak, &c);
+  if (r) return r;
+  out->a = c.a;
+  out->da = c.da;
+  out->a_end = c.a_end;
+  out->kpend = c.kpend;
+  out->a_grid = c.a_grid;
+  out->mode = c.mode;
+  out->state = c.state;
+  out->nsteps = c.nsteps;
+  out->max_steps = c.max_steps;
+  return 0;
+}
+
+int pm_get_stats(pm_engine* e, int peak, pm_stats_info* out) {
+  if (!e || peak < 0 || peak >= e->npeaks || !out) return -2000;
+  CU(cudaSetDevice(e->device));
+  PeakStats s;
+  int err = 0;
+  CU(cudaMemcpyAsync(&s, e->d_stats + peak, sizeof(PeakStats), cudaMemcpyDeviceToHost, e->stream));
+  CU(cudaMemcpyAsync(&err, e->sort.err, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+  CU(cudaStreamSynchronize(e->stream));
+  const PeakDesc& P = e->peaks[peak];
+  out->rho_max_over_mean = (double)s.max_fix / (double)PM_FIX_ONE / P.n_mean;
+  out->delta_max = out->rho_max_over_mean - 1.0;
+  out->mass_defect = (double)s.mass_defect / (double)PM_FIX_ONE;
+  out->status = s.status | (err ? 2u : 0u);
+  return (int)(out->status != 0);
+}
+
+int pm_interp64(const double* F, const double* X, long long n, int N, double L, double* out) {
+  if (!F || !X || !out || n < 0 || N < 1 || !(L > 0)) return -2000;
+  if (n == 0) return 0;
+  launch_interp64(F, X, n, N, L / N, out, 0);
+  CU(cudaGetLastError());
+  CU(cudaDeviceSynchronize());
+  return 0;
+}
+
+int pm_sort_u64(const unsigned long long* keys, unsigned long long* keys_out, unsigned int* perm_out,
+                unsigned long long* tmp_keys, unsigned int* tmp_vals, long long n, int lo, int hi) {
+  if (!keys || !keys_out || !perm_out || !tmp_keys || !tmp_vals || n < 0) return -2000;
+  if (lo < 0 || hi > 64 || hi <= lo) return -2001;
+  if (n >= (1LL << 32)) return -2002;
+  if (n == 0) return 0;
+  SortSeg seg{0, n, lo, hi, 1, 0};
+  SortPlan plan;
+  const int npass = (hi - lo + 7) / 8;
+  int r = sort_plan_create(&plan, &seg, 1, npass);
+  if (r) {
+    sort_plan_destroy(&plan);
+    return r;
+  }
+  // Even pass counts land in the first pair, odd in the second: route so that the final
+  // pass writes (keys_out, perm_out).
+  u64* k0 = (u64*)tmp_keys;
+  u32* v0 = tmp_vals;
+  u64* k1 = (u64*)keys_out;
+  u32* v1 = perm_out;
+  if ((npass & 1) == 0) {
+    k0 = (u64*)keys_out;
+    v0 = perm_out;
+    k1 = (u64*)tmp_keys;
+    v1 = tmp_vals;
+  }
+  cudaError_t ce = cudaMemcpy(k0, keys, sizeof(u64) * n, cudaMemcpyDeviceToDevice);
+  if (ce == cudaSuccess) {
+    r = sort_run(&plan, k0, v0, k1, v1, true, true, 0);
+    ce = cudaDeviceSynchronize();
+  }
+  int err = 0;
+  if (ce == cudaSuccess) ce = cudaMemcpy(&err, plan.err, sizeof(int), cudaMemcpyDeviceToHost);
+  sort_plan_destroy(&plan);
+  if (ce != cudaSuccess) return -(int)ce;
+  if (r) return r;
+  return err ? 1 : 0;
+}
+
+int pm_cell_keys(const int* cells, long long n, int N, int tile, unsigned int* keys_out) {
+  // Host-side helper (plain host pointers): the key layout used by the sort.
+  if (!cells || !keys_out || n < 0) return -2000;
+  const int l2 = ilog2(N);
+  const int T = tile > 0 ? tile : std::min(16, N);
+  if (l2 < 1 || ilog2(T) < 1 || T > N) return -2001;
+  PeakDesc P{};
+  P.N = N;
+  P.log2N = l2;
+  P.T = T;
+  P.log2T = ilog2(T);
+  P.local_bits = 3 * P.log2T;
+  for (long long i = 0; i < n; ++i) {
+    const int c = cells[i];
+    keys_out[i] = pm_cell_key(P, c >> (2 * l2), (c >> l2) & (N - 1), c & (N - 1));
+  }
+  return 0;
+}
+
+}  // extern "C"

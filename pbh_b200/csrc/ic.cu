@@ -1,0 +1,309 @@
+// Initial conditions on the GPU in float64: PM3D.make_ic (pbhgr/pbhgr/pm3d.py:40-73) and the
+// benchmark's Gaussian-peak recipe, both ending in the reference's Zel'dovich tail
+// (pm3d.py:59-72): delta_k -> displacement potential -> psi = -grad phi -> CIC-interpolated
+// displacements of the quiet-start lattice.
+#include <cufft.h>
+
+#include <cmath>
+#include <vector>
+
+#include "../../include/pmb200.h"
+#include "common.cuh"
+
+namespace {
+
+constexpr double kTwoPi = 6.283185307179586476925286766559;
+constexpr double kPi = 3.14159265358979323846264338328;
+constexpr int kThreads = 256;
+
+#define CU(x)                                         \
+  do {                                                \
+    cudaError_t e_ = (x);                             \
+    if (e_ != cudaSuccess) { rc = -(int)e_; goto done; } \
+  } while (0)
+#define CF(x)                                         \
+  do {                                                \
+    cufftResult r_ = (x);                             \
+    if (r_ != CUFFT_SUCCESS) { rc = -1000 - (int)r_; goto done; } \
+  } while (0)
+
+__device__ __forceinline__ double kline(int i, int N, double kf) { return kf * (double)(i < N / 2 ? i : i - N); }
+
+// Piecewise cubic (scipy PPoly layout: c[k*m + i] multiplies (r - x_i)^(3-k)); interval by
+// searchsorted(x, r, 'right') - 1 clipped to [0, m-1], as CubicSpline.__call__ does.
+__device__ double spline_eval(const double* __restrict__ xs, const double* __restrict__ c, int m, double r) {
+  int lo = 0, hi = m;  // find last i in [0, m] with xs[i] <= r
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (xs[mid] <= r) lo = mid; else hi = mid - 1;
+  }
+  int i = lo;
+  if (i > m - 1) i = m - 1;
+  if (i < 0) i = 0;
+  const double t = r - xs[i];
+  return ((c[i] * t + c[m + i]) * t + c[2 * m + i]) * t + c[3 * m + i];
+}
+
+// Field on the centred cell grid x = (i + 1/2) dx - L/2 (pm3d.py:42-46).
+__global__ void k_field(int N, double L, int kind, double amp, double a0, double a1, double a2,
+                        const double* __restrict__ xs, const double* __restrict__ c, int m, double* __restrict__ out) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long N3 = (long long)N * N * N;
+  if (g >= N3) return;
+  const int iz = (int)(g % N), iy = (int)((g / N) % N), ix = (int)(g / ((long long)N * N));
+  const double dx = L / N;
+  const double X = (ix + 0.5) * dx - L / 2, Y = (iy + 0.5) * dx - L / 2, Z = (iz + 0.5) * dx - L / 2;
+  if (kind == 0) {
+    const double r = sqrt((X / a0) * (X / a0) + (Y / a1) * (Y / a1) + (Z / a2) * (Z / a2));
+    out[g] = amp * spline_eval(xs, c, m, fmin(r, xs[m]));
+  } else {
+    out[g] = amp * exp(-(X * X / (2 * a0 * a0) + Y * Y / (2 * a1 * a1) + Z * Z / (2 * a2 * a2)));
+  }
+}
+
+// Noise spectrum shaping.  kind 0: band-limited P flat in ln k (pm3d.py:49-54);
+// kind 1: sqrt(P) = 1/k, P(0) = 0 (benchmark recipe).
+__global__ void k_shape(cufftDoubleComplex* __restrict__ s, int N, double L, int kind, double tail_rms, double k1,
+                        double k2) {
+  const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int Nh = N / 2 + 1;
+  const long long M = (long long)N * N * Nh;
+  if (m >= M) return;
+  const int kz = (int)(m % Nh), iy = (int)((m / Nh) % N), ix = (int)(m / ((long long)Nh * N));
+  const double kf = kTwoPi / L;
+  const double kx = kline(ix, N, kf), ky = kline(iy, N, kf), kzv = kf * kz;
+  const double kk = m == 0 ? 0.0 : sqrt(kx * kx + ky * ky + kzv * kzv);
+  double f;
+  if (kind == 0) {
+    const bool band = kk >= k1 && kk <= k2;
+    const double P = band ? 2 * kPi * kPi * tail_rms * tail_rms / (fmax(kk, 1e-30) * fmax(kk, 1e-30) * fmax(kk, 1e-30) * log(k2 / k1)) : 0.0;
+    f = sqrt(P * (double)N * N * N / (L * L * L));
+  } else {
+    f = m == 0 ? 0.0 : 1.0 / kk;
+  }
+  s[m].x *= f;
+  s[m].y *= f;
+}
+
+__global__ void k_axpy_spec(cufftDoubleComplex* __restrict__ y, const cufftDoubleComplex* __restrict__ x, double a,
+                            long long M) {
+  const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= M) return;
+  y[m].x += a * x[m].x;
+  y[m].y += a * x[m].y;
+}
+
+// delta_k (kind 0: 0.4 k^2 zeta_k / H_i^2, pm3d.py:59), zero mode removed; then the four
+// spectra inverted at once: delta_lin = irfftn(dk) (pm3d.py:70) and psi_c = -irfftn(i k_c phi),
+// phi = -dk/k^2 (pm3d.py:61-62).  Each spectrum carries numpy's 1/N^3 and, in the kz = 0 and
+// kz = N/2 planes, its Hermitian part (numpy's irfftn uses only that part there).
+__device__ __forceinline__ void four_spectra(const cufftDoubleComplex z, int kind, double kx, double ky, double kz,
+                                            long long m, double* re, double* im) {
+  const double k2 = m == 0 ? 1.0 : kx * kx + ky * ky + kz * kz;
+  double dr = z.x, di = z.y;
+  if (kind == 0) {
+    const double f = 0.4 * k2 / (PM_H_I * PM_H_I);
+    dr *= f;
+    di *= f;
+  }
+  if (m == 0) dr = di = 0.0;
+  const double pr = -dr / k2, pi = -di / k2;
+  re[0] = dr;
+  im[0] = di;
+  const double kc[3] = {kx, ky, kz};
+  for (int c = 0; c < 3; ++c) {  // -(i k phi) = (k pi, -k pr)
+    re[c + 1] = kc[c] * pi;
+    im[c + 1] = -kc[c] * pr;
+  }
+}
+
+__global__ void k_disp_spectra(const cufftDoubleComplex* __restrict__ s, int N, double L, int kind,
+                               cufftDoubleComplex* __restrict__ out) {
+  const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int Nh = N / 2 + 1;
+  const long long M = (long long)N * N * Nh;
+  if (m >= M) return;
+  const int kz = (int)(m % Nh), iy = (int)((m / Nh) % N), ix = (int)(m / ((long long)Nh * N));
+  const double kf = kTwoPi / L;
+  const double kx = kline(ix, N, kf), ky = kline(iy, N, kf), kzv = kf * kz;
+  double re[4], im[4];
+  four_spectra(s[m], kind, kx, ky, kzv, m, re, im);
+  if (kz == 0 || kz == N / 2) {
+    const int px = (-ix) & (N - 1), py = (-iy) & (N - 1);
+    const long long mp = ((long long)px * N + py) * Nh + kz;
+    double rp[4], ip[4];
+    four_spectra(s[mp], kind, kline(px, N, kf), kline(py, N, kf), kzv, mp, rp, ip);
+    for (int c = 0; c < 4; ++c) {
+      re[c] = 0.5 * (re[c] + rp[c]);
+      im[c] = 0.5 * (im[c] - ip[c]);
+    }
+  }
+  const double inv = 1.0 / ((double)N * N * N);
+  for (int c = 0; c < 4; ++c) {
+    out[c * M + m].x = re[c] * inv;
+    out[c * M + m].y = im[c] * inv;
+  }
+}
+
+// Lattice (pm3d.py:64-65), CIC displacement at (Q + L/2) % L (pm3d.py:66), x and p
+// (pm3d.py:67-68).  Python's float % is x - L*floor(x/L).
+__device__ __forceinline__ double pymod(double x, double L) {
+  double r = fmod(x, L);
+  if (r != 0.0 && ((r < 0) != (L < 0))) r += L;
+  return r;
+}
+
+__global__ void k_lattice(int N, int Np, double L, const double* __restrict__ psi, double* __restrict__ x,
+                          double* __restrict__ p) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n = (long long)Np * Np * Np;
+  if (i >= n) return;
+  const int jz = (int)(i % Np), jy = (int)((i / Np) % Np), jx = (int)(i / ((long long)Np * Np));
+  const double dq = L / Np, dx = L / N;
+  const double Q[3] = {(jx + 0.5) * dq - L / 2, (jy + 0.5) * dq - L / 2, (jz + 0.5) * dq - L / 2};
+  long long i0[3], i1[3];
+  double f[3];
+  for (int d = 0; d < 3; ++d) {
+    const double at = pymod(Q[d] + L / 2, L);
+    const double g = at / dx - 0.5;
+    const double fl = floor(g);
+    const long long c = (long long)fl;
+    f[d] = g - fl;
+    i0[d] = ((c % N) + N) % N;
+    i1[d] = (((c + 1) % N) + N) % N;
+  }
+  const long long N3 = (long long)N * N * N;
+  double disp[3] = {0.0, 0.0, 0.0};
+  for (int c = 0; c < 8; ++c) {
+    const int cx = c >> 2, cy = (c >> 1) & 1, cz = c & 1;
+    const long long o = ((cx ? i1[0] : i0[0]) * N + (cy ? i1[1] : i0[1])) * N + (cz ? i1[2] : i0[2]);
+    const double w = (cx ? f[0] : 1.0 - f[0]) * (cy ? f[1] : 1.0 - f[1]) * (cz ? f[2] : 1.0 - f[2]);
+    for (int d = 0; d < 3; ++d) disp[d] += psi[(1 + d) * N3 + o] * w;
+  }
+  for (int d = 0; d < 3; ++d) {
+    x[3 * i + d] = pymod(Q[d] + disp[d] + L / 2, L);
+    p[3 * i + d] = PM_H_I * disp[d];
+  }
+}
+
+// Block partial sums of x and (x - mean)^2 for numpy's std (mean first, then the spread).
+__global__ void k_partial(const double* __restrict__ v, long long n, double mean, int squares, double* __restrict__ part) {
+  __shared__ double sh[kThreads];
+  double s = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double d = squares ? v[i] - mean : v[i];
+    s += squares ? d * d : d;
+  }
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = kThreads / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+int grid_std(const double* v, long long n, double* out) {
+  const int nb = 1024;
+  double* part = nullptr;
+  std::vector<double> h(nb);
+  double mean = 0.0, var = 0.0;
+  int rc = 0;
+  CU(cudaMalloc(&part, sizeof(double) * nb));
+  k_partial<<<nb, kThreads>>>(v, n, 0.0, 0, part);
+  CU(cudaMemcpy(h.data(), part, sizeof(double) * nb, cudaMemcpyDeviceToHost));
+  for (double d : h) mean += d;
+  mean /= (double)n;
+  k_partial<<<nb, kThreads>>>(v, n, mean, 1, part);
+  CU(cudaMemcpy(h.data(), part, sizeof(double) * nb, cudaMemcpyDeviceToHost));
+  for (double d : h) var += d;
+  *out = std::sqrt(var / (double)n);
+done:
+  cudaFree(part);
+  return rc;
+}
+
+unsigned nblk(long long n) { return (unsigned)((n + kThreads - 1) / kThreads); }
+
+}  // namespace
+
+extern "C" int pm_make_ic(const pm_ic_params* prm, double* x_out, double* p_out, double* delta_lin_out,
+                          double* noise_rms_out) {
+  if (!prm || !x_out || !p_out) return -2000;
+  const int N = prm->N, Np = prm->Np;
+  if (N < 4 || (N & (N - 1)) || Np < 1 || !(prm->L > 0)) return -2001;
+  if (prm->kind == 0 && (!prm->spline_x || !prm->spline_c || prm->spline_m < 1)) return -2002;
+  if (prm->kind != 0 && prm->kind != 1) return -2003;
+  const long long N3 = (long long)N * N * N, M = (long long)N * N * (N / 2 + 1);
+  const double L = prm->L;
+  int rc = 0;
+  double *field = nullptr, *xs = nullptr, *cs = nullptr, *real4 = nullptr, *tmp_real = nullptr;
+  cufftDoubleComplex *spec = nullptr, *nspec = nullptr, *spec4 = nullptr, *tmp_spec = nullptr;
+  cufftHandle d2z = 0, z2d = 0, z2d4 = 0;
+  bool has_d2z = false, has_z2d = false, has_z2d4 = false;
+  double noise_rms = 0.0;
+  const bool noisy = prm->noise && ((prm->kind == 0 && prm->tail_rms > 0) || (prm->kind == 1 && prm->noise_frac > 0));
+
+  CU(cudaMalloc(&field, sizeof(double) * N3));
+  CU(cudaMalloc(&spec, sizeof(cufftDoubleComplex) * M));
+  CU(cudaMalloc(&spec4, sizeof(cufftDoubleComplex) * 4 * M));
+  CU(cudaMalloc(&real4, sizeof(double) * 4 * N3));
+  if (prm->kind == 0) {
+    const int m = prm->spline_m;
+    CU(cudaMalloc(&xs, sizeof(double) * (m + 1)));
+    CU(cudaMalloc(&cs, sizeof(double) * 4 * m));
+    CU(cudaMemcpy(xs, prm->spline_x, sizeof(double) * (m + 1), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(cs, prm->spline_c, sizeof(double) * 4 * m, cudaMemcpyHostToDevice));
+  }
+  CF(cufftPlan3d(&d2z, N, N, N, CUFFT_D2Z));
+  has_d2z = true;
+  {
+    int n3[3] = {N, N, N};
+    CF(cufftPlanMany(&z2d4, 3, n3, nullptr, 1, 0, nullptr, 1, 0, CUFFT_Z2D, 4));
+    has_z2d4 = true;
+  }
+  k_field<<<nblk(N3), kThreads>>>(N, L, prm->kind, prm->amp, prm->axes[0], prm->axes[1], prm->axes[2], xs, cs,
+                                  prm->kind == 0 ? prm->spline_m : 0, field);
+  CU(cudaGetLastError());
+  CF(cufftExecD2Z(d2z, field, spec));
+  if (noisy) {
+    CU(cudaMalloc(&nspec, sizeof(cufftDoubleComplex) * M));
+    CU(cudaMalloc(&tmp_spec, sizeof(cufftDoubleComplex) * M));
+    CU(cudaMalloc(&tmp_real, sizeof(double) * N3));
+    CF(cufftPlan3d(&z2d, N, N, N, CUFFT_Z2D));
+    has_z2d = true;
+    CF(cufftExecD2Z(d2z, (double*)prm->noise, nspec));
+    k_shape<<<nblk(M), kThreads>>>(nspec, N, L, prm->kind, prm->tail_rms, prm->k1, prm->k2);
+    CU(cudaGetLastError());
+    CU(cudaMemcpy(tmp_spec, nspec, sizeof(cufftDoubleComplex) * M, cudaMemcpyDeviceToDevice));
+    CF(cufftExecZ2D(z2d, tmp_spec, tmp_real));  // unnormalised inverse; numpy divides by N^3
+    rc = grid_std(tmp_real, N3, &noise_rms);
+    if (rc) goto done;
+    noise_rms /= (double)N3;
+    const double scale = prm->kind == 0 ? 1.0 : prm->noise_frac * prm->amp / noise_rms;
+    k_axpy_spec<<<nblk(M), kThreads>>>(spec, nspec, scale, M);
+    CU(cudaGetLastError());
+  }
+  k_disp_spectra<<<nblk(M), kThreads>>>(spec, N, L, prm->kind, spec4);
+  CU(cudaGetLastError());
+  CF(cufftExecZ2D(z2d4, spec4, real4));
+  k_lattice<<<nblk((long long)Np * Np * Np), kThreads>>>(N, Np, L, real4, x_out, p_out);
+  CU(cudaGetLastError());
+  if (delta_lin_out) CU(cudaMemcpy(delta_lin_out, real4, sizeof(double) * N3, cudaMemcpyDeviceToDevice));
+  CU(cudaDeviceSynchronize());
+  if (noise_rms_out) *noise_rms_out = noise_rms;
+done:
+  if (has_d2z) cufftDestroy(d2z);
+  if (has_z2d) cufftDestroy(z2d);
+  if (has_z2d4) cufftDestroy(z2d4);
+  cudaFree(field);
+  cudaFree(xs);
+  cudaFree(cs);
+  cudaFree(real4);
+  cudaFree(tmp_real);
+  cudaFree(spec);
+  cudaFree(nspec);
+  cudaFree(spec4);
+  cudaFree(tmp_spec);
+  return rc;
+}

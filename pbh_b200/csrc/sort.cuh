@@ -1,0 +1,56 @@
+// Segmented, stable LSD radix sort of 64-bit keys with 32-bit values (sm_100a).
+//
+// One launch per 8-bit digit.  Each CTA ranks a tile of SORT_TILE keys with warp-level
+// multi-split (match.any + popc), publishes its digit counts and resolves its global
+// offsets by decoupled look-back over the preceding tiles of the same segment, so every
+// pass reads and writes each key once.  Tiles are claimed in order through an atomic
+// counter, which guarantees that every tile a CTA waits on is already running.  Waits are
+// bounded: a CTA that gives up sets the error word and proceeds.
+//
+// A segment is a contiguous key range sorted independently (one peak of the ensemble).
+// Because every key of a segment carries the same high word (the peak id), sorting the
+// segments separately over the low-word bit range [lo, lo + 8*npass) produces exactly the
+// order of a stable sort of the full 64-bit keys.  A plan whose single segment has lo = 0
+// and npass = 8 is a plain sort of arbitrary 64-bit keys.
+#pragma once
+#include "common.cuh"
+
+#define SORT_THREADS 256
+#define SORT_WARPS (SORT_THREADS / 32)
+#define SORT_IPT 16
+#define SORT_TILE (SORT_THREADS * SORT_IPT)
+#define SORT_RADIX 256
+#define SORT_MAX_PASSES 8
+
+struct SortSeg {
+  long long begin, end;  // key range
+  int lo;                // first key bit sorted in this segment
+  int hi;                // one past the last key bit sorted (bits >= hi are ignored)
+  int active;            // 0: skip (the segment's buffers are left untouched)
+  int pad;
+};
+
+struct SortPlan {
+  int nseg;
+  int ntiles;
+  int npass;             // digit passes (the same for every segment)
+  SortSeg* seg;          // [nseg] (device)
+  int* tile_seg;         // [ntiles]
+  long long* tile_begin; // [ntiles]
+  int* tile_first;       // [ntiles] 1 when the tile opens its segment
+  u32* hist;             // [nseg][SORT_MAX_PASSES][256]
+  long long* base;       // [nseg][SORT_MAX_PASSES][256]
+  u64* status;           // [ntiles][256] look-back words: epoch<<34 | flag<<32 | count
+  u32* counters;         // [SORT_MAX_PASSES] tile claims, then the epoch word
+  int* err;              // nonzero after a bounded wait gave up
+};
+
+// Host side (sort.cu).  `segs` is a host array.
+int sort_plan_create(SortPlan* plan, const SortSeg* segs, int nseg, int npass);
+void sort_plan_destroy(SortPlan* plan);
+// Runs plan->npass passes, ping-ponging (k0,v0) -> (k1,v1) -> (k0,v0) ...  The sorted
+// result is in (k0,v0) when npass is even, (k1,v1) when odd.  identity_vals ignores the
+// contents of v0 and uses value = global index.  write_last_keys = false skips writing the
+// keys on the last pass (only the permutation is then produced).
+int sort_run(const SortPlan* plan, u64* k0, u32* v0, u64* k1, u32* v1, bool identity_vals,
+             bool write_last_keys, cudaStream_t s);
