@@ -1,0 +1,331 @@
+#!/usr/bin/env python
+"""Benchmark of the pm3d particle-mesh step on B200: PM particle-steps/s of the batched
+ensemble (64 peaks, meshes 32^3..256^3, one graph replay per step), with the plain single-run
+path on the same peaks, per-kernel HBM roofline, an end-to-end job through the public API,
+and the CPU reference timed on the host.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload batched|plain256|plain512]
+    python bench.py --impl reference ...      # the reference algorithm on the host cores
+
+One JSON line on stdout (rank 0).  Multi-GPU runs (torchrun) give every rank its own
+ensemble (independent peaks, no data-path collective): weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+METRIC = "PM particle-steps/s batched vs plain on 1 B200 at FP64-oracle tol; p50/p99 latency"
+UNIT = "particle-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["batched", "plain256", "plain512"], default="batched")
+    ap.add_argument("--npeaks", type=int, default=64)
+    ap.add_argument("--seed", type=int, default=1234)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--bucket-sort", action="store_true", help="sort only the bucket bits each step")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------------------ workloads
+def workload_specs(name: str, npeaks: int, seed: int, rank: int):
+    from pbh_b200 import recipe
+    if name == "batched":
+        specs = recipe.ensemble(npeaks=npeaks, steps=150, seed=seed + 1000 * rank)
+        desc = {"workload": f"batched ensemble: {npeaks} peaks, meshes from {{32,64,128,256}}^3 with particles = "
+                            "cells, e~U[0,0.3], p~U[-0.1,0.1], delta0 log-uniform over collapse a in [0.3,1], "
+                            "150 KDK steps over a_cfg 0.01..1, seeded k^-2 noise"}
+    elif name == "plain256":
+        specs = [recipe.single_peak(N=256, steps=200, seed=seed + rank)]
+        desc = {"workload": "plain single run: 256^3 mesh, 256^3 particles, R=(0.10,0.09,0.08)L, "
+                            "collapse of the first axis at a_cfg=0.8, 200 steps"}
+    else:
+        specs = [recipe.large_peak(N=512, steps=300, seed=seed + rank)]
+        desc = {"workload": "large single run: 512^3 mesh and particles, e=0.3, p=0.1, collapse a_cfg=0.5, 300 steps"}
+    return specs, desc
+
+
+# ------------------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait()
+        rows = [r.split(",") for r in Path(self.path).read_text().strip().splitlines() if r.strip()]
+        os.unlink(self.path)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows if len(r) >= 9 for k in range(4) if r[5 + k].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------------------------ CPU side
+def _cpu_worker(args):
+    """One peak of the recipe on the CPU oracle (float64 numpy restatement of pm3d):
+    IC, `warmup` untimed steps, then `steps` timed steps.  Returns (n, seconds)."""
+    N, R, delta0, seed, ratio, steps, warmup = args
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    import warnings
+    warnings.filterwarnings("ignore")
+    from oracle import pm3d_oracle as O
+    from oracle.recipe_oracle import recipe_ic
+    mesh = O.Mesh(N, 1.0, N)
+    ic = recipe_ic(mesh, R, delta0, 0.01, seed)
+    tr = O.Trajectory(mesh, ic["x"], ic["p"])
+    a = 1.0
+    for _ in range(warmup):
+        a, _d = tr.step(a, a * ratio)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        a, _d = tr.step(a, a * ratio)
+    return N ** 3, time.perf_counter() - t0
+
+
+def cpu_rate(specs, steps: int, warmup: int, max_mesh: int, workers: int | None = None) -> dict:
+    """The oracle port of the reference path on the host cores, one peak per worker process
+    (spawned), the reference's own pattern for many runs (pbhgr/pbhgr/scan.py:223-232)."""
+    import multiprocessing as mp
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    workers = workers or cores
+    sample = [s for s in specs if s.N <= max_mesh] or specs
+    tasks = [(s.N, tuple(s.R), s.delta0, s.seed, s.ratio(), steps, warmup) for s in
+             (sample * (workers // len(sample) + 1))[:workers]]
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(len(tasks)) as pool:
+        res = pool.map(_cpu_worker, tasks)
+    wall = time.perf_counter() - t0
+    ps = sum(n * steps for n, _ in res)
+    tmax = max(t for _, t in res)
+    import platform
+    return {"value": ps / tmax, "unit": UNIT, "cores": len(tasks), "kind": "port",
+            "sample": f"{len(tasks)} peaks (one per core) with meshes {sorted({t[0] for t in tasks})}^3 from the "
+                      f"same recipe, {steps} timed KDK steps each after {warmup} untimed, float64 numpy oracle",
+            "host_cpus": cores, "cpu": platform.processor() or platform.machine(), "wall_s": wall}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    specs, desc = workload_specs(args.workload, args.npeaks, args.seed, 0)
+    max_mesh = 128 if args.workload == "batched" else 64
+    cb = cpu_rate(specs, args.steps, args.warmup, max_mesh)
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(desc, sample_meshes_max=max_mesh),
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------ GPU side
+# Algorithmic bytes per launch of each kernel: n = particles, m = modes.
+def algorithmic_bytes(phase: str, n: int, cells: int, modes: int, npass: int) -> float:
+    if phase == "push":
+        return n * (32 + 32 + 8) + cells * 12.0
+    if phase == "sort":
+        return n * (8.0 + npass * 24.0 - 4.0)
+    if phase == "deposit":
+        return n * 16.0 + cells * 4.0
+    if phase == "green":
+        return modes * 32.0
+    if phase == "bucket":
+        return n * 8.0
+    return 0.0
+
+
+PHASES = ["push", "advance", "sort", "bucket", "deposit", "r2c", "green", "c2r"]
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    from pbh_b200 import _lib
+    from pbh_b200.batch import Ensemble, plain_rate
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    specs, desc = workload_specs(args.workload, args.npeaks, args.seed, rank)
+    need = 1 + args.warmup + args.steps
+    if need > min(s.steps for s in specs):
+        raise SystemExit(f"warmup + steps ({need}) exceed the run length ({min(s.steps for s in specs)})")
+    ens = Ensemble(specs, device=local, bucket_sort=args.bucket_sort)
+    lib = _lib.load()
+    info = (np.zeros(6, dtype=np.int64))
+    lib.pm_engine_info(ens.engine._h, info.ctypes.data)
+    npass = int(info[3])
+    ens.load()
+    ens.step(1 + args.warmup)                     # prime + warm-up steps
+    stream = torch.cuda.ExternalStream(lib.pm_engine_stream(ens.engine._h), device=local)
+    n_step = ens.active_particles()
+    assert n_step == ens.n_particles, "every peak must be stepping during the timed region"
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    ens.engine.sync()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    e0.record(stream)
+    ens.step(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    t = e0.elapsed_time(e1) / 1e3
+    if dist:
+        tt = torch.tensor([t], device=f"cuda:{local}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t = float(tt.item())
+    value = world * n_step * args.steps / t
+    ms_per_step = t / args.steps * 1e3
+
+    # Per-kernel device times: a few ungraphed steps with events between phases, same stream.
+    ph = ens.timed_phases(3)
+    cells = sum(s.N ** 3 for s in specs)
+    modes = sum(s.N * s.N * (s.N // 2 + 1) for s in specs)
+    kern = {}
+    for k, name in enumerate(PHASES):
+        b = algorithmic_bytes(name, n_step, cells, modes, npass)
+        kern[name] = {"ms": ph[k], "algorithmic_bytes": b, "gbs": (b / (ph[k] / 1e3) / 1e9) if b and ph[k] > 0 else None}
+    peaks_file = ROOT / "MEASURED_PEAKS.json"
+    if peaks_file.exists():
+        hbm = float(json.loads(peaks_file.read_text())["hbm_gbs"])
+        hbm_src = "measured"
+    else:
+        hbm, hbm_src = 6650.0, "fallback"
+    ours = {k: v for k, v in kern.items() if k in ("push", "sort", "deposit", "green", "bucket")}
+    top = max(ours, key=lambda k: ours[k]["ms"])
+    roofline = {"bound": "hbm", "kernel": top, "achieved": kern[top]["gbs"], "peak": hbm, "unit": "GB/s",
+                "frac": kern[top]["gbs"] / hbm, "traffic": None, "peak_source": hbm_src,
+                "per_kernel": {k: {"ms": round(v["ms"], 4), "gbs": None if v["gbs"] is None else round(v["gbs"], 1),
+                                   "frac": None if v["gbs"] is None else round(v["gbs"] / hbm, 3)}
+                               for k, v in kern.items()},
+                "fft_ms": round(ph[5] + ph[7], 4), "step_ms_ungraphed": round(float(ph.sum()), 4)}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (fields, offsets, momenta; i32 cells; i64 fixed-point density sums)",
+            "data": "synthetic (recipe peaks, seeded numpy noise)",
+            "config": dict(desc, particles_per_gpu=n_step, peaks=len(specs), l2="inputs larger than L2 (126 MB)",
+                           sort_bits="bucket" if args.bucket_sort else "full key", parallelism=f"replicas x{world}"),
+            "clocks": clocks, "gpu_launches": args.steps * (7 + npass), "roofline": roofline}
+
+    if rank == 0 and not args.no_plain and args.workload == "batched":
+        pr = plain_rate(specs, steps=8, warmup=3, device=local)
+        line["plain"] = dict(pr, batched_over_plain=value / world / pr["particle_steps_per_s"],
+                             how="each peak alone in a single-peak engine, sequentially, same kernels")
+
+    if not args.no_e2e:
+        line["e2e"] = e2e_job(ens, specs, torch, local)
+    ens.close()
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cb = cpu_rate(specs, steps=2, warmup=1, max_mesh=128 if args.workload == "batched" else 64)
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def e2e_job(ens, specs, torch, device):
+    """The whole job through the public batch API: per-peak noise fields start in pinned host
+    memory, are copied to the device, turned into particles (device IC), then every step runs
+    and its per-peak statistics are read back to the host."""
+    import numpy as np
+    noises = []
+    for s in specs:
+        h = torch.empty((s.N,) * 3, dtype=torch.float64).pin_memory()
+        h.numpy()[...] = np.random.default_rng(s.seed).standard_normal((s.N,) * 3)
+        noises.append(h)
+    h2d = sum(int(h.numel()) * 8 for h in noises)
+    steps = min(s.steps for s in specs)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ens.load(noises=noises)
+    stats_bytes = 0
+    done = 0
+    for _ in range(steps + 2):                   # prime + steps + closing kick
+        ens.step(1)
+        st = ens.stats()
+        stats_bytes += len(st) * 32
+        done += 1
+    torch.cuda.synchronize()
+    t = time.perf_counter() - t0
+    del noises
+    ps = sum(s.n for s in specs) * steps
+    return {"value": ps / t, "unit": UNIT, "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step": stats_bytes / done,
+            "job_steps": steps, "seconds": t,
+            "how": "public Ensemble API: pinned host noise -> device IC -> all steps, per-step stats to host; wall clock"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -57,6 +57,7 @@ typedef struct {
   double kpend;   /* pending closing-kick coefficient (0 when p is complete) */
   double a_grid;  /* expansion factor the force grids were computed for */
   int mode, state, nsteps, max_steps;
+  double a_collapse; /* first a at which max delta reached the collapse threshold, -1 if not yet */
 } pm_clock_info;
 
 typedef struct {
@@ -86,6 +87,15 @@ int pm_set_particles(pm_engine* e, int peak, const double* x, const double* p, d
  * Replaces: the driver loop of pbhgr/scripts/pm3d_peak.py:26-28. */
 int pm_run(pm_engine* e, int nsteps);
 
+/* pm_run without the graph, with a CUDA event between kernel phases on the engine's stream;
+ * adds each phase's device time (ms) into phase_ms[8]: push, advance, sort, bucket starts,
+ * deposit, R2C, Green, C2R.  Used for per-kernel roofline figures. */
+int pm_run_timed(pm_engine* e, int nsteps, double* phase_ms);
+/* The engine's CUDA stream (cudaStream_t), for events and stream ordering by callers. */
+void* pm_engine_stream(pm_engine* e);
+/* info[6]: npeaks, particles, tiles, sort passes per step, mesh classes, device bytes. */
+int pm_engine_info(const pm_engine* e, long long* info);
+
 /* PM3D.step(a, da) for one peak (pm3d.py:117-129): a KDK step from a to a + da.  Forces at
  * a are reused when the peak's current state is at a (pm3d.py:119), else recomputed. */
 int pm_step_explicit(pm_engine* e, int peak, double a, double da);
@@ -99,8 +109,14 @@ int pm_get_acc(pm_engine* e, int peak, double a, double* acc);
 int pm_get_delta(pm_engine* e, int peak, float* delta);
 /* Float64 CIC counts of the current positions (N^3): PM3D.deposit(PM3D.x) (pm3d.py:81-89). */
 int pm_get_counts(pm_engine* e, int peak, double* counts);
+/* Collapse time tracking: the first a at which max delta of the peak's deposit reaches
+ * delta_collapse is recorded on the device (pm_clock_info.a_collapse).  <= 0 disables. */
+int pm_set_collapse_threshold(pm_engine* e, int peak, double delta_collapse);
 int pm_get_clock(pm_engine* e, int peak, pm_clock_info* out);   /* host struct */
 int pm_get_stats(pm_engine* e, int peak, pm_stats_info* out);   /* host struct */
+/* All peaks at once (host arrays of npeaks); the return value counts flagged peaks. */
+int pm_get_stats_all(pm_engine* e, pm_stats_info* out);
+int pm_get_clocks_all(pm_engine* e, pm_clock_info* out);
 
 /* Initial particles on the GPU in float64 (setup call: allocates and frees its temporaries).
  * kind 0 = PM3D.make_ic(mu, profile_spline, e, p, tail_rms, tail_k) (pm3d.py:40-73): amp = mu,

@@ -24,7 +24,7 @@ class PeakCfg(C.Structure):
 class ClockInfo(C.Structure):
     _fields_ = [("a", C.c_double), ("da", C.c_double), ("a_end", C.c_double), ("kpend", C.c_double),
                 ("a_grid", C.c_double), ("mode", C.c_int), ("state", C.c_int), ("nsteps", C.c_int),
-                ("max_steps", C.c_int)]
+                ("max_steps", C.c_int), ("a_collapse", C.c_double)]
 
 
 class StatsInfo(C.Structure):
@@ -48,11 +48,17 @@ _SIGS = {
     "pm_set_particles": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_int, C.c_double,
                                    C.c_double, C.c_int]),
     "pm_run": (C.c_int, [C.c_void_p, C.c_int]),
+    "pm_run_timed": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "pm_engine_stream": (C.c_void_p, [C.c_void_p]),
+    "pm_engine_info": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "pm_get_stats_all": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "pm_get_clocks_all": (C.c_int, [C.c_void_p, C.c_void_p]),
     "pm_step_explicit": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double]),
     "pm_get_particles": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "pm_get_acc": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_void_p]),
     "pm_get_delta": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "pm_get_counts": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "pm_set_collapse_threshold": (C.c_int, [C.c_void_p, C.c_int, C.c_double]),
     "pm_get_clock": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(ClockInfo)]),
     "pm_get_stats": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(StatsInfo)]),
     "pm_make_ic": (C.c_int, [C.POINTER(ICParams), C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]),

@@ -77,6 +77,8 @@ struct PeakClock {
   int dep;         // 1 when this step re-deposits (set by the advance kernel)
   int has_delta;   // delta/grids hold data
   int pad;
+  double delta_collapse;  // collapse threshold on max delta (<= 0: not tracked)
+  double a_collapse;      // first a whose deposit reached delta_collapse (-1: not yet)
 };
 
 // Per-peak device statistics.  Integer fields are reduced with integer atomics

@@ -117,6 +117,36 @@ struct pm_engine {
     return 0;
   }
 
+  // The step with an event between phases, for per-kernel device times (phase_ms accumulates).
+  int launch_step_timed(cudaEvent_t* ev, double* phase_ms) {
+    const StepArgs A = args();
+    CU(cudaEventRecord(ev[0], stream));
+    launch_push(A, ntiles, smem_push, stream);
+    CU(cudaEventRecord(ev[1], stream));
+    launch_advance(A, stream);
+    CU(cudaEventRecord(ev[2], stream));
+    int r = sort_run(&sort, keys[0], vals[0], keys[1], vals[1], true, true, stream);
+    if (r) return r;
+    CU(cudaEventRecord(ev[3], stream));
+    launch_bucket_starts(A, ntot, stream);
+    CU(cudaEventRecord(ev[4], stream));
+    launch_deposit(A, ntiles, smem_dep, nullptr, stream);
+    CU(cudaEventRecord(ev[5], stream));
+    for (auto& c : classes) CF(cufftExecR2C(c.r2c, c.delta, (cufftComplex*)c.spec));
+    CU(cudaEventRecord(ev[6], stream));
+    launch_green(A, nmodeblk, stream);
+    CU(cudaEventRecord(ev[7], stream));
+    for (auto& c : classes) CF(cufftExecC2R(c.c2r, (cufftComplex*)c.gspec, c.force));
+    CU(cudaEventRecord(ev[8], stream));
+    CU(cudaEventSynchronize(ev[8]));
+    for (int k = 0; k < 8; ++k) {
+      float ms = 0.f;
+      CU(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+      phase_ms[k] += ms;
+    }
+    return 0;
+  }
+
   int step() {
     if (flags & 2) {
       if (!graph) {
@@ -302,6 +332,7 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   for (auto& c : clocks) {
     c = PeakClock{};
     c.state = PS_IDLE;
+    c.a_collapse = -1.0;
   }
   CU(cudaMemcpy(E->d_clocks, clocks.data(), sizeof(PeakClock) * npeaks, cudaMemcpyHostToDevice));
   CU(cudaMemset(E->d_stats, 0, sizeof(PeakStats) * npeaks));
@@ -393,6 +424,71 @@ int pm_run(pm_engine* e, int nsteps) {
   return 0;
 }
 
+int pm_run_timed(pm_engine* e, int nsteps, double* phase_ms) {
+  if (!e || nsteps < 0 || !phase_ms) return -2000;
+  CU(cudaSetDevice(e->device));
+  cudaEvent_t ev[9];
+  for (int k = 0; k < 9; ++k) CU(cudaEventCreate(&ev[k]));
+  int r = 0;
+  for (int s = 0; s < nsteps && !r; ++s) r = e->launch_step_timed(ev, phase_ms);
+  for (int k = 0; k < 9; ++k) cudaEventDestroy(ev[k]);
+  return r;
+}
+
+void* pm_engine_stream(pm_engine* e) { return e ? (void*)e->stream : nullptr; }
+
+int pm_engine_info(const pm_engine* e, long long* info) {
+  if (!e || !info) return -2000;
+  info[0] = e->npeaks;
+  info[1] = e->ntot;
+  info[2] = e->ntiles;
+  info[3] = e->sort.npass;
+  info[4] = (long long)e->classes.size();
+  info[5] = e->bytes;
+  return 0;
+}
+
+int pm_get_stats_all(pm_engine* e, pm_stats_info* out) {
+  if (!e || !out) return -2000;
+  CU(cudaSetDevice(e->device));
+  std::vector<PeakStats> s(e->npeaks);
+  int err = 0;
+  CU(cudaMemcpyAsync(s.data(), e->d_stats, sizeof(PeakStats) * e->npeaks, cudaMemcpyDeviceToHost, e->stream));
+  CU(cudaMemcpyAsync(&err, e->sort.err, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+  CU(cudaStreamSynchronize(e->stream));
+  int flagged = 0;
+  for (int i = 0; i < e->npeaks; ++i) {
+    const PeakDesc& P = e->peaks[i];
+    out[i].rho_max_over_mean = (double)s[i].max_fix / (double)PM_FIX_ONE / P.n_mean;
+    out[i].delta_max = out[i].rho_max_over_mean - 1.0;
+    out[i].mass_defect = (double)s[i].mass_defect / (double)PM_FIX_ONE;
+    out[i].status = s[i].status | (err ? 2u : 0u);
+    flagged += out[i].status != 0;
+  }
+  return flagged;
+}
+
+int pm_get_clocks_all(pm_engine* e, pm_clock_info* out) {
+  if (!e || !out) return -2000;
+  CU(cudaSetDevice(e->device));
+  std::vector<PeakClock> c(e->npeaks);
+  CU(cudaMemcpyAsync(c.data(), e->d_clocks, sizeof(PeakClock) * e->npeaks, cudaMemcpyDeviceToHost, e->stream));
+  CU(cudaStreamSynchronize(e->stream));
+  for (int i = 0; i < e->npeaks; ++i) {
+    out[i].a = c[i].a;
+    out[i].da = c[i].da;
+    out[i].a_end = c[i].a_end;
+    out[i].kpend = c[i].kpend;
+    out[i].a_grid = c[i].a_grid;
+    out[i].mode = c[i].mode;
+    out[i].state = c[i].state;
+    out[i].nsteps = c[i].nsteps;
+    out[i].max_steps = c[i].max_steps;
+    out[i].a_collapse = c[i].a_collapse;
+  }
+  return 0;
+}
+
 int pm_step_explicit(pm_engine* e, int peak, double a, double da) {
   if (!e || peak < 0 || peak >= e->npeaks) return -2000;
   if (!(a > 0) || !(da > 0)) return -2001;
@@ -475,6 +571,16 @@ int pm_get_counts(pm_engine* e, int peak, double* counts) {
   return 0;
 }
 
+int pm_set_collapse_threshold(pm_engine* e, int peak, double delta_collapse) {
+  if (!e || peak < 0 || peak >= e->npeaks) return -2000;
+  CU(cudaSetDevice(e->device));
+  PeakClock c;
+  int r;
+  if ((r = e->read_clock(peak, &c))) return r;
+  c.delta_collapse = delta_collapse;
+  return e->write_clock(peak, c);
+}
+
 int pm_get_clock(pm_engine* e, int peak, pm_clock_info* out) {
   if (!e || peak < 0 || peak >= e->npeaks || !out) return -2000;
   CU(cudaSetDevice(e->device));
@@ -490,6 +596,7 @@ int pm_get_clock(pm_engine* e, int peak, pm_clock_info* out) {
   out->state = c.state;
   out->nsteps = c.nsteps;
   out->max_steps = c.max_steps;
+  out->a_collapse = c.a_collapse;
   return 0;
 }
 

@@ -144,6 +144,12 @@ __global__ void k_advance(StepArgs A) {
   for (int pk = threadIdx.x; pk < A.npeaks; pk += blockDim.x) {
     PeakClock c = A.clocks[pk];
     int dep = 0;
+    // Collapse detection on the deposit of the current positions (made by the previous step).
+    if (c.has_delta && c.delta_collapse > 0 && c.a_collapse < 0 && c.state != PS_PRIME) {
+      const PeakDesc& P = A.peaks[pk];
+      const double dmax = (double)A.stats[pk].max_fix / (double)PM_FIX_ONE / P.n_mean - 1.0;
+      if (dmax >= c.delta_collapse) c.a_collapse = c.a;
+    }
     switch (c.state) {
       case PS_PRIME:
         dep = 1;
@@ -421,6 +427,7 @@ __global__ void k_reset_peak(StepArgs A, int pk, double a0, int mode, double par
   c.state = PS_PRIME;
   c.has_delta = 0;
   c.dep = 0;
+  c.a_collapse = -1.0;
   if (mode == SCHED_RATIO) c.da = a0 * param;
   else if (mode == SCHED_FRAC) c.da = fmin(param * a0, a_end - a0);
   else c.da = 0.0;

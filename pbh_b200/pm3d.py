@@ -21,6 +21,7 @@ import numpy as np
 from . import _lib
 from ._lib import check
 from .engine import Engine, PeakConfig, interp64
+from .ic import make_particles
 
 H_I = 5.0                                   # pm3d.py:15-17
 T_I = 2.0 / (3.0 * H_I)
@@ -79,39 +80,15 @@ class PM3D:
 
     # ------------------------------------------------------------------ initial data
     def _ic(self, kind, amp, axes, spline=None, noise=None, tail_rms=0.0, tail_k=(2.0, 10.0), noise_frac=0.0):
-        torch = self._torch
-        dev = f"cuda:{self.device}"
-        n = self.Np ** 3
-        x = torch.empty((n, 3), dtype=torch.float64, device=dev)
-        p = torch.empty_like(x)
-        dl = torch.empty((self.N,) * 3, dtype=torch.float64, device=dev)
-        prm = _lib.ICParams()
-        prm.N, prm.Np, prm.L, prm.kind, prm.amp = self.N, self.Np, self.L, kind, float(amp)
-        prm.axes = (C.c_double * 3)(*[float(v) for v in axes])
-        keep = []
-        if spline is not None:
-            xs = np.ascontiguousarray(spline.x, dtype=np.float64)
-            cs = np.ascontiguousarray(spline.c, dtype=np.float64)
-            if cs.shape[0] != 4:
-                raise ValueError("profile_spline must be a cubic piecewise polynomial (scipy CubicSpline)")
-            keep += [xs, cs]
-            prm.spline_x = xs.ctypes.data_as(C.c_void_p)
-            prm.spline_c = cs.ctypes.data_as(C.c_void_p)
-            prm.spline_m = cs.shape[1]
-        nt = None
-        if noise is not None:
-            nt = torch.as_tensor(noise, dtype=torch.float64, device=dev).contiguous()
-            prm.noise = nt.data_ptr()
-        prm.tail_rms, prm.k1, prm.k2, prm.noise_frac = float(tail_rms), float(tail_k[0]), float(tail_k[1]), float(noise_frac)
-        rms = C.c_double(0.0)
-        torch.cuda.synchronize(dev)
-        check(_lib.load().pm_make_ic(C.byref(prm), x.data_ptr(), p.data_ptr(), dl.data_ptr(), C.byref(rms)), "pm_make_ic")
+        x, p, dl, rms = make_particles(self.N, self.Np, self.L, kind, amp, axes, spline=spline, noise=noise,
+                                       tail_rms=tail_rms, tail_k=tail_k, noise_frac=noise_frac,
+                                       device=self.device, delta_lin=True)
         self._engine.set_particles(0, x, p, 1.0)
         self._loaded = True
         self._delta_lin = dl
         self._ic_xp = (x, p) if getattr(self, "keep_ic", False) else None
         self.A = np.asarray(axes, dtype=np.float64)
-        return float(rms.value)
+        return rms
 
     def make_ic(self, mu, profile_spline, e=0.0, p=0.0, tail_rms=0.0, tail_k=(2.0, 10.0)):
         """Zel'dovich particles of one triaxial peak (pm3d.py:40-73), computed on the GPU in float64."""

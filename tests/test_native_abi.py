@@ -9,7 +9,7 @@ ROOT = Path(__file__).resolve().parent.parent
 
 def header_symbols():
     text = (ROOT / "include" / "pmb200.h").read_text()
-    return sorted(set(re.findall(r"^\s*(?:int|long long)\s+(pm_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|long long|void\*)\s+(pm_\w+)\s*\(", text, re.M)))
 
 
 def test_library_exports_header_symbols():
