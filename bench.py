@@ -42,7 +42,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
-    ap.add_argument("--bucket-sort", action="store_true", help="sort only the bucket bits each step")
+    ap.add_argument("--full-sort", action="store_true", help="sort the whole cell key every step")
     return ap.parse_args()
 
 
@@ -205,7 +205,7 @@ def run_ours(args):
     need = 1 + args.warmup + args.steps
     if need > min(s.steps for s in specs):
         raise SystemExit(f"warmup + steps ({need}) exceed the run length ({min(s.steps for s in specs)})")
-    ens = Ensemble(specs, device=local, bucket_sort=args.bucket_sort)
+    ens = Ensemble(specs, device=local, bucket_sort=not args.full_sort)
     lib = _lib.load()
     info = (np.zeros(6, dtype=np.int64))
     lib.pm_engine_info(ens.engine._h, info.ctypes.data)
@@ -267,7 +267,7 @@ def run_ours(args):
             "vs_baseline": None, "dtype": "f32 (fields, offsets, momenta; i32 cells; i64 fixed-point density sums)",
             "data": "synthetic (recipe peaks, seeded numpy noise)",
             "config": dict(desc, particles_per_gpu=n_step, peaks=len(specs), l2="inputs larger than L2 (126 MB)",
-                           sort_bits="bucket" if args.bucket_sort else "full key", parallelism=f"replicas x{world}"),
+                           sort_bits="full key every step" if args.full_sort else "bucket bits each step, full key every 16th", parallelism=f"replicas x{world}"),
             "clocks": clocks, "gpu_launches": args.steps * (7 + npass), "roofline": roofline}
 
     if rank == 0 and not args.no_plain and args.workload == "batched":

@@ -18,7 +18,7 @@ from .ic import recipe_particles
 
 
 class Ensemble:
-    def __init__(self, specs, device: int = 0, graph: bool = True, bucket_sort: bool = False, tiles=None,
+    def __init__(self, specs, device: int = 0, graph: bool = True, bucket_sort: bool = True, tiles=None,
                  delta_collapse: float = 0.0):
         self.specs = list(specs)
         tiles = tiles or {}

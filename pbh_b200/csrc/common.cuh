@@ -41,7 +41,9 @@ enum ScheduleMode : int {
 };
 
 struct PeakDesc {
-  int N, log2N, T, log2T;
+  int N, log2N, T, log2T;  // T: bucket tile side (sort buckets, deposit tiles)
+  int TP, log2TP;          // push super-tile side, a multiple of T (its sub-tiles are contiguous buckets)
+  int nptiles;             // (N/TP)^3
   int log2NT;       // log2(N/T)
   int ntiles;       // (N/T)^3
   int nb;           // buckets = ntiles*8
@@ -53,6 +55,7 @@ struct PeakDesc {
   double inv_fix_nmean;    // 2^-40 / n_mean
   long long p_off, n;      // particle range in the arena
   long long tile_base;     // first global tile index of this peak
+  long long ptile_base;    // first global push super-tile index of this peak
   long long bucket_off;    // offset of this peak's bucket-start array (nb + 1 entries)
   long long mode_base;     // first global mode-block of this peak (Green kernel)
   long long nmodes;        // N*N*(N/2+1)

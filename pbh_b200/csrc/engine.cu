@@ -52,7 +52,7 @@ struct pm_engine {
   int npeaks = 0;
   std::vector<PeakDesc> peaks;
   std::vector<MeshClass> classes;
-  long long ntot = 0, ntiles = 0, nmodeblk = 0, nbuckets = 0;
+  long long ntot = 0, ntiles = 0, nptiles = 0, nmodeblk = 0, nbuckets = 0;
   int Tmax = 0;
   size_t smem_dep = 0, smem_push = 0;
   // device arrays
@@ -60,16 +60,20 @@ struct pm_engine {
   PeakClock* d_clocks = nullptr;
   PeakStats* d_stats = nullptr;
   long long* d_tile_base = nullptr;
+  long long* d_ptile_base = nullptr;
   long long* d_p_base = nullptr;
   long long* d_mode_base = nullptr;
   int4* pos[2] = {nullptr, nullptr};
   float4* mom[2] = {nullptr, nullptr};
-  u64* keys[2] = {nullptr, nullptr};
+  u32* keys[2] = {nullptr, nullptr};
   u32* vals[2] = {nullptr, nullptr};
   u32* bstart = nullptr;
-  SortPlan sort{};
-  int sort_result = 0;  // which (keys, vals) pair holds the sorted output
-  cudaGraphExec_t graph = nullptr;
+  SortPlan sort{};       // per-step sort: bucket bits only when full_every > 1
+  SortPlan sort_full{};  // whole cell key
+  int full_every = 1;    // full-key sort every this many steps
+  long long replays = 0;
+  int sort_result = 0;  // which (keys, vals) pair holds the sorted output (same for both plans)
+  cudaGraphExec_t graph = nullptr, graph_full = nullptr;
   long long bytes = 0;
 
   StepArgs args() const {
@@ -78,7 +82,9 @@ struct pm_engine {
     A.clocks = d_clocks;
     A.stats = d_stats;
     A.sortseg = sort.seg;
+    A.sortseg_full = sort_full.seg;
     A.tile_base = d_tile_base;
+    A.ptile_base = d_ptile_base;
     A.p_base = d_p_base;
     A.mode_base = d_mode_base;
     A.npeaks = npeaks;
@@ -102,14 +108,15 @@ struct pm_engine {
     return 0;
   }
 
-  int launch_step() {
+  int launch_step(bool full) {
     const StepArgs A = args();
-    launch_push(A, ntiles, smem_push, stream);
+    SortPlan& plan = full ? sort_full : sort;
+    launch_push(A, nptiles, smem_push, stream);
     launch_advance(A, stream);
-    int r = sort_run(&sort, keys[0], vals[0], keys[1], vals[1], true, true, stream);
+    int r = sort_run<u32>(&plan, keys[0], vals[0], keys[1], vals[1], true, true, stream);
     if (r) return r;
     launch_bucket_starts(A, ntot, stream);
-    launch_deposit(A, ntiles, smem_dep, nullptr, stream);
+    launch_deposit(A, nptiles, smem_dep, nullptr, stream);
     for (auto& c : classes) CF(cufftExecR2C(c.r2c, c.delta, (cufftComplex*)c.spec));
     launch_green(A, nmodeblk, stream);
     for (auto& c : classes) CF(cufftExecC2R(c.c2r, (cufftComplex*)c.gspec, c.force));
@@ -117,20 +124,26 @@ struct pm_engine {
     return 0;
   }
 
+  // Whether this engine step sorts the full cell key (the in-tile Morton order is refreshed)
+  // or only the bucket bits the deposit and push depend on.
+  bool next_full() const { return full_every <= 1 || (replays % full_every) == 0; }
+
   // The step with an event between phases, for per-kernel device times (phase_ms accumulates).
   int launch_step_timed(cudaEvent_t* ev, double* phase_ms) {
     const StepArgs A = args();
     CU(cudaEventRecord(ev[0], stream));
-    launch_push(A, ntiles, smem_push, stream);
+    launch_push(A, nptiles, smem_push, stream);
     CU(cudaEventRecord(ev[1], stream));
     launch_advance(A, stream);
     CU(cudaEventRecord(ev[2], stream));
-    int r = sort_run(&sort, keys[0], vals[0], keys[1], vals[1], true, true, stream);
+    const bool full = next_full();
+    ++replays;
+    int r = sort_run<u32>(full ? &sort_full : &sort, keys[0], vals[0], keys[1], vals[1], true, true, stream);
     if (r) return r;
     CU(cudaEventRecord(ev[3], stream));
     launch_bucket_starts(A, ntot, stream);
     CU(cudaEventRecord(ev[4], stream));
-    launch_deposit(A, ntiles, smem_dep, nullptr, stream);
+    launch_deposit(A, nptiles, smem_dep, nullptr, stream);
     CU(cudaEventRecord(ev[5], stream));
     for (auto& c : classes) CF(cufftExecR2C(c.r2c, c.delta, (cufftComplex*)c.spec));
     CU(cudaEventRecord(ev[6], stream));
@@ -148,21 +161,24 @@ struct pm_engine {
   }
 
   int step() {
+    const bool full = next_full();
+    ++replays;
     if (flags & 2) {
-      if (!graph) {
-        cudaGraph_t g = nullptr;
+      cudaGraphExec_t& g = full ? graph_full : graph;
+      if (!g) {
+        cudaGraph_t cg = nullptr;
         CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-        int r = launch_step();
-        cudaError_t ce = cudaStreamEndCapture(stream, &g);
+        int r = launch_step(full);
+        cudaError_t ce = cudaStreamEndCapture(stream, &cg);
         if (r) return r;
         CU(ce);
-        CU(cudaGraphInstantiate(&graph, g, 0));
-        cudaGraphDestroy(g);
+        CU(cudaGraphInstantiate(&g, cg, 0));
+        cudaGraphDestroy(cg);
       }
-      CU(cudaGraphLaunch(graph, stream));
+      CU(cudaGraphLaunch(g, stream));
       return 0;
     }
-    return launch_step();
+    return launch_step(full);
   }
 
   int read_clock(int pk, PeakClock* c) {
@@ -178,6 +194,7 @@ struct pm_engine {
 
   ~pm_engine() {
     if (graph) cudaGraphExecDestroy(graph);
+    if (graph_full) cudaGraphExecDestroy(graph_full);
     for (auto& c : classes) {
       if (c.plans) {
         cufftDestroy(c.r2c);
@@ -189,10 +206,12 @@ struct pm_engine {
       cudaFree(c.force);
     }
     sort_plan_destroy(&sort);
+    sort_plan_destroy(&sort_full);
     cudaFree(d_peaks);
     cudaFree(d_clocks);
     cudaFree(d_stats);
     cudaFree(d_tile_base);
+    cudaFree(d_ptile_base);
     cudaFree(d_p_base);
     cudaFree(d_mode_base);
     for (int b = 0; b < 2; ++b) {
@@ -212,10 +231,10 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   E->npeaks = npeaks;
   E->peaks.resize(npeaks);
   std::map<int, int> class_of;
-  long long poff = 0, tb = 0, mb = 0, bo = 0;
-  int Tmax = 1;
+  long long poff = 0, tb = 0, mb = 0, bo = 0, ptb = 0;
+  int Tmax = 1, TPmax = 1;
   int max_bits = 0, min_lo = 64;
-  std::vector<long long> tile_base(npeaks + 1), p_base(npeaks + 1), mode_base(npeaks + 1);
+  std::vector<long long> tile_base(npeaks + 1), p_base(npeaks + 1), mode_base(npeaks + 1), ptile_base(npeaks + 1);
   for (int i = 0; i < npeaks; ++i) {
     const pm_peak_cfg& c = cfg[i];
     const int l2 = ilog2(c.N);
@@ -223,8 +242,11 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
     const long long npart = c.n > 0 ? c.n : (long long)c.Np * c.Np * c.Np;
     if (c.Np < 1 || npart >= (1LL << 31)) return -2002;
     if (!(c.L > 0)) return -2003;
-    int T = c.tile > 0 ? c.tile : std::min(16, c.N);
-    if (ilog2(T) < 1 || T > c.N) return -2004;
+    // Bucket tiles of 8^3 (4^3 below 32^3); push super-tiles of 16^3 (the mesh when smaller).
+    int T = c.tile > 0 ? c.tile : (c.N >= 32 ? 8 : std::max(2, c.N / 4));
+    if (ilog2(T) < 1 || T > 8 || T > c.N) return -2004;
+    // The push/deposit super-tile is 2T per side (8 bucket tiles), or T when the mesh is one tile.
+    const int TP = std::min(2 * T, c.N);
     PeakDesc& P = E->peaks[i];
     P = PeakDesc{};
     P.N = c.N;
@@ -233,6 +255,10 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
     P.log2T = ilog2(T);
     P.log2NT = l2 - P.log2T;
     P.ntiles = 1 << (3 * P.log2NT);
+    P.TP = TP;
+    P.log2TP = ilog2(TP);
+    P.nptiles = 1 << (3 * (l2 - P.log2TP));
+    P.ptile_base = ptb;
     P.nb = P.ntiles * 8;
     P.local_bits = 3 * P.log2T;
     P.key_bits = 3 * l2 + 3;
@@ -252,6 +278,8 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
     P.nmodes = (long long)c.N * c.N * (c.N / 2 + 1);
     P.mode_base = mb;
     tile_base[i] = tb;
+    ptile_base[i] = ptb;
+    ptb += P.nptiles;
     p_base[i] = poff;
     mode_base[i] = mb;
     poff += P.n;
@@ -259,6 +287,7 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
     bo += P.nb + 1;
     mb += (P.nmodes + PM_THREADS - 1) / PM_THREADS;
     Tmax = std::max(Tmax, T);
+    TPmax = std::max(TPmax, TP);
     max_bits = std::max(max_bits, P.key_bits);
     min_lo = std::min(min_lo, P.local_bits);
     if (!class_of.count(c.N)) {
@@ -269,6 +298,8 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
     E->classes[class_of[c.N]].peaks.push_back(i);
   }
   tile_base[npeaks] = tb;
+  ptile_base[npeaks] = ptb;
+  E->nptiles = ptb;
   p_base[npeaks] = poff;
   mode_base[npeaks] = mb;
   if (poff >= (1LL << 32)) return -2005;
@@ -278,8 +309,8 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   E->nbuckets = bo;
   E->Tmax = Tmax;
   if (int rk = pm_kernels_init()) return rk;
-  E->smem_dep = pm_deposit_smem(Tmax);
-  E->smem_push = pm_push_smem(Tmax);
+  E->smem_dep = pm_deposit_smem(TPmax);
+  E->smem_push = pm_push_smem(TPmax);
 
   // Mesh arenas, one per mesh size, peaks of a class contiguous for batched cuFFT plans.
   for (auto& mc : E->classes) {
@@ -315,6 +346,7 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   if ((r = E->alloc(&E->d_clocks, npeaks))) return r;
   if ((r = E->alloc(&E->d_stats, npeaks))) return r;
   if ((r = E->alloc(&E->d_tile_base, npeaks + 1))) return r;
+  if ((r = E->alloc(&E->d_ptile_base, npeaks + 1))) return r;
   if ((r = E->alloc(&E->d_p_base, npeaks + 1))) return r;
   if ((r = E->alloc(&E->d_mode_base, npeaks + 1))) return r;
   for (int b = 0; b < 2; ++b) {
@@ -326,6 +358,7 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   if ((r = E->alloc(&E->bstart, E->nbuckets))) return r;
   CU(cudaMemcpy(E->d_peaks, E->peaks.data(), sizeof(PeakDesc) * npeaks, cudaMemcpyHostToDevice));
   CU(cudaMemcpy(E->d_tile_base, tile_base.data(), sizeof(long long) * (npeaks + 1), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(E->d_ptile_base, ptile_base.data(), sizeof(long long) * (npeaks + 1), cudaMemcpyHostToDevice));
   CU(cudaMemcpy(E->d_p_base, p_base.data(), sizeof(long long) * (npeaks + 1), cudaMemcpyHostToDevice));
   CU(cudaMemcpy(E->d_mode_base, mode_base.data(), sizeof(long long) * (npeaks + 1), cudaMemcpyHostToDevice));
   std::vector<PeakClock> clocks(npeaks);
@@ -338,23 +371,28 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   CU(cudaMemset(E->d_stats, 0, sizeof(PeakStats) * npeaks));
   CU(cudaMemset(E->bstart, 0, sizeof(u32) * E->nbuckets));
 
-  // Sort plan: one segment per peak.  The whole cell key is sorted every step (bits
-  // [0, key_bits)); with flag bit 0 only the bucket bits [local_bits, key_bits) are.
-  std::vector<SortSeg> segs(npeaks);
-  int max_span = 0;
+  // Sort plans: one segment per peak.  The full plan sorts the whole cell key [0, key_bits);
+  // the per-step plan, when flag bit 0 asks for it, only the bucket bits [local_bits, key_bits)
+  // that the deposit and push group by, keeping the previous in-bucket order (stable).  Both
+  // plans use pass counts of the same parity so the result always lands in the same buffers.
+  E->full_every = (E->flags & 1) ? std::max(1, (E->flags >> 8) & 0xFF) : 1;
+  if ((E->flags & 1) && ((E->flags >> 8) & 0xFF) == 0) E->full_every = 16;
+  std::vector<SortSeg> segs(npeaks), fsegs(npeaks);
+  int span_b = 0, span_f = 0;
   for (int i = 0; i < npeaks; ++i) {
     const PeakDesc& P = E->peaks[i];
-    segs[i].begin = P.p_off;
-    segs[i].end = P.p_off + P.n;
-    segs[i].lo = (E->flags & 1) ? P.local_bits : 0;
-    segs[i].hi = P.key_bits;
-    segs[i].active = 0;
-    max_span = std::max(max_span, P.key_bits - segs[i].lo);
+    fsegs[i] = SortSeg{P.p_off, P.p_off + P.n, 0, P.key_bits, 0, 0};
+    segs[i] = SortSeg{P.p_off, P.p_off + P.n, (E->flags & 1) ? P.local_bits : 0, P.key_bits, 0, 0};
+    span_b = std::max(span_b, P.key_bits - segs[i].lo);
+    span_f = std::max(span_f, P.key_bits);
   }
-  const int npass = (max_span + 7) / 8;
-  if ((r = sort_plan_create(&E->sort, segs.data(), npeaks, npass))) return r;
-  E->bytes += (long long)E->sort.ntiles * SORT_RADIX * 8;
-  E->sort_result = npass & 1;
+  const int np_b = (span_b + SORT_MAX_BITS - 1) / SORT_MAX_BITS;
+  int np_f = (span_f + SORT_MAX_BITS - 1) / SORT_MAX_BITS;
+  if ((np_f & 1) != (np_b & 1)) ++np_f;
+  if ((r = sort_plan_create(&E->sort, segs.data(), npeaks, np_b, span_b))) return r;
+  if ((r = sort_plan_create(&E->sort_full, fsegs.data(), npeaks, np_f, span_f))) return r;
+  E->bytes += (long long)E->sort.ntiles * 8 * ((1LL << E->sort.bits) + (1LL << E->sort_full.bits));
+  E->sort_result = np_b & 1;
   CU(cudaDeviceSynchronize());
   return 0;
 }
@@ -452,9 +490,11 @@ int pm_get_stats_all(pm_engine* e, pm_stats_info* out) {
   if (!e || !out) return -2000;
   CU(cudaSetDevice(e->device));
   std::vector<PeakStats> s(e->npeaks);
-  int err = 0;
+  int err = 0, err2 = 0;
   CU(cudaMemcpyAsync(s.data(), e->d_stats, sizeof(PeakStats) * e->npeaks, cudaMemcpyDeviceToHost, e->stream));
   CU(cudaMemcpyAsync(&err, e->sort.err, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+  CU(cudaMemcpyAsync(&err2, e->sort_full.err, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+  err |= err2;
   CU(cudaStreamSynchronize(e->stream));
   int flagged = 0;
   for (int i = 0; i < e->npeaks; ++i) {
@@ -564,7 +604,7 @@ int pm_get_counts(pm_engine* e, int peak, double* counts) {
   st.mass_defect = 0;
   CU(cudaMemcpy(e->d_stats + peak, &st, sizeof(PeakStats), cudaMemcpyHostToDevice));
   // Same kernel with the extra float64 output; delta is rewritten with identical values.
-  launch_deposit(e->args(), e->ntiles, e->smem_dep, counts, e->stream);
+  launch_deposit(e->args(), e->nptiles, e->smem_dep, counts, e->stream);
   CU(cudaGetLastError());
   CU(cudaStreamSynchronize(e->stream));
   CU(cudaMemcpy(e->d_clocks, all.data(), sizeof(PeakClock) * e->npeaks, cudaMemcpyHostToDevice));
@@ -604,9 +644,11 @@ int pm_get_stats(pm_engine* e, int peak, pm_stats_info* out) {
   if (!e || peak < 0 || peak >= e->npeaks || !out) return -2000;
   CU(cudaSetDevice(e->device));
   PeakStats s;
-  int err = 0;
+  int err = 0, err2 = 0;
   CU(cudaMemcpyAsync(&s, e->d_stats + peak, sizeof(PeakStats), cudaMemcpyDeviceToHost, e->stream));
   CU(cudaMemcpyAsync(&err, e->sort.err, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+  CU(cudaMemcpyAsync(&err2, e->sort_full.err, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+  err |= err2;
   CU(cudaStreamSynchronize(e->stream));
   const PeakDesc& P = e->peaks[peak];
   out->rho_max_over_mean = (double)s.max_fix / (double)PM_FIX_ONE / P.n_mean;
@@ -634,7 +676,7 @@ int pm_sort_u64(const unsigned long long* keys, unsigned long long* keys_out, un
   SortSeg seg{0, n, lo, hi, 1, 0};
   SortPlan plan;
   const int npass = (hi - lo + 7) / 8;
-  int r = sort_plan_create(&plan, &seg, 1, npass);
+  int r = sort_plan_create(&plan, &seg, 1, npass, hi - lo);
   if (r) {
     sort_plan_destroy(&plan);
     return r;
@@ -653,7 +695,7 @@ int pm_sort_u64(const unsigned long long* keys, unsigned long long* keys_out, un
   }
   cudaError_t ce = cudaMemcpy(k0, keys, sizeof(u64) * n, cudaMemcpyDeviceToDevice);
   if (ce == cudaSuccess) {
-    r = sort_run(&plan, k0, v0, k1, v1, true, true, 0);
+    r = sort_run<u64>(&plan, k0, v0, k1, v1, true, true, 0);
     ce = cudaDeviceSynchronize();
   }
   int err = 0;

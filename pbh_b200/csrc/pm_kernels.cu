@@ -18,19 +18,24 @@ __device__ __forceinline__ u64 shfl_up_u64(u64 v, int d) {
   return ((u64)hi << 32) | lo;
 }
 
+// Buffer selection without indexing the kernel-parameter arrays dynamically (which would
+// copy the whole parameter struct to local memory).
+__device__ __forceinline__ int4* posb(const StepArgs& A, int b) { return b ? A.pos[1] : A.pos[0]; }
+__device__ __forceinline__ float4* momb(const StepArgs& A, int b) { return b ? A.mom[1] : A.mom[0]; }
+
 // Locate the peak and tile of this CTA (uniform across the block).
 struct TileRef {
   int pk;
   long long t;
 };
 
-__device__ __forceinline__ TileRef find_tile(const StepArgs& A) {
+__device__ __forceinline__ TileRef find_tile(const long long* base, int npeaks) {
   __shared__ int s_pk;
-  if (threadIdx.x == 0) s_pk = pm_find(A.tile_base, A.npeaks, (long long)blockIdx.x);
+  if (threadIdx.x == 0) s_pk = pm_find(base, npeaks, (long long)blockIdx.x);
   __syncthreads();
   TileRef r;
   r.pk = s_pk;
-  r.t = (long long)blockIdx.x - A.tile_base[r.pk];
+  r.t = (long long)blockIdx.x - base[r.pk];
   return r;
 }
 
@@ -40,102 +45,145 @@ __device__ __forceinline__ TileRef find_tile(const StepArgs& A) {
 // One CTA per tile: the (T+1)^3 node patch of all three grids is staged in shared memory,
 // then every particle whose CIC cell lies in the tile reads its 8 corners from there.
 // Output is written in sorted order into the other state buffer, with the new cell key.
-__global__ void __launch_bounds__(PM_THREADS) k_push(StepArgs A) {
+struct PushCoef {
+  float kA, kB, D, gscale;
+};
+
+template <int T>
+__device__ __forceinline__ void push_one(const PeakDesc& P, const float* __restrict__ s_f, const PushCoef& K,
+                                         bool run, int tx, int ty, int tz, int4 ps, float4 m, long long j,
+                                         int4* __restrict__ pout, float4* __restrict__ mout, u32* __restrict__ kout,
+                                         bool& bad) {
+  constexpr int T1 = T + 1, T13 = T1 * T1 * T1;
+  const int N = P.N, l2 = P.log2N;
+  const int ix = ps.x >> (2 * l2), iy = (ps.x >> l2) & (N - 1), iz = ps.x & (N - 1);
+  const int lx = ix - tx * T, ly = iy - ty * T, lz = iz - tz * T;
+  if ((unsigned)lx >= (unsigned)T || (unsigned)ly >= (unsigned)T || (unsigned)lz >= (unsigned)T) {
+    bad = true;  // state and sort disagree: flag it, never index outside the patch
+    return;
+  }
+  float fx = __int_as_float(ps.y), fy = __int_as_float(ps.z), fz = __int_as_float(ps.w);
+  const float gx = 1.0f - fx, gy = 1.0f - fy, gz = 1.0f - fz;
+  const int o = (lx * T1 + ly) * T1 + lz;
+  float ax = 0.f, ay = 0.f, az = 0.f;
+#define PM_CORNER(w, d)                       \
+  {                                           \
+    const float w_ = (w);                     \
+    ax = fmaf(w_, s_f[o + (d)], ax);          \
+    ay = fmaf(w_, s_f[T13 + o + (d)], ay);    \
+    az = fmaf(w_, s_f[2 * T13 + o + (d)], az); \
+  }
+  const float w00 = gx * gy, w01 = gx * fy, w10 = fx * gy, w11 = fx * fy;
+  PM_CORNER(w00 * gz, 0)
+  PM_CORNER(w00 * fz, 1)
+  PM_CORNER(w01 * gz, T1)
+  PM_CORNER(w01 * fz, T1 + 1)
+  PM_CORNER(w10 * gz, T1 * T1)
+  PM_CORNER(w10 * fz, T1 * T1 + 1)
+  PM_CORNER(w11 * gz, T1 * T1 + T1)
+  PM_CORNER(w11 * fz, T1 * T1 + T1 + 1)
+#undef PM_CORNER
+  ax *= K.gscale;
+  ay *= K.gscale;
+  az *= K.gscale;
+  float px = m.x + K.kA * ax, py = m.y + K.kA * ay, pz = m.z + K.kA * az;
+  int nx = ix, ny = iy, nz = iz;
+  if (run) {
+    px += K.kB * ax;
+    py += K.kB * ay;
+    pz += K.kB * az;
+#define PM_DRIFT(f, p, i)                 \
+  {                                       \
+    float fn = f + K.D * p;               \
+    float c = floorf(fn);                 \
+    fn -= c;                              \
+    if (fn >= 1.0f) {                     \
+      fn -= 1.0f;                         \
+      c += 1.0f;                          \
+    }                                     \
+    f = fn;                               \
+    i = (i + (int)c) & (N - 1);           \
+  }
+    PM_DRIFT(fx, px, nx)
+    PM_DRIFT(fy, py, ny)
+    PM_DRIFT(fz, pz, nz)
+#undef PM_DRIFT
+  }
+  bad |= !(isfinite(px) && isfinite(py) && isfinite(pz));
+  pout[j] = make_int4((nx << (2 * l2)) | (ny << l2) | nz, __float_as_int(fx), __float_as_int(fy), __float_as_int(fz));
+  mout[j] = make_float4(px, py, pz, m.w);
+  kout[j] = pm_cell_key(P, nx, ny, nz);
+}
+
+template <int T>
+__device__ __forceinline__ void push_tile(const StepArgs& A, const PeakDesc& P, const PeakClock& C, int pk, u32 tc,
+                                          long long b, long long e, float* s_f, const PushCoef& K) {
+  constexpr int T1 = T + 1, T12 = T1 * T1, T13 = T1 * T1 * T1;
+  const int N = P.N;
+  const int tx = pm_compact3(tc >> 2), ty = pm_compact3(tc >> 1), tz = pm_compact3(tc);
+  const long long N3 = (long long)N * N * N;
+  for (int i = threadIdx.x; i < 3 * T13; i += PUSH_THREADS) {
+    const int comp = i / T13, r = i - comp * T13;
+    const int lx = r / T12, r2 = r - lx * T12;
+    const int ly = r2 / T1, lz = r2 - ly * T1;
+    const int gx = (tx * T + lx) & (N - 1), gy = (ty * T + ly) & (N - 1), gz = (tz * T + lz) & (N - 1);
+    s_f[i] = __ldg(P.force + comp * N3 + ((long long)gx * N + gy) * N + gz);
+  }
+  __syncthreads();
+  const bool run = C.state == PS_RUN;
+  const int buf = C.buf;
+  const int4* __restrict__ pin = posb(A, buf);
+  const float4* __restrict__ min_ = momb(A, buf);
+  int4* __restrict__ pout = posb(A, buf ^ 1);
+  float4* __restrict__ mout = momb(A, buf ^ 1);
+  u32* __restrict__ kout = A.keys_push;
+  bool bad = false;
+  // Two particles per thread per iteration: both gathers are in flight before either is used.
+  for (long long j = b + threadIdx.x; j < e; j += 2 * PUSH_THREADS) {
+    const long long j2 = j + PUSH_THREADS;
+    const bool has2 = j2 < e;
+    const u32 q1 = A.perm[j];
+    const u32 q2 = has2 ? A.perm[j2] : q1;
+    const int4 p1 = pin[q1];
+    const float4 m1 = min_[q1];
+    const int4 p2 = pin[q2];
+    const float4 m2 = min_[q2];
+    push_one<T>(P, s_f, K, run, tx, ty, tz, p1, m1, j, pout, mout, kout, bad);
+    if (has2) push_one<T>(P, s_f, K, run, tx, ty, tz, p2, m2, j2, pout, mout, kout, bad);
+  }
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&A.stats[pk].status, 1u);
+}
+
+// One CTA per push super-tile of TP^3 cells: its (TP/T)^3 bucket tiles are consecutive Morton
+// codes, so its particles are one contiguous range of the sorted order.
+__global__ void __launch_bounds__(PUSH_THREADS) k_push(StepArgs A) {
   extern __shared__ float s_f[];
-  __shared__ float s_coef[5];
-  const TileRef tr = find_tile(A);
+  __shared__ PushCoef s_k;
+  const TileRef tr = find_tile(A.ptile_base, A.npeaks);
   const PeakClock C = A.clocks[tr.pk];
   if (C.state != PS_RUN && C.state != PS_FINALIZE) return;
   const PeakDesc& P = A.peaks[tr.pk];
-  const int N = P.N, T = P.T, T1 = T + 1, T13 = T1 * T1 * T1;
-  const u32 tc = (u32)tr.t;
+  const u32 st = (u32)tr.t;
+  const u32 R = 1u << (3 * (P.log2TP - P.log2T));
   const u32* bs = A.bstart + P.bucket_off;
-  const long long b = bs[tc * 8], e = bs[tc * 8 + 8];
+  const long long b = bs[st * R * 8], e = bs[(st + 1) * R * 8];
   if (b == e) return;
-  const int tx = pm_compact3(tc >> 2), ty = pm_compact3(tc >> 1), tz = pm_compact3(tc);
-  const long long N3 = (long long)N * N * N;
-  // Stage the force patch, one row of T+1 nodes per warp iteration.
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int row = warp; row < 3 * T1 * T1; row += PM_THREADS / 32) {
-    const int comp = row / (T1 * T1);
-    const int rem = row - comp * T1 * T1;
-    const int lx = rem / T1, ly = rem - (rem / T1) * T1;
-    const int gx = (tx * T + lx) & (N - 1), gy = (ty * T + ly) & (N - 1);
-    const float* src = P.force + comp * N3 + ((long long)gx * N + gy) * N;
-    for (int lz = lane; lz < T1; lz += 32) s_f[comp * T13 + (lx * T1 + ly) * T1 + lz] = src[(tz * T + lz) & (N - 1)];
-  }
   if (threadIdx.x == 0) {
     const double a = C.a, da = C.da;
     const bool run = C.state == PS_RUN;
-    const double kB = run ? 0.5 * da / (a * pm_hubble(a)) : 0.0;
     const double amid = a + 0.5 * da;
-    const double D = run ? da / (amid * amid * amid * pm_hubble(amid)) / P.dx : 0.0;
-    s_coef[0] = (float)C.kpend;
-    s_coef[1] = (float)kB;
-    s_coef[2] = (float)D;
-    s_coef[3] = (float)(C.a_grid / a);
+    s_k.kA = (float)C.kpend;
+    s_k.kB = run ? (float)(0.5 * da / (a * pm_hubble(a))) : 0.f;
+    s_k.D = run ? (float)(da / (amid * amid * amid * pm_hubble(amid)) / P.dx) : 0.f;
+    s_k.gscale = (float)(C.a_grid / a);
   }
   __syncthreads();
-  const float kA = s_coef[0], kB = s_coef[1], D = s_coef[2], gscale = s_coef[3];
-  const bool run = C.state == PS_RUN;
-  const int buf = C.buf;
-  const int4* __restrict__ pin = A.pos[buf];
-  const float4* __restrict__ min_ = A.mom[buf];
-  int4* __restrict__ pout = A.pos[buf ^ 1];
-  float4* __restrict__ mout = A.mom[buf ^ 1];
-  const int l2 = 2 * P.log2N;
-  bool bad = false;
-  for (long long j = b + threadIdx.x; j < e; j += PM_THREADS) {
-    const u32 q = A.perm[j];
-    const int4 ps = pin[q];
-    const float4 m = min_[q];
-    int ix = ps.x >> l2, iy = (ps.x >> P.log2N) & (N - 1), iz = ps.x & (N - 1);
-    float f[3] = {__int_as_float(ps.y), __int_as_float(ps.z), __int_as_float(ps.w)};
-    const int lx = ix - tx * T, ly = iy - ty * T, lz = iz - tz * T;
-    if ((unsigned)lx >= (unsigned)T || (unsigned)ly >= (unsigned)T || (unsigned)lz >= (unsigned)T) {
-      bad = true;  // state and sort disagree: flag it, never index outside the patch
-      continue;
-    }
-    const float wx[2] = {1.0f - f[0], f[0]}, wy[2] = {1.0f - f[1], f[1]}, wz[2] = {1.0f - f[2], f[2]};
-    float acc[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      const int cx = c >> 2, cy = (c >> 1) & 1, cz = c & 1;
-      const float w = wx[cx] * wy[cy] * wz[cz];
-      const int o = ((lx + cx) * T1 + ly + cy) * T1 + lz + cz;
-      acc[0] += w * s_f[o];
-      acc[1] += w * s_f[T13 + o];
-      acc[2] += w * s_f[2 * T13 + o];
-    }
-    float p[3] = {m.x, m.y, m.z};
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      const float g = acc[d] * gscale;
-      p[d] += kA * g;
-      if (run) p[d] += kB * g;
-    }
-    bad |= !(isfinite(p[0]) && isfinite(p[1]) && isfinite(p[2]));
-    int ii[3] = {ix, iy, iz};
-    if (run) {
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        float fn = f[d] + D * p[d];
-        float cfl = floorf(fn);
-        fn -= cfl;
-        if (fn >= 1.0f) {
-          fn -= 1.0f;
-          cfl += 1.0f;
-        }
-        f[d] = fn;
-        ii[d] = (ii[d] + (int)cfl) & (N - 1);
-      }
-    }
-    const int cell = (ii[0] << l2) | (ii[1] << P.log2N) | ii[2];
-    pout[j] = make_int4(cell, __float_as_int(f[0]), __float_as_int(f[1]), __float_as_int(f[2]));
-    mout[j] = make_float4(p[0], p[1], p[2], m.w);
-    A.keys_push[j] = ((u64)tr.pk << 32) | pm_cell_key(P, ii[0], ii[1], ii[2]);
+  const PushCoef K = s_k;
+  switch (P.TP) {
+    case 4: push_tile<4>(A, P, C, tr.pk, st, b, e, s_f, K); break;
+    case 8: push_tile<8>(A, P, C, tr.pk, st, b, e, s_f, K); break;
+    default: push_tile<16>(A, P, C, tr.pk, st, b, e, s_f, K); break;
   }
-  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&A.stats[tr.pk].status, 1u);
 }
 
 // Clock advance (one thread per peak): applies the step that the push kernel just made,
@@ -189,6 +237,7 @@ __global__ void k_advance(StepArgs A) {
     c.dep = dep;
     A.clocks[pk] = c;
     A.sortseg[pk].active = dep;
+    A.sortseg_full[pk].active = dep;
     if (dep) {
       A.stats[pk].max_fix = 0;
       A.stats[pk].mass_defect = 0;
@@ -204,128 +253,224 @@ __global__ void k_bucket_starts(StepArgs A, long long ntot) {
   if (!A.clocks[pk].dep) return;
   const PeakDesc& P = A.peaks[pk];
   u32* bs = A.bstart + P.bucket_off;
-  const int b = (int)((u32)A.keys_sorted[j] >> P.local_bits);
-  const int bprev = j == P.p_off ? -1 : (int)((u32)A.keys_sorted[j - 1] >> P.local_bits);
+  const int b = (int)(A.keys_sorted[j] >> P.local_bits);
+  const int bprev = j == P.p_off ? -1 : (int)(A.keys_sorted[j - 1] >> P.local_bits);
   for (int bb = bprev + 1; bb <= b; ++bb) bs[bb] = (u32)j;
   if (j == P.p_off + P.n - 1)
     for (int bb = b + 1; bb <= P.nb; ++bb) bs[bb] = (u32)(P.p_off + P.n);
 }
 
 // ------------------------------------------------------------------------------------------
-// Deterministic CIC deposit (pm3d.py:81-89, 103-104).  One CTA owns the T^3 nodes of one
-// tile and accumulates, in 64-bit fixed point in shared memory, every particle contribution
-// that lands on them: the tile's own particles (corners outside the tile are left to their
-// owners) and, from the 7 lower neighbour tiles, only the boundary-layer buckets whose
-// corners reach into this tile.  Consecutive particles in the same cell are first combined
-// by a warp-shuffle segmented scan, so dense cells cost one shared-memory update per run.
-// Every node is written exactly once as FP32 delta = S/n_mean - 1, with no global atomics.
-__global__ void __launch_bounds__(PM_THREADS) k_deposit(StepArgs A, double* rho64) {
-  extern __shared__ u64 s_acc[];
-  __shared__ long long s_rb[16], s_re[16];
-  __shared__ int s_ro[16];
+// Deterministic CIC deposit (pm3d.py:81-89, 103-104).  One CTA owns the TS^3 nodes of one push
+// super-tile (TS = 16: 8 bucket tiles of 8^3).  It reads the super-tile's own particles (one
+// contiguous sorted range) and, from the 7 lower neighbour super-tiles, only the buckets of
+// their boundary-layer cells whose corners reach into it.  Per particle the 8 CIC weights are
+// formed in 64-bit fixed point with 40 fractional bits, the 8th corner taking the remainder so
+// each particle deposits exactly 2^40; consecutive particles of one cell are first combined by
+// a warp-shuffle segmented scan.  Each node accumulates in shared memory as two native 32-bit
+// words (the signed weight's bits >= 20 and its low 20 bits), which cannot overflow within a
+// chunk of fewer than 2048 particles, and is folded into a 64-bit register accumulator after
+// every chunk.
+// Integer sums make the result independent of particle order, bit for bit; no global atomics.
+// Every node is written once as FP32 delta = S/n_mean - 1.
+template <int TS>
+__device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc& P, int pk, u32 st, u32* smem,
+                                              double* rho64) {
+  constexpr int TS3 = TS * TS * TS;
+  constexpr int NPT = (TS3 + DEP_THREADS - 1) / DEP_THREADS;  // nodes per thread
+  constexpr int NCAND = 7 * 64;                                // (neighbour o, sub-tile, mask) candidates
+  u32* acc_hi = smem;
+  u32* acc_lo = smem + TS3;
+  __shared__ long long s_rb[72], s_rp[73];
+  __shared__ int s_ro[72];
   __shared__ int s_nr;
-  __shared__ long long s_red[PM_THREADS / 32];
-  __shared__ long long s_max[PM_THREADS / 32];
-  const TileRef tr = find_tile(A);
-  if (!A.clocks[tr.pk].dep) return;
-  const PeakDesc& P = A.peaks[tr.pk];
-  const int N = P.N, T = P.T, T3 = T * T * T, NT = N >> P.log2T;
-  const u32 tc = (u32)tr.t;
-  const int tx = pm_compact3(tc >> 2), ty = pm_compact3(tc >> 1), tz = pm_compact3(tc);
-  for (int i = threadIdx.x; i < T3; i += PM_THREADS) s_acc[i] = 0ull;
-  if (threadIdx.x == 0) {
-    const u32* bs = A.bstart + P.bucket_off;
-    int nr = 0;
-    s_rb[0] = bs[tc * 8];
-    s_re[0] = bs[tc * 8 + 8];
-    s_ro[0] = 0;
-    nr = s_re[0] > s_rb[0] ? 1 : 0;
-    for (int o = 1; o < 8; ++o) {
-      const u32 nx = (tx - (o & 1)) & (NT - 1), ny = (ty - ((o >> 1) & 1)) & (NT - 1),
-                nz = (tz - ((o >> 2) & 1)) & (NT - 1);
-      const u32 tn = pm_morton3(nx, ny, nz);
-      for (int m = 0; m < 8; ++m) {
-        if ((m & o) != o) continue;
-        const long long rb = bs[tn * 8 + m], re = bs[tn * 8 + m + 1];
-        if (re <= rb) continue;
-        if (nr > 0 && s_ro[nr - 1] == o && s_re[nr - 1] == rb) {
-          s_re[nr - 1] = re;
-        } else {
-          s_rb[nr] = rb;
-          s_re[nr] = re;
-          s_ro[nr] = o;
-          ++nr;
-        }
+  __shared__ u32 s_wc[DEP_THREADS / 32];
+  __shared__ long long s_red[DEP_THREADS / 32];
+  __shared__ long long s_max[DEP_THREADS / 32];
+  const int N = P.N, l2 = P.log2N;
+  const int rb = P.log2TP - P.log2T;      // log2 of sub-tiles per axis: 0 or 1
+  const int RS = 1 << (3 * rb);           // sub-tiles per super-tile: 1 or 8
+  const int NS = N / TS;                  // super-tiles per axis
+  const int sx = pm_compact3(st >> 2), sy = pm_compact3(st >> 1), sz = pm_compact3(st);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const u32* bs = A.bstart + P.bucket_off;
+  for (int i = threadIdx.x; i < 2 * TS3; i += DEP_THREADS) smem[i] = 0u;
+  // Range table: candidate k = (o - 1) * 64 + s * 8 + m over sub-tiles s of the neighbour
+  // super-tile at offset -o that touch this one, and masks m covering o.
+  long long cb = 0, ce = 0;
+  bool use = false;
+  int co = 0;
+  if (threadIdx.x < NCAND) {
+    const int o = threadIdx.x / 64 + 1, s = (threadIdx.x >> 3) & 7, m = threadIdx.x & 7;
+    if (s < RS && (m & o) == o) {
+      const int sxl = pm_compact3((u32)s >> 2), syl = pm_compact3((u32)s >> 1), szl = pm_compact3((u32)s);
+      const int last = (1 << rb) - 1;
+      if ((!(o & 1) || sxl == last) && (!(o & 2) || syl == last) && (!(o & 4) || szl == last)) {
+        const u32 nx = (sx - (o & 1)) & (NS - 1), ny = (sy - ((o >> 1) & 1)) & (NS - 1), nz = (sz - ((o >> 2) & 1)) & (NS - 1);
+        const u32 b = (pm_morton3(nx, ny, nz) * (u32)RS + (u32)s) * 8 + m;
+        cb = bs[b];
+        ce = bs[b + 1];
+        use = ce > cb;
+        co = o;
       }
     }
-    s_nr = nr;
+  }
+  // Compact the non-empty candidates (block-wide ballot prefix) behind the own range.
+  const u32 bal = __ballot_sync(0xffffffffu, use);
+  if (lane == 0) s_wc[warp] = __popc(bal);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    u32 run = 1;
+    for (int w = 0; w < DEP_THREADS / 32; ++w) {
+      const u32 c = s_wc[w];
+      s_wc[w] = run;
+      run += c;
+    }
+    s_nr = (int)run;
+    s_rb[0] = bs[st * RS * 8];
+    s_rp[0] = bs[(st + 1) * RS * 8] - s_rb[0];  // length for now
+    s_ro[0] = 0;
   }
   __syncthreads();
-  const int4* __restrict__ pos = A.pos[A.clocks[tr.pk].buf];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int l2 = 2 * P.log2N;
-  const u32 le = lanemask_le();
-  const double fix_one = (double)PM_FIX_ONE;
-  for (int r = 0; r < s_nr; ++r) {
-    const long long rb = s_rb[r], re = s_re[r];
-    const int o = s_ro[r];
-    for (long long j0 = rb + warp * 32; j0 < re; j0 += PM_THREADS) {
-      const long long j = j0 + lane;
-      const bool valid = j < re;
-      const int4 ps = valid ? pos[A.perm[j]] : make_int4(-1, 0, 0, 0);
-      const int ix = ps.x >> l2, iy = (ps.x >> P.log2N) & (N - 1), iz = ps.x & (N - 1);
-      const int lx = (o & 1) ? -1 : ix - tx * T;
-      const int ly = (o & 2) ? -1 : iy - ty * T;
-      const int lz = (o & 4) ? -1 : iz - tz * T;
-      const double fx = __int_as_float(ps.y), fy = __int_as_float(ps.z), fz = __int_as_float(ps.w);
-      const double wx[2] = {1.0 - fx, fx}, wy[2] = {1.0 - fy, fy}, wz[2] = {1.0 - fz, fz};
-      u64 W[8];
-      u64 s7 = 0;
-#pragma unroll
-      for (int c = 0; c < 7; ++c) {
-        W[c] = valid ? (u64)__double2ll_rn(wx[c >> 2] * wy[(c >> 1) & 1] * wz[c & 1] * fix_one) : 0ull;
-        s7 += W[c];
+  if (use) {
+    const int slot = s_wc[warp] + __popc(bal & ((1u << lane) - 1u));
+    s_rb[slot] = cb;
+    s_rp[slot] = ce - cb;
+    s_ro[slot] = co;
+  }
+  __syncthreads();
+  const int nr = s_nr;
+  if (warp == 0) {  // lengths -> exclusive prefix (nr <= 72)
+    long long carry = 0;
+    for (int base = 0; base < nr; base += 32) {
+      const int i = base + lane;
+      const long long len = i < nr ? s_rp[i] : 0;
+      long long incl = len;
+      for (int d = 1; d < 32; d <<= 1) {
+        const long long v = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += v;
       }
-      // The eighth corner takes the remainder so each particle deposits exactly 2^40.
-      W[7] = valid ? PM_FIX_ONE - s7 : 0ull;
-      const int prev = __shfl_up_sync(0xffffffffu, ps.x, 1);
-      const bool head = !(valid && lane > 0 && prev == ps.x);
+      if (i < nr) s_rp[i] = carry + incl - len;
+      carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    if (lane == 0) s_rp[nr] = carry;
+  }
+  __syncthreads();
+  const long long total = s_rp[nr];
+  const int4* __restrict__ pos = posb(A, A.clocks[pk].buf);
+  const u32 le = lanemask_le();
+  u64 acc[NPT];
+#pragma unroll
+  for (int k = 0; k < NPT; ++k) acc[k] = 0ull;
+  // A node takes at most one contribution per particle of a chunk.  With CHUNK < 2^11 the high
+  // words (each at most 2^20, or -1 for a remainder corner a few units below zero) sum inside
+  // int32 and the low words (each < 2^20) inside uint32, so both are exact.
+  constexpr long long CHUNK = 2016;
+  for (long long c0 = 0; c0 < total; c0 += CHUNK) {
+    const long long c1 = min(c0 + CHUNK, total);
+    for (long long k0 = c0 + warp * 32; k0 < c1; k0 += DEP_THREADS) {
+      const long long k = k0 + lane;
+      const bool valid = k < c1;
+      int r = 0;
+      if (valid) {
+        int lo = 0, hi = nr - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (s_rp[mid] <= k) lo = mid; else hi = mid - 1;
+        }
+        r = lo;
+      }
+      const int4 ps = valid ? pos[A.perm[s_rb[r] + (k - s_rp[r])]] : make_int4(-1, 0, 0, 0);
+      const int o = s_ro[r];
+      const int ix = ps.x >> (2 * l2), iy = (ps.x >> l2) & (N - 1), iz = ps.x & (N - 1);
+      const int lx = (o & 1) ? -1 : ix - sx * TS;
+      const int ly = (o & 2) ? -1 : iy - sy * TS;
+      const int lz = (o & 4) ? -1 : iz - sz * TS;
+      const double fx = __int_as_float(ps.y), fy = __int_as_float(ps.z), fz = __int_as_float(ps.w);
+      const double gx = 1.0 - fx, gy = 1.0 - fy, gz = 1.0 - fz;
+      const double one = (double)PM_FIX_ONE;
+      const double w00 = gx * gy * one, w01 = gx * fy * one, w10 = fx * gy * one, w11 = fx * fy * one;
+      u64 W0 = 0, W1 = 0, W2 = 0, W3 = 0, W4 = 0, W5 = 0, W6 = 0, W7 = 0;
+      if (valid) {
+        W0 = (u64)__double2ll_rn(w00 * gz);
+        W1 = (u64)__double2ll_rn(w00 * fz);
+        W2 = (u64)__double2ll_rn(w01 * gz);
+        W3 = (u64)__double2ll_rn(w01 * fz);
+        W4 = (u64)__double2ll_rn(w10 * gz);
+        W5 = (u64)__double2ll_rn(w10 * fz);
+        W6 = (u64)__double2ll_rn(w11 * gz);
+        W7 = PM_FIX_ONE - (W0 + W1 + W2 + W3 + W4 + W5 + W6);
+      }
+      // Warp-shuffle segmented scan over runs of the same cell (a cell lies in one bucket, so
+      // equal cells also share the range and its neighbour offset o).
+      const int key = valid ? ps.x : -1 - lane;
+      const int prev = __shfl_up_sync(0xffffffffu, key, 1);
+      const bool head = lane == 0 || prev != key;
       const u32 heads = __ballot_sync(0xffffffffu, head);
       bool tail = true;
       if (heads != 0xffffffffu) {
         const int sstart = 31 - __clz(heads & le);
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
-#pragma unroll
-          for (int c = 0; c < 8; ++c) {
-            const u64 v = shfl_up_u64(W[c], d);
-            if (lane - d >= sstart) W[c] += v;
-          }
+          const bool take = lane - d >= sstart;
+#define PM_SEG(W)                              \
+  {                                            \
+    const u64 v_ = shfl_up_u64(W, d);          \
+    if (take) W += v_;                         \
+  }
+          PM_SEG(W0) PM_SEG(W1) PM_SEG(W2) PM_SEG(W3) PM_SEG(W4) PM_SEG(W5) PM_SEG(W6) PM_SEG(W7)
+#undef PM_SEG
         }
         tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
       }
       if (valid && tail) {
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {
-          const int cx = lx + (c >> 2), cy = ly + ((c >> 1) & 1), cz = lz + (c & 1);
-          if ((unsigned)cx < (unsigned)T && (unsigned)cy < (unsigned)T && (unsigned)cz < (unsigned)T)
-            atomicAdd(&s_acc[(cx * T + cy) * T + cz], W[c]);
-        }
+        const bool x0 = (unsigned)lx < (unsigned)TS, x1 = (unsigned)(lx + 1) < (unsigned)TS;
+        const bool y0 = (unsigned)ly < (unsigned)TS, y1 = (unsigned)(ly + 1) < (unsigned)TS;
+        const bool z0 = (unsigned)lz < (unsigned)TS, z1 = (unsigned)(lz + 1) < (unsigned)TS;
+        const int nb = (lx * TS + ly) * TS + lz;
+#define PM_ADD(cond, off, W)                                                  \
+  if (cond) {                                                                 \
+    atomicAdd(&acc_hi[nb + (off)], (u32)(int)((long long)(W) >> 20));        \
+    atomicAdd(&acc_lo[nb + (off)], (u32)((W) & 0xFFFFFu));                   \
+  }
+        PM_ADD(x0 && y0 && z0, 0, W0)
+        PM_ADD(x0 && y0 && z1, 1, W1)
+        PM_ADD(x0 && y1 && z0, TS, W2)
+        PM_ADD(x0 && y1 && z1, TS + 1, W3)
+        PM_ADD(x1 && y0 && z0, TS * TS, W4)
+        PM_ADD(x1 && y0 && z1, TS * TS + 1, W5)
+        PM_ADD(x1 && y1 && z0, TS * TS + TS, W6)
+        PM_ADD(x1 && y1 && z1, TS * TS + TS + 1, W7)
+#undef PM_ADD
       }
     }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NPT; ++k) {
+      const int node = threadIdx.x + k * DEP_THREADS;
+      if (node < TS3) {
+        acc[k] += (u64)((long long)(int)acc_hi[node] * (1LL << 20)) + (u64)acc_lo[node];
+        acc_hi[node] = 0u;
+        acc_lo[node] = 0u;
+      }
+    }
+    __syncthreads();
   }
-  __syncthreads();
   long long dsum = 0, smax = 0;
-  const long long base = ((long long)tx * T * N + (long long)ty * T) * N + tz * T;
-  for (int i = threadIdx.x; i < T3; i += PM_THREADS) {
-    const int lz = i & (T - 1), ly = (i >> P.log2T) & (T - 1), lx = i >> (2 * P.log2T);
-    const long long S = (long long)s_acc[i];
-    const long long Dv = S - P.n_mean_fix;
-    const long long g = base + ((long long)lx * N + ly) * N + lz;
-    P.delta[g] = (float)((double)Dv * P.inv_fix_nmean);
-    if (rho64) rho64[g] = (double)S * (1.0 / (double)PM_FIX_ONE);
-    dsum += Dv;
-    smax = S > smax ? S : smax;
+  const long long base = ((long long)sx * TS * N + (long long)sy * TS) * N + sz * TS;
+#pragma unroll
+  for (int k = 0; k < NPT; ++k) {
+    const int node = threadIdx.x + k * DEP_THREADS;
+    if (node < TS3) {
+      const int nz = node & (TS - 1), ny = (node / TS) & (TS - 1), nx = node / (TS * TS);
+      const long long S = (long long)acc[k];
+      const long long Dv = S - P.n_mean_fix;
+      const long long g = base + ((long long)nx * N + ny) * N + nz;
+      P.delta[g] = (float)((double)Dv * P.inv_fix_nmean);
+      if (rho64) rho64[g] = (double)S * (1.0 / (double)PM_FIX_ONE);
+      dsum += Dv;
+      smax = S > smax ? S : smax;
+    }
   }
   for (int d = 16; d > 0; d >>= 1) {
     dsum += __shfl_xor_sync(0xffffffffu, dsum, d);
@@ -339,12 +484,24 @@ __global__ void __launch_bounds__(PM_THREADS) k_deposit(StepArgs A, double* rho6
   __syncthreads();
   if (threadIdx.x == 0) {
     long long ts = 0, tm = 0;
-    for (int w = 0; w < PM_THREADS / 32; ++w) {
+    for (int w = 0; w < DEP_THREADS / 32; ++w) {
       ts += s_red[w];
       tm = s_max[w] > tm ? s_max[w] : tm;
     }
-    atomicAdd((unsigned long long*)&A.stats[tr.pk].mass_defect, (unsigned long long)ts);
-    atomicMax(&A.stats[tr.pk].max_fix, (u64)tm);
+    atomicAdd((unsigned long long*)&A.stats[pk].mass_defect, (unsigned long long)ts);
+    atomicMax(&A.stats[pk].max_fix, (u64)tm);
+  }
+}
+
+__global__ void __launch_bounds__(DEP_THREADS) k_deposit(StepArgs A, double* rho64) {
+  extern __shared__ __align__(16) u32 s_dep[];
+  const TileRef tr = find_tile(A.ptile_base, A.npeaks);
+  if (!A.clocks[tr.pk].dep) return;
+  const PeakDesc& P = A.peaks[tr.pk];
+  switch (P.TP) {
+    case 4: deposit_super<4>(A, P, tr.pk, (u32)tr.t, s_dep, rho64); break;
+    case 8: deposit_super<8>(A, P, tr.pk, (u32)tr.t, s_dep, rho64); break;
+    default: deposit_super<16>(A, P, tr.pk, (u32)tr.t, s_dep, rho64); break;
   }
 }
 
@@ -357,21 +514,28 @@ __global__ void __launch_bounds__(PM_THREADS) k_deposit(StepArgs A, double* rho6
 // of its input (it takes the real part after the two complex inverse transforms).  Those two
 // planes are therefore written as (G(k) + conj G(-k))/2, which any correct C2R turns into
 // exactly numpy's field.
-__device__ __forceinline__ double kline(int i, int N, double kf) { return kf * (double)(i < N / 2 ? i : i - N); }
+__device__ __forceinline__ float kline(int i, int N, float kf) { return kf * (float)(i < N / 2 ? i : i - N); }
 
-__device__ __forceinline__ double grad_k(double k, double dx, int mode) {
-  if (mode == 1) return sin(k * dx) / dx;
-  if (mode == 2) return (8.0 * sin(k * dx) - sin(2.0 * k * dx)) / (6.0 * dx);
+// Gradient operator in k-space: spectral -i k (the reference), or the transfer function of the
+// 2-point / 4-point central differences.
+__device__ __forceinline__ float grad_k(float k, float dx, int mode) {
+  if (mode == 1) return sinf(k * dx) / dx;
+  if (mode == 2) return (8.0f * sinf(k * dx) - sinf(2.0f * k * dx)) / (6.0f * dx);
   return k;
 }
 
 __global__ void __launch_bounds__(PM_THREADS) k_green(StepArgs A) {
   __shared__ int s_pk;
-  if (threadIdx.x == 0) s_pk = pm_find(A.mode_base, A.npeaks, (long long)blockIdx.x);
+  __shared__ float s_c;
+  if (threadIdx.x == 0) {
+    s_pk = pm_find(A.mode_base, A.npeaks, (long long)blockIdx.x);
+    const PeakDesc& P = A.peaks[s_pk];
+    const double n3 = (double)P.N * P.N * P.N;
+    s_c = (float)(-1.5 * PM_H_I * PM_H_I / A.clocks[s_pk].a_grid / n3);
+  }
   __syncthreads();
   const int pk = s_pk;
-  const PeakClock& C = A.clocks[pk];
-  if (!C.has_delta) return;
+  if (!A.clocks[pk].has_delta) return;
   const PeakDesc& P = A.peaks[pk];
   const long long m = ((long long)blockIdx.x - A.mode_base[pk]) * PM_THREADS + threadIdx.x;
   if (m >= P.nmodes) return;
@@ -379,38 +543,38 @@ __global__ void __launch_bounds__(PM_THREADS) k_green(StepArgs A) {
   const int kz = (int)(m % Nh);
   const long long rest = m / Nh;
   const int iy = (int)(rest & (N - 1)), ix = (int)(rest >> P.log2N);
-  const double kf = kTwoPi / P.L;
-  const double kx = kline(ix, N, kf), ky = kline(iy, N, kf), kzv = kf * kz;
-  const double k2 = kx * kx + ky * ky + kzv * kzv;
+  const float kf = (float)(kTwoPi / P.L), dx = (float)P.dx;
+  const float kx = kline(ix, N, kf), ky = kline(iy, N, kf), kzv = kf * (float)kz;
+  const float k2 = kx * kx + ky * ky + kzv * kzv;
+  const long long M = P.nmodes;
   float2* out = P.gspec;
   if (m == 0) {
-    out[m] = out[P.nmodes + m] = out[2 * P.nmodes + m] = make_float2(0.f, 0.f);
+    out[0] = out[M] = out[2 * M] = make_float2(0.f, 0.f);
     return;
   }
-  double G = -1.5 * PM_H_I * PM_H_I / C.a_grid / k2;
-  if (P.smooth > 0) G *= exp(-0.5 * k2 * (P.smooth * P.dx) * (P.smooth * P.dx));
-  G /= (double)N * (double)N * (double)N;
-  const float2 d = P.spec[m];
-  const double kc[3] = {grad_k(kx, P.dx, P.gradient), grad_k(ky, P.dx, P.gradient), grad_k(kzv, P.dx, P.gradient)};
-  // -i k G d = (k G d.y, -k G d.x)
-  double vr[3], vi[3];
-  for (int c = 0; c < 3; ++c) {
-    vr[c] = kc[c] * G * (double)d.y;
-    vi[c] = -kc[c] * G * (double)d.x;
+  float G = s_c / k2;
+  if (P.smooth > 0) {
+    const float sd = (float)(P.smooth * P.dx);
+    G *= expf(-0.5f * k2 * sd * sd);
   }
+  const int gm = P.gradient;
+  const float gx = grad_k(kx, dx, gm) * G, gy = grad_k(ky, dx, gm) * G, gz = grad_k(kzv, dx, gm) * G;
+  const float2 d = P.spec[m];
+  // -i k G d = (k G d.y, -k G d.x)
+  float2 ox = make_float2(gx * d.y, -gx * d.x), oy = make_float2(gy * d.y, -gy * d.x),
+         oz = make_float2(gz * d.y, -gz * d.x);
   if (kz == 0 || kz == N / 2) {
     const int px = (-ix) & (N - 1), py = (-iy) & (N - 1);
-    const long long mp = ((long long)px * N + py) * Nh + kz;
-    const float2 dp = P.spec[mp];
-    const double kpx = kline(px, N, kf), kpy = kline(py, N, kf);
-    const double kpc[3] = {grad_k(kpx, P.dx, P.gradient), grad_k(kpy, P.dx, P.gradient), kc[2]};
-    for (int c = 0; c < 3; ++c) {
-      const double pr = kpc[c] * G * (double)dp.y, pi = -kpc[c] * G * (double)dp.x;
-      vr[c] = 0.5 * (vr[c] + pr);
-      vi[c] = 0.5 * (vi[c] - pi);
-    }
+    const float2 dp = P.spec[((long long)px * N + py) * Nh + kz];
+    const float hx = grad_k(kline(px, N, kf), dx, gm) * G, hy = grad_k(kline(py, N, kf), dx, gm) * G;
+    // (v + conj(v_partner)) / 2 with v_partner = (h dp.y, -h dp.x)
+    ox = make_float2(0.5f * (ox.x + hx * dp.y), 0.5f * (ox.y + hx * dp.x));
+    oy = make_float2(0.5f * (oy.x + hy * dp.y), 0.5f * (oy.y + hy * dp.x));
+    oz = make_float2(0.5f * (oz.x + gz * dp.y), 0.5f * (oz.y + gz * dp.x));
   }
-  for (int c = 0; c < 3; ++c) out[c * P.nmodes + m] = make_float2((float)vr[c], (float)vi[c]);
+  out[m] = ox;
+  out[M + m] = oy;
+  out[2 * M + m] = oz;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -457,9 +621,9 @@ __global__ void k_set_particles(StepArgs A, int pk, PeakDesc P, const double* __
   }
   const int cell = (ii[0] << (2 * P.log2N)) | (ii[1] << P.log2N) | ii[2];
   const long long g = P.p_off + i;
-  A.pos[buf][g] = make_int4(cell, __float_as_int(ff[0]), __float_as_int(ff[1]), __float_as_int(ff[2]));
-  A.mom[buf][g] = make_float4((float)p[3 * i], (float)p[3 * i + 1], (float)p[3 * i + 2], __int_as_float((int)i));
-  A.keys_push[g] = ((u64)pk << 32) | pm_cell_key(P, ii[0], ii[1], ii[2]);
+  posb(A, buf)[g] = make_int4(cell, __float_as_int(ff[0]), __float_as_int(ff[1]), __float_as_int(ff[2]));
+  momb(A, buf)[g] = make_float4((float)p[3 * i], (float)p[3 * i + 1], (float)p[3 * i + 2], __int_as_float((int)i));
+  A.keys_push[g] = pm_cell_key(P, ii[0], ii[1], ii[2]);
 }
 
 // Current state -> float64 x, p (lattice order).  p includes the pending closing kick; acc
@@ -469,8 +633,8 @@ __global__ void k_get_particles(StepArgs A, int pk, PeakDesc P, double* __restri
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P.n) return;
   const PeakClock C = A.clocks[pk];
-  const int4 ps = A.pos[C.buf][P.p_off + i];
-  const float4 m = A.mom[C.buf][P.p_off + i];
+  const int4 ps = posb(A, C.buf)[P.p_off + i];
+  const float4 m = momb(A, C.buf)[P.p_off + i];
   const int N = P.N;
   const int ii[3] = {ps.x >> (2 * P.log2N), (ps.x >> P.log2N) & (N - 1), ps.x & (N - 1)};
   const float f[3] = {__int_as_float(ps.y), __int_as_float(ps.z), __int_as_float(ps.w)};
@@ -526,8 +690,8 @@ __global__ void k_interp64(const double* __restrict__ F, const double* __restric
 
 }  // namespace
 
-size_t pm_deposit_smem(int Tmax) { return sizeof(u64) * (size_t)Tmax * Tmax * Tmax; }
-size_t pm_push_smem(int Tmax) { return sizeof(float) * 3 * (size_t)(Tmax + 1) * (Tmax + 1) * (Tmax + 1); }
+size_t pm_deposit_smem(int TPmax) { return sizeof(u32) * 2 * (size_t)TPmax * TPmax * TPmax; }
+size_t pm_push_smem(int TPmax) { return sizeof(float) * 3 * (size_t)(TPmax + 1) * (TPmax + 1) * (TPmax + 1); }
 
 int pm_kernels_init() {
   cudaError_t e = cudaFuncSetAttribute(k_push, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
@@ -535,15 +699,15 @@ int pm_kernels_init() {
   return e == cudaSuccess ? 0 : -(int)e;
 }
 
-void launch_push(const StepArgs& A, long long ntiles, size_t smem, cudaStream_t s) {
-  k_push<<<(unsigned)ntiles, PM_THREADS, smem, s>>>(A);
+void launch_push(const StepArgs& A, long long nptiles, size_t smem, cudaStream_t s) {
+  k_push<<<(unsigned)nptiles, PUSH_THREADS, smem, s>>>(A);
 }
 void launch_advance(const StepArgs& A, cudaStream_t s) { k_advance<<<1, 256, 0, s>>>(A); }
 void launch_bucket_starts(const StepArgs& A, long long ntot, cudaStream_t s) {
   k_bucket_starts<<<(unsigned)((ntot + PM_THREADS - 1) / PM_THREADS), PM_THREADS, 0, s>>>(A, ntot);
 }
-void launch_deposit(const StepArgs& A, long long ntiles, size_t smem, double* rho64, cudaStream_t s) {
-  k_deposit<<<(unsigned)ntiles, PM_THREADS, smem, s>>>(A, rho64);
+void launch_deposit(const StepArgs& A, long long nptiles, size_t smem, double* rho64, cudaStream_t s) {
+  k_deposit<<<(unsigned)nptiles, DEP_THREADS, smem, s>>>(A, rho64);
 }
 void launch_green(const StepArgs& A, long long nblocks, cudaStream_t s) {
   k_green<<<(unsigned)nblocks, PM_THREADS, 0, s>>>(A);

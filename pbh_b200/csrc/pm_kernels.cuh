@@ -4,6 +4,8 @@
 #include "sort.cuh"
 
 #define PM_THREADS 256
+#define PUSH_THREADS 512
+#define DEP_THREADS 512
 
 // Views of the engine's device arrays handed to every kernel.
 struct StepArgs {
@@ -11,15 +13,18 @@ struct StepArgs {
   PeakClock* clocks;
   PeakStats* stats;
   SortSeg* sortseg;            // sort activity flags, written by the advance kernel
+  SortSeg* sortseg_full;       // the same for the full-key plan
   const long long* tile_base;  // [npeaks + 1] prefix of tiles
+  const long long* ptile_base; // [npeaks + 1] prefix of push super-tiles
   const long long* p_base;     // [npeaks + 1] prefix of particles
   const long long* mode_base;  // [npeaks + 1] prefix of Green blocks
   int npeaks;
   int pad;
   int4* pos[2];
   float4* mom[2];
-  u64* keys_push;              // keys written by the push kernel (sort input)
-  const u64* keys_sorted;      // sort output keys
+  u32* keys_push;              // cell keys written by the push kernel (sort input); the
+                               // peak id, the high word of the 64-bit key, is the segment
+  const u32* keys_sorted;      // sort output keys
   const u32* perm;             // sort output permutation (index into the current buffer)
   u32* bstart;                 // bucket starts arena
 };
@@ -35,13 +40,13 @@ __device__ __forceinline__ int pm_find(const long long* base, int n, long long v
 }
 
 int pm_kernels_init();  // kernel attributes; call once per device before launching
-size_t pm_deposit_smem(int Tmax);
-size_t pm_push_smem(int Tmax);
+size_t pm_deposit_smem(int TPmax);
+size_t pm_push_smem(int TPmax);
 
-void launch_push(const StepArgs& A, long long ntiles, size_t smem, cudaStream_t s);
+void launch_push(const StepArgs& A, long long nptiles, size_t smem, cudaStream_t s);
 void launch_advance(const StepArgs& A, cudaStream_t s);
 void launch_bucket_starts(const StepArgs& A, long long ntot, cudaStream_t s);
-void launch_deposit(const StepArgs& A, long long ntiles, size_t smem, double* rho64, cudaStream_t s);
+void launch_deposit(const StepArgs& A, long long nptiles, size_t smem, double* rho64, cudaStream_t s);
 void launch_green(const StepArgs& A, long long nblocks, cudaStream_t s);
 
 // Host-requested per-peak operations.

@@ -17,9 +17,11 @@
 
 #define SORT_THREADS 256
 #define SORT_WARPS (SORT_THREADS / 32)
-#define SORT_IPT 16
+#define SORT_IPT 8
 #define SORT_TILE (SORT_THREADS * SORT_IPT)
-#define SORT_RADIX 256
+#define SORT_RADIX 256          // digit bins of the default 8-bit digit
+#define SORT_MAX_BITS 10        // digits of 8, 9 or 10 bits
+#define SORT_MAX_RADIX (1 << SORT_MAX_BITS)
 #define SORT_MAX_PASSES 8
 
 struct SortSeg {
@@ -34,23 +36,27 @@ struct SortPlan {
   int nseg;
   int ntiles;
   int npass;             // digit passes (the same for every segment)
+  int bits;              // digit width: 8, 9 or 10
   SortSeg* seg;          // [nseg] (device)
   int* tile_seg;         // [ntiles]
   long long* tile_begin; // [ntiles]
   int* tile_first;       // [ntiles] 1 when the tile opens its segment
-  u32* hist;             // [nseg][SORT_MAX_PASSES][256]
-  long long* base;       // [nseg][SORT_MAX_PASSES][256]
-  u64* status;           // [ntiles][256] look-back words: epoch<<34 | flag<<32 | count
+  u32* hist;             // [nseg][SORT_MAX_PASSES][radix]
+  long long* base;       // [nseg][SORT_MAX_PASSES][radix]
+  u64* status;           // [ntiles][radix] look-back words: epoch<<34 | flag<<32 | count
   u32* counters;         // [SORT_MAX_PASSES] tile claims, then the epoch word
   int* err;              // nonzero after a bounded wait gave up
 };
 
-// Host side (sort.cu).  `segs` is a host array.
-int sort_plan_create(SortPlan* plan, const SortSeg* segs, int nseg, int npass);
+// Host side (sort.cu).  `segs` is a host array.  The digit width is the smallest of 8..10 bits
+// that covers `span` key bits in `npass` passes (npass = 0: as few passes as 10-bit digits allow).
+int sort_plan_create(SortPlan* plan, const SortSeg* segs, int nseg, int npass, int span = 0);
 void sort_plan_destroy(SortPlan* plan);
 // Runs plan->npass passes, ping-ponging (k0,v0) -> (k1,v1) -> (k0,v0) ...  The sorted
 // result is in (k0,v0) when npass is even, (k1,v1) when odd.  identity_vals ignores the
 // contents of v0 and uses value = global index.  write_last_keys = false skips writing the
 // keys on the last pass (only the permutation is then produced).
-int sort_run(const SortPlan* plan, u64* k0, u32* v0, u64* k1, u32* v1, bool identity_vals,
-             bool write_last_keys, cudaStream_t s);
+// Key is u64 or u32 (the engine's cell keys fit 32 bits; the segment supplies the peak id).
+template <class K>
+int sort_run(const SortPlan* plan, K* k0, u32* v0, K* k1, u32* v1, bool identity_vals, bool write_last_keys,
+             cudaStream_t s);

@@ -42,7 +42,7 @@ def _ptr(t) -> int:
 
 
 class Engine:
-    def __init__(self, peaks, device: int = 0, bucket_sort: bool = False, graph: bool = True):
+    def __init__(self, peaks, device: int = 0, bucket_sort: bool = True, graph: bool = True, full_every: int = 16):
         torch = _lib.require_cuda()
         self._torch = torch
         lib = _lib.load()
@@ -51,7 +51,11 @@ class Engine:
         arr = (_lib.PeakCfg * len(self.cfgs))(*[c.cstruct() for c in self.cfgs])
         h = C.c_void_p()
         self.device = int(device)
-        flags = (_lib.FLAG_BUCKET_SORT if bucket_sort else 0) | (_lib.FLAG_GRAPH if graph else 0)
+        # bucket_sort: each step sorts only the bucket bits of the cell key (what the deposit and
+        # push group by); every `full_every` steps the whole key is sorted.  Results do not
+        # depend on the choice: the deposit is order-independent bit for bit.
+        flags = ((_lib.FLAG_BUCKET_SORT | (int(full_every) & 0xFF) << 8) if bucket_sort else 0) | \
+                (_lib.FLAG_GRAPH if graph else 0)
         torch.cuda.set_device(self.device)
         check(lib.pm_engine_create(arr, len(self.cfgs), self.device, flags, C.byref(h)), "pm_engine_create")
         self._h = h
