@@ -159,6 +159,24 @@ int pm_sort_u64(const unsigned long long* keys, unsigned long long* keys_out, un
 int pm_rell_keys(int Np, double L, const double* A, unsigned long long* keys);
 int pm_analyse_partials(const double* x, int Np, double L, const double* A, const double* centre,
                         const double* set_radii, const double* radii, int nblocks, double* partials);
+/* pm_sort_u64 for callers that cannot allocate device memory.  No counterpart in the reference
+ * (which has no GPU code).  Some callers must not call cudaMalloc or cudaFree: cudaFree waits
+ * for the whole device and both can stall on driver locks, so a latency-bound loop (such as a
+ * request loop between two steps) cannot afford them, and a process whose device memory is
+ * already held by another framework's allocator may have none to give.  This variant takes the
+ * same input and outputs but keeps all of its scratch in one static device array of
+ * PM_NOALLOC_SCRATCH_BYTES inside this library, which every GPU that loads the library holds
+ * until the process exits; it calls no allocating routine.  n must not exceed
+ * PM_NOALLOC_MAX_KEYS (larger n returns -2003 and touches nothing).  The first call on a device
+ * looks up the array's device address for that device (cudaGetSymbolAddress, with that device
+ * current), so make that first call before any stream capture.  Every call shares the array:
+ * calls that overlap on the GPU (from several streams or threads) race, and must be serialized
+ * by the caller.  Runs on `stream` (a cudaStream_t, NULL for the default stream) and returns
+ * after the sort has finished: 0, 1 if a bounded look-back wait gave up, < 0 on error. */
+#define PM_NOALLOC_MAX_KEYS (1LL << 18)
+#define PM_NOALLOC_SCRATCH_BYTES (3670016)
+int pm_sort_u64_noalloc(const unsigned long long* keys, unsigned long long* keys_out, unsigned int* perm_out,
+                        long long n, int lo, int hi, void* stream);
 /* Cell keys of split positions; used by tests to check the key layout. */
 int pm_cell_keys(const int* cells, long long n, int N, int tile, unsigned int* keys_out);
 

@@ -14,6 +14,7 @@ SCHED_RATIO, SCHED_FRAC, SCHED_EXPLICIT = 0, 1, 2
 STATE_IDLE, STATE_PRIME, STATE_RUN, STATE_FINALIZE, STATE_HOLD = 0, 1, 2, 3, 4
 FLAG_BUCKET_SORT = 1
 FLAG_GRAPH = 2
+NOALLOC_MAX_KEYS = 1 << 18          # PM_NOALLOC_MAX_KEYS of include/pmb200.h
 
 
 class PeakCfg(C.Structure):
@@ -68,6 +69,8 @@ _SIGS = {
     "pm_interp64": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong, C.c_int, C.c_double, C.c_void_p]),
     "pm_sort_u64": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.c_int,
                               C.c_int]),
+    "pm_sort_u64_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.c_int, C.c_int,
+                                      C.c_void_p]),
     "pm_cell_keys": (C.c_int, [C.c_void_p, C.c_longlong, C.c_int, C.c_int, C.c_void_p]),
 }
 
