@@ -43,6 +43,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--full-sort", action="store_true", help="sort the whole cell key every step")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served-stream latency run")
+    ap.add_argument("--serve-seconds", type=float, default=10.0, help="arrival window of the served stream")
+    ap.add_argument("--serve-rate", type=float, default=20.0, help="mean request arrivals per second")
     return ap.parse_args()
 
 
@@ -278,6 +281,9 @@ def run_ours(args):
     if not args.no_e2e:
         line["e2e"] = e2e_job(ens, specs, torch, local)
     ens.close()
+    del ens
+    if rank == 0 and not args.no_serve:
+        line["served"] = served_stream(args, local)
     if rank == 0 and world == 1 and not args.no_cpu:
         cb = cpu_rate(specs, steps=2, warmup=1, max_mesh=128 if args.workload == "batched" else 64)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
@@ -317,6 +323,32 @@ def e2e_job(ens, specs, torch, device):
     return {"value": ps / t, "unit": UNIT, "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step": stats_bytes / done,
             "job_steps": steps, "seconds": t,
             "how": "public Ensemble API: pinned host noise -> device IC -> all steps, per-step stats to host; wall clock"}
+
+
+def served_stream(args, device):
+    """The served form: Poisson arrivals of single-peak collapse runs (meshes 64^3-256^3,
+    (e, p, delta0) as the ensemble) admitted into a slot pool under a 150 GB HBM budget,
+    continuously batched, each run ending at its collapse (max delta >= 50) or last step."""
+    import numpy as np
+
+    from pbh_b200.serve import Server, ServerConfig, latency_summary, poisson_arrivals
+    arrivals = poisson_arrivals(rate=args.serve_rate, duration=args.serve_seconds, seed=args.seed, steps=150)
+    cfg = ServerConfig(slots={64: 32, 128: 32, 256: 24}, budget_bytes=150e9, delta_collapse=50.0, keep_delta=True,
+                       device=device)
+    srv = Server(cfg)
+    t0 = time.perf_counter()
+    done = srv.serve(arrivals, timeout=args.serve_seconds + 240.0)
+    wall = time.perf_counter() - t0
+    out = latency_summary(done)
+    out.update(requests=len(arrivals), rate_per_s=args.serve_rate, arrival_window_s=args.serve_seconds,
+               wall_s=wall, particle_steps_per_s=srv.particle_steps / wall, engine_steps=srv.engine_steps,
+               collapsed=int(sum(1 for r in done if r.a_collapse_cfg > 0)),
+               mean_steps=float(np.mean([r.steps for r in done])) if done else None,
+               slots={str(k): v for k, v in cfg.slots.items()}, budget_gb=cfg.budget_bytes / 1e9,
+               device_gb=srv.engine.device_bytes / 1e9,
+               how="latency = arrival to result (collapse a, final delta) on the host; wall-clock")
+    srv.close()
+    return out
 
 
 def main():

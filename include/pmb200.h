@@ -69,8 +69,10 @@ typedef struct {
 
 /* Create an engine holding npeaks independent peaks (a batched ensemble; npeaks = 1 is the
  * plain single run).  Allocates all device memory and cuFFT plans up front; no later call
- * allocates.  flags: bit 0 = sort only the bucket bits of the key each step (the full
- * 64-bit key is sorted at priming); bit 1 = record the step as a CUDA graph. */
+ * allocates.  flags: bit 0 = sort only the bucket bits of the key each step, with the whole
+ * key sorted every (flags >> 8 & 0xFF) steps (16 if 0); bit 1 = replay the step as a CUDA graph;
+ * bit 2 = dynamic mode for served runs: no graph, and each step's FFTs cover only the slots up
+ * to the highest one in use in each mesh size (slots are the peaks of one size, in order). */
 int pm_engine_create(const pm_peak_cfg* cfg, int npeaks, int device, int flags, pm_engine** out);
 int pm_engine_destroy(pm_engine* e);
 int pm_engine_sync(pm_engine* e);
@@ -110,8 +112,11 @@ int pm_get_delta(pm_engine* e, int peak, float* delta);
 /* Float64 CIC counts of the current positions (N^3): PM3D.deposit(PM3D.x) (pm3d.py:81-89). */
 int pm_get_counts(pm_engine* e, int peak, double* counts);
 /* Collapse time tracking: the first a at which max delta of the peak's deposit reaches
- * delta_collapse is recorded on the device (pm_clock_info.a_collapse).  <= 0 disables. */
-int pm_set_collapse_threshold(pm_engine* e, int peak, double delta_collapse);
+ * delta_collapse is recorded on the device (pm_clock_info.a_collapse); <= 0 disables.  With
+ * stop != 0 the run ends there (the peak finalizes and goes idle). */
+int pm_set_collapse_threshold(pm_engine* e, int peak, double delta_collapse, int stop);
+/* Free a peak's slot: it goes idle, its mesh is no longer transformed (dynamic mode). */
+int pm_release(pm_engine* e, int peak);
 int pm_get_clock(pm_engine* e, int peak, pm_clock_info* out);   /* host struct */
 int pm_get_stats(pm_engine* e, int peak, pm_stats_info* out);   /* host struct */
 /* All peaks at once (host arrays of npeaks); the return value counts flagged peaks. */
@@ -139,8 +144,13 @@ typedef struct {
   const double* noise;     /* device, N^3 standard normals, or NULL */
   double tail_rms, k1, k2;
   double noise_frac;
+  unsigned long long noise_seed;  /* noise == NULL and seed != 0: N^3 normals generated on the
+                                   * device (Philox4x32-10 + Box-Muller) instead of numpy's stream */
 } pm_ic_params;
 int pm_make_ic(const pm_ic_params* prm, double* x_out, double* p_out, double* delta_lin_out, double* noise_rms_out);
+/* pm_make_ic keeps its float64 work buffers and cuFFT plans per (device, N) after the first call;
+ * this frees them. */
+int pm_ic_release_cache(void);
 
 /* Stateless helpers. */
 /* PM3D.interp(F, X) (pm3d.py:91-99) in float64: F (N^3), X (n,3) -> out (n). */

@@ -14,6 +14,7 @@ SCHED_RATIO, SCHED_FRAC, SCHED_EXPLICIT = 0, 1, 2
 STATE_IDLE, STATE_PRIME, STATE_RUN, STATE_FINALIZE, STATE_HOLD = 0, 1, 2, 3, 4
 FLAG_BUCKET_SORT = 1
 FLAG_GRAPH = 2
+FLAG_DYNAMIC = 4
 NOALLOC_MAX_KEYS = 1 << 18          # PM_NOALLOC_MAX_KEYS of include/pmb200.h
 
 
@@ -37,7 +38,7 @@ class ICParams(C.Structure):
     _fields_ = [("N", C.c_int), ("Np", C.c_int), ("L", C.c_double), ("kind", C.c_int), ("amp", C.c_double),
                 ("axes", C.c_double * 3), ("spline_x", C.c_void_p), ("spline_c", C.c_void_p), ("spline_m", C.c_int),
                 ("noise", C.c_void_p), ("tail_rms", C.c_double), ("k1", C.c_double), ("k2", C.c_double),
-                ("noise_frac", C.c_double)]
+                ("noise_frac", C.c_double), ("noise_seed", C.c_ulonglong)]
 
 
 # name -> (restype, argtypes)
@@ -59,13 +60,15 @@ _SIGS = {
     "pm_get_acc": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_void_p]),
     "pm_get_delta": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "pm_get_counts": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
-    "pm_set_collapse_threshold": (C.c_int, [C.c_void_p, C.c_int, C.c_double]),
+    "pm_set_collapse_threshold": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int]),
+    "pm_release": (C.c_int, [C.c_void_p, C.c_int]),
     "pm_get_clock": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(ClockInfo)]),
     "pm_get_stats": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(StatsInfo)]),
     "pm_make_ic": (C.c_int, [C.POINTER(ICParams), C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]),
     "pm_rell_keys": (C.c_int, [C.c_int, C.c_double, C.c_void_p, C.c_void_p]),
     "pm_analyse_partials": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_int, C.c_void_p]),
+    "pm_ic_release_cache": (C.c_int, []),
     "pm_interp64": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong, C.c_int, C.c_double, C.c_void_p]),
     "pm_sort_u64": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.c_int,
                               C.c_int]),

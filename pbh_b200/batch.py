@@ -40,7 +40,7 @@ class Ensemble:
             x, p = recipe_particles(s, device=self.device, noise=None if noises is None else noises[j])
             self.engine.set_particles(i, x, p, 1.0, mode=_lib.SCHED_RATIO, param=s.ratio(), max_steps=s.steps)
             if self.delta_collapse > 0:
-                _lib.load().pm_set_collapse_threshold(self.engine._h, i, self.delta_collapse)
+                _lib.load().pm_set_collapse_threshold(self.engine._h, i, self.delta_collapse, 0)
             del x, p
 
     def step(self, k: int = 1):

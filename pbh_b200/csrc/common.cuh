@@ -59,6 +59,7 @@ struct PeakDesc {
   long long bucket_off;    // offset of this peak's bucket-start array (nb + 1 entries)
   long long mode_base;     // first global mode-block of this peak (Green kernel)
   long long nmodes;        // N*N*(N/2+1)
+  double inv_nh;           // 1/(N/2+1)
   float* delta;            // N^3 FP32 density contrast (R2C input)
   float2* spec;            // N*N*(N/2+1) complex spectrum (R2C output)
   float2* gspec;           // 3 gradient spectra
@@ -79,7 +80,7 @@ struct PeakClock {
   int buf;         // which particle buffer holds the current state
   int dep;         // 1 when this step re-deposits (set by the advance kernel)
   int has_delta;   // delta/grids hold data
-  int pad;
+  int stop_on_collapse;  // end the run (finalize) on the step that detects collapse
   double delta_collapse;  // collapse threshold on max delta (<= 0: not tracked)
   double a_collapse;      // first a whose deposit reached delta_collapse (-1: not yet)
 };

@@ -34,13 +34,16 @@ int ilog2(int v) {
 
 struct MeshClass {
   int N = 0;
-  std::vector<int> peaks;
+  std::vector<int> peaks;   // peak indices in slot order
   float* delta = nullptr;
   float2* spec = nullptr;
   float2* gspec = nullptr;
   float* force = nullptr;
   cufftHandle r2c = 0, c2r = 0;
   bool plans = false;
+  // Dynamic mode: plans for every batch size 1..B over the leading slots, one shared work area.
+  std::vector<cufftHandle> r2c_b, c2r_b;
+  void* work = nullptr;
 };
 
 }  // namespace
@@ -74,6 +77,7 @@ struct pm_engine {
   long long replays = 0;
   int sort_result = 0;  // which (keys, vals) pair holds the sorted output (same for both plans)
   cudaGraphExec_t graph = nullptr, graph_full = nullptr;
+  std::vector<char> occupied;  // host view: slots holding a run (dynamic mode FFT extents)
   long long bytes = 0;
 
   StepArgs args() const {
@@ -117,10 +121,41 @@ struct pm_engine {
     if (r) return r;
     launch_bucket_starts(A, ntot, stream);
     launch_deposit(A, nptiles, smem_dep, nullptr, stream);
-    for (auto& c : classes) CF(cufftExecR2C(c.r2c, c.delta, (cufftComplex*)c.spec));
+    int r2 = fft_r2c();
+    if (r2) return r2;
     launch_green(A, nmodeblk, stream);
-    for (auto& c : classes) CF(cufftExecC2R(c.c2r, (cufftComplex*)c.gspec, c.force));
+    if ((r2 = fft_c2r())) return r2;
     CU(cudaGetLastError());
+    return 0;
+  }
+
+  // Slots in use per class (dynamic mode): transforms run over slots [0, extent).
+  int extent(const MeshClass& c) const {
+    int x = 0;
+    for (int k = 0; k < (int)c.peaks.size(); ++k)
+      if (occupied[c.peaks[k]]) x = k + 1;
+    return x;
+  }
+  int fft_r2c() {
+    for (auto& c : classes) {
+      if (flags & 4) {
+        const int x = extent(c);
+        if (x) CF(cufftExecR2C(c.r2c_b[x - 1], c.delta, (cufftComplex*)c.spec));
+      } else {
+        CF(cufftExecR2C(c.r2c, c.delta, (cufftComplex*)c.spec));
+      }
+    }
+    return 0;
+  }
+  int fft_c2r() {
+    for (auto& c : classes) {
+      if (flags & 4) {
+        const int x = extent(c);
+        if (x) CF(cufftExecC2R(c.c2r_b[x - 1], (cufftComplex*)c.gspec, c.force));
+      } else {
+        CF(cufftExecC2R(c.c2r, (cufftComplex*)c.gspec, c.force));
+      }
+    }
     return 0;
   }
 
@@ -145,11 +180,11 @@ struct pm_engine {
     CU(cudaEventRecord(ev[4], stream));
     launch_deposit(A, nptiles, smem_dep, nullptr, stream);
     CU(cudaEventRecord(ev[5], stream));
-    for (auto& c : classes) CF(cufftExecR2C(c.r2c, c.delta, (cufftComplex*)c.spec));
+    if ((r = fft_r2c())) return r;
     CU(cudaEventRecord(ev[6], stream));
     launch_green(A, nmodeblk, stream);
     CU(cudaEventRecord(ev[7], stream));
-    for (auto& c : classes) CF(cufftExecC2R(c.c2r, (cufftComplex*)c.gspec, c.force));
+    if ((r = fft_c2r())) return r;
     CU(cudaEventRecord(ev[8], stream));
     CU(cudaEventSynchronize(ev[8]));
     for (int k = 0; k < 8; ++k) {
@@ -163,7 +198,7 @@ struct pm_engine {
   int step() {
     const bool full = next_full();
     ++replays;
-    if (flags & 2) {
+    if ((flags & 2) && !(flags & 4)) {
       cudaGraphExec_t& g = full ? graph_full : graph;
       if (!g) {
         cudaGraph_t cg = nullptr;
@@ -200,6 +235,9 @@ struct pm_engine {
         cufftDestroy(c.r2c);
         cufftDestroy(c.c2r);
       }
+      for (auto h : c.r2c_b) cufftDestroy(h);
+      for (auto h : c.c2r_b) cufftDestroy(h);
+      cudaFree(c.work);
       cudaFree(c.delta);
       cudaFree(c.spec);
       cudaFree(c.gspec);
@@ -230,6 +268,7 @@ namespace {
 int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   E->npeaks = npeaks;
   E->peaks.resize(npeaks);
+  E->occupied.assign(npeaks, 0);
   std::map<int, int> class_of;
   long long poff = 0, tb = 0, mb = 0, bo = 0, ptb = 0;
   int Tmax = 1, TPmax = 1;
@@ -276,6 +315,7 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
     P.tile_base = tb;
     P.bucket_off = bo;
     P.nmodes = (long long)c.N * c.N * (c.N / 2 + 1);
+    P.inv_nh = 1.0 / (double)(c.N / 2 + 1);
     P.mode_base = mb;
     tile_base[i] = tb;
     ptile_base[i] = ptb;
@@ -331,14 +371,41 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
       P.force = mc.force + 3 * k * N3;
     }
     int n[3] = {(int)N, (int)N, (int)N};
-    CF(cufftPlanMany(&mc.r2c, 3, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_R2C, B));
-    CF(cufftPlanMany(&mc.c2r, 3, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2R, 3 * B));
-    mc.plans = true;
-    CF(cufftSetStream(mc.r2c, E->stream));
-    CF(cufftSetStream(mc.c2r, E->stream));
-    size_t ws = 0;
-    if (cufftGetSize(mc.r2c, &ws) == CUFFT_SUCCESS) E->bytes += (long long)ws;
-    if (cufftGetSize(mc.c2r, &ws) == CUFFT_SUCCESS) E->bytes += (long long)ws;
+    if (E->flags & 4) {
+      // Dynamic mode: a plan per batch size, all sharing the largest work area, so a step
+      // transforms only the slots up to the highest one in use.
+      size_t wmax = 0;
+      for (int b = 1; b <= B; ++b) {
+        cufftHandle h1, h2;
+        size_t w1 = 0, w2 = 0;
+        CF(cufftCreate(&h1));
+        CF(cufftCreate(&h2));
+        CF(cufftSetAutoAllocation(h1, 0));
+        CF(cufftSetAutoAllocation(h2, 0));
+        CF(cufftMakePlanMany(h1, 3, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_R2C, b, &w1));
+        CF(cufftMakePlanMany(h2, 3, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2R, 3 * b, &w2));
+        CF(cufftSetStream(h1, E->stream));
+        CF(cufftSetStream(h2, E->stream));
+        mc.r2c_b.push_back(h1);
+        mc.c2r_b.push_back(h2);
+        wmax = std::max(wmax, std::max(w1, w2));
+      }
+      int rr;
+      if ((rr = E->alloc((char**)&mc.work, wmax))) return rr;
+      for (int b = 0; b < B; ++b) {
+        CF(cufftSetWorkArea(mc.r2c_b[b], mc.work));
+        CF(cufftSetWorkArea(mc.c2r_b[b], mc.work));
+      }
+    } else {
+      CF(cufftPlanMany(&mc.r2c, 3, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_R2C, B));
+      CF(cufftPlanMany(&mc.c2r, 3, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2R, 3 * B));
+      mc.plans = true;
+      CF(cufftSetStream(mc.r2c, E->stream));
+      CF(cufftSetStream(mc.c2r, E->stream));
+      size_t ws = 0;
+      if (cufftGetSize(mc.r2c, &ws) == CUFFT_SUCCESS) E->bytes += (long long)ws;
+      if (cufftGetSize(mc.c2r, &ws) == CUFFT_SUCCESS) E->bytes += (long long)ws;
+    }
   }
 
   int r;
@@ -447,6 +514,7 @@ int pm_set_particles(pm_engine* e, int peak, const double* x, const double* p, d
   const StepArgs A = e->args();
   launch_reset_peak(A, peak, a0, mode, param, a_end, max_steps, e->stream);
   launch_set_particles(A, peak, e->peaks[peak], x, p, e->stream);
+  e->occupied[peak] = 1;
   CU(cudaGetLastError());
   CU(cudaStreamSynchronize(e->stream));
   return 0;
@@ -611,14 +679,30 @@ int pm_get_counts(pm_engine* e, int peak, double* counts) {
   return 0;
 }
 
-int pm_set_collapse_threshold(pm_engine* e, int peak, double delta_collapse) {
+int pm_set_collapse_threshold(pm_engine* e, int peak, double delta_collapse, int stop) {
   if (!e || peak < 0 || peak >= e->npeaks) return -2000;
   CU(cudaSetDevice(e->device));
   PeakClock c;
   int r;
   if ((r = e->read_clock(peak, &c))) return r;
   c.delta_collapse = delta_collapse;
+  c.stop_on_collapse = stop ? 1 : 0;
   return e->write_clock(peak, c);
+}
+
+int pm_release(pm_engine* e, int peak) {
+  if (!e || peak < 0 || peak >= e->npeaks) return -2000;
+  CU(cudaSetDevice(e->device));
+  PeakClock c;
+  int r;
+  if ((r = e->read_clock(peak, &c))) return r;
+  c.state = PS_IDLE;
+  c.has_delta = 0;
+  c.dep = 0;
+  c.kpend = 0.0;
+  if ((r = e->write_clock(peak, c))) return r;
+  e->occupied[peak] = 0;
+  return 0;
 }
 
 int pm_get_clock(pm_engine* e, int peak, pm_clock_info* out) {

@@ -5,6 +5,9 @@
 #include <cufft.h>
 
 #include <cmath>
+#include <map>
+#include <mutex>
+#include <utility>
 #include <vector>
 
 #include "../../include/pmb200.h"
@@ -83,6 +86,49 @@ __global__ void k_shape(cufftDoubleComplex* __restrict__ s, int N, double L, int
   }
   s[m].x *= f;
   s[m].y *= f;
+}
+
+// Counter-based normal deviates for seeded noise generated on the device: Philox4x32-10
+// (Salmon, Moraes, Dror & Shaw, SC'11: 10 rounds of the two 32x32->64 multiplies with a Weyl-
+// sequence key schedule) feeding the Box-Muller transform.  Element i of the field is a
+// deterministic function of (seed, i), so a run is reproducible and independent of launch shape.
+__device__ __forceinline__ void philox_round(u32 (&c)[4], u32 k0, u32 k1) {
+  const u32 M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+  const u32 hi0 = __umulhi(M0, c[0]), lo0 = M0 * c[0];
+  const u32 hi1 = __umulhi(M1, c[2]), lo1 = M1 * c[2];
+  const u32 n0 = hi1 ^ c[1] ^ k0, n1 = lo1, n2 = hi0 ^ c[3] ^ k1, n3 = lo0;
+  c[0] = n0;
+  c[1] = n1;
+  c[2] = n2;
+  c[3] = n3;
+}
+
+__global__ void k_philox_normal(double* __restrict__ out, long long n, unsigned long long seed) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;  // one Philox call -> 4 normals
+  if (4 * q >= n) return;
+  u32 c[4] = {(u32)q, (u32)((unsigned long long)q >> 32), 0x5eedu, 0x1ce5u};
+  u32 k0 = (u32)seed, k1 = (u32)(seed >> 32);
+  for (int r = 0; r < 10; ++r) {
+    philox_round(c, k0, k1);
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  // 53-bit uniforms in (0, 1] from pairs of words, then Box-Muller pairs.
+  const double inv53 = 1.0 / 9007199254740992.0;
+  const double u0 = ((double)((((unsigned long long)c[0] << 32) | c[1]) >> 11) + 1.0) * inv53;
+  const double u1 = (double)((((unsigned long long)c[2] << 32) | c[3]) >> 11) * inv53;
+  const double r = sqrt(-2.0 * log(u0));
+  double sn, cs;
+  sincospi(2.0 * u1, &sn, &cs);
+  // The second pair reuses the words with halves swapped.
+  const double v0 = ((double)((((unsigned long long)c[3] << 32) | c[2]) >> 11) + 1.0) * inv53;
+  const double v1 = (double)((((unsigned long long)c[1] << 32) | c[0]) >> 11) * inv53;
+  const double r2 = sqrt(-2.0 * log(v0));
+  double sn2, cs2;
+  sincospi(2.0 * v1, &sn2, &cs2);
+  const double z[4] = {r * cs, r * sn, r2 * cs2, r2 * sn2};
+  for (int k = 0; k < 4; ++k)
+    if (4 * q + k < n) out[4 * q + k] = z[k];
 }
 
 __global__ void k_axpy_spec(cufftDoubleComplex* __restrict__ y, const cufftDoubleComplex* __restrict__ x, double a,
@@ -225,7 +271,70 @@ done:
 
 unsigned nblk(long long n) { return (unsigned)((n + kThreads - 1) / kThreads); }
 
+// Device buffers and FP64 cuFFT plans of pm_make_ic, kept per (device, N) after first use so
+// that repeated calls (a request loop) neither allocate nor plan again.
+struct ICWork {
+  double *field = nullptr, *real4 = nullptr, *tmp_real = nullptr, *noise = nullptr;
+  cufftDoubleComplex *spec = nullptr, *nspec = nullptr, *spec4 = nullptr, *tmp_spec = nullptr;
+  cufftHandle d2z = 0, z2d = 0, z2d4 = 0;
+  bool ok = false;
+};
+std::mutex g_ic_mu;
+std::map<std::pair<int, int>, ICWork> g_ic;
+
+int ic_work(int device, int N, ICWork** out) {
+  std::lock_guard<std::mutex> lock(g_ic_mu);
+  ICWork& w = g_ic[{device, N}];
+  if (!w.ok) {
+    const long long N3 = (long long)N * N * N, M = (long long)N * N * (N / 2 + 1);
+    int rc = 0;
+    int n3[3] = {N, N, N};
+    CU(cudaMalloc(&w.field, sizeof(double) * N3));
+    CU(cudaMalloc(&w.real4, sizeof(double) * 4 * N3));
+    CU(cudaMalloc(&w.tmp_real, sizeof(double) * N3));
+    CU(cudaMalloc(&w.noise, sizeof(double) * N3));
+    CU(cudaMalloc(&w.spec, sizeof(cufftDoubleComplex) * M));
+    CU(cudaMalloc(&w.nspec, sizeof(cufftDoubleComplex) * M));
+    CU(cudaMalloc(&w.spec4, sizeof(cufftDoubleComplex) * 4 * M));
+    CU(cudaMalloc(&w.tmp_spec, sizeof(cufftDoubleComplex) * M));
+    CF(cufftPlan3d(&w.d2z, N, N, N, CUFFT_D2Z));
+    CF(cufftPlan3d(&w.z2d, N, N, N, CUFFT_Z2D));
+    CF(cufftPlanMany(&w.z2d4, 3, n3, nullptr, 1, 0, nullptr, 1, 0, CUFFT_Z2D, 4));
+    w.ok = true;
+  done:
+    if (rc) {
+      g_ic.erase({device, N});
+      return rc;
+    }
+  }
+  *out = &w;
+  return 0;
+}
+
 }  // namespace
+
+extern "C" int pm_ic_release_cache(void) {
+  std::lock_guard<std::mutex> lock(g_ic_mu);
+  for (auto& kv : g_ic) {
+    ICWork& w = kv.second;
+    cudaSetDevice(kv.first.first);
+    cudaFree(w.field);
+    cudaFree(w.real4);
+    cudaFree(w.tmp_real);
+    cudaFree(w.noise);
+    cudaFree(w.spec);
+    cudaFree(w.nspec);
+    cudaFree(w.spec4);
+    cudaFree(w.tmp_spec);
+    if (w.ok) {
+      cufftDestroy(w.d2z);
+      cufftDestroy(w.z2d);
+      cufftDestroy(w.z2d4);
+    }
+  }
+  g_ic.clear();
+  return 0;
+}
 
 extern "C" int pm_make_ic(const pm_ic_params* prm, double* x_out, double* p_out, double* delta_lin_out,
                           double* noise_rms_out) {
@@ -236,18 +345,15 @@ extern "C" int pm_make_ic(const pm_ic_params* prm, double* x_out, double* p_out,
   if (prm->kind != 0 && prm->kind != 1) return -2003;
   const long long N3 = (long long)N * N * N, M = (long long)N * N * (N / 2 + 1);
   const double L = prm->L;
-  int rc = 0;
-  double *field = nullptr, *xs = nullptr, *cs = nullptr, *real4 = nullptr, *tmp_real = nullptr;
-  cufftDoubleComplex *spec = nullptr, *nspec = nullptr, *spec4 = nullptr, *tmp_spec = nullptr;
-  cufftHandle d2z = 0, z2d = 0, z2d4 = 0;
-  bool has_d2z = false, has_z2d = false, has_z2d4 = false;
+  int rc = 0, device = 0;
+  double *xs = nullptr, *cs = nullptr;
   double noise_rms = 0.0;
-  const bool noisy = prm->noise && ((prm->kind == 0 && prm->tail_rms > 0) || (prm->kind == 1 && prm->noise_frac > 0));
-
-  CU(cudaMalloc(&field, sizeof(double) * N3));
-  CU(cudaMalloc(&spec, sizeof(cufftDoubleComplex) * M));
-  CU(cudaMalloc(&spec4, sizeof(cufftDoubleComplex) * 4 * M));
-  CU(cudaMalloc(&real4, sizeof(double) * 4 * N3));
+  const bool want_noise = (prm->kind == 0 && prm->tail_rms > 0) || (prm->kind == 1 && prm->noise_frac > 0);
+  const bool noisy = want_noise && (prm->noise || prm->noise_seed);
+  ICWork* w = nullptr;
+  CU(cudaGetDevice(&device));
+  rc = ic_work(device, N, &w);
+  if (rc) return rc;
   if (prm->kind == 0) {
     const int m = prm->spline_m;
     CU(cudaMalloc(&xs, sizeof(double) * (m + 1)));
@@ -255,55 +361,37 @@ extern "C" int pm_make_ic(const pm_ic_params* prm, double* x_out, double* p_out,
     CU(cudaMemcpy(xs, prm->spline_x, sizeof(double) * (m + 1), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(cs, prm->spline_c, sizeof(double) * 4 * m, cudaMemcpyHostToDevice));
   }
-  CF(cufftPlan3d(&d2z, N, N, N, CUFFT_D2Z));
-  has_d2z = true;
-  {
-    int n3[3] = {N, N, N};
-    CF(cufftPlanMany(&z2d4, 3, n3, nullptr, 1, 0, nullptr, 1, 0, CUFFT_Z2D, 4));
-    has_z2d4 = true;
-  }
   k_field<<<nblk(N3), kThreads>>>(N, L, prm->kind, prm->amp, prm->axes[0], prm->axes[1], prm->axes[2], xs, cs,
-                                  prm->kind == 0 ? prm->spline_m : 0, field);
+                                  prm->kind == 0 ? prm->spline_m : 0, w->field);
   CU(cudaGetLastError());
-  CF(cufftExecD2Z(d2z, field, spec));
+  CF(cufftExecD2Z(w->d2z, w->field, w->spec));
   if (noisy) {
-    CU(cudaMalloc(&nspec, sizeof(cufftDoubleComplex) * M));
-    CU(cudaMalloc(&tmp_spec, sizeof(cufftDoubleComplex) * M));
-    CU(cudaMalloc(&tmp_real, sizeof(double) * N3));
-    CF(cufftPlan3d(&z2d, N, N, N, CUFFT_Z2D));
-    has_z2d = true;
-    CF(cufftExecD2Z(d2z, (double*)prm->noise, nspec));
-    k_shape<<<nblk(M), kThreads>>>(nspec, N, L, prm->kind, prm->tail_rms, prm->k1, prm->k2);
+    if (!prm->noise) {  // seeded device noise
+      k_philox_normal<<<nblk((N3 + 3) / 4), kThreads>>>(w->noise, N3, prm->noise_seed);
+      CU(cudaGetLastError());
+    }
+    CF(cufftExecD2Z(w->d2z, prm->noise ? (double*)prm->noise : w->noise, w->nspec));
+    k_shape<<<nblk(M), kThreads>>>(w->nspec, N, L, prm->kind, prm->tail_rms, prm->k1, prm->k2);
     CU(cudaGetLastError());
-    CU(cudaMemcpy(tmp_spec, nspec, sizeof(cufftDoubleComplex) * M, cudaMemcpyDeviceToDevice));
-    CF(cufftExecZ2D(z2d, tmp_spec, tmp_real));  // unnormalised inverse; numpy divides by N^3
-    rc = grid_std(tmp_real, N3, &noise_rms);
+    CU(cudaMemcpy(w->tmp_spec, w->nspec, sizeof(cufftDoubleComplex) * M, cudaMemcpyDeviceToDevice));
+    CF(cufftExecZ2D(w->z2d, w->tmp_spec, w->tmp_real));  // unnormalised inverse; numpy divides by N^3
+    rc = grid_std(w->tmp_real, N3, &noise_rms);
     if (rc) goto done;
     noise_rms /= (double)N3;
     const double scale = prm->kind == 0 ? 1.0 : prm->noise_frac * prm->amp / noise_rms;
-    k_axpy_spec<<<nblk(M), kThreads>>>(spec, nspec, scale, M);
+    k_axpy_spec<<<nblk(M), kThreads>>>(w->spec, w->nspec, scale, M);
     CU(cudaGetLastError());
   }
-  k_disp_spectra<<<nblk(M), kThreads>>>(spec, N, L, prm->kind, spec4);
+  k_disp_spectra<<<nblk(M), kThreads>>>(w->spec, N, L, prm->kind, w->spec4);
   CU(cudaGetLastError());
-  CF(cufftExecZ2D(z2d4, spec4, real4));
-  k_lattice<<<nblk((long long)Np * Np * Np), kThreads>>>(N, Np, L, real4, x_out, p_out);
+  CF(cufftExecZ2D(w->z2d4, w->spec4, w->real4));
+  k_lattice<<<nblk((long long)Np * Np * Np), kThreads>>>(N, Np, L, w->real4, x_out, p_out);
   CU(cudaGetLastError());
-  if (delta_lin_out) CU(cudaMemcpy(delta_lin_out, real4, sizeof(double) * N3, cudaMemcpyDeviceToDevice));
+  if (delta_lin_out) CU(cudaMemcpy(delta_lin_out, w->real4, sizeof(double) * N3, cudaMemcpyDeviceToDevice));
   CU(cudaDeviceSynchronize());
   if (noise_rms_out) *noise_rms_out = noise_rms;
 done:
-  if (has_d2z) cufftDestroy(d2z);
-  if (has_z2d) cufftDestroy(z2d);
-  if (has_z2d4) cufftDestroy(z2d4);
-  cudaFree(field);
   cudaFree(xs);
   cudaFree(cs);
-  cudaFree(real4);
-  cudaFree(tmp_real);
-  cudaFree(spec);
-  cudaFree(nspec);
-  cudaFree(spec4);
-  cudaFree(tmp_spec);
   return rc;
 }

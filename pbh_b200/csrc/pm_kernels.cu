@@ -138,16 +138,33 @@ __device__ __forceinline__ void push_tile(const StepArgs& A, const PeakDesc& P, 
   float4* __restrict__ mout = momb(A, buf ^ 1);
   u32* __restrict__ kout = A.keys_push;
   bool bad = false;
-  // Two particles per thread per iteration: both gathers are in flight before either is used.
-  for (long long j = b + threadIdx.x; j < e; j += 2 * PUSH_THREADS) {
+  // Two particles per thread per sweep, and the next sweep's pair is fetched before this one is
+  // computed, so four gathers are in flight while the arithmetic runs.
+  long long j = b + threadIdx.x;
+  int4 p1n = make_int4(0, 0, 0, 0), p2n = p1n;
+  float4 m1n = make_float4(0.f, 0.f, 0.f, 0.f), m2n = m1n;
+  if (j < e) {
+    const u32 q1 = A.perm[j];
+    const u32 q2 = j + PUSH_THREADS < e ? A.perm[j + PUSH_THREADS] : q1;
+    p1n = pin[q1];
+    m1n = min_[q1];
+    p2n = pin[q2];
+    m2n = min_[q2];
+  }
+  for (; j < e; j += 2 * PUSH_THREADS) {
     const long long j2 = j + PUSH_THREADS;
     const bool has2 = j2 < e;
-    const u32 q1 = A.perm[j];
-    const u32 q2 = has2 ? A.perm[j2] : q1;
-    const int4 p1 = pin[q1];
-    const float4 m1 = min_[q1];
-    const int4 p2 = pin[q2];
-    const float4 m2 = min_[q2];
+    const int4 p1 = p1n, p2 = p2n;
+    const float4 m1 = m1n, m2 = m2n;
+    const long long jn = j + 2 * PUSH_THREADS;
+    if (jn < e) {
+      const u32 q1 = A.perm[jn];
+      const u32 q2 = jn + PUSH_THREADS < e ? A.perm[jn + PUSH_THREADS] : q1;
+      p1n = pin[q1];
+      m1n = min_[q1];
+      p2n = pin[q2];
+      m2n = min_[q2];
+    }
     push_one<T>(P, s_f, K, run, tx, ty, tz, p1, m1, j, pout, mout, kout, bad);
     if (has2) push_one<T>(P, s_f, K, run, tx, ty, tz, p2, m2, j2, pout, mout, kout, bad);
   }
@@ -156,7 +173,7 @@ __device__ __forceinline__ void push_tile(const StepArgs& A, const PeakDesc& P, 
 
 // One CTA per push super-tile of TP^3 cells: its (TP/T)^3 bucket tiles are consecutive Morton
 // codes, so its particles are one contiguous range of the sorted order.
-__global__ void __launch_bounds__(PUSH_THREADS) k_push(StepArgs A) {
+__global__ void __launch_bounds__(PUSH_THREADS, 2) k_push(StepArgs A) {
   extern __shared__ float s_f[];
   __shared__ PushCoef s_k;
   const TileRef tr = find_tile(A.ptile_base, A.npeaks);
@@ -196,7 +213,10 @@ __global__ void k_advance(StepArgs A) {
     if (c.has_delta && c.delta_collapse > 0 && c.a_collapse < 0 && c.state != PS_PRIME) {
       const PeakDesc& P = A.peaks[pk];
       const double dmax = (double)A.stats[pk].max_fix / (double)PM_FIX_ONE / P.n_mean - 1.0;
-      if (dmax >= c.delta_collapse) c.a_collapse = c.a;
+      if (dmax >= c.delta_collapse) {
+        c.a_collapse = c.a;
+        if (c.stop_on_collapse && c.state == PS_RUN) c.state = PS_FINALIZE;
+      }
     }
     switch (c.state) {
       case PS_PRIME:
@@ -365,23 +385,33 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
   // A node takes at most one contribution per particle of a chunk.  With CHUNK < 2^11 the high
   // words (each at most 2^20, or -1 for a remainder corner a few units below zero) sum inside
   // int32 and the low words (each < 2^20) inside uint32, so both are exact.
-  constexpr long long CHUNK = 2016;
-  for (long long c0 = 0; c0 < total; c0 += CHUNK) {
-    const long long c1 = min(c0 + CHUNK, total);
-    for (long long k0 = c0 + warp * 32; k0 < c1; k0 += DEP_THREADS) {
-      const long long k = k0 + lane;
-      const bool valid = k < c1;
-      int r = 0;
-      if (valid) {
-        int lo = 0, hi = nr - 1;
-        while (lo < hi) {
-          const int mid = (lo + hi + 1) >> 1;
-          if (s_rp[mid] <= k) lo = mid; else hi = mid - 1;
-        }
-        r = lo;
-      }
-      const int4 ps = valid ? pos[A.perm[s_rb[r] + (k - s_rp[r])]] : make_int4(-1, 0, 0, 0);
-      const int o = s_ro[r];
+  constexpr int CH_IT = 3;  // sweeps of DEP_THREADS particles per chunk: CHUNK = 1536
+  static_assert(CH_IT * DEP_THREADS < 2048, "chunk too large for the split accumulators");
+  const long long nit = (total + DEP_THREADS - 1) / DEP_THREADS;
+  // Flat particle index k over the concatenated ranges; the range index only moves forward.
+  long long k = warp * 32 + lane;
+  int r = 0;
+  bool v_n = k < total;
+  int4 ps_n = make_int4(-1, 0, 0, 0);
+  int o_n = 0;
+  if (v_n) {
+    while (r + 1 < nr && s_rp[r + 1] <= k) ++r;
+    ps_n = pos[A.perm[s_rb[r] + (k - s_rp[r])]];
+    o_n = s_ro[r];
+  }
+  for (long long it = 0; it < nit; ++it) {
+    const int4 ps = ps_n;
+    const bool valid = v_n;
+    const int o = o_n;
+    // Prefetch the next sweep's particle before working on this one.
+    k += DEP_THREADS;
+    v_n = k < total;
+    if (v_n) {
+      while (r + 1 < nr && s_rp[r + 1] <= k) ++r;
+      ps_n = pos[A.perm[s_rb[r] + (k - s_rp[r])]];
+      o_n = s_ro[r];
+    }
+    {
       const int ix = ps.x >> (2 * l2), iy = (ps.x >> l2) & (N - 1), iz = ps.x & (N - 1);
       const int lx = (o & 1) ? -1 : ix - sx * TS;
       const int ly = (o & 2) ? -1 : iy - sy * TS;
@@ -444,17 +474,19 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
 #undef PM_ADD
       }
     }
-    __syncthreads();
+    if ((it + 1) % CH_IT == 0 || it + 1 == nit) {
+      __syncthreads();
 #pragma unroll
-    for (int k = 0; k < NPT; ++k) {
-      const int node = threadIdx.x + k * DEP_THREADS;
-      if (node < TS3) {
-        acc[k] += (u64)((long long)(int)acc_hi[node] * (1LL << 20)) + (u64)acc_lo[node];
-        acc_hi[node] = 0u;
-        acc_lo[node] = 0u;
+      for (int q = 0; q < NPT; ++q) {
+        const int node = threadIdx.x + q * DEP_THREADS;
+        if (node < TS3) {
+          acc[q] += (u64)((long long)(int)acc_hi[node] * (1LL << 20)) + (u64)acc_lo[node];
+          acc_hi[node] = 0u;
+          acc_lo[node] = 0u;
+        }
       }
+      __syncthreads();
     }
-    __syncthreads();
   }
   long long dsum = 0, smax = 0;
   const long long base = ((long long)sx * TS * N + (long long)sy * TS) * N + sz * TS;
@@ -540,8 +572,11 @@ __global__ void __launch_bounds__(PM_THREADS) k_green(StepArgs A) {
   const long long m = ((long long)blockIdx.x - A.mode_base[pk]) * PM_THREADS + threadIdx.x;
   if (m >= P.nmodes) return;
   const int N = P.N, Nh = N / 2 + 1;
-  const int kz = (int)(m % Nh);
-  const long long rest = m / Nh;
+  // m = row * Nh + kz without an integer division: the double quotient is off by at most one.
+  long long rest = (long long)((double)m * P.inv_nh);
+  if (rest * Nh > m) --rest;
+  else if ((rest + 1) * Nh <= m) ++rest;
+  const int kz = (int)(m - rest * Nh);
   const int iy = (int)(rest & (N - 1)), ix = (int)(rest >> P.log2N);
   const float kf = (float)(kTwoPi / P.L), dx = (float)P.dx;
   const float kx = kline(ix, N, kf), ky = kline(iy, N, kf), kzv = kf * (float)kz;
@@ -592,6 +627,7 @@ __global__ void k_reset_peak(StepArgs A, int pk, double a0, int mode, double par
   c.has_delta = 0;
   c.dep = 0;
   c.a_collapse = -1.0;
+  c.stop_on_collapse = 0;
   if (mode == SCHED_RATIO) c.da = a0 * param;
   else if (mode == SCHED_FRAC) c.da = fmin(param * a0, a_end - a0);
   else c.da = 0.0;

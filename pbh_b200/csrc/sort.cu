@@ -150,6 +150,9 @@ __global__ void __launch_bounds__(SORT_THREADS, 3) k_sort_pass(SortPlan P, int p
     // Publish this tile's own count first, so successors can look past it at once.
     st[(size_t)t * RADIX + d] = tag | ((P.tile_first[t] ? 2ull : 1ull) << 32) | r;
   }
+  // Look back over the predecessors of this segment, LB words per round trip: the loads of a
+  // window are independent, so the walk costs one memory latency per LB tiles.
+  constexpr int LB = 8;
 #pragma unroll
   for (int q = 0; q < DPT; ++q) {
     const int d = threadIdx.x + q * SORT_THREADS;
@@ -157,20 +160,29 @@ __global__ void __launch_bounds__(SORT_THREADS, 3) k_sort_pass(SortPlan P, int p
     if (!P.tile_first[t]) {
       int p = t - 1;
       int spins = 0;
-      while (true) {
-        const u64 w = st[(size_t)p * RADIX + d];
-        const u32 flag = (u32)(w >> 32) & 3u;
-        if ((w >> 34) != (u64)ep || flag == 0) {
-          if (++spins > kSpinLimit) {
-            atomicExch(P.err, 1);
-            break;
+      bool done = false;
+      while (!done) {
+        u64 w[LB];
+#pragma unroll
+        for (int i = 0; i < LB; ++i) w[i] = p - i >= S.first_tile ? st[(size_t)(p - i) * RADIX + d] : 0ull;
+#pragma unroll
+        for (int i = 0; i < LB; ++i) {
+          if (done || p - i < S.first_tile) continue;
+          u64 v = w[i];
+          while ((v >> 34) != (u64)ep || ((u32)(v >> 32) & 3u) == 0) {
+            if (++spins > kSpinLimit) {
+              atomicExch(P.err, 1);
+              v = tag | (2ull << 32);  // give up: treat as a zero inclusive prefix
+              break;
+            }
+            __nanosleep(20);
+            v = st[(size_t)(p - i) * RADIX + d];
           }
-          __nanosleep(20);
-          continue;
+          excl += (u32)v;
+          if (((u32)(v >> 32) & 3u) == 2u) done = true;
         }
-        excl += (u32)w;
-        if (flag == 2) break;
-        --p;
+        p -= LB;
+        if (p < S.first_tile) done = true;
       }
       st[(size_t)t * RADIX + d] = tag | (2ull << 32) | (excl + run[q]);
     }
@@ -202,7 +214,9 @@ int sort_plan_create(SortPlan* P, const SortSeg* segs, int nseg, int npass, int 
   P->bits = bits;
   std::vector<int> tseg, tfirst;
   std::vector<long long> tbeg;
+  std::vector<SortSeg> sg(segs, segs + nseg);
   for (int s = 0; s < nseg; ++s) {
+    sg[s].first_tile = (int)tseg.size();
     bool first = true;
     for (long long b = segs[s].begin; b < segs[s].end; b += SORT_TILE) {
       tseg.push_back(s);
@@ -225,7 +239,7 @@ int sort_plan_create(SortPlan* P, const SortSeg* segs, int nseg, int npass, int 
   PM_CHECK(cudaMalloc(&P->status, sizeof(u64) * nt * radix));
   PM_CHECK(cudaMalloc(&P->counters, sizeof(u32) * (SORT_MAX_PASSES + 1)));
   PM_CHECK(cudaMalloc(&P->err, sizeof(int)));
-  PM_CHECK(cudaMemcpy(P->seg, segs, sizeof(SortSeg) * nseg, cudaMemcpyHostToDevice));
+  PM_CHECK(cudaMemcpy(P->seg, sg.data(), sizeof(SortSeg) * nseg, cudaMemcpyHostToDevice));
   if (!tseg.empty()) {
     PM_CHECK(cudaMemcpy(P->tile_seg, tseg.data(), sizeof(int) * nt, cudaMemcpyHostToDevice));
     PM_CHECK(cudaMemcpy(P->tile_begin, tbeg.data(), sizeof(long long) * nt, cudaMemcpyHostToDevice));

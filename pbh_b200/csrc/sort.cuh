@@ -29,7 +29,7 @@ struct SortSeg {
   int lo;                // first key bit sorted in this segment
   int hi;                // one past the last key bit sorted (bits >= hi are ignored)
   int active;            // 0: skip (the segment's buffers are left untouched)
-  int pad;
+  int first_tile;        // global index of the segment's first tile (filled by the plan)
 };
 
 struct SortPlan {

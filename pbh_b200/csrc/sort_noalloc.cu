@@ -60,7 +60,7 @@ __global__ void k_noalloc_setup(unsigned char* base, long long n, int lo, int hi
   u32* hist = (u32*)(base + kOffHist);
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0) {
-    *seg = SortSeg{0, n, lo, hi, 1, 0};
+    *seg = SortSeg{0, n, lo, hi, 1, 0};  // first tile 0
     *(int*)(base + kOffErr) = 0;
   }
   if (i < ntiles) {

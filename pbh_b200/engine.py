@@ -42,7 +42,8 @@ def _ptr(t) -> int:
 
 
 class Engine:
-    def __init__(self, peaks, device: int = 0, bucket_sort: bool = True, graph: bool = True, full_every: int = 16):
+    def __init__(self, peaks, device: int = 0, bucket_sort: bool = True, graph: bool = True, full_every: int = 16,
+                 dynamic: bool = False):
         torch = _lib.require_cuda()
         self._torch = torch
         lib = _lib.load()
@@ -54,8 +55,10 @@ class Engine:
         # bucket_sort: each step sorts only the bucket bits of the cell key (what the deposit and
         # push group by); every `full_every` steps the whole key is sorted.  Results do not
         # depend on the choice: the deposit is order-independent bit for bit.
+        # dynamic: served runs; no graph, and each step's FFTs cover only the slots in use.
         flags = ((_lib.FLAG_BUCKET_SORT | (int(full_every) & 0xFF) << 8) if bucket_sort else 0) | \
-                (_lib.FLAG_GRAPH if graph else 0)
+                (_lib.FLAG_GRAPH if graph else 0) | (_lib.FLAG_DYNAMIC if dynamic else 0)
+        self.npeaks = len(self.cfgs)
         torch.cuda.set_device(self.device)
         check(lib.pm_engine_create(arr, len(self.cfgs), self.device, flags, C.byref(h)), "pm_engine_create")
         self._h = h
@@ -133,6 +136,9 @@ class Engine:
         torch.cuda.current_stream(self.device).synchronize()
         check(self._lib.pm_get_counts(self._h, peak, _ptr(out)), "pm_get_counts")
         return out
+
+    def release(self, peak: int):
+        check(self._lib.pm_release(self._h, peak), "pm_release")
 
     def clock(self, peak: int) -> _lib.ClockInfo:
         c = _lib.ClockInfo()

@@ -14,10 +14,10 @@ KIND_ZETA, KIND_GAUSS = 0, 1
 
 def make_particles(N: int, Np: int, L: float, kind: int, amp: float, axes, *, spline=None, noise=None,
                    tail_rms: float = 0.0, tail_k=(2.0, 10.0), noise_frac: float = 0.0, device: int = 0,
-                   delta_lin: bool = False):
+                   delta_lin: bool = False, noise_seed: int = 0):
     """Returns (x, p, delta_lin or None, noise_rms): x, p are (Np^3, 3) float64 CUDA tensors in
     lattice order.  `noise` (N^3 standard normals) may be a numpy array, a pinned CPU tensor or
-    a CUDA tensor."""
+    a CUDA tensor; without it, a nonzero `noise_seed` draws the normals on the device."""
     torch = _lib.require_cuda()
     dev = f"cuda:{device}"
     n = Np ** 3
@@ -43,6 +43,7 @@ def make_particles(N: int, Np: int, L: float, kind: int, amp: float, axes, *, sp
         prm.noise = nt.data_ptr()
     prm.tail_rms, prm.k1, prm.k2 = float(tail_rms), float(tail_k[0]), float(tail_k[1])
     prm.noise_frac = float(noise_frac)
+    prm.noise_seed = int(noise_seed) if noise is None else 0
     rms = C.c_double(0.0)
     torch.cuda.synchronize(dev)
     with torch.cuda.device(dev):
@@ -51,11 +52,13 @@ def make_particles(N: int, Np: int, L: float, kind: int, amp: float, axes, *, sp
     return x, p, dl, float(rms.value)
 
 
-def recipe_particles(spec, device: int = 0, noise=None):
-    """Particles of a recipe PeakSpec (pbh_b200.recipe); noise defaults to the peak's own
-    generator default_rng(seed).standard_normal((N, N, N))."""
-    if noise is None and spec.noise_frac > 0:
+def recipe_particles(spec, device: int = 0, noise=None, device_noise: bool = False):
+    """Particles of a recipe PeakSpec (pbh_b200.recipe).  Noise defaults to the peak's own
+    generator default_rng(seed).standard_normal((N, N, N)) (numpy's stream, as the reference
+    draws it); device_noise draws it on the GPU from the seed instead."""
+    if noise is None and spec.noise_frac > 0 and not device_noise:
         noise = np.random.default_rng(spec.seed).standard_normal((spec.N,) * 3)
     x, p, _, _ = make_particles(spec.N, spec.N, spec.L, KIND_GAUSS, spec.delta0, spec.R, noise=noise,
-                                noise_frac=spec.noise_frac, device=device)
+                                noise_frac=spec.noise_frac, device=device,
+                                noise_seed=(spec.seed + 1) if device_noise else 0)
     return x, p
