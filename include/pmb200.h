@@ -31,7 +31,7 @@ typedef struct pm_engine pm_engine;
 typedef struct {
   int N;          /* mesh side, power of two, 8..1024 */
   int Np;         /* particles per side (n = Np^3) */
-  int tile;       /* deposit/push tile side, power of two <= N (0: automatic) */
+  int tile;       /* super-tile side for push/deposit/grouping: 4, 8 or 16 (0: min(16, N)) */
   int gradient;   /* 0: spectral -i k (the reference, pm3d.py:111-112); 1: 2-point; 2: 4-point FD */
   double L;       /* box side */
   double smooth;  /* Gaussian force smoothing in cells (pm3d.py:107-108) */
@@ -64,13 +64,15 @@ typedef struct {
   double rho_max_over_mean;  /* max node count / n_mean of the last deposit (pm3d.py:158) */
   double delta_max;          /* max delta of the last deposit (pbhgr/scripts/pm3d_peak.py:30) */
   double mass_defect;        /* sum over nodes of (count - n_mean), exactly 0 unless corrupted */
-  unsigned status;           /* bit 0: non-finite momentum seen; bit 1: sort look-back gave up */
+  unsigned status;           /* bit 0: non-finite momentum or a particle outside its super-tile;
+                              * bit 1: sort look-back gave up; bit 2: regrouping lost count;
+                              * bit 3: a particle id outside the lattice */
 } pm_stats_info;
 
 /* Create an engine holding npeaks independent peaks (a batched ensemble; npeaks = 1 is the
  * plain single run).  Allocates all device memory and cuFFT plans up front; no later call
- * allocates.  flags: bit 0 = sort only the bucket bits of the key each step, with the whole
- * key sorted every (flags >> 8 & 0xFF) steps (16 if 0); bit 1 = replay the step as a CUDA graph;
+ * allocates.  flags: bits 8..15 = a full Morton-key radix sort every that many steps (16 if 0;
+ * the steps between regroup by re-binning); bit 1 = replay the step as a CUDA graph;
  * bit 2 = dynamic mode for served runs: no graph, and each step's FFTs cover only the slots up
  * to the highest one in use in each mesh size (slots are the peaks of one size, in order). */
 int pm_engine_create(const pm_peak_cfg* cfg, int npeaks, int device, int flags, pm_engine** out);
@@ -90,12 +92,12 @@ int pm_set_particles(pm_engine* e, int peak, const double* x, const double* p, d
 int pm_run(pm_engine* e, int nsteps);
 
 /* pm_run without the graph, with a CUDA event between kernel phases on the engine's stream;
- * adds each phase's device time (ms) into phase_ms[8]: push, advance, sort, bucket starts,
- * deposit, R2C, Green, C2R.  Used for per-kernel roofline figures. */
+ * adds each phase's device time (ms) into phase_ms[9]: push, advance, sort (with its
+ * permutation), re-binning, deposit, face fix-up, R2C, Green, C2R.  For per-kernel rooflines. */
 int pm_run_timed(pm_engine* e, int nsteps, double* phase_ms);
 /* The engine's CUDA stream (cudaStream_t), for events and stream ordering by callers. */
 void* pm_engine_stream(pm_engine* e);
-/* info[6]: npeaks, particles, tiles, sort passes per step, mesh classes, device bytes. */
+/* info[6]: npeaks, particles, super-tiles, sort passes, mesh classes, device bytes. */
 int pm_engine_info(const pm_engine* e, long long* info);
 
 /* PM3D.step(a, da) for one peak (pm3d.py:117-129): a KDK step from a to a + da.  Forces at
@@ -187,7 +189,7 @@ int pm_analyse_partials(const double* x, int Np, double L, const double* A, cons
 #define PM_NOALLOC_SCRATCH_BYTES (3670016)
 int pm_sort_u64_noalloc(const unsigned long long* keys, unsigned long long* keys_out, unsigned int* perm_out,
                         long long n, int lo, int hi, void* stream);
-/* Cell keys of split positions; used by tests to check the key layout. */
+/* Sort keys (Morton code of the CIC cell) of split positions, host pointers; for tests. */
 int pm_cell_keys(const int* cells, long long n, int N, int tile, unsigned int* keys_out);
 
 #ifdef __cplusplus

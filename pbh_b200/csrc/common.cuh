@@ -41,22 +41,25 @@ enum ScheduleMode : int {
 };
 
 struct PeakDesc {
-  int N, log2N, T, log2T;  // T: bucket tile side (sort buckets, deposit tiles)
-  int TP, log2TP;          // push super-tile side, a multiple of T (its sub-tiles are contiguous buckets)
-  int nptiles;             // (N/TP)^3
-  int log2NT;       // log2(N/T)
-  int ntiles;       // (N/T)^3
-  int nb;           // buckets = ntiles*8
-  int local_bits;   // 3*log2T
-  int key_bits;     // 3*log2N + 3
-  int gradient;     // 0 spectral (reference), 1 two-point finite difference, 2 four-point
+  int N, log2N;
+  int TS, log2TS;          // super-tile side: the unit of push, deposit and particle grouping
+  int NS;                  // super-tiles per axis (N / TS)
+  int nst;                 // super-tiles (NS^3)
+  int W;                   // re-binning classes per axis: min(NS, 5) (offsets 0, +1, +2, -1, -2)
+  int NC;                  // classes (W^3)
+  int key_bits;            // 3*log2N: Morton key of the CIC cell
+  int st_shift;            // 3*log2TS: key >> st_shift is the super-tile
+  int fc, hc;              // face nodes (any local coordinate 0) and upper-halo nodes per super-tile
+  int gradient;            // 0 spectral (reference), 1 two-point finite difference, 2 four-point
+  int full_every;          // a full Morton-key sort every this many steps (re-binning between)
   double L, dx, smooth, n_mean, m_part;
   long long n_mean_fix;    // round(n_mean * 2^40)
   double inv_fix_nmean;    // 2^-40 / n_mean
   long long p_off, n;      // particle range in the arena
-  long long tile_base;     // first global tile index of this peak
-  long long ptile_base;    // first global push super-tile index of this peak
-  long long bucket_off;    // offset of this peak's bucket-start array (nb + 1 entries)
+  long long st_base;       // first global super-tile index of this peak
+  long long sst_off;       // offset of this peak's super-tile start arrays (nst + 1 entries)
+  long long face_off;      // offset of this peak's face partials (nst * fc)
+  long long halo_off;      // offset of this peak's halo partials (nst * hc)
   long long mode_base;     // first global mode-block of this peak (Green kernel)
   long long nmodes;        // N*N*(N/2+1)
   double inv_nh;           // 1/(N/2+1)
@@ -77,8 +80,10 @@ struct PeakClock {
   int state;       // PeakState
   int nsteps;      // steps taken
   int max_steps;   // SCHED_RATIO length
-  int buf;         // which particle buffer holds the current state
+  int sbuf;        // which super-tile start array describes the current grouping
   int dep;         // 1 when this step re-deposits (set by the advance kernel)
+  int sortstep;    // 1 when this step regroups by a full Morton-key sort (else re-binning)
+  int pad2;
   int has_delta;   // delta/grids hold data
   int stop_on_collapse;  // end the run (finalize) on the step that detects collapse
   double delta_collapse;  // collapse threshold on max delta (<= 0: not tracked)
@@ -123,15 +128,8 @@ __host__ __device__ __forceinline__ u32 pm_morton3(u32 x, u32 y, u32 z) {
   return (pm_spread3(x) << 2) | (pm_spread3(y) << 1) | pm_spread3(z);
 }
 
-// Cell key of a node-lattice cell: [tile Morton | boundary mask (3) | in-tile Morton].
-// Bit b of the mask is set when the cell is the last layer of its tile along axis b
-// (x = bit 0, y = bit 1, z = bit 2); those cells also feed the next tile's nodes.
-__host__ __device__ __forceinline__ u32 pm_cell_key(const PeakDesc& P, int ix, int iy, int iz) {
-  const int m = P.T - 1;
-  u32 lx = ix & m, ly = iy & m, lz = iz & m;
-  u32 tx = ix >> P.log2T, ty = iy >> P.log2T, tz = iz >> P.log2T;
-  u32 mask = (lx == (u32)m ? 1u : 0u) | (ly == (u32)m ? 2u : 0u) | (lz == (u32)m ? 4u : 0u);
-  return (((pm_morton3(tx, ty, tz) << 3) | mask) << P.local_bits) | pm_morton3(lx, ly, lz);
-}
+// Cell key of a node-lattice cell: the Morton code of (ix, iy, iz), z in the lowest bit of each
+// triple.  Codes nest: key >> (3 log2 TS) is the Morton code of the super-tile.
+__host__ __device__ __forceinline__ u32 pm_cell_key(int ix, int iy, int iz) { return pm_morton3(ix, iy, iz); }
 
 __host__ __device__ __forceinline__ double pm_hubble(double a) { return PM_H_I / (a * sqrt(a)); }

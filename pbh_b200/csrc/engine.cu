@@ -55,28 +55,35 @@ struct pm_engine {
   int npeaks = 0;
   std::vector<PeakDesc> peaks;
   std::vector<MeshClass> classes;
-  long long ntot = 0, ntiles = 0, nptiles = 0, nmodeblk = 0, nbuckets = 0;
-  int Tmax = 0;
+  long long ntot = 0, nst = 0, nface = 0, nmodeblk = 0, nsst = 0, nfc = 0, nhc = 0;
+  int TSmax = 0;
   size_t smem_dep = 0, smem_push = 0;
   // device arrays
   PeakDesc* d_peaks = nullptr;
   PeakClock* d_clocks = nullptr;
   PeakStats* d_stats = nullptr;
-  long long* d_tile_base = nullptr;
-  long long* d_ptile_base = nullptr;
+  long long* d_st_base = nullptr;
   long long* d_p_base = nullptr;
   long long* d_mode_base = nullptr;
-  int4* pos[2] = {nullptr, nullptr};
-  float4* mom[2] = {nullptr, nullptr};
+  long long* d_face_base = nullptr;
+  int4* pos = nullptr;   // state, grouped by super-tile
+  float4* mom = nullptr;
+  int4* tpos = nullptr;  // push output / loading area
+  float4* tmom = nullptr;
+  unsigned char* cls = nullptr;
   u32* keys[2] = {nullptr, nullptr};
   u32* vals[2] = {nullptr, nullptr};
-  u32* bstart = nullptr;
-  SortPlan sort{};       // per-step sort: bucket bits only when full_every > 1
-  SortPlan sort_full{};  // whole cell key
-  int full_every = 1;    // full-key sort every this many steps
-  long long replays = 0;
-  int sort_result = 0;  // which (keys, vals) pair holds the sorted output (same for both plans)
-  cudaGraphExec_t graph = nullptr, graph_full = nullptr;
+  u32* sstart[2] = {nullptr, nullptr};
+  u32* counts = nullptr;
+  u32* lpre = nullptr;
+  u32* far_count = nullptr;
+  u32* far_fill = nullptr;
+  u32* totals = nullptr;
+  long long* face = nullptr;
+  long long* halo = nullptr;
+  SortPlan sort{};       // Morton-key sort used by priming and every full_every steps
+  int sort_result = 0;   // which (keys, vals) pair holds the sorted output
+  cudaGraphExec_t graph = nullptr;
   std::vector<char> occupied;  // host view: slots holding a run (dynamic mode FFT extents)
   long long bytes = 0;
 
@@ -86,20 +93,28 @@ struct pm_engine {
     A.clocks = d_clocks;
     A.stats = d_stats;
     A.sortseg = sort.seg;
-    A.sortseg_full = sort_full.seg;
-    A.tile_base = d_tile_base;
-    A.ptile_base = d_ptile_base;
+    A.st_base = d_st_base;
     A.p_base = d_p_base;
     A.mode_base = d_mode_base;
+    A.face_base = d_face_base;
     A.npeaks = npeaks;
-    A.pos[0] = pos[0];
-    A.pos[1] = pos[1];
-    A.mom[0] = mom[0];
-    A.mom[1] = mom[1];
+    A.pos = pos;
+    A.mom = mom;
+    A.tpos = tpos;
+    A.tmom = tmom;
+    A.cls = cls;
     A.keys_push = keys[0];
     A.keys_sorted = keys[sort_result];
     A.perm = vals[sort_result];
-    A.bstart = bstart;
+    A.sstart[0] = sstart[0];
+    A.sstart[1] = sstart[1];
+    A.counts = counts;
+    A.lpre = lpre;
+    A.far_count = far_count;
+    A.far_fill = far_fill;
+    A.totals = totals;
+    A.face = face;
+    A.halo = halo;
     return A;
   }
 
@@ -109,23 +124,6 @@ struct pm_engine {
     cudaError_t e = cudaMalloc((void**)p, b);
     if (e != cudaSuccess) return -(int)e;
     bytes += (long long)b;
-    return 0;
-  }
-
-  int launch_step(bool full) {
-    const StepArgs A = args();
-    SortPlan& plan = full ? sort_full : sort;
-    launch_push(A, nptiles, smem_push, stream);
-    launch_advance(A, stream);
-    int r = sort_run<u32>(&plan, keys[0], vals[0], keys[1], vals[1], true, true, stream);
-    if (r) return r;
-    launch_bucket_starts(A, ntot, stream);
-    launch_deposit(A, nptiles, smem_dep, nullptr, stream);
-    int r2 = fft_r2c();
-    if (r2) return r2;
-    launch_green(A, nmodeblk, stream);
-    if ((r2 = fft_c2r())) return r2;
-    CU(cudaGetLastError());
     return 0;
   }
 
@@ -159,61 +157,62 @@ struct pm_engine {
     return 0;
   }
 
-  // Whether this engine step sorts the full cell key (the in-tile Morton order is refreshed)
-  // or only the bucket bits the deposit and push depend on.
-  bool next_full() const { return full_every <= 1 || (replays % full_every) == 0; }
-
-  // The step with an event between phases, for per-kernel device times (phase_ms accumulates).
-  int launch_step_timed(cudaEvent_t* ev, double* phase_ms) {
+  // One step for every peak.  With ev != nullptr an event is recorded after each phase and the
+  // phase times (push, advance, sort, re-bin, deposit, fix-up, R2C, Green, C2R) are accumulated.
+  int launch_step(cudaEvent_t* ev = nullptr, double* phase_ms = nullptr) {
     const StepArgs A = args();
-    CU(cudaEventRecord(ev[0], stream));
-    launch_push(A, nptiles, smem_push, stream);
-    CU(cudaEventRecord(ev[1], stream));
+    int k = 0;
+    auto mark = [&]() -> cudaError_t { return ev ? cudaEventRecord(ev[k++], stream) : cudaSuccess; };
+    CU(mark());
+    launch_push(A, nst, smem_push, stream);
+    CU(mark());
     launch_advance(A, stream);
-    CU(cudaEventRecord(ev[2], stream));
-    const bool full = next_full();
-    ++replays;
-    int r = sort_run<u32>(full ? &sort_full : &sort, keys[0], vals[0], keys[1], vals[1], true, true, stream);
+    CU(mark());
+    int r = sort_run<u32>(&sort, keys[0], vals[0], keys[1], vals[1], true, true, stream);
     if (r) return r;
-    CU(cudaEventRecord(ev[3], stream));
-    launch_bucket_starts(A, ntot, stream);
-    CU(cudaEventRecord(ev[4], stream));
-    launch_deposit(A, nptiles, smem_dep, nullptr, stream);
-    CU(cudaEventRecord(ev[5], stream));
+    launch_permute(A, ntot, stream);
+    launch_st_starts(A, ntot, stream);
+    CU(mark());
+    launch_bin(A, nst, stream);
+    CU(mark());
+    launch_deposit(A, nst, smem_dep, nullptr, stream);
+    CU(mark());
+    launch_fixup(A, nface, nullptr, stream);
+    CU(mark());
     if ((r = fft_r2c())) return r;
-    CU(cudaEventRecord(ev[6], stream));
+    CU(mark());
     launch_green(A, nmodeblk, stream);
-    CU(cudaEventRecord(ev[7], stream));
+    CU(mark());
     if ((r = fft_c2r())) return r;
-    CU(cudaEventRecord(ev[8], stream));
-    CU(cudaEventSynchronize(ev[8]));
-    for (int k = 0; k < 8; ++k) {
-      float ms = 0.f;
-      CU(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
-      phase_ms[k] += ms;
+    CU(mark());
+    CU(cudaGetLastError());
+    if (ev) {
+      CU(cudaEventSynchronize(ev[k - 1]));
+      for (int q = 0; q + 1 < k; ++q) {
+        float ms = 0.f;
+        CU(cudaEventElapsedTime(&ms, ev[q], ev[q + 1]));
+        phase_ms[q] += ms;
+      }
     }
     return 0;
   }
 
   int step() {
-    const bool full = next_full();
-    ++replays;
     if ((flags & 2) && !(flags & 4)) {
-      cudaGraphExec_t& g = full ? graph_full : graph;
-      if (!g) {
+      if (!graph) {
         cudaGraph_t cg = nullptr;
         CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-        int r = launch_step(full);
+        int r = launch_step();
         cudaError_t ce = cudaStreamEndCapture(stream, &cg);
         if (r) return r;
         CU(ce);
-        CU(cudaGraphInstantiate(&g, cg, 0));
+        CU(cudaGraphInstantiate(&graph, cg, 0));
         cudaGraphDestroy(cg);
       }
-      CU(cudaGraphLaunch(g, stream));
+      CU(cudaGraphLaunch(graph, stream));
       return 0;
     }
-    return launch_step(full);
+    return launch_step();
   }
 
   int read_clock(int pk, PeakClock* c) {
@@ -229,7 +228,6 @@ struct pm_engine {
 
   ~pm_engine() {
     if (graph) cudaGraphExecDestroy(graph);
-    if (graph_full) cudaGraphExecDestroy(graph_full);
     for (auto& c : classes) {
       if (c.plans) {
         cufftDestroy(c.r2c);
@@ -244,21 +242,10 @@ struct pm_engine {
       cudaFree(c.force);
     }
     sort_plan_destroy(&sort);
-    sort_plan_destroy(&sort_full);
-    cudaFree(d_peaks);
-    cudaFree(d_clocks);
-    cudaFree(d_stats);
-    cudaFree(d_tile_base);
-    cudaFree(d_ptile_base);
-    cudaFree(d_p_base);
-    cudaFree(d_mode_base);
-    for (int b = 0; b < 2; ++b) {
-      cudaFree(pos[b]);
-      cudaFree(mom[b]);
-      cudaFree(keys[b]);
-      cudaFree(vals[b]);
-    }
-    cudaFree(bstart);
+    void* bufs[] = {d_peaks, d_clocks, d_stats, d_st_base, d_p_base, d_mode_base, d_face_base, pos, mom, tpos,
+                    tmom, cls, keys[0], keys[1], vals[0], vals[1], sstart[0], sstart[1], counts, lpre, far_count,
+                    far_fill, totals, face, halo};
+    for (void* b : bufs) cudaFree(b);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -270,10 +257,10 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   E->peaks.resize(npeaks);
   E->occupied.assign(npeaks, 0);
   std::map<int, int> class_of;
-  long long poff = 0, tb = 0, mb = 0, bo = 0, ptb = 0;
-  int Tmax = 1, TPmax = 1;
-  int max_bits = 0, min_lo = 64;
-  std::vector<long long> tile_base(npeaks + 1), p_base(npeaks + 1), mode_base(npeaks + 1), ptile_base(npeaks + 1);
+  long long poff = 0, stb = 0, mb = 0, sso = 0, fo = 0, ho = 0;
+  int TSmax = 1, max_bits = 0;
+  const int full_every = std::max(1, (E->flags >> 8) & 0xFF ? (E->flags >> 8) & 0xFF : 16);
+  std::vector<long long> st_base(npeaks + 1), p_base(npeaks + 1), mode_base(npeaks + 1), face_base(npeaks + 1);
   for (int i = 0; i < npeaks; ++i) {
     const pm_peak_cfg& c = cfg[i];
     const int l2 = ilog2(c.N);
@@ -281,27 +268,25 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
     const long long npart = c.n > 0 ? c.n : (long long)c.Np * c.Np * c.Np;
     if (c.Np < 1 || npart >= (1LL << 31)) return -2002;
     if (!(c.L > 0)) return -2003;
-    // Bucket tiles of 8^3 (4^3 below 32^3); push super-tiles of 16^3 (the mesh when smaller).
-    int T = c.tile > 0 ? c.tile : (c.N >= 32 ? 8 : std::max(2, c.N / 4));
-    if (ilog2(T) < 1 || T > 8 || T > c.N) return -2004;
-    // The push/deposit super-tile is 2T per side (8 bucket tiles), or T when the mesh is one tile.
-    const int TP = std::min(2 * T, c.N);
+    // Super-tile side: 16^3 cells (the whole mesh below that); 4 and 8 are also built.
+    const int TS = c.tile > 0 ? c.tile : std::min(16, c.N);
+    if (ilog2(TS) < 2 || TS > 16 || TS > c.N) return -2004;
     PeakDesc& P = E->peaks[i];
     P = PeakDesc{};
     P.N = c.N;
     P.log2N = l2;
-    P.T = T;
-    P.log2T = ilog2(T);
-    P.log2NT = l2 - P.log2T;
-    P.ntiles = 1 << (3 * P.log2NT);
-    P.TP = TP;
-    P.log2TP = ilog2(TP);
-    P.nptiles = 1 << (3 * (l2 - P.log2TP));
-    P.ptile_base = ptb;
-    P.nb = P.ntiles * 8;
-    P.local_bits = 3 * P.log2T;
-    P.key_bits = 3 * l2 + 3;
+    P.TS = TS;
+    P.log2TS = ilog2(TS);
+    P.NS = c.N / TS;
+    P.nst = P.NS * P.NS * P.NS;
+    P.W = std::min(P.NS, 5);
+    P.NC = P.W * P.W * P.W;
+    P.key_bits = 3 * l2;
+    P.st_shift = 3 * P.log2TS;
+    P.fc = TS * TS * TS - (TS - 1) * (TS - 1) * (TS - 1);
+    P.hc = (TS + 1) * (TS + 1) * (TS + 1) - TS * TS * TS;
     P.gradient = c.gradient;
+    P.full_every = full_every;
     P.L = c.L;
     P.dx = c.L / c.N;
     P.smooth = c.smooth;
@@ -312,24 +297,25 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
     P.inv_fix_nmean = 1.0 / ((double)PM_FIX_ONE * P.n_mean);
     P.p_off = poff;
     P.n = npart;
-    P.tile_base = tb;
-    P.bucket_off = bo;
+    P.st_base = stb;
+    P.sst_off = sso;
+    P.face_off = fo;
+    P.halo_off = ho;
     P.nmodes = (long long)c.N * c.N * (c.N / 2 + 1);
     P.inv_nh = 1.0 / (double)(c.N / 2 + 1);
     P.mode_base = mb;
-    tile_base[i] = tb;
-    ptile_base[i] = ptb;
-    ptb += P.nptiles;
+    st_base[i] = stb;
     p_base[i] = poff;
     mode_base[i] = mb;
+    face_base[i] = fo;
     poff += P.n;
-    tb += P.ntiles;
-    bo += P.nb + 1;
+    stb += P.nst;
+    sso += P.nst + 1;
+    fo += (long long)P.nst * P.fc;
+    ho += (long long)P.nst * P.hc;
     mb += (P.nmodes + PM_THREADS - 1) / PM_THREADS;
-    Tmax = std::max(Tmax, T);
-    TPmax = std::max(TPmax, TP);
+    TSmax = std::max(TSmax, TS);
     max_bits = std::max(max_bits, P.key_bits);
-    min_lo = std::min(min_lo, P.local_bits);
     if (!class_of.count(c.N)) {
       class_of[c.N] = (int)E->classes.size();
       E->classes.push_back(MeshClass{});
@@ -337,20 +323,22 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
     }
     E->classes[class_of[c.N]].peaks.push_back(i);
   }
-  tile_base[npeaks] = tb;
-  ptile_base[npeaks] = ptb;
-  E->nptiles = ptb;
+  st_base[npeaks] = stb;
   p_base[npeaks] = poff;
   mode_base[npeaks] = mb;
+  face_base[npeaks] = fo;
   if (poff >= (1LL << 32)) return -2005;
   E->ntot = poff;
-  E->ntiles = tb;
+  E->nst = stb;
+  E->nface = fo;
   E->nmodeblk = mb;
-  E->nbuckets = bo;
-  E->Tmax = Tmax;
+  E->nsst = sso;
+  E->nfc = fo;
+  E->nhc = ho;
+  E->TSmax = TSmax;
   if (int rk = pm_kernels_init()) return rk;
-  E->smem_dep = pm_deposit_smem(TPmax);
-  E->smem_push = pm_push_smem(TPmax);
+  E->smem_dep = pm_deposit_smem(TSmax);
+  E->smem_push = pm_push_smem(TSmax);
 
   // Mesh arenas, one per mesh size, peaks of a class contiguous for batched cuFFT plans.
   for (auto& mc : E->classes) {
@@ -412,22 +400,32 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   if ((r = E->alloc(&E->d_peaks, npeaks))) return r;
   if ((r = E->alloc(&E->d_clocks, npeaks))) return r;
   if ((r = E->alloc(&E->d_stats, npeaks))) return r;
-  if ((r = E->alloc(&E->d_tile_base, npeaks + 1))) return r;
-  if ((r = E->alloc(&E->d_ptile_base, npeaks + 1))) return r;
+  if ((r = E->alloc(&E->d_st_base, npeaks + 1))) return r;
   if ((r = E->alloc(&E->d_p_base, npeaks + 1))) return r;
   if ((r = E->alloc(&E->d_mode_base, npeaks + 1))) return r;
+  if ((r = E->alloc(&E->d_face_base, npeaks + 1))) return r;
+  if ((r = E->alloc(&E->pos, E->ntot))) return r;
+  if ((r = E->alloc(&E->mom, E->ntot))) return r;
+  if ((r = E->alloc(&E->tpos, E->ntot))) return r;
+  if ((r = E->alloc(&E->tmom, E->ntot))) return r;
+  if ((r = E->alloc(&E->cls, E->ntot))) return r;
   for (int b = 0; b < 2; ++b) {
-    if ((r = E->alloc(&E->pos[b], E->ntot))) return r;
-    if ((r = E->alloc(&E->mom[b], E->ntot))) return r;
     if ((r = E->alloc(&E->keys[b], E->ntot))) return r;
     if ((r = E->alloc(&E->vals[b], E->ntot))) return r;
+    if ((r = E->alloc(&E->sstart[b], E->nsst))) return r;
   }
-  if ((r = E->alloc(&E->bstart, E->nbuckets))) return r;
+  if ((r = E->alloc(&E->counts, E->nst * BIN_CLASSES))) return r;
+  if ((r = E->alloc(&E->lpre, E->nst * BIN_CLASSES))) return r;
+  if ((r = E->alloc(&E->far_count, E->nst))) return r;
+  if ((r = E->alloc(&E->far_fill, E->nst))) return r;
+  if ((r = E->alloc(&E->totals, E->nst))) return r;
+  if ((r = E->alloc(&E->face, E->nfc))) return r;
+  if ((r = E->alloc(&E->halo, E->nhc))) return r;
   CU(cudaMemcpy(E->d_peaks, E->peaks.data(), sizeof(PeakDesc) * npeaks, cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(E->d_tile_base, tile_base.data(), sizeof(long long) * (npeaks + 1), cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(E->d_ptile_base, ptile_base.data(), sizeof(long long) * (npeaks + 1), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(E->d_st_base, st_base.data(), sizeof(long long) * (npeaks + 1), cudaMemcpyHostToDevice));
   CU(cudaMemcpy(E->d_p_base, p_base.data(), sizeof(long long) * (npeaks + 1), cudaMemcpyHostToDevice));
   CU(cudaMemcpy(E->d_mode_base, mode_base.data(), sizeof(long long) * (npeaks + 1), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(E->d_face_base, face_base.data(), sizeof(long long) * (npeaks + 1), cudaMemcpyHostToDevice));
   std::vector<PeakClock> clocks(npeaks);
   for (auto& c : clocks) {
     c = PeakClock{};
@@ -436,30 +434,25 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   }
   CU(cudaMemcpy(E->d_clocks, clocks.data(), sizeof(PeakClock) * npeaks, cudaMemcpyHostToDevice));
   CU(cudaMemset(E->d_stats, 0, sizeof(PeakStats) * npeaks));
-  CU(cudaMemset(E->bstart, 0, sizeof(u32) * E->nbuckets));
+  CU(cudaMemset(E->pos, 0, sizeof(int4) * E->ntot));
+  CU(cudaMemset(E->mom, 0, sizeof(float4) * E->ntot));
+  CU(cudaMemset(E->tpos, 0, sizeof(int4) * E->ntot));
+  CU(cudaMemset(E->tmom, 0, sizeof(float4) * E->ntot));
+  CU(cudaMemset(E->far_count, 0, sizeof(u32) * E->nst));
+  CU(cudaMemset(E->far_fill, 0, sizeof(u32) * E->nst));
+  for (int b = 0; b < 2; ++b) CU(cudaMemset(E->sstart[b], 0, sizeof(u32) * E->nsst));
 
-  // Sort plans: one segment per peak.  The full plan sorts the whole cell key [0, key_bits);
-  // the per-step plan, when flag bit 0 asks for it, only the bucket bits [local_bits, key_bits)
-  // that the deposit and push group by, keeping the previous in-bucket order (stable).  Both
-  // plans use pass counts of the same parity so the result always lands in the same buffers.
-  E->full_every = (E->flags & 1) ? std::max(1, (E->flags >> 8) & 0xFF) : 1;
-  if ((E->flags & 1) && ((E->flags >> 8) & 0xFF) == 0) E->full_every = 16;
-  std::vector<SortSeg> segs(npeaks), fsegs(npeaks);
-  int span_b = 0, span_f = 0;
+  // Sort plan: one segment per peak over the whole Morton key (sorted at priming and every
+  // full_every steps; the segment of a peak is active only on those steps).
+  std::vector<SortSeg> segs(npeaks);
   for (int i = 0; i < npeaks; ++i) {
     const PeakDesc& P = E->peaks[i];
-    fsegs[i] = SortSeg{P.p_off, P.p_off + P.n, 0, P.key_bits, 0, 0};
-    segs[i] = SortSeg{P.p_off, P.p_off + P.n, (E->flags & 1) ? P.local_bits : 0, P.key_bits, 0, 0};
-    span_b = std::max(span_b, P.key_bits - segs[i].lo);
-    span_f = std::max(span_f, P.key_bits);
+    segs[i] = SortSeg{P.p_off, P.p_off + P.n, 0, P.key_bits, 0, 0};
   }
-  const int np_b = (span_b + SORT_MAX_BITS - 1) / SORT_MAX_BITS;
-  int np_f = (span_f + SORT_MAX_BITS - 1) / SORT_MAX_BITS;
-  if ((np_f & 1) != (np_b & 1)) ++np_f;
-  if ((r = sort_plan_create(&E->sort, segs.data(), npeaks, np_b, span_b))) return r;
-  if ((r = sort_plan_create(&E->sort_full, fsegs.data(), npeaks, np_f, span_f))) return r;
-  E->bytes += (long long)E->sort.ntiles * 8 * ((1LL << E->sort.bits) + (1LL << E->sort_full.bits));
-  E->sort_result = np_b & 1;
+  const int np = (max_bits + SORT_MAX_BITS - 1) / SORT_MAX_BITS;
+  if ((r = sort_plan_create(&E->sort, segs.data(), npeaks, np, max_bits))) return r;
+  E->bytes += (long long)E->sort.ntiles * 8 * (1LL << E->sort.bits);
+  E->sort_result = np & 1;
   CU(cudaDeviceSynchronize());
   return 0;
 }
@@ -533,11 +526,11 @@ int pm_run(pm_engine* e, int nsteps) {
 int pm_run_timed(pm_engine* e, int nsteps, double* phase_ms) {
   if (!e || nsteps < 0 || !phase_ms) return -2000;
   CU(cudaSetDevice(e->device));
-  cudaEvent_t ev[9];
-  for (int k = 0; k < 9; ++k) CU(cudaEventCreate(&ev[k]));
+  cudaEvent_t ev[10];
+  for (int k = 0; k < 10; ++k) CU(cudaEventCreate(&ev[k]));
   int r = 0;
-  for (int s = 0; s < nsteps && !r; ++s) r = e->launch_step_timed(ev, phase_ms);
-  for (int k = 0; k < 9; ++k) cudaEventDestroy(ev[k]);
+  for (int s = 0; s < nsteps && !r; ++s) r = e->launch_step(ev, phase_ms);
+  for (int k = 0; k < 10; ++k) cudaEventDestroy(ev[k]);
   return r;
 }
 
@@ -547,7 +540,7 @@ int pm_engine_info(const pm_engine* e, long long* info) {
   if (!e || !info) return -2000;
   info[0] = e->npeaks;
   info[1] = e->ntot;
-  info[2] = e->ntiles;
+  info[2] = e->nst;
   info[3] = e->sort.npass;
   info[4] = (long long)e->classes.size();
   info[5] = e->bytes;
@@ -558,11 +551,9 @@ int pm_get_stats_all(pm_engine* e, pm_stats_info* out) {
   if (!e || !out) return -2000;
   CU(cudaSetDevice(e->device));
   std::vector<PeakStats> s(e->npeaks);
-  int err = 0, err2 = 0;
+  int err = 0;
   CU(cudaMemcpyAsync(s.data(), e->d_stats, sizeof(PeakStats) * e->npeaks, cudaMemcpyDeviceToHost, e->stream));
   CU(cudaMemcpyAsync(&err, e->sort.err, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
-  CU(cudaMemcpyAsync(&err2, e->sort_full.err, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
-  err |= err2;
   CU(cudaStreamSynchronize(e->stream));
   int flagged = 0;
   for (int i = 0; i < e->npeaks; ++i) {
@@ -610,6 +601,9 @@ int pm_step_explicit(pm_engine* e, int peak, double a, double da) {
     if ((r = e->write_clock(peak, c)) || (r = e->step()) || (r = e->read_clock(peak, &c))) return r;
   }
   if (c.state == PS_IDLE || c.state == PS_PRIME || (c.state == PS_HOLD && !c.has_delta)) {
+    // A loaded peak (PRIME) has its particles in the loading area already; any other state
+    // holds them in the grouped state, from where they are reloaded for the priming sort.
+    if (c.state != PS_PRIME) launch_reload(e->args(), e->peaks[peak], e->stream);
     c.a = a;
     c.a_grid = a;
     c.mode = SCHED_EXPLICIT;
@@ -671,8 +665,9 @@ int pm_get_counts(pm_engine* e, int peak, double* counts) {
   st.max_fix = 0;
   st.mass_defect = 0;
   CU(cudaMemcpy(e->d_stats + peak, &st, sizeof(PeakStats), cudaMemcpyHostToDevice));
-  // Same kernel with the extra float64 output; delta is rewritten with identical values.
-  launch_deposit(e->args(), e->nptiles, e->smem_dep, counts, e->stream);
+  // Same kernels with the extra float64 output; delta is rewritten with identical values.
+  launch_deposit(e->args(), e->nst, e->smem_dep, counts, e->stream);
+  launch_fixup(e->args(), e->nface, counts, e->stream);
   CU(cudaGetLastError());
   CU(cudaStreamSynchronize(e->stream));
   CU(cudaMemcpy(e->d_clocks, all.data(), sizeof(PeakClock) * e->npeaks, cudaMemcpyHostToDevice));
@@ -728,11 +723,9 @@ int pm_get_stats(pm_engine* e, int peak, pm_stats_info* out) {
   if (!e || peak < 0 || peak >= e->npeaks || !out) return -2000;
   CU(cudaSetDevice(e->device));
   PeakStats s;
-  int err = 0, err2 = 0;
+  int err = 0;
   CU(cudaMemcpyAsync(&s, e->d_stats + peak, sizeof(PeakStats), cudaMemcpyDeviceToHost, e->stream));
   CU(cudaMemcpyAsync(&err, e->sort.err, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
-  CU(cudaMemcpyAsync(&err2, e->sort_full.err, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
-  err |= err2;
   CU(cudaStreamSynchronize(e->stream));
   const PeakDesc& P = e->peaks[peak];
   out->rho_max_over_mean = (double)s.max_fix / (double)PM_FIX_ONE / P.n_mean;
@@ -791,20 +784,14 @@ int pm_sort_u64(const unsigned long long* keys, unsigned long long* keys_out, un
 }
 
 int pm_cell_keys(const int* cells, long long n, int N, int tile, unsigned int* keys_out) {
-  // Host-side helper (plain host pointers): the key layout used by the sort.
+  // Host-side helper (plain host pointers): the key the sort orders particles by.  `tile` is
+  // accepted for the layout's super-tile but does not change the key (Morton codes nest).
   if (!cells || !keys_out || n < 0) return -2000;
   const int l2 = ilog2(N);
-  const int T = tile > 0 ? tile : std::min(16, N);
-  if (l2 < 1 || ilog2(T) < 1 || T > N) return -2001;
-  PeakDesc P{};
-  P.N = N;
-  P.log2N = l2;
-  P.T = T;
-  P.log2T = ilog2(T);
-  P.local_bits = 3 * P.log2T;
+  if (l2 < 1 || tile < 0 || tile > N) return -2001;
   for (long long i = 0; i < n; ++i) {
     const int c = cells[i];
-    keys_out[i] = pm_cell_key(P, c >> (2 * l2), (c >> l2) & (N - 1), c & (N - 1));
+    keys_out[i] = pm_cell_key(c >> (2 * l2), (c >> l2) & (N - 1), c & (N - 1));
   }
   return 0;
 }

@@ -1,5 +1,6 @@
-// Step kernels: push (CIC interp + kicks + drift), clock advance, bucket starts,
-// deterministic tiled CIC deposit, Green's function + gradient, and particle I/O.
+// Step kernels of the pm3d engine: push (CIC gather + kicks + drift, re-binning class),
+// clock advance, regrouping (re-binning scatter, or radix-sort permutation), halo-exchange CIC
+// deposit with its face fix-up, Green's function + gradient, and particle I/O.
 #include "pm_kernels.cuh"
 
 namespace {
@@ -11,6 +12,11 @@ __device__ __forceinline__ u32 lanemask_le() {
   asm("mov.u32 %0, %%lanemask_le;" : "=r"(m));
   return m;
 }
+__device__ __forceinline__ u32 lanemask_lt() {
+  u32 m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
 
 __device__ __forceinline__ u64 shfl_up_u64(u64 v, int d) {
   const u32 lo = __shfl_up_sync(0xffffffffu, (u32)v, d);
@@ -18,12 +24,11 @@ __device__ __forceinline__ u64 shfl_up_u64(u64 v, int d) {
   return ((u64)hi << 32) | lo;
 }
 
-// Buffer selection without indexing the kernel-parameter arrays dynamically (which would
-// copy the whole parameter struct to local memory).
-__device__ __forceinline__ int4* posb(const StepArgs& A, int b) { return b ? A.pos[1] : A.pos[0]; }
-__device__ __forceinline__ float4* momb(const StepArgs& A, int b) { return b ? A.mom[1] : A.mom[0]; }
+// Super-tile start arrays without indexing the kernel-parameter array dynamically (which would
+// copy the parameter struct to local memory).
+__device__ __forceinline__ u32* sst(const StepArgs& A, int b) { return b ? A.sstart[1] : A.sstart[0]; }
 
-// Locate the peak and tile of this CTA (uniform across the block).
+// Locate the peak and the peak-local index of this CTA (uniform across the block).
 struct TileRef {
   int pk;
   long long t;
@@ -39,38 +44,48 @@ __device__ __forceinline__ TileRef find_tile(const long long* base, int npeaks) 
   return r;
 }
 
+// Re-binning classes: per axis, the offset u = (destination - source) mod NS of the super-tile a
+// particle moved to is one of 0, +1, +2, -1, -2 (NS - 1, NS - 2), or any offset when NS <= 5.
+__device__ __forceinline__ int bin_digit(int u, int NS) {
+  if (NS <= 5 || u <= 2) return u;
+  if (u >= NS - 2) return 2 + (NS - u);
+  return -1;
+}
+__device__ __forceinline__ int bin_offset(int d, int NS) { return (NS <= 5 || d <= 2) ? d : NS - (d - 2); }
+
 // ------------------------------------------------------------------------------------------
 // Push: CIC gather of the three force grids (pm3d.py:91-99) fused with the pending closing
 // kick of the previous step, the opening kick and the drift of this one (pm3d.py:122-127).
-// One CTA per tile: the (T+1)^3 node patch of all three grids is staged in shared memory,
-// then every particle whose CIC cell lies in the tile reads its 8 corners from there.
-// Output is written in sorted order into the other state buffer, with the new cell key.
+// One CTA per super-tile: the (TS+1)^3 node patch of all three grids is staged in shared
+// memory, and the super-tile's particles -- one contiguous range -- read their 8 corners from
+// there.  Each result is written to the same position of the temporary state with the class of
+// its new super-tile; per-class counts feed the re-binning.
 struct PushCoef {
   float kA, kB, D, gscale;
+  int run, sortnext;
 };
 
 template <int T>
-__device__ __forceinline__ void push_one(const PeakDesc& P, const float* __restrict__ s_f, const PushCoef& K,
-                                         bool run, int tx, int ty, int tz, int4 ps, float4 m, long long j,
-                                         int4* __restrict__ pout, float4* __restrict__ mout, u32* __restrict__ kout,
-                                         bool& bad) {
+__device__ __forceinline__ void push_one(const StepArgs& A, const PeakDesc& P, const float* __restrict__ s_f,
+                                         const PushCoef& K, int sx, int sy, int sz, int4 ps, float4 m, long long j,
+                                         u32* s_cnt, bool& bad) {
   constexpr int T1 = T + 1, T13 = T1 * T1 * T1;
   const int N = P.N, l2 = P.log2N;
   const int ix = ps.x >> (2 * l2), iy = (ps.x >> l2) & (N - 1), iz = ps.x & (N - 1);
-  const int lx = ix - tx * T, ly = iy - ty * T, lz = iz - tz * T;
+  const int lx = ix - sx * T, ly = iy - sy * T, lz = iz - sz * T;
   if ((unsigned)lx >= (unsigned)T || (unsigned)ly >= (unsigned)T || (unsigned)lz >= (unsigned)T) {
-    bad = true;  // state and sort disagree: flag it, never index outside the patch
+    bad = true;  // grouping and state disagree: flag it, never index outside the patch
     return;
   }
   float fx = __int_as_float(ps.y), fy = __int_as_float(ps.z), fz = __int_as_float(ps.w);
   const float gx = 1.0f - fx, gy = 1.0f - fy, gz = 1.0f - fz;
   const int o = (lx * T1 + ly) * T1 + lz;
   float ax = 0.f, ay = 0.f, az = 0.f;
-#define PM_CORNER(w, d)                       \
-  {                                           \
-    const float w_ = (w);                     \
-    ax = fmaf(w_, s_f[o + (d)], ax);          \
-    ay = fmaf(w_, s_f[T13 + o + (d)], ay);    \
+#define PM_CORNER(w, d)                        \
+  {                                            \
+    const float w_ = (w);                      \
+    ax = fmaf(w_, s_f[o + (d)], ax);           \
+    ay = fmaf(w_, s_f[T13 + o + (d)], ay);     \
     az = fmaf(w_, s_f[2 * T13 + o + (d)], az); \
   }
   const float w00 = gx * gy, w01 = gx * fy, w10 = fx * gy, w11 = fx * fy;
@@ -88,21 +103,21 @@ __device__ __forceinline__ void push_one(const PeakDesc& P, const float* __restr
   az *= K.gscale;
   float px = m.x + K.kA * ax, py = m.y + K.kA * ay, pz = m.z + K.kA * az;
   int nx = ix, ny = iy, nz = iz;
-  if (run) {
+  if (K.run) {
     px += K.kB * ax;
     py += K.kB * ay;
     pz += K.kB * az;
-#define PM_DRIFT(f, p, i)                 \
-  {                                       \
-    float fn = f + K.D * p;               \
-    float c = floorf(fn);                 \
-    fn -= c;                              \
-    if (fn >= 1.0f) {                     \
-      fn -= 1.0f;                         \
-      c += 1.0f;                          \
-    }                                     \
-    f = fn;                               \
-    i = (i + (int)c) & (N - 1);           \
+#define PM_DRIFT(f, p, i)       \
+  {                             \
+    float fn = f + K.D * p;     \
+    float c = floorf(fn);       \
+    fn -= c;                    \
+    if (fn >= 1.0f) {           \
+      fn -= 1.0f;               \
+      c += 1.0f;                \
+    }                           \
+    f = fn;                     \
+    i = (i + (int)c) & (N - 1); \
   }
     PM_DRIFT(fx, px, nx)
     PM_DRIFT(fy, py, ny)
@@ -110,46 +125,58 @@ __device__ __forceinline__ void push_one(const PeakDesc& P, const float* __restr
 #undef PM_DRIFT
   }
   bad |= !(isfinite(px) && isfinite(py) && isfinite(pz));
-  pout[j] = make_int4((nx << (2 * l2)) | (ny << l2) | nz, __float_as_int(fx), __float_as_int(fy), __float_as_int(fz));
-  mout[j] = make_float4(px, py, pz, m.w);
-  kout[j] = pm_cell_key(P, nx, ny, nz);
+  A.tpos[j] = make_int4((nx << (2 * l2)) | (ny << l2) | nz, __float_as_int(fx), __float_as_int(fy), __float_as_int(fz));
+  A.tmom[j] = make_float4(px, py, pz, m.w);
+  if (K.sortnext) A.keys_push[j] = pm_cell_key(nx, ny, nz);
+  // Class of the destination super-tile.
+  const int NS = P.NS;
+  const int tx = nx >> P.log2TS, ty = ny >> P.log2TS, tz = nz >> P.log2TS;
+  const int dxc = bin_digit((tx - sx) & (NS - 1), NS), dyc = bin_digit((ty - sy) & (NS - 1), NS),
+            dzc = bin_digit((tz - sz) & (NS - 1), NS);
+  int c = BIN_FAR;
+  if (dxc >= 0 && dyc >= 0 && dzc >= 0) c = (dxc * P.W + dyc) * P.W + dzc;
+  A.cls[j] = (unsigned char)c;
+  const u32 am = __activemask();
+  const u32 peers = __match_any_sync(am, c);
+  if (c == BIN_FAR) {
+    // Far movers of one warp can be bound for different super-tiles: count each one at its own.
+    atomicAdd(&A.far_count[P.st_base + pm_morton3(tx, ty, tz)], 1u);
+  } else if ((peers & lanemask_lt()) == 0) {
+    atomicAdd(&s_cnt[c], (u32)__popc(peers));
+  }
 }
 
 template <int T>
-__device__ __forceinline__ void push_tile(const StepArgs& A, const PeakDesc& P, const PeakClock& C, int pk, u32 tc,
-                                          long long b, long long e, float* s_f, const PushCoef& K) {
+__device__ __forceinline__ void push_super(const StepArgs& A, const PeakDesc& P, const PeakClock& C, int pk, u32 st,
+                                           float* s_f, u32* s_cnt, const PushCoef& K) {
   constexpr int T1 = T + 1, T12 = T1 * T1, T13 = T1 * T1 * T1;
   const int N = P.N;
-  const int tx = pm_compact3(tc >> 2), ty = pm_compact3(tc >> 1), tz = pm_compact3(tc);
+  const int sx = pm_compact3(st >> 2), sy = pm_compact3(st >> 1), sz = pm_compact3(st);
   const long long N3 = (long long)N * N * N;
-  for (int i = threadIdx.x; i < 3 * T13; i += PUSH_THREADS) {
-    const int comp = i / T13, r = i - comp * T13;
-    const int lx = r / T12, r2 = r - lx * T12;
-    const int ly = r2 / T1, lz = r2 - ly * T1;
-    const int gx = (tx * T + lx) & (N - 1), gy = (ty * T + ly) & (N - 1), gz = (tz * T + lz) & (N - 1);
-    s_f[i] = __ldg(P.force + comp * N3 + ((long long)gx * N + gy) * N + gz);
+  const u32* ss = sst(A, C.sbuf) + P.sst_off;
+  const long long b = ss[st], e = ss[st + 1];
+  if (b < e) {
+    for (int i = threadIdx.x; i < 3 * T13; i += PUSH_THREADS) {
+      const int comp = i / T13, r = i - comp * T13;
+      const int lx = r / T12, r2 = r - lx * T12;
+      const int ly = r2 / T1, lz = r2 - ly * T1;
+      const int gx = (sx * T + lx) & (N - 1), gy = (sy * T + ly) & (N - 1), gz = (sz * T + lz) & (N - 1);
+      s_f[i] = __ldg(P.force + comp * N3 + ((long long)gx * N + gy) * N + gz);
+    }
   }
   __syncthreads();
-  const bool run = C.state == PS_RUN;
-  const int buf = C.buf;
-  const int4* __restrict__ pin = posb(A, buf);
-  const float4* __restrict__ min_ = momb(A, buf);
-  int4* __restrict__ pout = posb(A, buf ^ 1);
-  float4* __restrict__ mout = momb(A, buf ^ 1);
-  u32* __restrict__ kout = A.keys_push;
   bool bad = false;
-  // Two particles per thread per sweep, and the next sweep's pair is fetched before this one is
-  // computed, so four gathers are in flight while the arithmetic runs.
+  // Two particles per thread per sweep, the next sweep's pair fetched before this one is computed.
   long long j = b + threadIdx.x;
   int4 p1n = make_int4(0, 0, 0, 0), p2n = p1n;
   float4 m1n = make_float4(0.f, 0.f, 0.f, 0.f), m2n = m1n;
   if (j < e) {
-    const u32 q1 = A.perm[j];
-    const u32 q2 = j + PUSH_THREADS < e ? A.perm[j + PUSH_THREADS] : q1;
-    p1n = pin[q1];
-    m1n = min_[q1];
-    p2n = pin[q2];
-    m2n = min_[q2];
+    p1n = A.pos[j];
+    m1n = A.mom[j];
+    if (j + PUSH_THREADS < e) {
+      p2n = A.pos[j + PUSH_THREADS];
+      m2n = A.mom[j + PUSH_THREADS];
+    }
   }
   for (; j < e; j += 2 * PUSH_THREADS) {
     const long long j2 = j + PUSH_THREADS;
@@ -158,33 +185,29 @@ __device__ __forceinline__ void push_tile(const StepArgs& A, const PeakDesc& P, 
     const float4 m1 = m1n, m2 = m2n;
     const long long jn = j + 2 * PUSH_THREADS;
     if (jn < e) {
-      const u32 q1 = A.perm[jn];
-      const u32 q2 = jn + PUSH_THREADS < e ? A.perm[jn + PUSH_THREADS] : q1;
-      p1n = pin[q1];
-      m1n = min_[q1];
-      p2n = pin[q2];
-      m2n = min_[q2];
+      p1n = A.pos[jn];
+      m1n = A.mom[jn];
+      if (jn + PUSH_THREADS < e) {
+        p2n = A.pos[jn + PUSH_THREADS];
+        m2n = A.mom[jn + PUSH_THREADS];
+      }
     }
-    push_one<T>(P, s_f, K, run, tx, ty, tz, p1, m1, j, pout, mout, kout, bad);
-    if (has2) push_one<T>(P, s_f, K, run, tx, ty, tz, p2, m2, j2, pout, mout, kout, bad);
+    push_one<T>(A, P, s_f, K, sx, sy, sz, p1, m1, j, s_cnt, bad);
+    if (has2) push_one<T>(A, P, s_f, K, sx, sy, sz, p2, m2, j2, s_cnt, bad);
   }
   if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&A.stats[pk].status, 1u);
+  for (int c = threadIdx.x; c < P.NC; c += PUSH_THREADS) A.counts[(P.st_base + st) * BIN_CLASSES + c] = s_cnt[c];
 }
 
-// One CTA per push super-tile of TP^3 cells: its (TP/T)^3 bucket tiles are consecutive Morton
-// codes, so its particles are one contiguous range of the sorted order.
 __global__ void __launch_bounds__(PUSH_THREADS, 2) k_push(StepArgs A) {
   extern __shared__ float s_f[];
   __shared__ PushCoef s_k;
-  const TileRef tr = find_tile(A.ptile_base, A.npeaks);
+  __shared__ u32 s_cnt[BIN_CLASSES];
+  const TileRef tr = find_tile(A.st_base, A.npeaks);
   const PeakClock C = A.clocks[tr.pk];
   if (C.state != PS_RUN && C.state != PS_FINALIZE) return;
   const PeakDesc& P = A.peaks[tr.pk];
-  const u32 st = (u32)tr.t;
-  const u32 R = 1u << (3 * (P.log2TP - P.log2T));
-  const u32* bs = A.bstart + P.bucket_off;
-  const long long b = bs[st * R * 8], e = bs[(st + 1) * R * 8];
-  if (b == e) return;
+  if (threadIdx.x < BIN_CLASSES) s_cnt[threadIdx.x] = 0u;
   if (threadIdx.x == 0) {
     const double a = C.a, da = C.da;
     const bool run = C.state == PS_RUN;
@@ -193,25 +216,28 @@ __global__ void __launch_bounds__(PUSH_THREADS, 2) k_push(StepArgs A) {
     s_k.kB = run ? (float)(0.5 * da / (a * pm_hubble(a))) : 0.f;
     s_k.D = run ? (float)(da / (amid * amid * amid * pm_hubble(amid)) / P.dx) : 0.f;
     s_k.gscale = (float)(C.a_grid / a);
+    s_k.run = run ? 1 : 0;
+    s_k.sortnext = run && ((C.nsteps + 1) % P.full_every == 0) ? 1 : 0;
   }
   __syncthreads();
   const PushCoef K = s_k;
-  switch (P.TP) {
-    case 4: push_tile<4>(A, P, C, tr.pk, st, b, e, s_f, K); break;
-    case 8: push_tile<8>(A, P, C, tr.pk, st, b, e, s_f, K); break;
-    default: push_tile<16>(A, P, C, tr.pk, st, b, e, s_f, K); break;
+  const u32 st = (u32)tr.t;
+  switch (P.TS) {
+    case 4: push_super<4>(A, P, C, tr.pk, st, s_f, s_cnt, K); break;
+    case 8: push_super<8>(A, P, C, tr.pk, st, s_f, s_cnt, K); break;
+    default: push_super<16>(A, P, C, tr.pk, st, s_f, s_cnt, K); break;
   }
 }
 
 // Clock advance (one thread per peak): applies the step that the push kernel just made,
-// selects the next step size and sets which peaks re-deposit this step.
+// selects the next step size, whether this step regroups by sort, and which peaks re-deposit.
 __global__ void k_advance(StepArgs A) {
   for (int pk = threadIdx.x; pk < A.npeaks; pk += blockDim.x) {
     PeakClock c = A.clocks[pk];
+    const PeakDesc& P = A.peaks[pk];
     int dep = 0;
     // Collapse detection on the deposit of the current positions (made by the previous step).
     if (c.has_delta && c.delta_collapse > 0 && c.a_collapse < 0 && c.state != PS_PRIME) {
-      const PeakDesc& P = A.peaks[pk];
       const double dmax = (double)A.stats[pk].max_fix / (double)PM_FIX_ONE / P.n_mean - 1.0;
       if (dmax >= c.delta_collapse) {
         c.a_collapse = c.a;
@@ -221,6 +247,8 @@ __global__ void k_advance(StepArgs A) {
     switch (c.state) {
       case PS_PRIME:
         dep = 1;
+        c.sortstep = 1;
+        c.sbuf ^= 1;
         c.kpend = 0.0;
         c.a_grid = c.a;
         c.has_delta = 1;
@@ -232,7 +260,8 @@ __global__ void k_advance(StepArgs A) {
         c.a = an;
         c.a_grid = an;
         c.nsteps += 1;
-        c.buf ^= 1;
+        c.sortstep = (c.nsteps % P.full_every) == 0 ? 1 : 0;
+        c.sbuf ^= 1;
         dep = 1;
         if (c.mode == SCHED_RATIO) {
           if (c.nsteps >= c.max_steps) c.state = PS_FINALIZE;
@@ -247,7 +276,8 @@ __global__ void k_advance(StepArgs A) {
       }
       case PS_FINALIZE:
         c.kpend = 0.0;
-        c.buf ^= 1;
+        c.sortstep = 0;
+        c.sbuf ^= 1;
         dep = 1;
         c.state = PS_IDLE;
         break;
@@ -256,8 +286,7 @@ __global__ void k_advance(StepArgs A) {
     }
     c.dep = dep;
     A.clocks[pk] = c;
-    A.sortseg[pk].active = dep;
-    A.sortseg_full[pk].active = dep;
+    A.sortseg[pk].active = dep && c.sortstep;
     if (dep) {
       A.stats[pk].max_fix = 0;
       A.stats[pk].mass_defect = 0;
@@ -265,119 +294,189 @@ __global__ void k_advance(StepArgs A) {
   }
 }
 
-// Bucket starts from the sorted keys: bstart[b] = first sorted index whose bucket >= b.
-__global__ void k_bucket_starts(StepArgs A, long long ntot) {
+// ------------------------------------------------------------------------------------------
+// Regrouping by sort (priming and every full_every steps): gather the temporary state in
+// sorted order and find the super-tile starts in the sorted keys.
+__global__ void k_permute(StepArgs A, long long ntot) {
   const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= ntot) return;
   const int pk = pm_find(A.p_base, A.npeaks, j);
-  if (!A.clocks[pk].dep) return;
+  const PeakClock& C = A.clocks[pk];
+  if (!(C.dep && C.sortstep)) return;
+  const u32 q = A.perm[j];
+  A.pos[j] = A.tpos[q];
+  A.mom[j] = A.tmom[q];
+}
+
+__global__ void k_st_starts(StepArgs A, long long ntot) {
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ntot) return;
+  const int pk = pm_find(A.p_base, A.npeaks, j);
+  const PeakClock& C = A.clocks[pk];
+  if (!(C.dep && C.sortstep)) return;
   const PeakDesc& P = A.peaks[pk];
-  u32* bs = A.bstart + P.bucket_off;
-  const int b = (int)(A.keys_sorted[j] >> P.local_bits);
-  const int bprev = j == P.p_off ? -1 : (int)(A.keys_sorted[j - 1] >> P.local_bits);
-  for (int bb = bprev + 1; bb <= b; ++bb) bs[bb] = (u32)j;
+  u32* ss = sst(A, C.sbuf) + P.sst_off;
+  const int b = (int)(A.keys_sorted[j] >> P.st_shift);
+  const int bprev = j == P.p_off ? -1 : (int)(A.keys_sorted[j - 1] >> P.st_shift);
+  for (int bb = bprev + 1; bb <= b; ++bb) ss[bb] = (u32)j;
   if (j == P.p_off + P.n - 1)
-    for (int bb = b + 1; bb <= P.nb; ++bb) bs[bb] = (u32)(P.p_off + P.n);
+    for (int bb = b + 1; bb <= P.nst; ++bb) ss[bb] = (u32)(P.p_off + P.n);
 }
 
 // ------------------------------------------------------------------------------------------
-// Deterministic CIC deposit (pm3d.py:81-89, 103-104).  One CTA owns the TS^3 nodes of one push
-// super-tile (TS = 16: 8 bucket tiles of 8^3).  It reads the super-tile's own particles (one
-// contiguous sorted range) and, from the 7 lower neighbour super-tiles, only the buckets of
-// their boundary-layer cells whose corners reach into it.  Per particle the 8 CIC weights are
-// formed in 64-bit fixed point with 40 fractional bits, the 8th corner taking the remainder so
-// each particle deposits exactly 2^40; consecutive particles of one cell are first combined by
-// a warp-shuffle segmented scan.  Each node accumulates in shared memory as two native 32-bit
-// words (the signed weight's bits >= 20 and its low 20 bits), which cannot overflow within a
-// chunk of fewer than 2048 particles, and is folded into a 64-bit register accumulator after
-// every chunk.
-// Integer sums make the result independent of particle order, bit for bit; no global atomics.
-// Every node is written once as FP32 delta = S/n_mean - 1.
+// Regrouping by re-binning (the other steps).  Destination super-tile D takes, in class order,
+// the run of each source D - u(c) whose particles moved by u(c), then its far movers.
+// scan1: per destination, offsets of its incoming runs and its total.
+__global__ void __launch_bounds__(BIN_CLASSES) k_bin_scan1(StepArgs A) {
+  __shared__ u32 s_w[BIN_CLASSES / 32];
+  const TileRef tr = find_tile(A.st_base, A.npeaks);
+  const PeakClock& C = A.clocks[tr.pk];
+  if (!(C.dep && !C.sortstep)) return;
+  const PeakDesc& P = A.peaks[tr.pk];
+  const u32 D = (u32)tr.t;
+  const int dx = pm_compact3(D >> 2), dy = pm_compact3(D >> 1), dz = pm_compact3(D);
+  const int c = threadIdx.x, lane = c & 31, warp = c >> 5;
+  u32 v = 0, src = 0;
+  if (c < P.NC) {
+    const int W = P.W, NS = P.NS;
+    const int ux = bin_offset(c / (W * W), NS), uy = bin_offset((c / W) % W, NS), uz = bin_offset(c % W, NS);
+    src = pm_morton3((dx - ux) & (NS - 1), (dy - uy) & (NS - 1), (dz - uz) & (NS - 1));
+    v = A.counts[(P.st_base + src) * BIN_CLASSES + c];
+  }
+  u32 incl = v;
+  for (int d = 1; d < 32; d <<= 1) {
+    const u32 t = __shfl_up_sync(0xffffffffu, incl, d);
+    if (lane >= d) incl += t;
+  }
+  if (lane == 31) s_w[warp] = incl;
+  __syncthreads();
+  u32 off = 0;
+  for (int w = 0; w < warp; ++w) off += s_w[w];
+  if (c < P.NC) A.lpre[(P.st_base + src) * BIN_CLASSES + c] = off + incl - v;
+  if (c == BIN_CLASSES - 1) A.totals[P.st_base + D] = off + incl + A.far_count[P.st_base + D];
+}
+
+// scan2: per peak, super-tile starts from the totals.
+__global__ void __launch_bounds__(1024) k_bin_scan2(StepArgs A) {
+  __shared__ u32 s_w[32];
+  __shared__ long long s_carry;
+  const int pk = blockIdx.x;
+  const PeakClock& C = A.clocks[pk];
+  if (!(C.dep && !C.sortstep)) return;
+  const PeakDesc& P = A.peaks[pk];
+  u32* ss = sst(A, C.sbuf) + P.sst_off;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) s_carry = P.p_off;
+  __syncthreads();
+  for (int base = 0; base < P.nst; base += 1024) {
+    const int i = base + threadIdx.x;
+    const u32 v = i < P.nst ? A.totals[P.st_base + i] : 0u;
+    u32 incl = v;
+    for (int d = 1; d < 32; d <<= 1) {
+      const u32 t = __shfl_up_sync(0xffffffffu, incl, d);
+      if (lane >= d) incl += t;
+    }
+    if (lane == 31) s_w[warp] = incl;
+    __syncthreads();
+    u32 off = 0;
+    for (int w = 0; w < warp; ++w) off += s_w[w];
+    const long long carry = s_carry;
+    if (i < P.nst) ss[i] = (u32)(carry + off + incl - v);
+    __syncthreads();
+    if (threadIdx.x == 1023) s_carry = carry + off + incl;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    ss[P.nst] = (u32)(P.p_off + P.n);
+    if (s_carry != P.p_off + P.n) atomicOr(&A.stats[pk].status, 4u);  // counts lost a particle
+  }
+}
+
+// scatter: per source super-tile, every particle to its place in the new grouping.
+__global__ void __launch_bounds__(PUSH_THREADS) k_bin_scatter(StepArgs A) {
+  __shared__ u32 s_rank[BIN_CLASSES];
+  const TileRef tr = find_tile(A.st_base, A.npeaks);
+  const PeakClock& C = A.clocks[tr.pk];
+  if (!(C.dep && !C.sortstep)) return;
+  const PeakDesc& P = A.peaks[tr.pk];
+  const u32 S = (u32)tr.t;
+  const u32* old = sst(A, C.sbuf ^ 1) + P.sst_off;
+  const u32* ss = sst(A, C.sbuf) + P.sst_off;
+  if (threadIdx.x < BIN_CLASSES) s_rank[threadIdx.x] = 0u;
+  __syncthreads();
+  const int sx = pm_compact3(S >> 2), sy = pm_compact3(S >> 1), sz = pm_compact3(S);
+  const int NS = P.NS, W = P.W;
+  const long long b = old[S], e = old[S + 1];
+  for (long long j = b + threadIdx.x; j < e; j += PUSH_THREADS) {
+    const int c = A.cls[j];
+    const int4 ps = A.tpos[j];
+    const float4 m = A.tmom[j];
+    long long dest;
+    const u32 am = __activemask();
+    const u32 peers = __match_any_sync(am, c);
+    const int leader = __ffs(peers) - 1;
+    if (c != BIN_FAR) {
+      u32 base = 0;
+      if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(&s_rank[c], (u32)__popc(peers));
+      base = __shfl_sync(peers, base, leader);
+      const int ux = bin_offset(c / (W * W), NS), uy = bin_offset((c / W) % W, NS), uz = bin_offset(c % W, NS);
+      const u32 D = pm_morton3((sx + ux) & (NS - 1), (sy + uy) & (NS - 1), (sz + uz) & (NS - 1));
+      dest = (long long)ss[D] + A.lpre[(P.st_base + S) * BIN_CLASSES + c] + base + __popc(peers & lanemask_lt());
+    } else {
+      const int l2 = P.log2N;
+      const u32 D = pm_morton3((ps.x >> (2 * l2)) >> P.log2TS, ((ps.x >> l2) & (P.N - 1)) >> P.log2TS,
+                               (ps.x & (P.N - 1)) >> P.log2TS);
+      dest = (long long)ss[D + 1] - A.far_count[P.st_base + D] + atomicAdd(&A.far_fill[P.st_base + D], 1u);
+    }
+    if (dest < P.p_off || dest >= P.p_off + P.n) {  // counts and classes disagree: never write outside
+      atomicOr(&A.stats[tr.pk].status, 4u);
+      continue;
+    }
+    A.pos[dest] = ps;
+    A.mom[dest] = m;
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Deterministic CIC deposit (pm3d.py:81-89, 103-104).  One CTA per super-tile deposits its own
+// particles (one contiguous range) onto the (TS+1)^3 nodes they touch.  Per particle the 8 CIC
+// weights are formed in 64-bit fixed point with 40 fractional bits, the 8th corner taking the
+// remainder so each particle deposits exactly 2^40; consecutive particles of one cell are first
+// combined by a warp-shuffle segmented scan.  Each node accumulates in shared memory as two
+// native 32-bit words (the signed weight's bits >= 20 and its low 20 bits), which cannot
+// overflow within a chunk of fewer than 2048 particles, and is folded into a 64-bit register
+// accumulator after every chunk.  Interior nodes are then final and written as FP32
+// delta = S/n_mean - 1; nodes on the three lower faces (which neighbours also reach) and on the
+// upper halo (which belongs to the neighbours) are written as 64-bit partials for the fix-up.
+// Integer sums make the result independent of particle order, bit for bit; no float atomics.
+__device__ __forceinline__ int face_index(int lx, int ly, int lz, int T) {
+  if (lx == 0) return ly * T + lz;
+  if (ly == 0) return T * T + (lx - 1) * T + lz;
+  return T * T + (T - 1) * T + (lx - 1) * (T - 1) + (ly - 1);
+}
+__device__ __forceinline__ int halo_index(int lx, int ly, int lz, int T) {
+  if (lx == T) return ly * (T + 1) + lz;
+  if (ly == T) return (T + 1) * (T + 1) + lx * (T + 1) + lz;
+  return (T + 1) * (T + 1) + T * (T + 1) + lx * T + ly;
+}
+
 template <int TS>
-__device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc& P, int pk, u32 st, u32* smem,
-                                              double* rho64) {
-  constexpr int TS3 = TS * TS * TS;
-  constexpr int NPT = (TS3 + DEP_THREADS - 1) / DEP_THREADS;  // nodes per thread
-  constexpr int NCAND = 7 * 64;                                // (neighbour o, sub-tile, mask) candidates
+__device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc& P, const PeakClock& C, int pk,
+                                              u32 st, u32* smem, double* rho64) {
+  constexpr int T1 = TS + 1, NN = T1 * T1 * T1;
+  constexpr int NPT = (NN + DEP_THREADS - 1) / DEP_THREADS;  // nodes per thread
   u32* acc_hi = smem;
-  u32* acc_lo = smem + TS3;
-  __shared__ long long s_rb[72], s_rp[73];
-  __shared__ int s_ro[72];
-  __shared__ int s_nr;
-  __shared__ u32 s_wc[DEP_THREADS / 32];
+  u32* acc_lo = smem + NN;
   __shared__ long long s_red[DEP_THREADS / 32];
   __shared__ long long s_max[DEP_THREADS / 32];
   const int N = P.N, l2 = P.log2N;
-  const int rb = P.log2TP - P.log2T;      // log2 of sub-tiles per axis: 0 or 1
-  const int RS = 1 << (3 * rb);           // sub-tiles per super-tile: 1 or 8
-  const int NS = N / TS;                  // super-tiles per axis
   const int sx = pm_compact3(st >> 2), sy = pm_compact3(st >> 1), sz = pm_compact3(st);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const u32* bs = A.bstart + P.bucket_off;
-  for (int i = threadIdx.x; i < 2 * TS3; i += DEP_THREADS) smem[i] = 0u;
-  // Range table: candidate k = (o - 1) * 64 + s * 8 + m over sub-tiles s of the neighbour
-  // super-tile at offset -o that touch this one, and masks m covering o.
-  long long cb = 0, ce = 0;
-  bool use = false;
-  int co = 0;
-  if (threadIdx.x < NCAND) {
-    const int o = threadIdx.x / 64 + 1, s = (threadIdx.x >> 3) & 7, m = threadIdx.x & 7;
-    if (s < RS && (m & o) == o) {
-      const int sxl = pm_compact3((u32)s >> 2), syl = pm_compact3((u32)s >> 1), szl = pm_compact3((u32)s);
-      const int last = (1 << rb) - 1;
-      if ((!(o & 1) || sxl == last) && (!(o & 2) || syl == last) && (!(o & 4) || szl == last)) {
-        const u32 nx = (sx - (o & 1)) & (NS - 1), ny = (sy - ((o >> 1) & 1)) & (NS - 1), nz = (sz - ((o >> 2) & 1)) & (NS - 1);
-        const u32 b = (pm_morton3(nx, ny, nz) * (u32)RS + (u32)s) * 8 + m;
-        cb = bs[b];
-        ce = bs[b + 1];
-        use = ce > cb;
-        co = o;
-      }
-    }
-  }
-  // Compact the non-empty candidates (block-wide ballot prefix) behind the own range.
-  const u32 bal = __ballot_sync(0xffffffffu, use);
-  if (lane == 0) s_wc[warp] = __popc(bal);
+  for (int i = threadIdx.x; i < 2 * NN; i += DEP_THREADS) smem[i] = 0u;
+  const u32* ss = sst(A, C.sbuf) + P.sst_off;
+  const long long b = ss[st], e = ss[st + 1];
+  const long long total = e - b;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    u32 run = 1;
-    for (int w = 0; w < DEP_THREADS / 32; ++w) {
-      const u32 c = s_wc[w];
-      s_wc[w] = run;
-      run += c;
-    }
-    s_nr = (int)run;
-    s_rb[0] = bs[st * RS * 8];
-    s_rp[0] = bs[(st + 1) * RS * 8] - s_rb[0];  // length for now
-    s_ro[0] = 0;
-  }
-  __syncthreads();
-  if (use) {
-    const int slot = s_wc[warp] + __popc(bal & ((1u << lane) - 1u));
-    s_rb[slot] = cb;
-    s_rp[slot] = ce - cb;
-    s_ro[slot] = co;
-  }
-  __syncthreads();
-  const int nr = s_nr;
-  if (warp == 0) {  // lengths -> exclusive prefix (nr <= 72)
-    long long carry = 0;
-    for (int base = 0; base < nr; base += 32) {
-      const int i = base + lane;
-      const long long len = i < nr ? s_rp[i] : 0;
-      long long incl = len;
-      for (int d = 1; d < 32; d <<= 1) {
-        const long long v = __shfl_up_sync(0xffffffffu, incl, d);
-        if (lane >= d) incl += v;
-      }
-      if (i < nr) s_rp[i] = carry + incl - len;
-      carry += __shfl_sync(0xffffffffu, incl, 31);
-    }
-    if (lane == 0) s_rp[nr] = carry;
-  }
-  __syncthreads();
-  const long long total = s_rp[nr];
-  const int4* __restrict__ pos = posb(A, A.clocks[pk].buf);
   const u32 le = lanemask_le();
   u64 acc[NPT];
 #pragma unroll
@@ -388,40 +487,25 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
   constexpr int CH_IT = 3;  // sweeps of DEP_THREADS particles per chunk: CHUNK = 1536
   static_assert(CH_IT * DEP_THREADS < 2048, "chunk too large for the split accumulators");
   const long long nit = (total + DEP_THREADS - 1) / DEP_THREADS;
-  // Flat particle index k over the concatenated ranges; the range index only moves forward.
-  long long k = warp * 32 + lane;
-  int r = 0;
-  bool v_n = k < total;
-  int4 ps_n = make_int4(-1, 0, 0, 0);
-  int o_n = 0;
-  if (v_n) {
-    while (r + 1 < nr && s_rp[r + 1] <= k) ++r;
-    ps_n = pos[A.perm[s_rb[r] + (k - s_rp[r])]];
-    o_n = s_ro[r];
-  }
+  long long j = b + threadIdx.x;
+  int4 ps_n = j < e ? A.pos[j] : make_int4(-1, 0, 0, 0);
+  bool bad = false;
   for (long long it = 0; it < nit; ++it) {
     const int4 ps = ps_n;
-    const bool valid = v_n;
-    const int o = o_n;
-    // Prefetch the next sweep's particle before working on this one.
-    k += DEP_THREADS;
-    v_n = k < total;
-    if (v_n) {
-      while (r + 1 < nr && s_rp[r + 1] <= k) ++r;
-      ps_n = pos[A.perm[s_rb[r] + (k - s_rp[r])]];
-      o_n = s_ro[r];
-    }
+    const bool valid = j < e;
+    j += DEP_THREADS;
+    if (j < e) ps_n = A.pos[j];  // next sweep's particle, fetched before this one is used
     {
       const int ix = ps.x >> (2 * l2), iy = (ps.x >> l2) & (N - 1), iz = ps.x & (N - 1);
-      const int lx = (o & 1) ? -1 : ix - sx * TS;
-      const int ly = (o & 2) ? -1 : iy - sy * TS;
-      const int lz = (o & 4) ? -1 : iz - sz * TS;
+      const int lx = ix - sx * TS, ly = iy - sy * TS, lz = iz - sz * TS;
+      const bool in = valid && (unsigned)lx < (unsigned)TS && (unsigned)ly < (unsigned)TS && (unsigned)lz < (unsigned)TS;
+      bad |= valid && !in;
       const double fx = __int_as_float(ps.y), fy = __int_as_float(ps.z), fz = __int_as_float(ps.w);
       const double gx = 1.0 - fx, gy = 1.0 - fy, gz = 1.0 - fz;
       const double one = (double)PM_FIX_ONE;
       const double w00 = gx * gy * one, w01 = gx * fy * one, w10 = fx * gy * one, w11 = fx * fy * one;
       u64 W0 = 0, W1 = 0, W2 = 0, W3 = 0, W4 = 0, W5 = 0, W6 = 0, W7 = 0;
-      if (valid) {
+      if (in) {
         W0 = (u64)__double2ll_rn(w00 * gz);
         W1 = (u64)__double2ll_rn(w00 * fz);
         W2 = (u64)__double2ll_rn(w01 * gz);
@@ -431,9 +515,8 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
         W6 = (u64)__double2ll_rn(w11 * gz);
         W7 = PM_FIX_ONE - (W0 + W1 + W2 + W3 + W4 + W5 + W6);
       }
-      // Warp-shuffle segmented scan over runs of the same cell (a cell lies in one bucket, so
-      // equal cells also share the range and its neighbour offset o).
-      const int key = valid ? ps.x : -1 - lane;
+      // Warp-shuffle segmented scan over runs of the same cell.
+      const int key = in ? ps.x : -1 - lane;
       const int prev = __shfl_up_sync(0xffffffffu, key, 1);
       const bool head = lane == 0 || prev != key;
       const u32 heads = __ballot_sync(0xffffffffu, head);
@@ -443,34 +526,31 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
           const bool take = lane - d >= sstart;
-#define PM_SEG(W)                              \
-  {                                            \
-    const u64 v_ = shfl_up_u64(W, d);          \
-    if (take) W += v_;                         \
+#define PM_SEG(W)                     \
+  {                                   \
+    const u64 v_ = shfl_up_u64(W, d); \
+    if (take) W += v_;                \
   }
           PM_SEG(W0) PM_SEG(W1) PM_SEG(W2) PM_SEG(W3) PM_SEG(W4) PM_SEG(W5) PM_SEG(W6) PM_SEG(W7)
 #undef PM_SEG
         }
         tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
       }
-      if (valid && tail) {
-        const bool x0 = (unsigned)lx < (unsigned)TS, x1 = (unsigned)(lx + 1) < (unsigned)TS;
-        const bool y0 = (unsigned)ly < (unsigned)TS, y1 = (unsigned)(ly + 1) < (unsigned)TS;
-        const bool z0 = (unsigned)lz < (unsigned)TS, z1 = (unsigned)(lz + 1) < (unsigned)TS;
-        const int nb = (lx * TS + ly) * TS + lz;
-#define PM_ADD(cond, off, W)                                                  \
-  if (cond) {                                                                 \
-    atomicAdd(&acc_hi[nb + (off)], (u32)(int)((long long)(W) >> 20));        \
-    atomicAdd(&acc_lo[nb + (off)], (u32)((W) & 0xFFFFFu));                   \
+      if (in && tail) {
+        const int nb = (lx * T1 + ly) * T1 + lz;
+#define PM_ADD(off, W)                                                   \
+  {                                                                      \
+    atomicAdd(&acc_hi[nb + (off)], (u32)(int)((long long)(W) >> 20));   \
+    atomicAdd(&acc_lo[nb + (off)], (u32)((W) & 0xFFFFFu));              \
   }
-        PM_ADD(x0 && y0 && z0, 0, W0)
-        PM_ADD(x0 && y0 && z1, 1, W1)
-        PM_ADD(x0 && y1 && z0, TS, W2)
-        PM_ADD(x0 && y1 && z1, TS + 1, W3)
-        PM_ADD(x1 && y0 && z0, TS * TS, W4)
-        PM_ADD(x1 && y0 && z1, TS * TS + 1, W5)
-        PM_ADD(x1 && y1 && z0, TS * TS + TS, W6)
-        PM_ADD(x1 && y1 && z1, TS * TS + TS + 1, W7)
+        PM_ADD(0, W0)
+        PM_ADD(1, W1)
+        PM_ADD(T1, W2)
+        PM_ADD(T1 + 1, W3)
+        PM_ADD(T1 * T1, W4)
+        PM_ADD(T1 * T1 + 1, W5)
+        PM_ADD(T1 * T1 + T1, W6)
+        PM_ADD(T1 * T1 + T1 + 1, W7)
 #undef PM_ADD
       }
     }
@@ -479,7 +559,7 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
 #pragma unroll
       for (int q = 0; q < NPT; ++q) {
         const int node = threadIdx.x + q * DEP_THREADS;
-        if (node < TS3) {
+        if (node < NN) {
           acc[q] += (u64)((long long)(int)acc_hi[node] * (1LL << 20)) + (u64)acc_lo[node];
           acc_hi[node] = 0u;
           acc_lo[node] = 0u;
@@ -488,20 +568,29 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
       __syncthreads();
     }
   }
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&A.stats[pk].status, 1u);
   long long dsum = 0, smax = 0;
-  const long long base = ((long long)sx * TS * N + (long long)sy * TS) * N + sz * TS;
+  const long long gbase = ((long long)sx * TS * N + (long long)sy * TS) * N + sz * TS;
+  long long* face = A.face + P.face_off + (long long)st * P.fc;
+  long long* halo = A.halo + P.halo_off + (long long)st * P.hc;
 #pragma unroll
-  for (int k = 0; k < NPT; ++k) {
-    const int node = threadIdx.x + k * DEP_THREADS;
-    if (node < TS3) {
-      const int nz = node & (TS - 1), ny = (node / TS) & (TS - 1), nx = node / (TS * TS);
-      const long long S = (long long)acc[k];
-      const long long Dv = S - P.n_mean_fix;
-      const long long g = base + ((long long)nx * N + ny) * N + nz;
-      P.delta[g] = (float)((double)Dv * P.inv_fix_nmean);
-      if (rho64) rho64[g] = (double)S * (1.0 / (double)PM_FIX_ONE);
-      dsum += Dv;
-      smax = S > smax ? S : smax;
+  for (int q = 0; q < NPT; ++q) {
+    const int node = threadIdx.x + q * DEP_THREADS;
+    if (node < NN) {
+      const int lz = node % T1, ly = (node / T1) % T1, lx = node / (T1 * T1);
+      const long long S = (long long)acc[q];
+      if (lx == TS || ly == TS || lz == TS) {
+        halo[halo_index(lx, ly, lz, TS)] = S;
+      } else if (lx == 0 || ly == 0 || lz == 0) {
+        face[face_index(lx, ly, lz, TS)] = S;
+      } else {
+        const long long Dv = S - P.n_mean_fix;
+        const long long g = gbase + ((long long)lx * N + ly) * N + lz;
+        P.delta[g] = (float)((double)Dv * P.inv_fix_nmean);
+        if (rho64) rho64[g] = (double)S * (1.0 / (double)PM_FIX_ONE);
+        dsum += Dv;
+        smax = S > smax ? S : smax;
+      }
     }
   }
   for (int d = 16; d > 0; d >>= 1) {
@@ -522,18 +611,92 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
     }
     atomicAdd((unsigned long long*)&A.stats[pk].mass_defect, (unsigned long long)ts);
     atomicMax(&A.stats[pk].max_fix, (u64)tm);
+    A.far_count[P.st_base + st] = 0u;  // consumed by this step's regrouping
+    A.far_fill[P.st_base + st] = 0u;
   }
 }
 
 __global__ void __launch_bounds__(DEP_THREADS) k_deposit(StepArgs A, double* rho64) {
   extern __shared__ __align__(16) u32 s_dep[];
-  const TileRef tr = find_tile(A.ptile_base, A.npeaks);
-  if (!A.clocks[tr.pk].dep) return;
+  const TileRef tr = find_tile(A.st_base, A.npeaks);
+  const PeakClock C = A.clocks[tr.pk];
+  if (!C.dep) return;
   const PeakDesc& P = A.peaks[tr.pk];
-  switch (P.TP) {
-    case 4: deposit_super<4>(A, P, tr.pk, (u32)tr.t, s_dep, rho64); break;
-    case 8: deposit_super<8>(A, P, tr.pk, (u32)tr.t, s_dep, rho64); break;
-    default: deposit_super<16>(A, P, tr.pk, (u32)tr.t, s_dep, rho64); break;
+  switch (P.TS) {
+    case 4: deposit_super<4>(A, P, C, tr.pk, (u32)tr.t, s_dep, rho64); break;
+    case 8: deposit_super<8>(A, P, C, tr.pk, (u32)tr.t, s_dep, rho64); break;
+    default: deposit_super<16>(A, P, C, tr.pk, (u32)tr.t, s_dep, rho64); break;
+  }
+}
+
+// Face fix-up: a node on a lower face of super-tile S also receives particles of the
+// neighbours below it; their shares were written as those neighbours' upper-halo partials.
+__device__ __forceinline__ void face_coords(int f, int T, int& lx, int& ly, int& lz) {
+  if (f < T * T) {
+    lx = 0;
+    ly = f / T;
+    lz = f % T;
+  } else if (f < T * T + (T - 1) * T) {
+    const int r = f - T * T;
+    lx = 1 + r / T;
+    ly = 0;
+    lz = r % T;
+  } else {
+    const int r = f - T * T - (T - 1) * T;
+    lx = 1 + r / (T - 1);
+    ly = 1 + r % (T - 1);
+    lz = 0;
+  }
+}
+
+__global__ void __launch_bounds__(PM_THREADS) k_fixup(StepArgs A, long long nface, double* rho64) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool inr = g < nface;
+  int pk = 0;
+  bool act = false;
+  long long Dv = 0, S = 0;
+  if (inr) {
+    pk = pm_find(A.face_base, A.npeaks, g);
+    act = A.clocks[pk].dep != 0;
+  }
+  if (act) {
+    const PeakDesc& P = A.peaks[pk];
+    const int T = P.TS, NS = P.NS, N = P.N;
+    const long long local = g - A.face_base[pk];
+    const u32 st = (u32)(local / P.fc);
+    const int f = (int)(local - (long long)st * P.fc);
+    int lx, ly, lz;
+    face_coords(f, T, lx, ly, lz);
+    const int sx = pm_compact3(st >> 2), sy = pm_compact3(st >> 1), sz = pm_compact3(st);
+    S = A.face[P.face_off + local];
+    const int zmask = (lx == 0 ? 1 : 0) | (ly == 0 ? 2 : 0) | (lz == 0 ? 4 : 0);
+    for (int o = 1; o < 8; ++o) {
+      if (o & ~zmask) continue;
+      const int ox = o & 1, oy = (o >> 1) & 1, oz = (o >> 2) & 1;
+      const u32 sn = pm_morton3((sx - ox) & (NS - 1), (sy - oy) & (NS - 1), (sz - oz) & (NS - 1));
+      S += A.halo[P.halo_off + (long long)sn * P.hc + halo_index(lx + T * ox, ly + T * oy, lz + T * oz, T)];
+    }
+    Dv = S - P.n_mean_fix;
+    const long long node = ((long long)(sx * T + lx) * N + (sy * T + ly)) * N + (sz * T + lz);
+    P.delta[node] = (float)((double)Dv * P.inv_fix_nmean);
+    if (rho64) rho64[node] = (double)S * (1.0 / (double)PM_FIX_ONE);
+  }
+  // Statistics: one atomic per warp when the warp covers a single peak.
+  const int pk0 = __shfl_sync(0xffffffffu, pk, 0);
+  if (__all_sync(0xffffffffu, pk == pk0)) {
+    long long ds = act ? Dv : 0, sm = act ? S : 0;
+    for (int d = 16; d > 0; d >>= 1) {
+      ds += __shfl_xor_sync(0xffffffffu, ds, d);
+      const long long om = __shfl_xor_sync(0xffffffffu, sm, d);
+      sm = om > sm ? om : sm;
+    }
+    if ((threadIdx.x & 31) == 0 && inr && A.clocks[pk0].dep) {
+      atomicAdd((unsigned long long*)&A.stats[pk0].mass_defect, (unsigned long long)ds);
+      atomicMax(&A.stats[pk0].max_fix, (u64)(sm > 0 ? sm : 0));
+    }
+  } else if (act) {
+    atomicAdd((unsigned long long*)&A.stats[pk].mass_defect, (unsigned long long)Dv);
+    atomicMax(&A.stats[pk].max_fix, (u64)(S > 0 ? S : 0));
   }
 }
 
@@ -612,7 +775,6 @@ __global__ void __launch_bounds__(PM_THREADS) k_green(StepArgs A) {
   out[2 * M + m] = oz;
 }
 
-// ------------------------------------------------------------------------------------------
 __global__ void k_reset_peak(StepArgs A, int pk, double a0, int mode, double param, double a_end, int max_steps) {
   PeakClock c = A.clocks[pk];
   c.a = a0;
@@ -626,6 +788,7 @@ __global__ void k_reset_peak(StepArgs A, int pk, double a0, int mode, double par
   c.state = PS_PRIME;
   c.has_delta = 0;
   c.dep = 0;
+  c.sortstep = 0;
   c.a_collapse = -1.0;
   c.stop_on_collapse = 0;
   if (mode == SCHED_RATIO) c.da = a0 * param;
@@ -640,7 +803,6 @@ __global__ void k_set_particles(StepArgs A, int pk, PeakDesc P, const double* __
                                 const double* __restrict__ p) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P.n) return;
-  const int buf = A.clocks[pk].buf;
   int ii[3];
   float ff[3];
   for (int d = 0; d < 3; ++d) {
@@ -657,9 +819,22 @@ __global__ void k_set_particles(StepArgs A, int pk, PeakDesc P, const double* __
   }
   const int cell = (ii[0] << (2 * P.log2N)) | (ii[1] << P.log2N) | ii[2];
   const long long g = P.p_off + i;
-  posb(A, buf)[g] = make_int4(cell, __float_as_int(ff[0]), __float_as_int(ff[1]), __float_as_int(ff[2]));
-  momb(A, buf)[g] = make_float4((float)p[3 * i], (float)p[3 * i + 1], (float)p[3 * i + 2], __int_as_float((int)i));
-  A.keys_push[g] = pm_cell_key(P, ii[0], ii[1], ii[2]);
+  // Loaded into the temporary state in lattice order; the priming step sorts it into place.
+  A.tpos[g] = make_int4(cell, __float_as_int(ff[0]), __float_as_int(ff[1]), __float_as_int(ff[2]));
+  A.tmom[g] = make_float4((float)p[3 * i], (float)p[3 * i + 1], (float)p[3 * i + 2], __int_as_float((int)i));
+  A.keys_push[g] = pm_cell_key(ii[0], ii[1], ii[2]);
+}
+
+// Re-priming an existing state: copy it back to the loading area with its sort keys.
+__global__ void k_reload(StepArgs A, PeakDesc P) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.n) return;
+  const long long g = P.p_off + i;
+  const int4 ps = A.pos[g];
+  A.tpos[g] = ps;
+  A.tmom[g] = A.mom[g];
+  const int N = P.N, l2 = P.log2N;
+  A.keys_push[g] = pm_cell_key(ps.x >> (2 * l2), (ps.x >> l2) & (N - 1), ps.x & (N - 1));
 }
 
 // Current state -> float64 x, p (lattice order).  p includes the pending closing kick; acc
@@ -669,12 +844,18 @@ __global__ void k_get_particles(StepArgs A, int pk, PeakDesc P, double* __restri
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P.n) return;
   const PeakClock C = A.clocks[pk];
-  const int4 ps = posb(A, C.buf)[P.p_off + i];
-  const float4 m = momb(A, C.buf)[P.p_off + i];
+  // A peak loaded but not yet primed still has its particles in the loading area.
+  const bool loaded_only = C.state == PS_PRIME;
+  const int4 ps = loaded_only ? A.tpos[P.p_off + i] : A.pos[P.p_off + i];
+  const float4 m = loaded_only ? A.tmom[P.p_off + i] : A.mom[P.p_off + i];
   const int N = P.N;
   const int ii[3] = {ps.x >> (2 * P.log2N), (ps.x >> P.log2N) & (N - 1), ps.x & (N - 1)};
   const float f[3] = {__int_as_float(ps.y), __int_as_float(ps.z), __int_as_float(ps.w)};
   const long long id = (long long)__float_as_int(m.w);
+  if (id < 0 || id >= P.n) {  // never write through an id that is not a lattice index
+    atomicOr(&A.stats[pk].status, 8u);
+    return;
+  }
   double g[3] = {0.0, 0.0, 0.0};
   const bool need_g = C.has_delta && ((p && C.kpend != 0.0) || acc);
   if (need_g) {
@@ -726,8 +907,8 @@ __global__ void k_interp64(const double* __restrict__ F, const double* __restric
 
 }  // namespace
 
-size_t pm_deposit_smem(int TPmax) { return sizeof(u32) * 2 * (size_t)TPmax * TPmax * TPmax; }
-size_t pm_push_smem(int TPmax) { return sizeof(float) * 3 * (size_t)(TPmax + 1) * (TPmax + 1) * (TPmax + 1); }
+size_t pm_deposit_smem(int TSmax) { return sizeof(u32) * 2 * (size_t)(TSmax + 1) * (TSmax + 1) * (TSmax + 1); }
+size_t pm_push_smem(int TSmax) { return sizeof(float) * 3 * (size_t)(TSmax + 1) * (TSmax + 1) * (TSmax + 1); }
 
 int pm_kernels_init() {
   cudaError_t e = cudaFuncSetAttribute(k_push, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
@@ -735,15 +916,28 @@ int pm_kernels_init() {
   return e == cudaSuccess ? 0 : -(int)e;
 }
 
-void launch_push(const StepArgs& A, long long nptiles, size_t smem, cudaStream_t s) {
-  k_push<<<(unsigned)nptiles, PUSH_THREADS, smem, s>>>(A);
+static unsigned nb(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+void launch_push(const StepArgs& A, long long nst, size_t smem, cudaStream_t s) {
+  k_push<<<(unsigned)nst, PUSH_THREADS, smem, s>>>(A);
 }
 void launch_advance(const StepArgs& A, cudaStream_t s) { k_advance<<<1, 256, 0, s>>>(A); }
-void launch_bucket_starts(const StepArgs& A, long long ntot, cudaStream_t s) {
-  k_bucket_starts<<<(unsigned)((ntot + PM_THREADS - 1) / PM_THREADS), PM_THREADS, 0, s>>>(A, ntot);
+void launch_permute(const StepArgs& A, long long ntot, cudaStream_t s) {
+  k_permute<<<nb(ntot, PM_THREADS), PM_THREADS, 0, s>>>(A, ntot);
 }
-void launch_deposit(const StepArgs& A, long long nptiles, size_t smem, double* rho64, cudaStream_t s) {
-  k_deposit<<<(unsigned)nptiles, DEP_THREADS, smem, s>>>(A, rho64);
+void launch_st_starts(const StepArgs& A, long long ntot, cudaStream_t s) {
+  k_st_starts<<<nb(ntot, PM_THREADS), PM_THREADS, 0, s>>>(A, ntot);
+}
+void launch_bin(const StepArgs& A, long long nst, cudaStream_t s) {
+  k_bin_scan1<<<(unsigned)nst, BIN_CLASSES, 0, s>>>(A);
+  k_bin_scan2<<<(unsigned)A.npeaks, 1024, 0, s>>>(A);
+  k_bin_scatter<<<(unsigned)nst, PUSH_THREADS, 0, s>>>(A);
+}
+void launch_deposit(const StepArgs& A, long long nst, size_t smem, double* rho64, cudaStream_t s) {
+  k_deposit<<<(unsigned)nst, DEP_THREADS, smem, s>>>(A, rho64);
+}
+void launch_fixup(const StepArgs& A, long long nface, double* rho64, cudaStream_t s) {
+  k_fixup<<<nb(nface, PM_THREADS), PM_THREADS, 0, s>>>(A, nface, rho64);
 }
 void launch_green(const StepArgs& A, long long nblocks, cudaStream_t s) {
   k_green<<<(unsigned)nblocks, PM_THREADS, 0, s>>>(A);
@@ -754,12 +948,15 @@ void launch_reset_peak(const StepArgs& A, int pk, double a0, int mode, double pa
 }
 void launch_set_particles(const StepArgs& A, int pk, const PeakDesc& P, const double* x, const double* p,
                           cudaStream_t s) {
-  k_set_particles<<<(unsigned)((P.n + PM_THREADS - 1) / PM_THREADS), PM_THREADS, 0, s>>>(A, pk, P, x, p);
+  k_set_particles<<<nb(P.n, PM_THREADS), PM_THREADS, 0, s>>>(A, pk, P, x, p);
+}
+void launch_reload(const StepArgs& A, const PeakDesc& P, cudaStream_t s) {
+  k_reload<<<nb(P.n, PM_THREADS), PM_THREADS, 0, s>>>(A, P);
 }
 void launch_get_particles(const StepArgs& A, int pk, const PeakDesc& P, double* x, double* p, double* acc,
                           double a_acc, cudaStream_t s) {
-  k_get_particles<<<(unsigned)((P.n + PM_THREADS - 1) / PM_THREADS), PM_THREADS, 0, s>>>(A, pk, P, x, p, acc, a_acc);
+  k_get_particles<<<nb(P.n, PM_THREADS), PM_THREADS, 0, s>>>(A, pk, P, x, p, acc, a_acc);
 }
 void launch_interp64(const double* F, const double* X, long long n, int N, double dx, double* out, cudaStream_t s) {
-  k_interp64<<<(unsigned)((n + PM_THREADS - 1) / PM_THREADS), PM_THREADS, 0, s>>>(F, X, n, N, dx, out);
+  k_interp64<<<nb(n, PM_THREADS), PM_THREADS, 0, s>>>(F, X, n, N, dx, out);
 }

@@ -1,4 +1,18 @@
 // Kernels of one PM step (pbhgr/pbhgr/pm3d.py:101-129) over a batch of peaks.
+//
+// Particles live grouped by super-tile (TS^3 cells): super-tile S of a peak owns the contiguous
+// range [sstart[S], sstart[S+1]) of the state arrays.  One step:
+//   push       per super-tile: CIC gather of the forces, kicks, drift; output in place into the
+//              temporary state, tagged with the class of the super-tile the particle moved to
+//              (one of <= 125 neighbours) and counted per class
+//   advance    per peak clock (and which peaks regroup by sort this step)
+//   regroup    re-binning (scan of the class counts, then a scatter into the new grouping) for
+//              most steps; a full Morton-key radix sort plus a permutation every full_every
+//              steps and when particles are first loaded
+//   deposit    per super-tile: CIC density of its particles into (TS+1)^3 nodes; interior nodes
+//              final, face and upper-halo nodes as 64-bit partials
+//   fixup      face nodes: own partial + the neighbours' halo partials
+//   R2C, Green, C2R (x3)
 #pragma once
 #include "common.cuh"
 #include "sort.cuh"
@@ -6,6 +20,8 @@
 #define PM_THREADS 256
 #define PUSH_THREADS 512
 #define DEP_THREADS 512
+#define BIN_CLASSES 128   // stride of the per-super-tile class arrays (>= 125)
+#define BIN_FAR 255       // class of a particle that moved more than 2 super-tiles
 
 // Views of the engine's device arrays handed to every kernel.
 struct StepArgs {
@@ -13,20 +29,28 @@ struct StepArgs {
   PeakClock* clocks;
   PeakStats* stats;
   SortSeg* sortseg;            // sort activity flags, written by the advance kernel
-  SortSeg* sortseg_full;       // the same for the full-key plan
-  const long long* tile_base;  // [npeaks + 1] prefix of tiles
-  const long long* ptile_base; // [npeaks + 1] prefix of push super-tiles
+  const long long* st_base;    // [npeaks + 1] prefix of super-tiles
   const long long* p_base;     // [npeaks + 1] prefix of particles
   const long long* mode_base;  // [npeaks + 1] prefix of Green blocks
+  const long long* face_base;  // [npeaks + 1] prefix of face nodes (nst * fc)
   int npeaks;
   int pad;
-  int4* pos[2];
-  float4* mom[2];
-  u32* keys_push;              // cell keys written by the push kernel (sort input); the
-                               // peak id, the high word of the 64-bit key, is the segment
+  int4* pos;                   // state, grouped by super-tile
+  float4* mom;
+  int4* tpos;                  // push output (same order as the input), regrouped into pos/mom
+  float4* tmom;
+  unsigned char* cls;          // per particle: re-binning class or BIN_FAR
+  u32* keys_push;              // Morton keys written by push / set_particles (sort input)
   const u32* keys_sorted;      // sort output keys
-  const u32* perm;             // sort output permutation (index into the current buffer)
-  u32* bstart;                 // bucket starts arena
+  const u32* perm;             // sort output permutation
+  u32* sstart[2];              // super-tile starts, two generations (clock.sbuf selects)
+  u32* counts;                 // [super-tile][BIN_CLASSES] class counts of the source
+  u32* lpre;                   // [super-tile][BIN_CLASSES] offset of a run in its destination
+  u32* far_count;              // [super-tile] far movers arriving (destination)
+  u32* far_fill;               // [super-tile] far movers placed so far
+  u32* totals;                 // [super-tile] particles arriving
+  long long* face;             // face partials
+  long long* halo;             // upper-halo partials
 };
 
 // Binary search: largest i in [0, n) with base[i] <= v.
@@ -40,13 +64,16 @@ __device__ __forceinline__ int pm_find(const long long* base, int n, long long v
 }
 
 int pm_kernels_init();  // kernel attributes; call once per device before launching
-size_t pm_deposit_smem(int TPmax);
-size_t pm_push_smem(int TPmax);
+size_t pm_deposit_smem(int TSmax);
+size_t pm_push_smem(int TSmax);
 
-void launch_push(const StepArgs& A, long long nptiles, size_t smem, cudaStream_t s);
+void launch_push(const StepArgs& A, long long nst, size_t smem, cudaStream_t s);
 void launch_advance(const StepArgs& A, cudaStream_t s);
-void launch_bucket_starts(const StepArgs& A, long long ntot, cudaStream_t s);
-void launch_deposit(const StepArgs& A, long long nptiles, size_t smem, double* rho64, cudaStream_t s);
+void launch_permute(const StepArgs& A, long long ntot, cudaStream_t s);
+void launch_st_starts(const StepArgs& A, long long ntot, cudaStream_t s);
+void launch_bin(const StepArgs& A, long long nst, cudaStream_t s);
+void launch_deposit(const StepArgs& A, long long nst, size_t smem, double* rho64, cudaStream_t s);
+void launch_fixup(const StepArgs& A, long long nface, double* rho64, cudaStream_t s);
 void launch_green(const StepArgs& A, long long nblocks, cudaStream_t s);
 
 // Host-requested per-peak operations.
@@ -54,6 +81,7 @@ void launch_reset_peak(const StepArgs& A, int pk, double a0, int mode, double pa
                        int max_steps, cudaStream_t s);
 void launch_set_particles(const StepArgs& A, int pk, const PeakDesc& P, const double* x, const double* p,
                           cudaStream_t s);
+void launch_reload(const StepArgs& A, const PeakDesc& P, cudaStream_t s);  // state -> loading area + keys
 void launch_get_particles(const StepArgs& A, int pk, const PeakDesc& P, double* x, double* p, double* acc,
                           double a_acc, cudaStream_t s);
 void launch_interp64(const double* F, const double* X, long long n, int N, double dx, double* out, cudaStream_t s);

@@ -42,8 +42,8 @@ def _ptr(t) -> int:
 
 
 class Engine:
-    def __init__(self, peaks, device: int = 0, bucket_sort: bool = True, graph: bool = True, full_every: int = 16,
-                 dynamic: bool = False):
+    def __init__(self, peaks, device: int = 0, graph: bool = True, full_every: int = 16, dynamic: bool = False,
+                 bucket_sort: bool = True):
         torch = _lib.require_cuda()
         self._torch = torch
         lib = _lib.load()
@@ -52,12 +52,13 @@ class Engine:
         arr = (_lib.PeakCfg * len(self.cfgs))(*[c.cstruct() for c in self.cfgs])
         h = C.c_void_p()
         self.device = int(device)
-        # bucket_sort: each step sorts only the bucket bits of the cell key (what the deposit and
-        # push group by); every `full_every` steps the whole key is sorted.  Results do not
-        # depend on the choice: the deposit is order-independent bit for bit.
+        # Particles are regrouped each step by re-binning into neighbouring super-tiles, and every
+        # `full_every` steps by a full Morton-key radix sort (bucket_sort=False: every step).
+        # Results do not depend on the choice: the deposit is order-independent bit for bit.
         # dynamic: served runs; no graph, and each step's FFTs cover only the slots in use.
-        flags = ((_lib.FLAG_BUCKET_SORT | (int(full_every) & 0xFF) << 8) if bucket_sort else 0) | \
-                (_lib.FLAG_GRAPH if graph else 0) | (_lib.FLAG_DYNAMIC if dynamic else 0)
+        every = int(full_every) if bucket_sort else 1
+        flags = ((max(1, min(every, 255)) & 0xFF) << 8) | (_lib.FLAG_GRAPH if graph else 0) | \
+                (_lib.FLAG_DYNAMIC if dynamic else 0)
         self.npeaks = len(self.cfgs)
         torch.cuda.set_device(self.device)
         check(lib.pm_engine_create(arr, len(self.cfgs), self.device, flags, C.byref(h)), "pm_engine_create")

@@ -33,6 +33,7 @@ def engine(cfgs, **kw):
     return Engine([PeakConfig(**c) for c in cfgs], **kw)
 
 
+
 def test_sort_matches_numpy_stable():
     from pbh_b200.engine import sort_u64
     rng = np.random.default_rng(0)
@@ -59,7 +60,7 @@ def test_interp64_matches_oracle(golden):
     assert rel(out, g["Fi"]) < 1e-14
 
 
-@pytest.mark.parametrize("N,Np,tile", [(32, 32, 8), (32, 32, 4), (16, 8, 2), (64, 64, 8), (64, 48, 0)])
+@pytest.mark.parametrize("N,Np,tile", [(32, 32, 16), (32, 32, 8), (16, 8, 4), (64, 64, 16), (64, 48, 0), (64, 64, 4)])
 def test_deposit_forces_same_positions(N, Np, tile):
     mesh, ic = recipe(N, Np)
     eng = engine([dict(N=N, Np=Np, L=1.0, tile=tile)])
@@ -115,7 +116,7 @@ def test_trajectory_50_steps(graph):
 def test_explicit_steps_match_oracle():
     N = 16
     mesh, ic = recipe(N, delta0=0.05, seed=3)
-    eng = engine([dict(N=N, Np=N, L=1.0, tile=8)])
+    eng = engine([dict(N=N, Np=N, L=1.0, tile=4)])
     eng.set_particles(0, ic["x"], ic["p"], 1.0)
     x0, p0 = [t.cpu().numpy() for t in eng.particles(0)]
     tr = O.Trajectory(mesh, x0, p0)
@@ -167,3 +168,45 @@ def test_batched_peaks_equal_alone():
         xm, pm = [t.cpu().numpy() for t in mix.particles(i)]
         assert np.array_equal(xa, xm) and np.array_equal(pa, pm), i
         assert np.array_equal(alone.delta(0).cpu().numpy(), mix.delta(i).cpu().numpy()), i
+
+
+def test_regroup_by_rebinning_equals_sorting_every_step():
+    """Re-binning between sorts and a full Morton sort every step give the same run, bit for bit."""
+    from pbh_b200._lib import SCHED_RATIO
+    N = 32
+    mesh, ic = recipe(N, delta0=0.05, seed=8)
+    runs = []
+    for every in (1, 16):
+        eng = engine([dict(N=N, Np=N, L=1.0, tile=8)], full_every=every)
+        eng.set_particles(0, ic["x"], ic["p"], 1.0, mode=SCHED_RATIO, param=RATIO_100, max_steps=20)
+        eng.run(22)
+        x, p = [t.cpu().numpy() for t in eng.particles(0)]
+        runs.append((x, p, eng.delta(0).cpu().numpy()))
+        s = eng.stats(0)
+        assert s.mass_defect == 0.0 and s.status == 0
+    for a, b in zip(runs[0], runs[1]):
+        assert np.array_equal(a, b)
+
+
+def test_fast_particles_cross_several_super_tiles():
+    """Particles that move more than two super-tiles in one step take the far-mover path."""
+    N, Np = 64, 16
+    mesh = O.Mesh(N, 1.0, Np)
+    rng = np.random.default_rng(21)
+    x = rng.uniform(0.0, 1.0, size=(Np ** 3, 3))
+    p = rng.normal(0.0, 1.0, size=(Np ** 3, 3)) * 8.0      # drifts of up to ~25 cells in one step
+    eng = engine([dict(N=N, Np=Np, L=1.0, tile=4)])       # 16 super-tiles per axis
+    eng.set_particles(0, x, p, 1.0)
+    x0, p0 = [t.cpu().numpy() for t in eng.particles(0)]
+    tr = O.Trajectory(mesh, x0, p0)
+    a = 1.0
+    for _ in range(2):
+        eng.step_explicit(0, a, 0.05)
+        a, delta = tr.step(a, 0.05)
+    xg, pg = [t.cpu().numpy() for t in eng.particles(0)]
+    moved = np.max(np.abs(wrap(xg - x0, 1.0))) / mesh.dx
+    assert moved > 12.0                                   # some particle crossed > 2 super-tiles
+    assert np.max(np.abs(wrap(xg - tr.x, 1.0))) / mesh.dx < TOL_POS_CELLS
+    assert rel(eng.delta(0).cpu().numpy(), O.density_contrast(mesh, xg)) < TOL_DENSITY
+    s = eng.stats(0)
+    assert s.mass_defect == 0.0 and s.status == 0

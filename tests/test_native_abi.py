@@ -23,29 +23,25 @@ def test_library_exports_header_symbols():
 
 
 def test_cell_key_layout_host_helper():
-    # [tile Morton | boundary mask | in-tile Morton] for N = 32, tile 8
+    # Morton code of the CIC cell, z in the lowest bit of each triple (codes nest by super-tile)
     import ctypes as C
     from pbh_b200 import _lib
     lib = _lib.load()
-    N, T = 32, 8
+    N = 32
     ix, iy, iz = np.meshgrid(np.arange(N), np.arange(N), np.arange(N), indexing="ij")
     cells = ((ix * N + iy) * N + iz).astype(np.int32).ravel()
     keys = np.empty(cells.size, np.uint32)
-    rc = lib.pm_cell_keys(cells.ctypes.data_as(C.c_void_p), cells.size, N, T, keys.ctypes.data_as(C.c_void_p))
+    rc = lib.pm_cell_keys(cells.ctypes.data_as(C.c_void_p), cells.size, N, 16, keys.ctypes.data_as(C.c_void_p))
     assert rc == 0
     assert len(np.unique(keys)) == cells.size             # a bijection of cells
-    local = keys & np.uint32((1 << 9) - 1)
-    mask = (keys >> np.uint32(9)) & np.uint32(7)
-    tile = keys >> np.uint32(12)
 
     def spread(v):
         out = np.zeros_like(v)
         for b in range(10):
             out |= ((v >> b) & 1) << (3 * b)
         return out
-    lx, ly, lz = ix.ravel() % T, iy.ravel() % T, iz.ravel() % T
-    assert np.array_equal(local, (spread(lx) << 2) | (spread(ly) << 1) | spread(lz))
-    m = (lx == T - 1) * 1 + (ly == T - 1) * 2 + (lz == T - 1) * 4
-    assert np.array_equal(mask, m)
-    tx, ty, tz = ix.ravel() // T, iy.ravel() // T, iz.ravel() // T
-    assert np.array_equal(tile, (spread(tx) << 2) | (spread(ty) << 1) | spread(tz))
+    ref = (spread(ix.ravel()) << 2) | (spread(iy.ravel()) << 1) | spread(iz.ravel())
+    assert np.array_equal(keys, ref.astype(np.uint32))
+    # the top bits are the Morton code of the 16^3 super-tile
+    st = (spread(ix.ravel() // 16) << 2) | (spread(iy.ravel() // 16) << 1) | spread(iz.ravel() // 16)
+    assert np.array_equal(keys >> np.uint32(12), st.astype(np.uint32))
