@@ -170,23 +170,21 @@ def run_reference(args):
 # ------------------------------------------------------------------------------ GPU side
 # Algorithmic bytes per launch of each kernel phase: n particles, N^3 cells,
 # M modes; fc/hc: face and halo partials.
-def algorithmic_bytes(phase: str, n: int, cells: int, modes: int, npass: int, partials: int = 0) -> float:
+def algorithmic_bytes(phase: str, n: int, cells: int, modes: int, npass: int) -> float:
     if phase == "push":        # read state 32, write state 32 + class 1, force grids 12 per cell
         return n * (32 + 32 + 1) + cells * 12.0
     if phase == "sort":        # full Morton sort (every 16th step), amortised in the step time
         return n * (4.0 + npass * 16.0 - 4.0) + n * 64.0
     if phase == "bin":         # read class 1 + state 32, write state 32
         return n * 65.0
-    if phase == "deposit":     # read positions 16, write delta 4 per cell and the 64-bit partials
-        return n * 16.0 + cells * 4.0 + partials * 8.0
-    if phase == "green":
+    if phase == "deposit":     # read positions 16, write delta 4 per cell (face/halo partials are overhead)
+        return n * 16.0 + cells * 4.0
+    if phase == "green":       # read the spectrum 8, write three gradient spectra 24 per mode
         return modes * 32.0
-    if phase == "fixup":
-        return partials * 8.0
     return 0.0
 
 
-PHASES = ["push", "advance", "sort", "bin", "deposit", "fixup", "r2c", "green", "c2r"]
+PHASES = ["push", "advance", "sort", "bin", "deposit", "r2c", "green", "c2r"]
 
 
 def run_ours(args):
@@ -249,10 +247,9 @@ def run_ours(args):
     ph = ens.timed_phases(16)                     # one sort step and fifteen re-binning steps
     cells = sum(s.N ** 3 for s in specs)
     modes = sum(s.N * s.N * (s.N // 2 + 1) for s in specs)
-    partials = sum((s.N // min(16, s.N)) ** 3 * 2 * (3 * min(16, s.N) ** 2 + 1) for s in specs)
     kern = {}
     for k, name in enumerate(PHASES):
-        b = algorithmic_bytes(name, n_step, cells, modes, npass, partials)
+        b = algorithmic_bytes(name, n_step, cells, modes, npass)
         if name == "sort":
             b /= 16.0
         kern[name] = {"ms": ph[k], "algorithmic_bytes": b, "gbs": (b / (ph[k] / 1e3) / 1e9) if b and ph[k] > 0 else None}
@@ -262,14 +259,14 @@ def run_ours(args):
         hbm_src = "measured"
     else:
         hbm, hbm_src = 6650.0, "fallback"
-    ours = {k: v for k, v in kern.items() if k in ("push", "sort", "bin", "deposit", "fixup", "green")}
+    ours = {k: v for k, v in kern.items() if k in ("push", "sort", "bin", "deposit", "green")}
     top = max(ours, key=lambda k: ours[k]["ms"])
     roofline = {"bound": "hbm", "kernel": top, "achieved": kern[top]["gbs"], "peak": hbm, "unit": "GB/s",
                 "frac": kern[top]["gbs"] / hbm, "traffic": None, "peak_source": hbm_src,
                 "per_kernel": {k: {"ms": round(v["ms"], 4), "gbs": None if v["gbs"] is None else round(v["gbs"], 1),
                                    "frac": None if v["gbs"] is None else round(v["gbs"] / hbm, 3)}
                                for k, v in kern.items()},
-                "fft_ms": round(ph[6] + ph[8], 4), "step_ms_ungraphed": round(float(ph.sum()), 4)}
+                "fft_ms": round(ph[5] + ph[7], 4), "step_ms_ungraphed": round(float(ph.sum()), 4)}
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",

@@ -55,7 +55,7 @@ struct pm_engine {
   int npeaks = 0;
   std::vector<PeakDesc> peaks;
   std::vector<MeshClass> classes;
-  long long ntot = 0, nst = 0, nface = 0, nmodeblk = 0, nsst = 0, nfc = 0, nhc = 0;
+  long long ntot = 0, nst = 0, nmodeblk = 0, nsst = 0, nfc = 0, nhc = 0;
   int TSmax = 0;
   size_t smem_dep = 0, smem_push = 0;
   // device arrays
@@ -65,7 +65,6 @@ struct pm_engine {
   long long* d_st_base = nullptr;
   long long* d_p_base = nullptr;
   long long* d_mode_base = nullptr;
-  long long* d_face_base = nullptr;
   int4* pos = nullptr;   // state, grouped by super-tile
   float4* mom = nullptr;
   int4* tpos = nullptr;  // push output / loading area
@@ -78,6 +77,8 @@ struct pm_engine {
   u32* lpre = nullptr;
   u32* far_count = nullptr;
   u32* far_fill = nullptr;
+  u32* arrive = nullptr;     // per super-tile face arrivals of the deposit (0 between steps)
+  u32* sort_gate = nullptr;  // one word: any peak sorts this step
   u32* totals = nullptr;
   long long* face = nullptr;
   long long* halo = nullptr;
@@ -96,7 +97,7 @@ struct pm_engine {
     A.st_base = d_st_base;
     A.p_base = d_p_base;
     A.mode_base = d_mode_base;
-    A.face_base = d_face_base;
+    A.arrive = arrive;
     A.npeaks = npeaks;
     A.pos = pos;
     A.mom = mom;
@@ -112,6 +113,7 @@ struct pm_engine {
     A.lpre = lpre;
     A.far_count = far_count;
     A.far_fill = far_fill;
+    A.sort_gate = sort_gate;
     A.totals = totals;
     A.face = face;
     A.halo = halo;
@@ -158,7 +160,8 @@ struct pm_engine {
   }
 
   // One step for every peak.  With ev != nullptr an event is recorded after each phase and the
-  // phase times (push, advance, sort, re-bin, deposit, fix-up, R2C, Green, C2R) are accumulated.
+  // phase times (push, advance, sort, re-bin, deposit with its face fix-up, R2C, Green, C2R) are
+  // accumulated.
   int launch_step(cudaEvent_t* ev = nullptr, double* phase_ms = nullptr) {
     const StepArgs A = args();
     int k = 0;
@@ -176,8 +179,6 @@ struct pm_engine {
     launch_bin(A, nst, stream);
     CU(mark());
     launch_deposit(A, nst, smem_dep, nullptr, stream);
-    CU(mark());
-    launch_fixup(A, nface, nullptr, stream);
     CU(mark());
     if ((r = fft_r2c())) return r;
     CU(mark());
@@ -242,9 +243,9 @@ struct pm_engine {
       cudaFree(c.force);
     }
     sort_plan_destroy(&sort);
-    void* bufs[] = {d_peaks, d_clocks, d_stats, d_st_base, d_p_base, d_mode_base, d_face_base, pos, mom, tpos,
+    void* bufs[] = {d_peaks, d_clocks, d_stats, d_st_base, d_p_base, d_mode_base, arrive, pos, mom, tpos,
                     tmom, cls, keys[0], keys[1], vals[0], vals[1], sstart[0], sstart[1], counts, lpre, far_count,
-                    far_fill, totals, face, halo};
+                    far_fill, sort_gate, totals, face, halo};
     for (void* b : bufs) cudaFree(b);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -260,7 +261,7 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   long long poff = 0, stb = 0, mb = 0, sso = 0, fo = 0, ho = 0;
   int TSmax = 1, max_bits = 0;
   const int full_every = std::max(1, (E->flags >> 8) & 0xFF ? (E->flags >> 8) & 0xFF : 16);
-  std::vector<long long> st_base(npeaks + 1), p_base(npeaks + 1), mode_base(npeaks + 1), face_base(npeaks + 1);
+  std::vector<long long> st_base(npeaks + 1), p_base(npeaks + 1), mode_base(npeaks + 1);
   for (int i = 0; i < npeaks; ++i) {
     const pm_peak_cfg& c = cfg[i];
     const int l2 = ilog2(c.N);
@@ -307,7 +308,6 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
     st_base[i] = stb;
     p_base[i] = poff;
     mode_base[i] = mb;
-    face_base[i] = fo;
     poff += P.n;
     stb += P.nst;
     sso += P.nst + 1;
@@ -326,11 +326,9 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   st_base[npeaks] = stb;
   p_base[npeaks] = poff;
   mode_base[npeaks] = mb;
-  face_base[npeaks] = fo;
   if (poff >= (1LL << 32)) return -2005;
   E->ntot = poff;
   E->nst = stb;
-  E->nface = fo;
   E->nmodeblk = mb;
   E->nsst = sso;
   E->nfc = fo;
@@ -403,7 +401,6 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   if ((r = E->alloc(&E->d_st_base, npeaks + 1))) return r;
   if ((r = E->alloc(&E->d_p_base, npeaks + 1))) return r;
   if ((r = E->alloc(&E->d_mode_base, npeaks + 1))) return r;
-  if ((r = E->alloc(&E->d_face_base, npeaks + 1))) return r;
   if ((r = E->alloc(&E->pos, E->ntot))) return r;
   if ((r = E->alloc(&E->mom, E->ntot))) return r;
   if ((r = E->alloc(&E->tpos, E->ntot))) return r;
@@ -418,6 +415,8 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   if ((r = E->alloc(&E->lpre, E->nst * BIN_CLASSES))) return r;
   if ((r = E->alloc(&E->far_count, E->nst))) return r;
   if ((r = E->alloc(&E->far_fill, E->nst))) return r;
+  if ((r = E->alloc(&E->arrive, E->nst))) return r;
+  if ((r = E->alloc(&E->sort_gate, 1))) return r;
   if ((r = E->alloc(&E->totals, E->nst))) return r;
   if ((r = E->alloc(&E->face, E->nfc))) return r;
   if ((r = E->alloc(&E->halo, E->nhc))) return r;
@@ -425,7 +424,6 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   CU(cudaMemcpy(E->d_st_base, st_base.data(), sizeof(long long) * (npeaks + 1), cudaMemcpyHostToDevice));
   CU(cudaMemcpy(E->d_p_base, p_base.data(), sizeof(long long) * (npeaks + 1), cudaMemcpyHostToDevice));
   CU(cudaMemcpy(E->d_mode_base, mode_base.data(), sizeof(long long) * (npeaks + 1), cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(E->d_face_base, face_base.data(), sizeof(long long) * (npeaks + 1), cudaMemcpyHostToDevice));
   std::vector<PeakClock> clocks(npeaks);
   for (auto& c : clocks) {
     c = PeakClock{};
@@ -440,6 +438,8 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   CU(cudaMemset(E->tmom, 0, sizeof(float4) * E->ntot));
   CU(cudaMemset(E->far_count, 0, sizeof(u32) * E->nst));
   CU(cudaMemset(E->far_fill, 0, sizeof(u32) * E->nst));
+  CU(cudaMemset(E->arrive, 0, sizeof(u32) * E->nst));
+  CU(cudaMemset(E->sort_gate, 0, sizeof(u32)));
   for (int b = 0; b < 2; ++b) CU(cudaMemset(E->sstart[b], 0, sizeof(u32) * E->nsst));
 
   // Sort plan: one segment per peak over the whole Morton key (sorted at priming and every
@@ -451,6 +451,7 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   }
   const int np = (max_bits + SORT_MAX_BITS - 1) / SORT_MAX_BITS;
   if ((r = sort_plan_create(&E->sort, segs.data(), npeaks, np, max_bits))) return r;
+  E->sort.gate = E->sort_gate;
   E->bytes += (long long)E->sort.ntiles * 8 * (1LL << E->sort.bits);
   E->sort_result = np & 1;
   CU(cudaDeviceSynchronize());
@@ -667,7 +668,6 @@ int pm_get_counts(pm_engine* e, int peak, double* counts) {
   CU(cudaMemcpy(e->d_stats + peak, &st, sizeof(PeakStats), cudaMemcpyHostToDevice));
   // Same kernels with the extra float64 output; delta is rewritten with identical values.
   launch_deposit(e->args(), e->nst, e->smem_dep, counts, e->stream);
-  launch_fixup(e->args(), e->nface, counts, e->stream);
   CU(cudaGetLastError());
   CU(cudaStreamSynchronize(e->stream));
   CU(cudaMemcpy(e->d_clocks, all.data(), sizeof(PeakClock) * e->npeaks, cudaMemcpyHostToDevice));

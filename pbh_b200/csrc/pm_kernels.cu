@@ -1,11 +1,29 @@
 // Step kernels of the pm3d engine: push (CIC gather + kicks + drift, re-binning class),
 // clock advance, regrouping (re-binning scatter, or radix-sort permutation), halo-exchange CIC
 // deposit with its face fix-up, Green's function + gradient, and particle I/O.
+#include <algorithm>
+
 #include "pm_kernels.cuh"
 
 namespace {
 
 constexpr double kTwoPi = 6.283185307179586476925286766559;
+
+// Shared-memory layout of a (TS+1)^3 node patch: node (lx, ly, lz) at lx*PS + ly*RS + lz.  The
+// strides are padded so that the 8 corners read (push) or added to (deposit) by a warp of 32
+// Morton-consecutive cells fall in 32 distinct banks, and so that rows start on 16 bytes
+// (asynchronous 16-byte copies).
+__host__ __device__ constexpr int patch_rs(int TS) { return TS == 4 ? 8 : TS == 8 ? 12 : 20; }
+__host__ __device__ constexpr int patch_ps(int TS) { return TS == 4 ? 44 : TS == 8 ? 112 : 368; }
+__host__ __device__ constexpr int patch_size(int TS) { return (TS + 1) * patch_ps(TS); }
+
+__device__ __forceinline__ void cp_async16(unsigned dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async4(unsigned dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 __device__ __forceinline__ u32 lanemask_le() {
   u32 m;
@@ -69,7 +87,7 @@ template <int T>
 __device__ __forceinline__ void push_one(const StepArgs& A, const PeakDesc& P, const float* __restrict__ s_f,
                                          const PushCoef& K, int sx, int sy, int sz, int4 ps, float4 m, long long j,
                                          u32* s_cnt, bool& bad) {
-  constexpr int T1 = T + 1, T13 = T1 * T1 * T1;
+  constexpr int RS = patch_rs(T), PS = patch_ps(T), CS = patch_size(T);
   const int N = P.N, l2 = P.log2N;
   const int ix = ps.x >> (2 * l2), iy = (ps.x >> l2) & (N - 1), iz = ps.x & (N - 1);
   const int lx = ix - sx * T, ly = iy - sy * T, lz = iz - sz * T;
@@ -79,24 +97,24 @@ __device__ __forceinline__ void push_one(const StepArgs& A, const PeakDesc& P, c
   }
   float fx = __int_as_float(ps.y), fy = __int_as_float(ps.z), fz = __int_as_float(ps.w);
   const float gx = 1.0f - fx, gy = 1.0f - fy, gz = 1.0f - fz;
-  const int o = (lx * T1 + ly) * T1 + lz;
+  const int o = lx * PS + ly * RS + lz;
   float ax = 0.f, ay = 0.f, az = 0.f;
-#define PM_CORNER(w, d)                        \
-  {                                            \
-    const float w_ = (w);                      \
-    ax = fmaf(w_, s_f[o + (d)], ax);           \
-    ay = fmaf(w_, s_f[T13 + o + (d)], ay);     \
-    az = fmaf(w_, s_f[2 * T13 + o + (d)], az); \
+#define PM_CORNER(w, d)                       \
+  {                                           \
+    const float w_ = (w);                     \
+    ax = fmaf(w_, s_f[o + (d)], ax);          \
+    ay = fmaf(w_, s_f[CS + o + (d)], ay);     \
+    az = fmaf(w_, s_f[2 * CS + o + (d)], az); \
   }
   const float w00 = gx * gy, w01 = gx * fy, w10 = fx * gy, w11 = fx * fy;
   PM_CORNER(w00 * gz, 0)
   PM_CORNER(w00 * fz, 1)
-  PM_CORNER(w01 * gz, T1)
-  PM_CORNER(w01 * fz, T1 + 1)
-  PM_CORNER(w10 * gz, T1 * T1)
-  PM_CORNER(w10 * fz, T1 * T1 + 1)
-  PM_CORNER(w11 * gz, T1 * T1 + T1)
-  PM_CORNER(w11 * fz, T1 * T1 + T1 + 1)
+  PM_CORNER(w01 * gz, RS)
+  PM_CORNER(w01 * fz, RS + 1)
+  PM_CORNER(w10 * gz, PS)
+  PM_CORNER(w10 * fz, PS + 1)
+  PM_CORNER(w11 * gz, PS + RS)
+  PM_CORNER(w11 * fz, PS + RS + 1)
 #undef PM_CORNER
   ax *= K.gscale;
   ay *= K.gscale;
@@ -149,20 +167,29 @@ __device__ __forceinline__ void push_one(const StepArgs& A, const PeakDesc& P, c
 template <int T>
 __device__ __forceinline__ void push_super(const StepArgs& A, const PeakDesc& P, const PeakClock& C, int pk, u32 st,
                                            float* s_f, u32* s_cnt, const PushCoef& K) {
-  constexpr int T1 = T + 1, T12 = T1 * T1, T13 = T1 * T1 * T1;
+  constexpr int T1 = T + 1, RS = patch_rs(T), PS = patch_ps(T), CS = patch_size(T);
+  constexpr int CH = T / 4 + 1;  // per patch row: T/4 copies of 16 bytes, then the (wrapped) last node
   const int N = P.N;
   const int sx = pm_compact3(st >> 2), sy = pm_compact3(st >> 1), sz = pm_compact3(st);
   const long long N3 = (long long)N * N * N;
   const u32* ss = sst(A, C.sbuf) + P.sst_off;
   const long long b = ss[st], e = ss[st + 1];
   if (b < e) {
-    for (int i = threadIdx.x; i < 3 * T13; i += PUSH_THREADS) {
-      const int comp = i / T13, r = i - comp * T13;
-      const int lx = r / T12, r2 = r - lx * T12;
-      const int ly = r2 / T1, lz = r2 - ly * T1;
-      const int gx = (sx * T + lx) & (N - 1), gy = (sy * T + ly) & (N - 1), gz = (sz * T + lz) & (N - 1);
-      s_f[i] = __ldg(P.force + comp * N3 + ((long long)gx * N + gy) * N + gz);
+    // Asynchronous copies of the patch rows (every row start is 16-byte aligned on both sides:
+    // z0 = sz*T is a multiple of 4 and the grids are 256-byte aligned).
+    const unsigned sbase = (unsigned)__cvta_generic_to_shared(s_f);
+    const int z0 = sz * T, zl = (sz * T + T) & (N - 1);
+    for (int i = threadIdx.x; i < 3 * T1 * T1 * CH; i += PUSH_THREADS) {
+      const int row = i / CH, part = i - row * CH;
+      const int comp = row / (T1 * T1), r = row - comp * (T1 * T1);
+      const int lx = r / T1, ly = r - lx * T1;
+      const int gx = (sx * T + lx) & (N - 1), gy = (sy * T + ly) & (N - 1);
+      const float* src = P.force + comp * N3 + ((long long)gx * N + gy) * N;
+      const unsigned dst = sbase + 4u * (unsigned)(comp * CS + lx * PS + ly * RS + part * 4);
+      if (part < T / 4) cp_async16(dst, src + z0 + part * 4);
+      else cp_async4(dst, src + zl);
     }
+    cp_async_wait_all();
   }
   __syncthreads();
   bool bad = false;
@@ -200,7 +227,7 @@ __device__ __forceinline__ void push_super(const StepArgs& A, const PeakDesc& P,
 }
 
 __global__ void __launch_bounds__(PUSH_THREADS, 2) k_push(StepArgs A) {
-  extern __shared__ float s_f[];
+  extern __shared__ __align__(16) float s_f[];
   __shared__ PushCoef s_k;
   __shared__ u32 s_cnt[BIN_CLASSES];
   const TileRef tr = find_tile(A.st_base, A.npeaks);
@@ -232,6 +259,7 @@ __global__ void __launch_bounds__(PUSH_THREADS, 2) k_push(StepArgs A) {
 // Clock advance (one thread per peak): applies the step that the push kernel just made,
 // selects the next step size, whether this step regroups by sort, and which peaks re-deposit.
 __global__ void k_advance(StepArgs A) {
+  int any_sort = 0;
   for (int pk = threadIdx.x; pk < A.npeaks; pk += blockDim.x) {
     PeakClock c = A.clocks[pk];
     const PeakDesc& P = A.peaks[pk];
@@ -287,40 +315,47 @@ __global__ void k_advance(StepArgs A) {
     c.dep = dep;
     A.clocks[pk] = c;
     A.sortseg[pk].active = dep && c.sortstep;
+    any_sort |= dep && c.sortstep;
     if (dep) {
       A.stats[pk].max_fix = 0;
       A.stats[pk].mass_defect = 0;
     }
   }
+  any_sort = __syncthreads_or(any_sort);
+  if (threadIdx.x == 0) *A.sort_gate = any_sort ? 1u : 0u;
 }
 
 // ------------------------------------------------------------------------------------------
 // Regrouping by sort (priming and every full_every steps): gather the temporary state in
 // sorted order and find the super-tile starts in the sorted keys.
+// Both are grid-stride loops over a grid of a few CTAs per SM and return at once on the steps
+// where no peak sorts.
 __global__ void k_permute(StepArgs A, long long ntot) {
-  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= ntot) return;
-  const int pk = pm_find(A.p_base, A.npeaks, j);
-  const PeakClock& C = A.clocks[pk];
-  if (!(C.dep && C.sortstep)) return;
-  const u32 q = A.perm[j];
-  A.pos[j] = A.tpos[q];
-  A.mom[j] = A.tmom[q];
+  if (*A.sort_gate == 0u) return;
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < ntot; j += (long long)gridDim.x * blockDim.x) {
+    const int pk = pm_find(A.p_base, A.npeaks, j);
+    const PeakClock& C = A.clocks[pk];
+    if (!(C.dep && C.sortstep)) continue;
+    const u32 q = A.perm[j];
+    A.pos[j] = A.tpos[q];
+    A.mom[j] = A.tmom[q];
+  }
 }
 
 __global__ void k_st_starts(StepArgs A, long long ntot) {
-  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= ntot) return;
-  const int pk = pm_find(A.p_base, A.npeaks, j);
-  const PeakClock& C = A.clocks[pk];
-  if (!(C.dep && C.sortstep)) return;
-  const PeakDesc& P = A.peaks[pk];
-  u32* ss = sst(A, C.sbuf) + P.sst_off;
-  const int b = (int)(A.keys_sorted[j] >> P.st_shift);
-  const int bprev = j == P.p_off ? -1 : (int)(A.keys_sorted[j - 1] >> P.st_shift);
-  for (int bb = bprev + 1; bb <= b; ++bb) ss[bb] = (u32)j;
-  if (j == P.p_off + P.n - 1)
-    for (int bb = b + 1; bb <= P.nst; ++bb) ss[bb] = (u32)(P.p_off + P.n);
+  if (*A.sort_gate == 0u) return;
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < ntot; j += (long long)gridDim.x * blockDim.x) {
+    const int pk = pm_find(A.p_base, A.npeaks, j);
+    const PeakClock& C = A.clocks[pk];
+    if (!(C.dep && C.sortstep)) continue;
+    const PeakDesc& P = A.peaks[pk];
+    u32* ss = sst(A, C.sbuf) + P.sst_off;
+    const int b = (int)(A.keys_sorted[j] >> P.st_shift);
+    const int bprev = j == P.p_off ? -1 : (int)(A.keys_sorted[j - 1] >> P.st_shift);
+    for (int bb = bprev + 1; bb <= b; ++bb) ss[bb] = (u32)j;
+    if (j == P.p_off + P.n - 1)
+      for (int bb = b + 1; bb <= P.nst; ++bb) ss[bb] = (u32)(P.p_off + P.n);
+  }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -447,7 +482,13 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_bin_scatter(StepArgs A) {
 // overflow within a chunk of fewer than 2048 particles, and is folded into a 64-bit register
 // accumulator after every chunk.  Interior nodes are then final and written as FP32
 // delta = S/n_mean - 1; nodes on the three lower faces (which neighbours also reach) and on the
-// upper halo (which belongs to the neighbours) are written as 64-bit partials for the fix-up.
+// upper halo (which belongs to the neighbours) are written as 64-bit partials.
+//
+// Face fix-up in the same launch: super-tile Y's face nodes are complete once Y and its 7 lower
+// neighbours have written their partials.  Every CTA, after its partials, counts itself in at
+// Y = S + o for the 8 offsets o in {0,1}^3 (a bijection per o, so each Y is counted exactly 8
+// times per step); the CTA that arrives 8th finishes Y's faces (own partial + the neighbours'
+// halo partials, still in L2) and clears the counter.  No CTA waits on another.
 // Integer sums make the result independent of particle order, bit for bit; no float atomics.
 __device__ __forceinline__ int face_index(int lx, int ly, int lz, int T) {
   if (lx == 0) return ly * T + lz;
@@ -459,20 +500,71 @@ __device__ __forceinline__ int halo_index(int lx, int ly, int lz, int T) {
   if (ly == T) return (T + 1) * (T + 1) + lx * (T + 1) + lz;
   return (T + 1) * (T + 1) + T * (T + 1) + lx * T + ly;
 }
+// Inverse of face_index.
+template <int T>
+__device__ __forceinline__ void face_coords(int f, int& lx, int& ly, int& lz) {
+  if (f < T * T) {
+    lx = 0;
+    ly = f / T;
+    lz = f % T;
+  } else if (f < T * T + (T - 1) * T) {
+    const int r = f - T * T;
+    lx = 1 + r / T;
+    ly = 0;
+    lz = r % T;
+  } else {
+    const int r = f - T * T - (T - 1) * T;
+    lx = 1 + r / (T - 1);
+    ly = 1 + r % (T - 1);
+    lz = 0;
+  }
+}
+
+// Finish the face nodes of super-tile Y (whole CTA).  Adds to the caller's statistics.
+template <int TS>
+__device__ __forceinline__ void fixup_faces(const StepArgs& A, const PeakDesc& P, u32 Y, double* rho64,
+                                            long long& dsum, long long& smax) {
+  constexpr int FC = TS * TS * TS - (TS - 1) * (TS - 1) * (TS - 1);
+  const int NS = P.NS, N = P.N;
+  const int sx = pm_compact3(Y >> 2), sy = pm_compact3(Y >> 1), sz = pm_compact3(Y);
+  const long long* face = A.face + P.face_off + (long long)Y * FC;
+  const long long* halo = A.halo + P.halo_off;
+  for (int f = threadIdx.x; f < FC; f += DEP_THREADS) {
+    int lx, ly, lz;
+    face_coords<TS>(f, lx, ly, lz);
+    long long S = __ldcg(face + f);
+    const int zmask = (lx == 0 ? 1 : 0) | (ly == 0 ? 2 : 0) | (lz == 0 ? 4 : 0);
+#pragma unroll
+    for (int o = 1; o < 8; ++o) {
+      if (o & ~zmask) continue;
+      const int ox = o & 1, oy = (o >> 1) & 1, oz = (o >> 2) & 1;
+      const u32 sn = pm_morton3((sx - ox) & (NS - 1), (sy - oy) & (NS - 1), (sz - oz) & (NS - 1));
+      S += __ldcg(halo + (long long)sn * P.hc + halo_index(lx + TS * ox, ly + TS * oy, lz + TS * oz, TS));
+    }
+    const long long Dv = S - P.n_mean_fix;
+    const long long node = ((long long)(sx * TS + lx) * N + (sy * TS + ly)) * N + (sz * TS + lz);
+    P.delta[node] = (float)((double)Dv * P.inv_fix_nmean);
+    if (rho64) rho64[node] = (double)S * (1.0 / (double)PM_FIX_ONE);
+    dsum += Dv;
+    smax = S > smax ? S : smax;
+  }
+}
 
 template <int TS>
 __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc& P, const PeakClock& C, int pk,
                                               u32 st, u32* smem, double* rho64) {
   constexpr int T1 = TS + 1, NN = T1 * T1 * T1;
+  constexpr int RS = patch_rs(TS), PS = patch_ps(TS), SZ = patch_size(TS);
   constexpr int NPT = (NN + DEP_THREADS - 1) / DEP_THREADS;  // nodes per thread
   u32* acc_hi = smem;
-  u32* acc_lo = smem + NN;
+  u32* acc_lo = smem + SZ;
   __shared__ long long s_red[DEP_THREADS / 32];
   __shared__ long long s_max[DEP_THREADS / 32];
+  __shared__ u32 s_last;
   const int N = P.N, l2 = P.log2N;
   const int sx = pm_compact3(st >> 2), sy = pm_compact3(st >> 1), sz = pm_compact3(st);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int i = threadIdx.x; i < 2 * NN; i += DEP_THREADS) smem[i] = 0u;
+  for (int i = threadIdx.x; i < 2 * SZ; i += DEP_THREADS) smem[i] = 0u;
   const u32* ss = sst(A, C.sbuf) + P.sst_off;
   const long long b = ss[st], e = ss[st + 1];
   const long long total = e - b;
@@ -537,7 +629,7 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
         tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
       }
       if (in && tail) {
-        const int nb = (lx * T1 + ly) * T1 + lz;
+        const int nb = lx * PS + ly * RS + lz;
 #define PM_ADD(off, W)                                                   \
   {                                                                      \
     atomicAdd(&acc_hi[nb + (off)], (u32)(int)((long long)(W) >> 20));   \
@@ -545,12 +637,12 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
   }
         PM_ADD(0, W0)
         PM_ADD(1, W1)
-        PM_ADD(T1, W2)
-        PM_ADD(T1 + 1, W3)
-        PM_ADD(T1 * T1, W4)
-        PM_ADD(T1 * T1 + 1, W5)
-        PM_ADD(T1 * T1 + T1, W6)
-        PM_ADD(T1 * T1 + T1 + 1, W7)
+        PM_ADD(RS, W2)
+        PM_ADD(RS + 1, W3)
+        PM_ADD(PS, W4)
+        PM_ADD(PS + 1, W5)
+        PM_ADD(PS + RS, W6)
+        PM_ADD(PS + RS + 1, W7)
 #undef PM_ADD
       }
     }
@@ -560,9 +652,10 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
       for (int q = 0; q < NPT; ++q) {
         const int node = threadIdx.x + q * DEP_THREADS;
         if (node < NN) {
-          acc[q] += (u64)((long long)(int)acc_hi[node] * (1LL << 20)) + (u64)acc_lo[node];
-          acc_hi[node] = 0u;
-          acc_lo[node] = 0u;
+          const int ad = (node / (T1 * T1)) * PS + ((node / T1) % T1) * RS + node % T1;
+          acc[q] += (u64)((long long)(int)acc_hi[ad] * (1LL << 20)) + (u64)acc_lo[ad];
+          acc_hi[ad] = 0u;
+          acc_lo[ad] = 0u;
         }
       }
       __syncthreads();
@@ -593,6 +686,28 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
       }
     }
   }
+  // Count this tile in at the 8 super-tiles whose faces it feeds; finish those it completes.
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = 0u;
+  __syncthreads();
+  const int NS = P.NS;
+  if (threadIdx.x < 8) {
+    const int o = threadIdx.x;
+    const u32 Y = pm_morton3((sx + (o & 1)) & (NS - 1), (sy + ((o >> 1) & 1)) & (NS - 1), (sz + ((o >> 2) & 1)) & (NS - 1));
+    if (atomicAdd(&A.arrive[P.st_base + Y], 1u) == 7u) atomicOr(&s_last, 1u << o);
+  }
+  __syncthreads();
+  const u32 last = s_last;
+  if (last) {
+    __threadfence();
+    for (int o = 0; o < 8; ++o) {
+      if (!((last >> o) & 1u)) continue;
+      const u32 Y = pm_morton3((sx + (o & 1)) & (NS - 1), (sy + ((o >> 1) & 1)) & (NS - 1), (sz + ((o >> 2) & 1)) & (NS - 1));
+      fixup_faces<TS>(A, P, Y, rho64, dsum, smax);
+      if (threadIdx.x == 0) A.arrive[P.st_base + Y] = 0u;  // all 8 arrivals of this step are in
+    }
+  }
   for (int d = 16; d > 0; d >>= 1) {
     dsum += __shfl_xor_sync(0xffffffffu, dsum, d);
     const long long om = __shfl_xor_sync(0xffffffffu, smax, d);
@@ -616,7 +731,7 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
   }
 }
 
-__global__ void __launch_bounds__(DEP_THREADS) k_deposit(StepArgs A, double* rho64) {
+__global__ void __launch_bounds__(DEP_THREADS, 2) k_deposit(StepArgs A, double* rho64) {
   extern __shared__ __align__(16) u32 s_dep[];
   const TileRef tr = find_tile(A.st_base, A.npeaks);
   const PeakClock C = A.clocks[tr.pk];
@@ -626,77 +741,6 @@ __global__ void __launch_bounds__(DEP_THREADS) k_deposit(StepArgs A, double* rho
     case 4: deposit_super<4>(A, P, C, tr.pk, (u32)tr.t, s_dep, rho64); break;
     case 8: deposit_super<8>(A, P, C, tr.pk, (u32)tr.t, s_dep, rho64); break;
     default: deposit_super<16>(A, P, C, tr.pk, (u32)tr.t, s_dep, rho64); break;
-  }
-}
-
-// Face fix-up: a node on a lower face of super-tile S also receives particles of the
-// neighbours below it; their shares were written as those neighbours' upper-halo partials.
-__device__ __forceinline__ void face_coords(int f, int T, int& lx, int& ly, int& lz) {
-  if (f < T * T) {
-    lx = 0;
-    ly = f / T;
-    lz = f % T;
-  } else if (f < T * T + (T - 1) * T) {
-    const int r = f - T * T;
-    lx = 1 + r / T;
-    ly = 0;
-    lz = r % T;
-  } else {
-    const int r = f - T * T - (T - 1) * T;
-    lx = 1 + r / (T - 1);
-    ly = 1 + r % (T - 1);
-    lz = 0;
-  }
-}
-
-__global__ void __launch_bounds__(PM_THREADS) k_fixup(StepArgs A, long long nface, double* rho64) {
-  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool inr = g < nface;
-  int pk = 0;
-  bool act = false;
-  long long Dv = 0, S = 0;
-  if (inr) {
-    pk = pm_find(A.face_base, A.npeaks, g);
-    act = A.clocks[pk].dep != 0;
-  }
-  if (act) {
-    const PeakDesc& P = A.peaks[pk];
-    const int T = P.TS, NS = P.NS, N = P.N;
-    const long long local = g - A.face_base[pk];
-    const u32 st = (u32)(local / P.fc);
-    const int f = (int)(local - (long long)st * P.fc);
-    int lx, ly, lz;
-    face_coords(f, T, lx, ly, lz);
-    const int sx = pm_compact3(st >> 2), sy = pm_compact3(st >> 1), sz = pm_compact3(st);
-    S = A.face[P.face_off + local];
-    const int zmask = (lx == 0 ? 1 : 0) | (ly == 0 ? 2 : 0) | (lz == 0 ? 4 : 0);
-    for (int o = 1; o < 8; ++o) {
-      if (o & ~zmask) continue;
-      const int ox = o & 1, oy = (o >> 1) & 1, oz = (o >> 2) & 1;
-      const u32 sn = pm_morton3((sx - ox) & (NS - 1), (sy - oy) & (NS - 1), (sz - oz) & (NS - 1));
-      S += A.halo[P.halo_off + (long long)sn * P.hc + halo_index(lx + T * ox, ly + T * oy, lz + T * oz, T)];
-    }
-    Dv = S - P.n_mean_fix;
-    const long long node = ((long long)(sx * T + lx) * N + (sy * T + ly)) * N + (sz * T + lz);
-    P.delta[node] = (float)((double)Dv * P.inv_fix_nmean);
-    if (rho64) rho64[node] = (double)S * (1.0 / (double)PM_FIX_ONE);
-  }
-  // Statistics: one atomic per warp when the warp covers a single peak.
-  const int pk0 = __shfl_sync(0xffffffffu, pk, 0);
-  if (__all_sync(0xffffffffu, pk == pk0)) {
-    long long ds = act ? Dv : 0, sm = act ? S : 0;
-    for (int d = 16; d > 0; d >>= 1) {
-      ds += __shfl_xor_sync(0xffffffffu, ds, d);
-      const long long om = __shfl_xor_sync(0xffffffffu, sm, d);
-      sm = om > sm ? om : sm;
-    }
-    if ((threadIdx.x & 31) == 0 && inr && A.clocks[pk0].dep) {
-      atomicAdd((unsigned long long*)&A.stats[pk0].mass_defect, (unsigned long long)ds);
-      atomicMax(&A.stats[pk0].max_fix, (u64)(sm > 0 ? sm : 0));
-    }
-  } else if (act) {
-    atomicAdd((unsigned long long*)&A.stats[pk].mass_defect, (unsigned long long)Dv);
-    atomicMax(&A.stats[pk].max_fix, (u64)(S > 0 ? S : 0));
   }
 }
 
@@ -907,8 +951,9 @@ __global__ void k_interp64(const double* __restrict__ F, const double* __restric
 
 }  // namespace
 
-size_t pm_deposit_smem(int TSmax) { return sizeof(u32) * 2 * (size_t)(TSmax + 1) * (TSmax + 1) * (TSmax + 1); }
-size_t pm_push_smem(int TSmax) { return sizeof(float) * 3 * (size_t)(TSmax + 1) * (TSmax + 1) * (TSmax + 1); }
+// Dynamic shared memory of the largest super-tile in use (the smaller ones fit inside).
+size_t pm_deposit_smem(int TSmax) { return sizeof(u32) * 2 * (size_t)patch_size(TSmax); }
+size_t pm_push_smem(int TSmax) { return sizeof(float) * 3 * (size_t)patch_size(TSmax); }
 
 int pm_kernels_init() {
   cudaError_t e = cudaFuncSetAttribute(k_push, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
@@ -918,15 +963,27 @@ int pm_kernels_init() {
 
 static unsigned nb(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 
+// Grid of a grid-stride kernel: enough CTAs to fill every SM `per_sm` times, fewer for small n.
+static unsigned stride_grid(long long n, int t, int per_sm) {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+      sms = 148;
+  }
+  const long long g = std::min<long long>((long long)nb(n, t), (long long)sms * per_sm);
+  return (unsigned)std::max<long long>(g, 1);
+}
+
 void launch_push(const StepArgs& A, long long nst, size_t smem, cudaStream_t s) {
   k_push<<<(unsigned)nst, PUSH_THREADS, smem, s>>>(A);
 }
 void launch_advance(const StepArgs& A, cudaStream_t s) { k_advance<<<1, 256, 0, s>>>(A); }
 void launch_permute(const StepArgs& A, long long ntot, cudaStream_t s) {
-  k_permute<<<nb(ntot, PM_THREADS), PM_THREADS, 0, s>>>(A, ntot);
+  k_permute<<<stride_grid(ntot, PM_THREADS, 8), PM_THREADS, 0, s>>>(A, ntot);
 }
 void launch_st_starts(const StepArgs& A, long long ntot, cudaStream_t s) {
-  k_st_starts<<<nb(ntot, PM_THREADS), PM_THREADS, 0, s>>>(A, ntot);
+  k_st_starts<<<stride_grid(ntot, PM_THREADS, 8), PM_THREADS, 0, s>>>(A, ntot);
 }
 void launch_bin(const StepArgs& A, long long nst, cudaStream_t s) {
   k_bin_scan1<<<(unsigned)nst, BIN_CLASSES, 0, s>>>(A);
@@ -935,9 +992,6 @@ void launch_bin(const StepArgs& A, long long nst, cudaStream_t s) {
 }
 void launch_deposit(const StepArgs& A, long long nst, size_t smem, double* rho64, cudaStream_t s) {
   k_deposit<<<(unsigned)nst, DEP_THREADS, smem, s>>>(A, rho64);
-}
-void launch_fixup(const StepArgs& A, long long nface, double* rho64, cudaStream_t s) {
-  k_fixup<<<nb(nface, PM_THREADS), PM_THREADS, 0, s>>>(A, nface, rho64);
 }
 void launch_green(const StepArgs& A, long long nblocks, cudaStream_t s) {
   k_green<<<(unsigned)nblocks, PM_THREADS, 0, s>>>(A);

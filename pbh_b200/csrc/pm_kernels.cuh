@@ -10,8 +10,9 @@
 //              most steps; a full Morton-key radix sort plus a permutation every full_every
 //              steps and when particles are first loaded
 //   deposit    per super-tile: CIC density of its particles into (TS+1)^3 nodes; interior nodes
-//              final, face and upper-halo nodes as 64-bit partials
-//   fixup      face nodes: own partial + the neighbours' halo partials
+//              final, face and upper-halo nodes as 64-bit partials; the last of the 8 tiles
+//              that feed a super-tile's lower faces finishes them (own partial + neighbours'
+//              halo partials) in the same launch
 //   R2C, Green, C2R (x3)
 #pragma once
 #include "common.cuh"
@@ -29,10 +30,11 @@ struct StepArgs {
   PeakClock* clocks;
   PeakStats* stats;
   SortSeg* sortseg;            // sort activity flags, written by the advance kernel
+  u32* sort_gate;              // 1 when any peak regroups by sort this step (advance kernel)
   const long long* st_base;    // [npeaks + 1] prefix of super-tiles
   const long long* p_base;     // [npeaks + 1] prefix of particles
   const long long* mode_base;  // [npeaks + 1] prefix of Green blocks
-  const long long* face_base;  // [npeaks + 1] prefix of face nodes (nst * fc)
+  u32* arrive;                 // [super-tile] deposits counted in at its faces this step (0..8)
   int npeaks;
   int pad;
   int4* pos;                   // state, grouped by super-tile
@@ -73,7 +75,6 @@ void launch_permute(const StepArgs& A, long long ntot, cudaStream_t s);
 void launch_st_starts(const StepArgs& A, long long ntot, cudaStream_t s);
 void launch_bin(const StepArgs& A, long long nst, cudaStream_t s);
 void launch_deposit(const StepArgs& A, long long nst, size_t smem, double* rho64, cudaStream_t s);
-void launch_fixup(const StepArgs& A, long long nface, double* rho64, cudaStream_t s);
 void launch_green(const StepArgs& A, long long nblocks, cudaStream_t s);
 
 // Host-requested per-peak operations.

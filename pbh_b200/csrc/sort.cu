@@ -1,6 +1,7 @@
 // Segmented stable LSD radix sort (see sort.cuh for the design).
 #include "sort.cuh"
 
+#include <algorithm>
 #include <vector>
 
 namespace {
@@ -21,35 +22,40 @@ __device__ __forceinline__ u32 digit_of(K k, int shift, int hi, bool valid) {
   return (u32)(k >> shift) & ((1u << width) - 1u);
 }
 
-// Digit histograms of every pass in one read of the keys.
+__device__ __forceinline__ bool gate_closed(const SortPlan& P) { return P.gate && *P.gate == 0u; }
+
+// Digit histograms of every pass in one read of the keys (grid-stride over the tiles).
 template <class K, int BITS>
 __global__ void __launch_bounds__(SORT_THREADS) k_sort_hist(SortPlan P, const K* __restrict__ keys) {
   constexpr int RADIX = 1 << BITS;
   extern __shared__ u32 sh[];  // [npass][RADIX]
-  const int t = blockIdx.x;
-  const int seg = P.tile_seg[t];
-  const SortSeg S = P.seg[seg];
-  if (!S.active) return;
-  for (int i = threadIdx.x; i < P.npass * RADIX; i += SORT_THREADS) sh[i] = 0;
-  __syncthreads();
-  const long long begin = P.tile_begin[t];
-  const long long end = min(begin + (long long)SORT_TILE, S.end);
+  if (gate_closed(P)) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const long long wb = begin + (long long)warp * 32 * SORT_IPT;
-  for (int j = 0; j < SORT_IPT; ++j) {
-    const long long idx = wb + j * 32 + lane;
-    const bool valid = idx < end;
-    const K k = valid ? keys[idx] : (K)0;
-    for (int pass = 0; pass < P.npass; ++pass) {
-      const u32 d = digit_of<BITS>(k, S.lo + BITS * pass, S.hi, valid);
-      const u32 peers = __match_any_sync(0xffffffffu, d);
-      if (d < RADIX && (peers & lanemask_lt()) == 0) atomicAdd(&sh[pass * RADIX + d], __popc(peers));
+  for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
+    const int seg = P.tile_seg[t];
+    const SortSeg S = P.seg[seg];
+    if (!S.active) continue;
+    for (int i = threadIdx.x; i < P.npass * RADIX; i += SORT_THREADS) sh[i] = 0;
+    __syncthreads();
+    const long long begin = P.tile_begin[t];
+    const long long end = min(begin + (long long)SORT_TILE, S.end);
+    const long long wb = begin + (long long)warp * 32 * SORT_IPT;
+    for (int j = 0; j < SORT_IPT; ++j) {
+      const long long idx = wb + j * 32 + lane;
+      const bool valid = idx < end;
+      const K k = valid ? keys[idx] : (K)0;
+      for (int pass = 0; pass < P.npass; ++pass) {
+        const u32 d = digit_of<BITS>(k, S.lo + BITS * pass, S.hi, valid);
+        const u32 peers = __match_any_sync(0xffffffffu, d);
+        if (d < RADIX && (peers & lanemask_lt()) == 0) atomicAdd(&sh[pass * RADIX + d], __popc(peers));
+      }
     }
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < P.npass * RADIX; i += SORT_THREADS) {
-    const u32 c = sh[i];
-    if (c) atomicAdd(&P.hist[(size_t)seg * SORT_MAX_PASSES * RADIX + i], c);
+    __syncthreads();
+    for (int i = threadIdx.x; i < P.npass * RADIX; i += SORT_THREADS) {
+      const u32 c = sh[i];
+      if (c) atomicAdd(&P.hist[(size_t)seg * SORT_MAX_PASSES * RADIX + i], c);
+    }
+    __syncthreads();
   }
 }
 
@@ -59,6 +65,7 @@ template <int BITS>
 __global__ void k_sort_scan(SortPlan P) {
   constexpr int RADIX = 1 << BITS;
   __shared__ u32 wsum[RADIX / 32];
+  if (gate_closed(P)) return;
   const int seg = blockIdx.x;
   const SortSeg S = P.seg[seg];
   if (seg == 0 && threadIdx.x < SORT_MAX_PASSES) P.counters[threadIdx.x] = 0;
@@ -92,113 +99,117 @@ __global__ void __launch_bounds__(SORT_THREADS, 3) k_sort_pass(SortPlan P, int p
   __shared__ u32 s_tile;
   __shared__ u32 whist[SORT_WARPS][RADIX];
   __shared__ long long s_gbase[RADIX];
-  if (threadIdx.x == 0) s_tile = atomicAdd(&P.counters[pass], 1u);
-  for (int i = threadIdx.x; i < SORT_WARPS * RADIX; i += SORT_THREADS) (&whist[0][0])[i] = 0;
-  __syncthreads();
-  const int t = (int)s_tile;
-  if (t >= P.ntiles) return;
-  const int seg = P.tile_seg[t];
-  const SortSeg S = P.seg[seg];
-  if (!S.active) return;
-  const int shift = S.lo + BITS * pass;
-  const long long begin = P.tile_begin[t];
-  const long long end = min(begin + (long long)SORT_TILE, S.end);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const long long wb = begin + (long long)warp * 32 * SORT_IPT;
-  const u32 lt = lanemask_lt();
+  if (gate_closed(P)) return;
+  for (;;) {
+    __syncthreads();  // the previous tile's readers of s_tile, whist and s_gbase are done
+    if (threadIdx.x == 0) s_tile = atomicAdd(&P.counters[pass], 1u);
+    for (int i = threadIdx.x; i < SORT_WARPS * RADIX; i += SORT_THREADS) (&whist[0][0])[i] = 0;
+    __syncthreads();
+    const int t = (int)s_tile;
+    if (t >= P.ntiles) return;
+    const int seg = P.tile_seg[t];
+    const SortSeg S = P.seg[seg];
+    if (!S.active) continue;
+    const int shift = S.lo + BITS * pass;
+    const long long begin = P.tile_begin[t];
+    const long long end = min(begin + (long long)SORT_TILE, S.end);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long wb = begin + (long long)warp * 32 * SORT_IPT;
+    const u32 lt = lanemask_lt();
 
-  K k[SORT_IPT];
-  u32 v[SORT_IPT];
-  u32 rd[SORT_IPT];  // warp-local rank (low 16 bits) | digit (high 16 bits)
+    K k[SORT_IPT];
+    u32 v[SORT_IPT];
+    u32 rd[SORT_IPT];  // warp-local rank (low 16 bits) | digit (high 16 bits)
 #pragma unroll
-  for (int j = 0; j < SORT_IPT; ++j) {
-    const long long idx = wb + j * 32 + lane;
-    const bool valid = idx < end;
-    k[j] = valid ? kin[idx] : (K)0;
-    v[j] = valid ? (vin ? vin[idx] : (u32)idx) : 0u;
-  }
-#pragma unroll
-  for (int j = 0; j < SORT_IPT; ++j) {
-    const long long idx = wb + j * 32 + lane;
-    const u32 d = digit_of<BITS>(k[j], shift, S.hi, idx < end);
-    const u32 peers = __match_any_sync(0xffffffffu, d);
-    const u32 below = __popc(peers & lt);
-    const u32 prev = d < RADIX ? whist[warp][d] : 0u;
-    __syncwarp();
-    if (d < RADIX && below == 0) whist[warp][d] = prev + __popc(peers);
-    __syncwarp();
-    rd[j] = (prev + below) | (d << 16);
-  }
-  __syncthreads();
-
-  // Per digit: warp offsets inside the tile, then the tile's offset inside the segment.
-  const u32 ep = (P.counters[SORT_MAX_PASSES] * SORT_MAX_PASSES + (u32)pass) & 0x3FFFFFFFu;
-  const u64 tag = (u64)ep << 34;
-  volatile u64* st = (volatile u64*)P.status;
-  u32 run[DPT];
-#pragma unroll
-  for (int q = 0; q < DPT; ++q) {
-    const int d = threadIdx.x + q * SORT_THREADS;
-    u32 r = 0;
-#pragma unroll
-    for (int w = 0; w < SORT_WARPS; ++w) {
-      const u32 c = whist[w][d];
-      whist[w][d] = r;
-      r += c;
+    for (int j = 0; j < SORT_IPT; ++j) {
+      const long long idx = wb + j * 32 + lane;
+      const bool valid = idx < end;
+      k[j] = valid ? kin[idx] : (K)0;
+      v[j] = valid ? (vin ? vin[idx] : (u32)idx) : 0u;
     }
-    run[q] = r;
-    // Publish this tile's own count first, so successors can look past it at once.
-    st[(size_t)t * RADIX + d] = tag | ((P.tile_first[t] ? 2ull : 1ull) << 32) | r;
-  }
-  // Look back over the predecessors of this segment, LB words per round trip: the loads of a
-  // window are independent, so the walk costs one memory latency per LB tiles.
-  constexpr int LB = 8;
 #pragma unroll
-  for (int q = 0; q < DPT; ++q) {
-    const int d = threadIdx.x + q * SORT_THREADS;
-    u32 excl = 0;
-    if (!P.tile_first[t]) {
-      int p = t - 1;
-      int spins = 0;
-      bool done = false;
-      while (!done) {
-        u64 w[LB];
+    for (int j = 0; j < SORT_IPT; ++j) {
+      const long long idx = wb + j * 32 + lane;
+      const u32 d = digit_of<BITS>(k[j], shift, S.hi, idx < end);
+      const u32 peers = __match_any_sync(0xffffffffu, d);
+      const u32 below = __popc(peers & lt);
+      const u32 prev = d < RADIX ? whist[warp][d] : 0u;
+      __syncwarp();
+      if (d < RADIX && below == 0) whist[warp][d] = prev + __popc(peers);
+      __syncwarp();
+      rd[j] = (prev + below) | (d << 16);
+    }
+    __syncthreads();
+
+    // Per digit: warp offsets inside the tile, then the tile's offset inside the segment.
+    const u32 ep = (P.counters[SORT_MAX_PASSES] * SORT_MAX_PASSES + (u32)pass) & 0x3FFFFFFFu;
+    const u64 tag = (u64)ep << 34;
+    volatile u64* st = (volatile u64*)P.status;
+    u32 run[DPT];
 #pragma unroll
-        for (int i = 0; i < LB; ++i) w[i] = p - i >= S.first_tile ? st[(size_t)(p - i) * RADIX + d] : 0ull;
+    for (int q = 0; q < DPT; ++q) {
+      const int d = threadIdx.x + q * SORT_THREADS;
+      u32 r = 0;
 #pragma unroll
-        for (int i = 0; i < LB; ++i) {
-          if (done || p - i < S.first_tile) continue;
-          u64 v = w[i];
-          while ((v >> 34) != (u64)ep || ((u32)(v >> 32) & 3u) == 0) {
-            if (++spins > kSpinLimit) {
-              atomicExch(P.err, 1);
-              v = tag | (2ull << 32);  // give up: treat as a zero inclusive prefix
-              break;
-            }
-            __nanosleep(20);
-            v = st[(size_t)(p - i) * RADIX + d];
-          }
-          excl += (u32)v;
-          if (((u32)(v >> 32) & 3u) == 2u) done = true;
-        }
-        p -= LB;
-        if (p < S.first_tile) done = true;
+      for (int w = 0; w < SORT_WARPS; ++w) {
+        const u32 c = whist[w][d];
+        whist[w][d] = r;
+        r += c;
       }
-      st[(size_t)t * RADIX + d] = tag | (2ull << 32) | (excl + run[q]);
+      run[q] = r;
+      // Publish this tile's own count first, so successors can look past it at once.
+      st[(size_t)t * RADIX + d] = tag | ((P.tile_first[t] ? 2ull : 1ull) << 32) | r;
     }
-    s_gbase[d] = P.base[((size_t)seg * SORT_MAX_PASSES + pass) * RADIX + d] + excl;
-  }
-  __syncthreads();
+    // Look back over the predecessors of this segment, LB words per round trip: the loads of a
+    // window are independent, so the walk costs one memory latency per LB tiles.
+    constexpr int LB = 8;
+#pragma unroll
+    for (int q = 0; q < DPT; ++q) {
+      const int d = threadIdx.x + q * SORT_THREADS;
+      u32 excl = 0;
+      if (!P.tile_first[t]) {
+        int p = t - 1;
+        int spins = 0;
+        bool done = false;
+        while (!done) {
+          u64 w[LB];
+#pragma unroll
+          for (int i = 0; i < LB; ++i) w[i] = p - i >= S.first_tile ? st[(size_t)(p - i) * RADIX + d] : 0ull;
+#pragma unroll
+          for (int i = 0; i < LB; ++i) {
+            if (done || p - i < S.first_tile) continue;
+            u64 v = w[i];
+            while ((v >> 34) != (u64)ep || ((u32)(v >> 32) & 3u) == 0) {
+              if (++spins > kSpinLimit) {
+                atomicExch(P.err, 1);
+                v = tag | (2ull << 32);  // give up: treat as a zero inclusive prefix
+                break;
+              }
+              __nanosleep(20);
+              v = st[(size_t)(p - i) * RADIX + d];
+            }
+            excl += (u32)v;
+            if (((u32)(v >> 32) & 3u) == 2u) done = true;
+          }
+          p -= LB;
+          if (p < S.first_tile) done = true;
+        }
+        st[(size_t)t * RADIX + d] = tag | (2ull << 32) | (excl + run[q]);
+      }
+      s_gbase[d] = P.base[((size_t)seg * SORT_MAX_PASSES + pass) * RADIX + d] + excl;
+    }
+    __syncthreads();
 
 #pragma unroll
-  for (int j = 0; j < SORT_IPT; ++j) {
-    const u32 d = rd[j] >> 16;
-    if (d < RADIX) {
-      const long long pos = s_gbase[d] + whist[warp][d] + (rd[j] & 0xFFFFu);
-      if (kout) kout[pos] = k[j];
-      vout[pos] = v[j];
+    for (int j = 0; j < SORT_IPT; ++j) {
+      const u32 d = rd[j] >> 16;
+      if (d < RADIX) {
+        const long long pos = s_gbase[d] + whist[warp][d] + (rd[j] & 0xFFFFu);
+        if (kout) kout[pos] = k[j];
+        vout[pos] = v[j];
+      }
     }
-  }
+  }  // next tile
 }
 
 }  // namespace
@@ -226,6 +237,7 @@ int sort_plan_create(SortPlan* P, const SortSeg* segs, int nseg, int npass, int 
     }
   }
   P->nseg = nseg;
+  P->gate = nullptr;
   P->ntiles = (int)tseg.size();
   P->npass = npass;
   const size_t nt = tseg.empty() ? 1 : tseg.size();
@@ -269,7 +281,15 @@ template <class K, int BITS>
 static int sort_run_bits(const SortPlan* P, K* k0, u32* v0, K* k1, u32* v1, bool identity_vals, bool write_last_keys,
                          cudaStream_t s) {
   constexpr int RADIX = 1 << BITS;
-  k_sort_hist<K, BITS><<<P->ntiles, SORT_THREADS, sizeof(u32) * P->npass * RADIX, s>>>(*P, k0);
+  // Persistent grids: as many CTAs as are resident at once (the passes rely on every claimed
+  // tile being held by a running CTA, which a grid of at most this size guarantees).
+  int dev = 0, sms = 0, per_sm = 0;
+  PM_CHECK(cudaGetDevice(&dev));
+  PM_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  PM_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sort_pass<K, BITS>, SORT_THREADS, 0));
+  const int grid_pass = std::max(1, std::min(P->ntiles, sms * std::max(per_sm, 1)));
+  const int grid_hist = std::max(1, std::min(P->ntiles, sms * 4));
+  k_sort_hist<K, BITS><<<grid_hist, SORT_THREADS, sizeof(u32) * P->npass * RADIX, s>>>(*P, k0);
   k_sort_scan<BITS><<<P->nseg, RADIX, 0, s>>>(*P);
   K* kin = k0;
   u32* vin = v0;
@@ -277,7 +297,7 @@ static int sort_run_bits(const SortPlan* P, K* k0, u32* v0, K* k1, u32* v1, bool
   u32* vout = v1;
   for (int pass = 0; pass < P->npass; ++pass) {
     const bool last = pass == P->npass - 1;
-    k_sort_pass<K, BITS><<<P->ntiles, SORT_THREADS, 0, s>>>(*P, pass, kin, (pass == 0 && identity_vals) ? nullptr : vin,
+    k_sort_pass<K, BITS><<<grid_pass, SORT_THREADS, 0, s>>>(*P, pass, kin, (pass == 0 && identity_vals) ? nullptr : vin,
                                                             (last && !write_last_keys) ? nullptr : kout, vout);
     K* tk = kin;
     kin = kout;

@@ -1,11 +1,14 @@
 // Segmented, stable LSD radix sort of 64-bit keys with 32-bit values (sm_100a).
 //
-// One launch per 8-bit digit.  Each CTA ranks a tile of SORT_TILE keys with warp-level
-// multi-split (match.any + popc), publishes its digit counts and resolves its global
-// offsets by decoupled look-back over the preceding tiles of the same segment, so every
-// pass reads and writes each key once.  Tiles are claimed in order through an atomic
-// counter, which guarantees that every tile a CTA waits on is already running.  Waits are
-// bounded: a CTA that gives up sets the error word and proceeds.
+// One launch per digit.  A persistent grid (as many CTAs as fit on the GPU at once) claims
+// tiles of SORT_TILE keys in order through an atomic counter; for each tile a CTA ranks the
+// keys with warp-level multi-split (match.any + popc), publishes its digit counts and resolves
+// its global offsets by decoupled look-back over the preceding tiles of the same segment, so
+// every pass reads and writes each key once.  Claiming in order guarantees that every tile a
+// CTA waits on is held by a running CTA that waits only on earlier tiles.  Waits are bounded:
+// a CTA that gives up sets the error word and proceeds.  A plan may carry a device gate word:
+// when it reads 0 (no segment active this step) every launch returns at once, so a sort
+// captured in a graph costs a few microseconds on the steps that do not need it.
 //
 // A segment is a contiguous key range sorted independently (one peak of the ensemble).
 // Because every key of a segment carries the same high word (the peak id), sorting the
@@ -46,6 +49,7 @@ struct SortPlan {
   u64* status;           // [ntiles][radix] look-back words: epoch<<34 | flag<<32 | count
   u32* counters;         // [SORT_MAX_PASSES] tile claims, then the epoch word
   int* err;              // nonzero after a bounded wait gave up
+  const u32* gate;       // optional (device): when *gate == 0 every launch of the sort returns at once
 };
 
 // Host side (sort.cu).  `segs` is a host array.  The digit width is the smallest of 8..10 bits
