@@ -67,6 +67,17 @@ typedef struct {
   unsigned status;           /* bit 0: non-finite momentum or a particle outside its super-tile;
                               * bit 1: sort look-back gave up; bit 2: regrouping lost count;
                               * bit 3: a particle id outside the lattice */
+  /* Energy check (no counterpart in pm3d.py; its equations of motion, pm3d.py:3-6): sampled at
+   * every step's synchronised positions and momenta, from compensated FP64 sums in a fixed order.
+   * Layzer-Irvine: a (K + W) + int_{a0}^{a} K da is constant; li_residual is its change since
+   * the first sample, li_scale = a (K + |W|) the size to compare it with. */
+  int energy_samples;        /* samples since the peak was loaded (0: fields below are 0) */
+  double a_energy;           /* expansion factor of the last sample */
+  double momentum[3];        /* m_p sum p (canonical momentum) */
+  double kinetic;            /* K = m_p / (2 a^2) sum p^2 */
+  double potential;          /* W = (1/2) rho_b a^3 dx^3 sum_nodes delta Phi (the PM mesh potential) */
+  double li_residual;
+  double li_scale;
 } pm_stats_info;
 
 /* Create an engine holding npeaks independent peaks (a batched ensemble; npeaks = 1 is the

@@ -127,6 +127,34 @@ def hubble(a: float) -> float:
     return H_I * a ** -1.5
 
 
+def energies(mesh: Mesh, x: np.ndarray, p: np.ndarray, a: float):
+    """Total momentum, kinetic and mesh potential energy at expansion factor ``a``.
+
+    ``pm3d.py`` has no energy diagnostic; this follows from its equations of motion
+    (pm3d.py:3-6: p = a^2 dx/dt, dp/dt = -grad Phi, lap Phi = (3/2) H_i^2 delta / a) and its
+    mesh potential (pm3d.py:103-109): K = m_p/(2 a^2) sum p^2 (peculiar velocity p/a) and
+    W = (1/2) rho_b a^3 dx^3 sum_nodes delta Phi.  They obey the Layzer-Irvine equation
+    d[a (K + W)]/da = -K.
+    """
+    mom = mesh.m_part * p.sum(axis=0)
+    kin = mesh.m_part / (2.0 * a * a) * float((p * p).sum())
+    delta = density_contrast(mesh, x)
+    phi = _irfftn(potential_k(mesh, np.fft.rfftn(delta), a), mesh.N)
+    pot = 0.5 * RHO_A3 * mesh.dx ** 3 * float((delta * phi).sum())
+    return mom, kin, pot
+
+
+def layzer_irvine(samples):
+    """a (K + W) + int K da - a0 (K0 + W0) at the last of ``samples`` [(a, K, W), ...], the
+    integral by the trapezoid rule between consecutive samples."""
+    a0, k0, w0 = samples[0]
+    integral = 0.0
+    for (a1, k1, _), (a2, k2, _) in zip(samples[:-1], samples[1:]):
+        integral += 0.5 * (k1 + k2) * (a2 - a1)
+    a, k, w = samples[-1]
+    return a * (k + w) + integral - a0 * (k0 + w0)
+
+
 class Trajectory:
     """Particle state and the KDK leapfrog in a of ``PM3D.step`` (pm3d.py:117-129)."""
 

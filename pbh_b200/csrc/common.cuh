@@ -96,8 +96,41 @@ struct PeakStats {
   u64 max_fix;            // max node count in fixed point
   long long mass_defect;  // sum over nodes of (S - n_mean_fix): 0 when mass is exact
   u32 status;             // bit 0: non-finite force/momentum, bit 1: fixed-point overflow
-  u32 pad;
+  u32 nsamples;           // energy samples taken since the peak was loaded
+  // Energy and momentum at a_e, from compensated FP64 sums in a fixed reduction order.  With
+  // p = a^2 dx/dt, dp/dt = -grad Phi (pbhgr/pbhgr/pm3d.py:3-6) the Layzer-Irvine equation reads
+  // d[a (K + W)]/da = -K, so a (K + W) + int_{a0}^{a} K da stays equal to a0 (K0 + W0).
+  double a_e;             // expansion factor of the last sample
+  double mom[3];          // total canonical momentum m_p sum p
+  double kin;             // K = m_p/(2 a^2) sum p^2 (peculiar velocity p/a)
+  double pot;             // W = (1/2) rho_b a^3 dx^3 sum_nodes delta Phi (mesh potential energy)
+  double li_int;          // int K da over the samples so far (trapezoid rule)
+  double li_e0;           // a0 (K0 + W0) at the first sample
 };
+
+// Neumaier-compensated FP64 sum (s + c is the running total).
+struct CSum {
+  double s, c;
+};
+__device__ __forceinline__ void csum_add(CSum& a, double x) {
+  const double t = a.s + x;
+  a.c += fabs(a.s) >= fabs(x) ? (a.s - t) + x : (x - t) + a.s;
+  a.s = t;
+}
+__device__ __forceinline__ void csum_merge(CSum& a, const CSum& b) {
+  csum_add(a, b.s);
+  a.c += b.c;
+}
+// Warp-level merge (lane 0 holds the warp's total); a fixed butterfly, so the order is fixed.
+__device__ __forceinline__ CSum csum_warp(CSum v) {
+  for (int d = 16; d > 0; d >>= 1) {
+    CSum o;
+    o.s = __shfl_down_sync(0xffffffffu, v.s, d);
+    o.c = __shfl_down_sync(0xffffffffu, v.c, d);
+    csum_merge(v, o);
+  }
+  return v;
+}
 
 #define PM_CHECK(x)                                  \
   do {                                               \

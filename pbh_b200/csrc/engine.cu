@@ -78,6 +78,10 @@ struct pm_engine {
   u32* far_count = nullptr;
   u32* far_fill = nullptr;
   u32* arrive = nullptr;     // per super-tile face arrivals of the deposit (0 between steps)
+  double2* epart = nullptr;  // push partials of the energy sums
+  double2* wpart = nullptr;  // Green partials of the potential energy
+  double2* eslice = nullptr; // energy slice partials
+  u32* ecount = nullptr;     // energy slices done per peak
   u32* sort_gate = nullptr;  // one word: any peak sorts this step
   u32* totals = nullptr;
   long long* face = nullptr;
@@ -98,6 +102,10 @@ struct pm_engine {
     A.p_base = d_p_base;
     A.mode_base = d_mode_base;
     A.arrive = arrive;
+    A.epart = epart;
+    A.wpart = wpart;
+    A.eslice = eslice;
+    A.ecount = ecount;
     A.npeaks = npeaks;
     A.pos = pos;
     A.mom = mom;
@@ -169,6 +177,7 @@ struct pm_engine {
     CU(mark());
     launch_push(A, nst, smem_push, stream);
     CU(mark());
+    launch_energy(A, stream);
     launch_advance(A, stream);
     CU(mark());
     int r = sort_run<u32>(&sort, keys[0], vals[0], keys[1], vals[1], true, true, stream);
@@ -243,7 +252,7 @@ struct pm_engine {
       cudaFree(c.force);
     }
     sort_plan_destroy(&sort);
-    void* bufs[] = {d_peaks, d_clocks, d_stats, d_st_base, d_p_base, d_mode_base, arrive, pos, mom, tpos,
+    void* bufs[] = {d_peaks, d_clocks, d_stats, d_st_base, d_p_base, d_mode_base, arrive, epart, wpart, eslice, ecount, pos, mom, tpos,
                     tmom, cls, keys[0], keys[1], vals[0], vals[1], sstart[0], sstart[1], counts, lpre, far_count,
                     far_fill, sort_gate, totals, face, halo};
     for (void* b : bufs) cudaFree(b);
@@ -252,6 +261,16 @@ struct pm_engine {
 };
 
 namespace {
+
+void fill_energy(const PeakStats& s, pm_stats_info* o) {
+  o->energy_samples = (int)s.nsamples;
+  o->a_energy = s.nsamples ? s.a_e : 0.0;
+  for (int k = 0; k < 3; ++k) o->momentum[k] = s.nsamples ? s.mom[k] : 0.0;
+  o->kinetic = s.nsamples ? s.kin : 0.0;
+  o->potential = s.nsamples ? s.pot : 0.0;
+  o->li_residual = s.nsamples ? s.a_e * (s.kin + s.pot) + s.li_int - s.li_e0 : 0.0;
+  o->li_scale = s.nsamples ? s.a_e * (s.kin + fabs(s.pot)) : 0.0;
+}
 
 int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   E->npeaks = npeaks;
@@ -313,7 +332,7 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
     sso += P.nst + 1;
     fo += (long long)P.nst * P.fc;
     ho += (long long)P.nst * P.hc;
-    mb += (P.nmodes + PM_THREADS - 1) / PM_THREADS;
+    mb += (P.nmodes + PM_THREADS * GREEN_MODES - 1) / (PM_THREADS * GREEN_MODES);
     TSmax = std::max(TSmax, TS);
     max_bits = std::max(max_bits, P.key_bits);
     if (!class_of.count(c.N)) {
@@ -416,6 +435,10 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   if ((r = E->alloc(&E->far_count, E->nst))) return r;
   if ((r = E->alloc(&E->far_fill, E->nst))) return r;
   if ((r = E->alloc(&E->arrive, E->nst))) return r;
+  if ((r = E->alloc(&E->epart, 4 * E->nst))) return r;
+  if ((r = E->alloc(&E->wpart, E->nmodeblk))) return r;
+  if ((r = E->alloc(&E->eslice, (size_t)npeaks * ENERGY_SLICES * 5))) return r;
+  if ((r = E->alloc(&E->ecount, npeaks))) return r;
   if ((r = E->alloc(&E->sort_gate, 1))) return r;
   if ((r = E->alloc(&E->totals, E->nst))) return r;
   if ((r = E->alloc(&E->face, E->nfc))) return r;
@@ -439,6 +462,9 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   CU(cudaMemset(E->far_count, 0, sizeof(u32) * E->nst));
   CU(cudaMemset(E->far_fill, 0, sizeof(u32) * E->nst));
   CU(cudaMemset(E->arrive, 0, sizeof(u32) * E->nst));
+  CU(cudaMemset(E->epart, 0, sizeof(double2) * 4 * E->nst));
+  CU(cudaMemset(E->wpart, 0, sizeof(double2) * E->nmodeblk));
+  CU(cudaMemset(E->ecount, 0, sizeof(u32) * npeaks));
   CU(cudaMemset(E->sort_gate, 0, sizeof(u32)));
   for (int b = 0; b < 2; ++b) CU(cudaMemset(E->sstart[b], 0, sizeof(u32) * E->nsst));
 
@@ -563,6 +589,7 @@ int pm_get_stats_all(pm_engine* e, pm_stats_info* out) {
     out[i].delta_max = out[i].rho_max_over_mean - 1.0;
     out[i].mass_defect = (double)s[i].mass_defect / (double)PM_FIX_ONE;
     out[i].status = s[i].status | (err ? 2u : 0u);
+    fill_energy(s[i], &out[i]);
     flagged += out[i].status != 0;
   }
   return flagged;
@@ -732,6 +759,7 @@ int pm_get_stats(pm_engine* e, int peak, pm_stats_info* out) {
   out->delta_max = out->rho_max_over_mean - 1.0;
   out->mass_defect = (double)s.mass_defect / (double)PM_FIX_ONE;
   out->status = s.status | (err ? 2u : 0u);
+  fill_energy(s, out);
   return (int)(out->status != 0);
 }
 

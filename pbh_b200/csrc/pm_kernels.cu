@@ -86,7 +86,7 @@ struct PushCoef {
 template <int T>
 __device__ __forceinline__ void push_one(const StepArgs& A, const PeakDesc& P, const float* __restrict__ s_f,
                                          const PushCoef& K, int sx, int sy, int sz, int4 ps, float4 m, long long j,
-                                         u32* s_cnt, bool& bad) {
+                                         u32* s_cnt, bool& bad, double4& acc_e) {
   constexpr int RS = patch_rs(T), PS = patch_ps(T), CS = patch_size(T);
   const int N = P.N, l2 = P.log2N;
   const int ix = ps.x >> (2 * l2), iy = (ps.x >> l2) & (N - 1), iz = ps.x & (N - 1);
@@ -120,6 +120,15 @@ __device__ __forceinline__ void push_one(const StepArgs& A, const PeakDesc& P, c
   ay *= K.gscale;
   az *= K.gscale;
   float px = m.x + K.kA * ax, py = m.y + K.kA * ay, pz = m.z + K.kA * az;
+  // Momentum synchronised with the positions (after the closing kick): energy and momentum sums.
+  {
+    double4 t = acc_e;
+    t.x += (double)px;
+    t.y += (double)py;
+    t.z += (double)pz;
+    t.w += (double)px * px + (double)py * py + (double)pz * pz;
+    acc_e = t;
+  }
   int nx = ix, ny = iy, nz = iz;
   if (K.run) {
     px += K.kB * ax;
@@ -193,37 +202,48 @@ __device__ __forceinline__ void push_super(const StepArgs& A, const PeakDesc& P,
   }
   __syncthreads();
   bool bad = false;
-  // Two particles per thread per sweep, the next sweep's pair fetched before this one is computed.
+  double4 acc_e = make_double4(0.0, 0.0, 0.0, 0.0);  // this thread's momentum and p^2 sums
+  // One particle per thread per sweep, the next two sweeps' particles in flight meanwhile.
   long long j = b + threadIdx.x;
-  int4 p1n = make_int4(0, 0, 0, 0), p2n = p1n;
-  float4 m1n = make_float4(0.f, 0.f, 0.f, 0.f), m2n = m1n;
+  int4 pa = make_int4(0, 0, 0, 0), pb = pa;
+  float4 ma = make_float4(0.f, 0.f, 0.f, 0.f), mb = ma;
   if (j < e) {
-    p1n = A.pos[j];
-    m1n = A.mom[j];
-    if (j + PUSH_THREADS < e) {
-      p2n = A.pos[j + PUSH_THREADS];
-      m2n = A.mom[j + PUSH_THREADS];
-    }
+    pa = A.pos[j];
+    ma = A.mom[j];
   }
-  for (; j < e; j += 2 * PUSH_THREADS) {
-    const long long j2 = j + PUSH_THREADS;
-    const bool has2 = j2 < e;
-    const int4 p1 = p1n, p2 = p2n;
-    const float4 m1 = m1n, m2 = m2n;
-    const long long jn = j + 2 * PUSH_THREADS;
-    if (jn < e) {
-      p1n = A.pos[jn];
-      m1n = A.mom[jn];
-      if (jn + PUSH_THREADS < e) {
-        p2n = A.pos[jn + PUSH_THREADS];
-        m2n = A.mom[jn + PUSH_THREADS];
-      }
+  if (j + PUSH_THREADS < e) {
+    pb = A.pos[j + PUSH_THREADS];
+    mb = A.mom[j + PUSH_THREADS];
+  }
+  for (; j < e; j += PUSH_THREADS) {
+    const int4 p0 = pa;
+    const float4 m0 = ma;
+    pa = pb;
+    ma = mb;
+    if (j + 2 * PUSH_THREADS < e) {
+      pb = A.pos[j + 2 * PUSH_THREADS];
+      mb = A.mom[j + 2 * PUSH_THREADS];
     }
-    push_one<T>(A, P, s_f, K, sx, sy, sz, p1, m1, j, s_cnt, bad);
-    if (has2) push_one<T>(A, P, s_f, K, sx, sy, sz, p2, m2, j2, s_cnt, bad);
+    push_one<T>(A, P, s_f, K, sx, sy, sz, p0, m0, j, s_cnt, bad, acc_e);
   }
   if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&A.stats[pk].status, 1u);
   for (int c = threadIdx.x; c < P.NC; c += PUSH_THREADS) A.counts[(P.st_base + st) * BIN_CLASSES + c] = s_cnt[c];
+  // Super-tile partials of the momentum and p^2 sums (compensated, fixed order).
+  __shared__ CSum s_e[PUSH_THREADS / 32][4];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const double4 ev = acc_e;
+  const double ea[4] = {ev.x, ev.y, ev.z, ev.w};
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const CSum v = csum_warp(CSum{ea[q], 0.0});
+    if (lane == 0) s_e[warp][q] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    CSum t = s_e[0][threadIdx.x];
+    for (int w = 1; w < PUSH_THREADS / 32; ++w) csum_merge(t, s_e[w][threadIdx.x]);
+    A.epart[(P.st_base + st) * 4 + threadIdx.x] = make_double2(t.s, t.c);
+  }
 }
 
 __global__ void __launch_bounds__(PUSH_THREADS, 2) k_push(StepArgs A) {
@@ -323,6 +343,88 @@ __global__ void k_advance(StepArgs A) {
   }
   any_sort = __syncthreads_or(any_sort);
   if (threadIdx.x == 0) *A.sort_gate = any_sort ? 1u : 0u;
+}
+
+// ------------------------------------------------------------------------------------------
+// Energy and momentum of every peak that was just pushed (before the clock advances): the push
+// partials give K and sum p at the positions' a, the previous step's Green partials give W at
+// the same a (the grids were computed there).  ENERGY_SLICES CTAs per peak each reduce a slice
+// of the partials; the last one to finish (atomic ticket) merges the slices in slice order and
+// updates the statistics.  All sums are compensated, every order fixed.  The Layzer-Irvine
+// integral int K da advances by the trapezoid rule between samples.
+__global__ void __launch_bounds__(PM_THREADS) k_energy(StepArgs A) {
+  const int pk = blockIdx.y, sl = blockIdx.x;
+  const PeakClock C = A.clocks[pk];
+  if (C.state != PS_RUN && C.state != PS_FINALIZE) return;
+  const PeakDesc& P = A.peaks[pk];
+  __shared__ CSum s_w[PM_THREADS / 32][5];
+  __shared__ u32 s_last;
+  CSum v[5];
+#pragma unroll
+  for (int q = 0; q < 5; ++q) v[q] = CSum{0.0, 0.0};
+  const long long t0 = P.nst * sl / ENERGY_SLICES, t1 = P.nst * (sl + 1) / ENERGY_SLICES;
+  for (long long t = t0 + threadIdx.x; t < t1; t += PM_THREADS) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const double2 e = A.epart[(P.st_base + t) * 4 + q];
+      csum_merge(v[q], CSum{e.x, e.y});
+    }
+  }
+  const long long nblk = (P.nmodes + PM_THREADS * GREEN_MODES - 1) / (PM_THREADS * GREEN_MODES);  // Green blocks
+  const long long g0 = nblk * sl / ENERGY_SLICES, g1 = nblk * (sl + 1) / ENERGY_SLICES;
+  for (long long t = g0 + threadIdx.x; t < g1; t += PM_THREADS) {
+    const double2 e = A.wpart[P.mode_base + t];
+    csum_merge(v[4], CSum{e.x, e.y});
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    const CSum r = csum_warp(v[q]);
+    if (lane == 0) s_w[warp][q] = r;
+  }
+  __syncthreads();
+  double2* slice = A.eslice + ((long long)pk * ENERGY_SLICES) * 5;
+  if (threadIdx.x < 5) {
+    CSum t = s_w[0][threadIdx.x];
+    for (int w = 1; w < PM_THREADS / 32; ++w) csum_merge(t, s_w[w][threadIdx.x]);
+    slice[sl * 5 + threadIdx.x] = make_double2(t.s, t.c);
+    __threadfence();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(&A.ecount[pk], 1u) == ENERGY_SLICES - 1 ? 1u : 0u;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  __shared__ double s_tot[5];
+  if (threadIdx.x < 5) {
+    CSum t = CSum{0.0, 0.0};
+    for (int q = 0; q < ENERGY_SLICES; ++q) {
+      const double2 e = __ldcg(slice + q * 5 + threadIdx.x);
+      csum_merge(t, CSum{e.x, e.y});
+    }
+    s_tot[threadIdx.x] = t.s + t.c;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    A.ecount[pk] = 0u;
+    PeakStats& S = A.stats[pk];
+    const double a = C.a;
+    const double kin = P.m_part / (2.0 * a * a) * s_tot[3];
+    const double pot = 0.5 * (3.0 * PM_H_I * PM_H_I / (8.0 * M_PI)) * P.dx * P.dx * P.dx * s_tot[4];
+    if (S.nsamples == 0) {
+      S.li_int = 0.0;
+      S.li_e0 = a * (kin + pot);
+    } else {
+      S.li_int += 0.5 * (S.kin + kin) * (a - S.a_e);
+    }
+    S.a_e = a;
+    S.mom[0] = P.m_part * s_tot[0];
+    S.mom[1] = P.m_part * s_tot[1];
+    S.mom[2] = P.m_part * s_tot[2];
+    S.kin = kin;
+    S.pot = pot;
+    S.nsamples += 1;
+  }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -525,21 +627,28 @@ template <int TS>
 __device__ __forceinline__ void fixup_faces(const StepArgs& A, const PeakDesc& P, u32 Y, double* rho64,
                                             long long& dsum, long long& smax) {
   constexpr int FC = TS * TS * TS - (TS - 1) * (TS - 1) * (TS - 1);
+  constexpr int HC = (TS + 1) * (TS + 1) * (TS + 1) - TS * TS * TS;
+  // Halo partials of the lower neighbour Y - o, o = (ox, oy, oz) in {0,1}^3 \ 0, seen from Y's
+  // face node (lx, ly, lz) with (lx, ly, lz) zero where o is one: node (lx + TS ox, ...) of the
+  // neighbour, which lies on its upper halo.
+  __shared__ const long long* s_nb[8];
   const int NS = P.NS, N = P.N;
   const int sx = pm_compact3(Y >> 2), sy = pm_compact3(Y >> 1), sz = pm_compact3(Y);
+  __syncthreads();  // s_nb of a previous call has been read
+  if (threadIdx.x < 8) {
+    const int o = threadIdx.x, ox = o & 1, oy = (o >> 1) & 1, oz = (o >> 2) & 1;
+    const u32 sn = pm_morton3((sx - ox) & (NS - 1), (sy - oy) & (NS - 1), (sz - oz) & (NS - 1));
+    s_nb[o] = A.halo + P.halo_off + (long long)sn * HC;
+  }
+  __syncthreads();
   const long long* face = A.face + P.face_off + (long long)Y * FC;
-  const long long* halo = A.halo + P.halo_off;
   for (int f = threadIdx.x; f < FC; f += DEP_THREADS) {
     int lx, ly, lz;
     face_coords<TS>(f, lx, ly, lz);
     long long S = __ldcg(face + f);
     const int zmask = (lx == 0 ? 1 : 0) | (ly == 0 ? 2 : 0) | (lz == 0 ? 4 : 0);
-#pragma unroll
-    for (int o = 1; o < 8; ++o) {
-      if (o & ~zmask) continue;
-      const int ox = o & 1, oy = (o >> 1) & 1, oz = (o >> 2) & 1;
-      const u32 sn = pm_morton3((sx - ox) & (NS - 1), (sy - oy) & (NS - 1), (sz - oz) & (NS - 1));
-      S += __ldcg(halo + (long long)sn * P.hc + halo_index(lx + TS * ox, ly + TS * oy, lz + TS * oz, TS));
+    for (int o = zmask; o; o = (o - 1) & zmask) {  // non-empty subsets of zmask
+      S += __ldcg(s_nb[o] + halo_index(lx + TS * (o & 1), ly + TS * ((o >> 1) & 1), lz + TS * (o >> 2), TS));
     }
     const long long Dv = S - P.n_mean_fix;
     const long long node = ((long long)(sx * TS + lx) * N + (sy * TS + ly)) * N + (sz * TS + lz);
@@ -573,11 +682,13 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
   u64 acc[NPT];
 #pragma unroll
   for (int k = 0; k < NPT; ++k) acc[k] = 0ull;
-  // A node takes at most one contribution per particle of a chunk.  With CHUNK < 2^11 the high
-  // words (each at most 2^20, or -1 for a remainder corner a few units below zero) sum inside
-  // int32 and the low words (each < 2^20) inside uint32, so both are exact.
-  constexpr int CH_IT = 3;  // sweeps of DEP_THREADS particles per chunk: CHUNK = 1536
-  static_assert(CH_IT * DEP_THREADS < 2048, "chunk too large for the split accumulators");
+  // A node takes at most one contribution per particle of a chunk.  The high word of a
+  // contribution is in [-1, 2^20] (-1 for a remainder corner a few units below zero), the low
+  // word in [0, 2^20).  With CHUNK < 4096 the low sums stay below 2^32 and the high sums in
+  // [-CHUNK, CHUNK * 2^20], an interval shorter than 2^32 - 4096: kept modulo 2^32 in a u32,
+  // a value at or above 2^32 - 4096 is the negative one.  Both are exact.
+  constexpr int CH_IT = 4095 / DEP_THREADS;  // sweeps of DEP_THREADS particles per chunk
+  static_assert(CH_IT >= 1 && CH_IT * DEP_THREADS < 4096, "chunk too large for the split accumulators");
   const long long nit = (total + DEP_THREADS - 1) / DEP_THREADS;
   long long j = b + threadIdx.x;
   int4 ps_n = j < e ? A.pos[j] : make_int4(-1, 0, 0, 0);
@@ -613,7 +724,9 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
       const bool head = lane == 0 || prev != key;
       const u32 heads = __ballot_sync(0xffffffffu, head);
       bool tail = true;
-      if (heads != 0xffffffffu) {
+      // A few same-cell neighbours cost a few serialised shared-memory atomics; the scan (about
+      // 250 instructions per lane) pays only when runs are long, as in collapsed regions.
+      if (__popc(heads) < 24) {
         const int sstart = 31 - __clz(heads & le);
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
@@ -653,7 +766,9 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
         const int node = threadIdx.x + q * DEP_THREADS;
         if (node < NN) {
           const int ad = (node / (T1 * T1)) * PS + ((node / T1) % T1) * RS + node % T1;
-          acc[q] += (u64)((long long)(int)acc_hi[ad] * (1LL << 20)) + (u64)acc_lo[ad];
+          const u32 h = acc_hi[ad];
+          const long long hs = h >= 0xFFFFF000u ? (long long)h - (1LL << 32) : (long long)h;
+          acc[q] += (u64)(hs * (1LL << 20)) + (u64)acc_lo[ad];
           acc_hi[ad] = 0u;
           acc_lo[ad] = 0u;
         }
@@ -763,21 +878,7 @@ __device__ __forceinline__ float grad_k(float k, float dx, int mode) {
   return k;
 }
 
-__global__ void __launch_bounds__(PM_THREADS) k_green(StepArgs A) {
-  __shared__ int s_pk;
-  __shared__ float s_c;
-  if (threadIdx.x == 0) {
-    s_pk = pm_find(A.mode_base, A.npeaks, (long long)blockIdx.x);
-    const PeakDesc& P = A.peaks[s_pk];
-    const double n3 = (double)P.N * P.N * P.N;
-    s_c = (float)(-1.5 * PM_H_I * PM_H_I / A.clocks[s_pk].a_grid / n3);
-  }
-  __syncthreads();
-  const int pk = s_pk;
-  if (!A.clocks[pk].has_delta) return;
-  const PeakDesc& P = A.peaks[pk];
-  const long long m = ((long long)blockIdx.x - A.mode_base[pk]) * PM_THREADS + threadIdx.x;
-  if (m >= P.nmodes) return;
+__device__ __forceinline__ double green_mode(const PeakDesc& P, long long m, float s_c) {
   const int N = P.N, Nh = N / 2 + 1;
   // m = row * Nh + kz without an integer division: the double quotient is off by at most one.
   long long rest = (long long)((double)m * P.inv_nh);
@@ -792,7 +893,7 @@ __global__ void __launch_bounds__(PM_THREADS) k_green(StepArgs A) {
   float2* out = P.gspec;
   if (m == 0) {
     out[0] = out[M] = out[2 * M] = make_float2(0.f, 0.f);
-    return;
+    return 0.0;
   }
   float G = s_c / k2;
   if (P.smooth > 0) {
@@ -817,6 +918,42 @@ __global__ void __launch_bounds__(PM_THREADS) k_green(StepArgs A) {
   out[m] = ox;
   out[M + m] = oy;
   out[2 * M + m] = oz;
+  // Potential-energy term: sum_x delta Phi = sum_k |delta_k|^2 G_k over the full spectrum; the
+  // half spectrum counts each kz in (0, N/2) twice.
+  const double wk = (kz == 0 || kz == N / 2) ? 1.0 : 2.0;
+  return wk * (double)G * ((double)d.x * d.x + (double)d.y * d.y);
+}
+
+__global__ void __launch_bounds__(PM_THREADS) k_green(StepArgs A) {
+  __shared__ int s_pk;
+  __shared__ float s_c;
+  __shared__ CSum s_w[PM_THREADS / 32];
+  if (threadIdx.x == 0) {
+    s_pk = pm_find(A.mode_base, A.npeaks, (long long)blockIdx.x);
+    const PeakDesc& P = A.peaks[s_pk];
+    const double n3 = (double)P.N * P.N * P.N;
+    s_c = (float)(-1.5 * PM_H_I * PM_H_I / A.clocks[s_pk].a_grid / n3);
+  }
+  __syncthreads();
+  const int pk = s_pk;
+  if (!A.clocks[pk].has_delta) return;
+  const PeakDesc& P = A.peaks[pk];
+  const long long m0 = ((long long)blockIdx.x - A.mode_base[pk]) * (PM_THREADS * GREEN_MODES) + threadIdx.x;
+  double w = 0.0;
+#pragma unroll
+  for (int k = 0; k < GREEN_MODES; ++k) {
+    const long long m = m0 + k * PM_THREADS;
+    if (m < P.nmodes) w += green_mode(P, m, s_c);
+  }
+  // Within the block a plain FP64 tree (at most 1024 terms); across blocks the compensated sum.
+  for (int d = 16; d > 0; d >>= 1) w += __shfl_down_sync(0xffffffffu, w, d);
+  if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = CSum{w, 0.0};
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    CSum t = s_w[0];
+    for (int q = 1; q < PM_THREADS / 32; ++q) csum_merge(t, s_w[q]);
+    A.wpart[blockIdx.x] = make_double2(t.s, t.c);
+  }
 }
 
 __global__ void k_reset_peak(StepArgs A, int pk, double a0, int mode, double param, double a_end, int max_steps) {
@@ -840,6 +977,7 @@ __global__ void k_reset_peak(StepArgs A, int pk, double a0, int mode, double par
   else c.da = 0.0;
   A.clocks[pk] = c;
   A.stats[pk].status = 0;
+  A.stats[pk].nsamples = 0;
 }
 
 // Particles (n,3) float64 in lattice order -> split state + cell keys (pm3d.py:76-79 convention).
@@ -979,6 +1117,9 @@ void launch_push(const StepArgs& A, long long nst, size_t smem, cudaStream_t s) 
   k_push<<<(unsigned)nst, PUSH_THREADS, smem, s>>>(A);
 }
 void launch_advance(const StepArgs& A, cudaStream_t s) { k_advance<<<1, 256, 0, s>>>(A); }
+void launch_energy(const StepArgs& A, cudaStream_t s) {
+  k_energy<<<dim3(ENERGY_SLICES, A.npeaks), PM_THREADS, 0, s>>>(A);
+}
 void launch_permute(const StepArgs& A, long long ntot, cudaStream_t s) {
   k_permute<<<stride_grid(ntot, PM_THREADS, 8), PM_THREADS, 0, s>>>(A, ntot);
 }

@@ -5,6 +5,7 @@
 //   push       per super-tile: CIC gather of the forces, kicks, drift; output in place into the
 //              temporary state, tagged with the class of the super-tile the particle moved to
 //              (one of <= 125 neighbours) and counted per class
+//   energy     per peak: momentum, kinetic and potential energy, Layzer-Irvine integral
 //   advance    per peak clock (and which peaks regroup by sort this step)
 //   regroup    re-binning (scan of the class counts, then a scatter into the new grouping) for
 //              most steps; a full Morton-key radix sort plus a permutation every full_every
@@ -21,6 +22,8 @@
 #define PM_THREADS 256
 #define PUSH_THREADS 512
 #define DEP_THREADS 512
+#define GREEN_MODES 4      // modes per thread of the Green kernel (a block covers PM_THREADS * GREEN_MODES)
+#define ENERGY_SLICES 16   // CTAs per peak of the energy reduction
 #define BIN_CLASSES 128   // stride of the per-super-tile class arrays (>= 125)
 #define BIN_FAR 255       // class of a particle that moved more than 2 super-tiles
 
@@ -53,6 +56,10 @@ struct StepArgs {
   u32* totals;                 // [super-tile] particles arriving
   long long* face;             // face partials
   long long* halo;             // upper-halo partials
+  double2* epart;              // [super-tile][4] push partials (sum, compensation): p_x, p_y, p_z, p^2
+  double2* wpart;              // [Green block] partials of sum_k w_k |delta_k|^2 G_k
+  double2* eslice;             // [peak][ENERGY_SLICES][5] slice partials of the energy kernel
+  u32* ecount;                 // [peak] energy slices finished this step (0 between steps)
 };
 
 // Binary search: largest i in [0, n) with base[i] <= v.
@@ -71,6 +78,7 @@ size_t pm_push_smem(int TSmax);
 
 void launch_push(const StepArgs& A, long long nst, size_t smem, cudaStream_t s);
 void launch_advance(const StepArgs& A, cudaStream_t s);
+void launch_energy(const StepArgs& A, cudaStream_t s);
 void launch_permute(const StepArgs& A, long long ntot, cudaStream_t s);
 void launch_st_starts(const StepArgs& A, long long ntot, cudaStream_t s);
 void launch_bin(const StepArgs& A, long long nst, cudaStream_t s);

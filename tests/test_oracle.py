@@ -87,3 +87,28 @@ def test_momentum_and_mass_invariants(golden):
         a, delta = tr.step(a, 0.05 * a)
     assert np.all(np.abs(tr.p.sum(axis=0) - P0) < 1e-12 * np.abs(tr.p).sum())
     assert abs(O.deposit(tr.x, m["N"], mesh.dx).sum() - m["Np"] ** 3) < 1e-8
+
+
+def test_oracle_energy_identities():
+    """The energy diagnostic of the oracle: W on the mesh equals (1/2) m_p sum_i Phi(x_i) with Phi
+    CIC-interpolated (deposit and interpolation share one kernel), the total momentum stays ~0,
+    and the Layzer-Irvine residual of a short linear-regime run stays at the PM scheme's level."""
+    from oracle.recipe_oracle import recipe_ic
+    N = 16
+    mesh = O.Mesh(N, 1.0, N)
+    ic = recipe_ic(mesh, R=(0.12, 0.1, 0.09), delta0=0.2, noise_frac=0.02, seed=4)
+    x, p = ic["x"], ic["p"]
+    mom, kin, pot = O.energies(mesh, x, p, 1.0)
+    delta = O.density_contrast(mesh, x)
+    phi = O._irfftn(O.potential_k(mesh, np.fft.rfftn(delta), 1.0), N)
+    pot_particles = 0.5 * mesh.m_part * float(O.interp(phi, x, N, mesh.dx).sum())
+    assert abs(pot - pot_particles) <= 1e-12 * abs(pot)
+    assert kin > 0 and pot < 0
+    tr = O.Trajectory(mesh, x, p)
+    a, samples = 1.0, [(1.0, kin, pot)]
+    for _ in range(10):
+        a, _ = tr.step(a, 0.05 * a)
+        m, k, w = O.energies(mesh, tr.x, tr.p, a)
+        samples.append((a, k, w))
+    assert np.max(np.abs(m)) <= 1e-12 * mesh.m_part * mesh.Np ** 3
+    assert abs(O.layzer_irvine(samples)) <= 2e-2 * a * (k + abs(w))
