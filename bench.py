@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--no-serve", action="store_true", help="skip the served-stream latency run")
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="arrival window of the served stream")
     ap.add_argument("--serve-rate", type=float, default=20.0, help="mean request arrivals per second")
+    ap.add_argument("--tiles", default="auto", help="super-tile side: 'auto' (autotuned per mesh size) or 4/8/16")
     return ap.parse_args()
 
 
@@ -186,6 +187,11 @@ def algorithmic_bytes(phase: str, n: int, cells: int, modes: int, npass: int) ->
 
 PHASES = ["push", "advance", "sort", "bin", "deposit", "r2c", "green", "c2r"]
 
+# DRAM bytes (read + write) per launch from one ncu capture of the plain 256^3 run
+# (profiles/kernels_plain256.md), per particle (per mode for Green), scaled to a launch by the
+# particles (modes) it processes.
+NCU_TRAFFIC = {"push": 78.35, "bin": 62.27, "deposit": 22.45, "green_per_mode": 25.77}
+
 
 def run_ours(args):
     import numpy as np
@@ -209,7 +215,12 @@ def run_ours(args):
     need = 1 + args.warmup + args.steps
     if need > min(s.steps for s in specs):
         raise SystemExit(f"warmup + steps ({need}) exceed the run length ({min(s.steps for s in specs)})")
-    ens = Ensemble(specs, device=local, bucket_sort=not args.full_sort)
+    if args.tiles == "auto":
+        from pbh_b200.tune import autotune
+        tiles = autotune({s.N for s in specs} | ({64, 128, 256} if not args.no_serve else set()), device=local)
+    else:
+        tiles = {s.N: min(int(args.tiles), s.N) for s in specs}
+    ens = Ensemble(specs, device=local, bucket_sort=not args.full_sort, tiles=tiles)
     lib = _lib.load()
     info = (np.zeros(6, dtype=np.int64))
     lib.pm_engine_info(ens.engine._h, info.ctypes.data)
@@ -261,8 +272,15 @@ def run_ours(args):
         hbm, hbm_src = 6650.0, "fallback"
     ours = {k: v for k, v in kern.items() if k in ("push", "sort", "bin", "deposit", "green")}
     top = max(ours, key=lambda k: ours[k]["ms"])
+    def traffic(name):
+        if name == "green":
+            return NCU_TRAFFIC["green_per_mode"] * modes
+        return NCU_TRAFFIC[name] * n_step if name in NCU_TRAFFIC else None
     roofline = {"bound": "hbm", "kernel": top, "achieved": kern[top]["gbs"], "peak": hbm, "unit": "GB/s",
-                "frac": kern[top]["gbs"] / hbm, "traffic": None, "peak_source": hbm_src,
+                "frac": kern[top]["gbs"] / hbm, "traffic": traffic(top),
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the plain 256^3 capture, "
+                                  "per particle, times this launch's particles",
+                "algorithmic_bytes": kern[top]["algorithmic_bytes"], "peak_source": hbm_src,
                 "per_kernel": {k: {"ms": round(v["ms"], 4), "gbs": None if v["gbs"] is None else round(v["gbs"], 1),
                                    "frac": None if v["gbs"] is None else round(v["gbs"] / hbm, 3)}
                                for k, v in kern.items()},
@@ -274,11 +292,12 @@ def run_ours(args):
             "data": "synthetic (recipe peaks, seeded numpy noise)",
             "config": dict(desc, particles_per_gpu=n_step, peaks=len(specs), l2="inputs larger than L2 (126 MB)",
                            regroup="Morton radix sort every step" if args.full_sort else
-                           "re-binning each step, Morton radix sort every 16th", parallelism=f"replicas x{world}"),
+                           "re-binning each step, Morton radix sort every 16th", parallelism=f"replicas x{world}",
+                           super_tiles={str(k): v for k, v in sorted(tiles.items())}),
             "clocks": clocks, "gpu_launches": args.steps * (11 + npass), "roofline": roofline}
 
     if rank == 0 and not args.no_plain and args.workload == "batched":
-        pr = plain_rate(specs, steps=8, warmup=3, device=local)
+        pr = plain_rate(specs, steps=8, warmup=3, device=local, tiles=tiles)
         line["plain"] = dict(pr, batched_over_plain=value / world / pr["particle_steps_per_s"],
                              how="each peak alone in a single-peak engine, sequentially, same kernels")
 
@@ -287,7 +306,7 @@ def run_ours(args):
     ens.close()
     del ens
     if rank == 0 and not args.no_serve:
-        line["served"] = served_stream(args, local)
+        line["served"] = served_stream(args, local, tiles)
     if rank == 0 and world == 1 and not args.no_cpu:
         cb = cpu_rate(specs, steps=2, warmup=1, max_mesh=128 if args.workload == "batched" else 64)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
@@ -329,7 +348,7 @@ def e2e_job(ens, specs, torch, device):
             "how": "public Ensemble API: pinned host noise -> device IC -> all steps, per-step stats to host; wall clock"}
 
 
-def served_stream(args, device):
+def served_stream(args, device, tiles=None):
     """The served form: Poisson arrivals of single-peak collapse runs (meshes 64^3-256^3,
     (e, p, delta0) as the ensemble) admitted into a slot pool under a 150 GB HBM budget,
     continuously batched, each run ending at its collapse (max delta >= 50) or last step."""
@@ -338,7 +357,7 @@ def served_stream(args, device):
     from pbh_b200.serve import Server, ServerConfig, latency_summary, poisson_arrivals
     arrivals = poisson_arrivals(rate=args.serve_rate, duration=args.serve_seconds, seed=args.seed, steps=150)
     cfg = ServerConfig(slots={64: 32, 128: 32, 256: 24}, budget_bytes=150e9, delta_collapse=50.0, keep_delta=True,
-                       device=device)
+                       device=device, tiles=tiles)
     srv = Server(cfg)
     t0 = time.perf_counter()
     done = srv.serve(arrivals, timeout=args.serve_seconds + 240.0)

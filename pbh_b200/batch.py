@@ -21,7 +21,11 @@ class Ensemble:
     def __init__(self, specs, device: int = 0, graph: bool = True, bucket_sort: bool = True, tiles=None,
                  delta_collapse: float = 0.0):
         self.specs = list(specs)
+        if tiles == "auto":                      # per mesh size, timed on this GPU (pbh_b200.tune)
+            from .tune import autotune
+            tiles = autotune({sp.N for sp in self.specs}, device=device)
         tiles = tiles or {}
+        self.tiles = {int(k): int(v) for k, v in tiles.items()}
         self.cfgs = [PeakConfig(N=s.N, Np=s.N, L=s.L, tile=int(tiles.get(s.N, 0))) for s in self.specs]
         self.engine = Engine(self.cfgs, device=device, bucket_sort=bucket_sort, graph=graph)
         self.device = device

@@ -16,10 +16,10 @@
 typedef unsigned long long u64;
 typedef unsigned int u32;
 
-// Density is accumulated as unsigned 64-bit fixed point with 40 fractional bits: integer
+// Density is accumulated as unsigned 64-bit fixed point with 38 fractional bits: integer
 // sums are associative, so the deposit is bitwise deterministic in any order, and
 // delta = S/n_mean - 1 keeps full FP32 relative precision even where |delta| << 1.
-#define PM_FIX_BITS 40
+#define PM_FIX_BITS 38
 #define PM_FIX_ONE (1ULL << PM_FIX_BITS)
 
 #define PM_H_I 5.0
@@ -53,8 +53,8 @@ struct PeakDesc {
   int gradient;            // 0 spectral (reference), 1 two-point finite difference, 2 four-point
   int full_every;          // a full Morton-key sort every this many steps (re-binning between)
   double L, dx, smooth, n_mean, m_part;
-  long long n_mean_fix;    // round(n_mean * 2^40)
-  double inv_fix_nmean;    // 2^-40 / n_mean
+  long long n_mean_fix;    // round(n_mean * 2^38)
+  double inv_fix_nmean;    // 2^-38 / n_mean
   long long p_off, n;      // particle range in the arena
   long long st_base;       // first global super-tile index of this peak
   long long sst_off;       // offset of this peak's super-tile start arrays (nst + 1 entries)

@@ -577,14 +577,14 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_bin_scatter(StepArgs A) {
 // ------------------------------------------------------------------------------------------
 // Deterministic CIC deposit (pm3d.py:81-89, 103-104).  One CTA per super-tile deposits its own
 // particles (one contiguous range) onto the (TS+1)^3 nodes they touch.  Per particle the 8 CIC
-// weights are formed in 64-bit fixed point with 40 fractional bits, the 8th corner taking the
-// remainder so each particle deposits exactly 2^40; consecutive particles of one cell are first
+// weights are formed in 64-bit fixed point with 38 fractional bits, the 8th corner taking the
+// remainder so each particle deposits exactly 2^38; consecutive particles of one cell are first
 // combined by a warp-shuffle segmented scan.  Each node accumulates in shared memory as two
-// native 32-bit words (the signed weight's bits >= 20 and its low 20 bits), which cannot
-// overflow within a chunk of fewer than 2048 particles, and is folded into a 64-bit register
-// accumulator after every chunk.  Interior nodes are then final and written as FP32
-// delta = S/n_mean - 1; nodes on the three lower faces (which neighbours also reach) and on the
-// upper halo (which belongs to the neighbours) are written as 64-bit partials.
+// native 32-bit words (the signed weight's bits >= 19 and its low 19 bits), exact within a chunk
+// of up to 8191 particles, and is folded into a 64-bit register accumulator after every chunk.
+// Interior nodes are then final and written as FP32 delta = S/n_mean - 1; nodes on the three
+// lower faces (which neighbours also reach) and on the upper halo (which belongs to the
+// neighbours) are written as 64-bit partials.
 //
 // Face fix-up in the same launch: super-tile Y's face nodes are complete once Y and its 7 lower
 // neighbours have written their partials.  Every CTA, after its partials, counts itself in at
@@ -659,6 +659,19 @@ __device__ __forceinline__ void fixup_faces(const StepArgs& A, const PeakDesc& P
   }
 }
 
+// Shared-memory address of node number `node` (z fastest) of a (TS+1)^3 patch.
+template <int TS>
+__device__ __forceinline__ int dep_addr(int node) {
+  constexpr int T1 = TS + 1;
+  const int lx = node / (T1 * T1), r = node - lx * (T1 * T1), ly = r / T1, lz = r - ly * T1;
+  return lx * patch_ps(TS) + ly * patch_rs(TS) + lz;
+}
+// A node's chunk sum from its split accumulators (high word modulo 2^32, see deposit_super).
+__device__ __forceinline__ long long chunk_sum(u32 hi, u32 lo) {
+  const long long hs = hi >= 0xFFFFE000u ? (long long)hi - (1LL << 32) : (long long)hi;
+  return hs * (1LL << 19) + (long long)lo;
+}
+
 template <int TS>
 __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc& P, const PeakClock& C, int pk,
                                               u32 st, u32* smem, double* rho64) {
@@ -679,20 +692,23 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
   const long long total = e - b;
   __syncthreads();
   const u32 le = lanemask_le();
-  u64 acc[NPT];
+  u64 acc[NPT];  // nodes' sums of the chunks folded so far
 #pragma unroll
   for (int k = 0; k < NPT; ++k) acc[k] = 0ull;
-  // A node takes at most one contribution per particle of a chunk.  The high word of a
-  // contribution is in [-1, 2^20] (-1 for a remainder corner a few units below zero), the low
-  // word in [0, 2^20).  With CHUNK < 4096 the low sums stay below 2^32 and the high sums in
-  // [-CHUNK, CHUNK * 2^20], an interval shorter than 2^32 - 4096: kept modulo 2^32 in a u32,
-  // a value at or above 2^32 - 4096 is the negative one.  Both are exact.
-  constexpr int CH_IT = 4095 / DEP_THREADS;  // sweeps of DEP_THREADS particles per chunk
-  static_assert(CH_IT >= 1 && CH_IT * DEP_THREADS < 4096, "chunk too large for the split accumulators");
+  // Split accumulators.  A weight W (at most 2^38, at least -3 for a remainder corner) goes in as
+  // hi = W >> 19 in [-1, 2^19] and lo = W & (2^19 - 1).  A node takes at most one contribution
+  // per particle of a chunk, so with CHUNK <= 8191 the low sums stay below 2^32 and the high
+  // sums lie in [-CHUNK, CHUNK * 2^19], an interval shorter than 2^32 - 8192: kept modulo 2^32
+  // in a u32, a value at or above 2^32 - 8192 is the negative one.  Both are exact.  A typical
+  // super-tile (about TS^3 particles) is a single chunk.
+  constexpr int CH_IT = 8191 / DEP_THREADS;  // sweeps of DEP_THREADS particles per chunk
+  static_assert(CH_IT >= 1 && CH_IT * DEP_THREADS <= 8191, "chunk too large for the split accumulators");
+  static_assert(PM_FIX_BITS == 38, "the split accumulators assume 38 fractional bits");
   const long long nit = (total + DEP_THREADS - 1) / DEP_THREADS;
   long long j = b + threadIdx.x;
   int4 ps_n = j < e ? A.pos[j] : make_int4(-1, 0, 0, 0);
   bool bad = false;
+  int left = CH_IT;
   for (long long it = 0; it < nit; ++it) {
     const int4 ps = ps_n;
     const bool valid = j < e;
@@ -745,8 +761,8 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
         const int nb = lx * PS + ly * RS + lz;
 #define PM_ADD(off, W)                                                   \
   {                                                                      \
-    atomicAdd(&acc_hi[nb + (off)], (u32)(int)((long long)(W) >> 20));   \
-    atomicAdd(&acc_lo[nb + (off)], (u32)((W) & 0xFFFFFu));              \
+    atomicAdd(&acc_hi[nb + (off)], (u32)(int)((long long)(W) >> 19));   \
+    atomicAdd(&acc_lo[nb + (off)], (u32)((W) & 0x7FFFFu));              \
   }
         PM_ADD(0, W0)
         PM_ADD(1, W1)
@@ -759,16 +775,15 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
 #undef PM_ADD
       }
     }
-    if ((it + 1) % CH_IT == 0 || it + 1 == nit) {
+    if (--left == 0 && it + 1 < nit) {  // chunk full and more to come: fold it into registers
+      left = CH_IT;
       __syncthreads();
 #pragma unroll
       for (int q = 0; q < NPT; ++q) {
         const int node = threadIdx.x + q * DEP_THREADS;
         if (node < NN) {
-          const int ad = (node / (T1 * T1)) * PS + ((node / T1) % T1) * RS + node % T1;
-          const u32 h = acc_hi[ad];
-          const long long hs = h >= 0xFFFFF000u ? (long long)h - (1LL << 32) : (long long)h;
-          acc[q] += (u64)(hs * (1LL << 20)) + (u64)acc_lo[ad];
+          const int ad = dep_addr<TS>(node);
+          acc[q] += (u64)chunk_sum(acc_hi[ad], acc_lo[ad]);
           acc_hi[ad] = 0u;
           acc_lo[ad] = 0u;
         }
@@ -777,6 +792,7 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
     }
   }
   if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&A.stats[pk].status, 1u);
+  // Last chunk folded straight into the output: interior nodes final, the rest as partials.
   long long dsum = 0, smax = 0;
   const long long gbase = ((long long)sx * TS * N + (long long)sy * TS) * N + sz * TS;
   long long* face = A.face + P.face_off + (long long)st * P.fc;
@@ -785,8 +801,9 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
   for (int q = 0; q < NPT; ++q) {
     const int node = threadIdx.x + q * DEP_THREADS;
     if (node < NN) {
-      const int lz = node % T1, ly = (node / T1) % T1, lx = node / (T1 * T1);
-      const long long S = (long long)acc[q];
+      const int lx = node / (T1 * T1), r = node - lx * (T1 * T1), ly = r / T1, lz = r - ly * T1;
+      const int ad = lx * PS + ly * RS + lz;
+      const long long S = (long long)(acc[q] + (u64)chunk_sum(acc_hi[ad], acc_lo[ad]));
       if (lx == TS || ly == TS || lz == TS) {
         halo[halo_index(lx, ly, lz, TS)] = S;
       } else if (lx == 0 || ly == 0 || lz == 0) {

@@ -56,6 +56,7 @@ def slot_bytes(N: int) -> int:
 @dataclass
 class ServerConfig:
     slots: dict = field(default_factory=lambda: {64: 32, 128: 32, 256: 32})
+    tiles: object = None            # {N: super-tile side}, "auto" (autotuned) or None (default 16)
     budget_bytes: float = 150e9
     delta_collapse: float = 50.0
     keep_delta: bool = True
@@ -67,10 +68,15 @@ class Server:
         self.cfg = cfg
         torch = _lib.require_cuda()
         self._torch = torch
+        tiles = cfg.tiles
+        if tiles == "auto":
+            from .tune import autotune
+            tiles = autotune(cfg.slots, device=cfg.device)
+        tiles = tiles or {}
         peaks, self.slot_N = [], []
         for N in sorted(cfg.slots):
             for _ in range(cfg.slots[N]):
-                peaks.append(PeakConfig(N=N, Np=N, L=1.0))
+                peaks.append(PeakConfig(N=N, Np=N, L=1.0, tile=int(tiles.get(N, 0))))
                 self.slot_N.append(N)
         pool = sum(slot_bytes(N) for N in self.slot_N)
         if pool > cfg.budget_bytes:

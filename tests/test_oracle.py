@@ -112,3 +112,27 @@ def test_oracle_energy_identities():
         samples.append((a, k, w))
     assert np.max(np.abs(m)) <= 1e-12 * mesh.m_part * mesh.Np ** 3
     assert abs(O.layzer_irvine(samples)) <= 2e-2 * a * (k + abs(w))
+
+
+def test_torch64_oracle_matches_numpy_oracle():
+    """The float64 torch restatement (used for meshes too large for numpy) against the numpy
+    oracle on the CPU: forces, density and a few KDK steps."""
+    import torch
+    from oracle.pm3d_torch64 import TorchMesh, TorchTrajectory
+    from oracle.recipe_oracle import recipe_ic
+    N = 16
+    mesh = O.Mesh(N, 1.0, N, smooth=0.5)
+    ic = recipe_ic(mesh, R=(0.12, 0.1, 0.09), delta0=0.4, noise_frac=0.02, seed=6)
+    tm = TorchMesh(N, 1.0, N, smooth=0.5, device="cpu")
+    acc_t, d_t = tm.forces(torch.from_numpy(ic["x"]), 1.3)
+    acc_n, d_n = O.accelerations(mesh, ic["x"], 1.3)
+    assert np.max(np.abs(acc_t.numpy() - acc_n)) <= 1e-12 * np.max(np.abs(acc_n))
+    assert np.max(np.abs(d_t.numpy() - d_n)) <= 1e-12
+    tr_n = O.Trajectory(mesh, ic["x"], ic["p"])
+    tr_t = TorchTrajectory(tm, ic["x"], ic["p"])
+    a = 1.0
+    for _ in range(5):
+        tr_n.step(a, 0.05 * a)
+        a, _ = tr_t.step(a, 0.05 * a)
+    assert np.max(np.abs(tr_t.x.numpy() - tr_n.x)) <= 1e-12
+    assert np.max(np.abs(tr_t.p.numpy() - tr_n.p)) <= 1e-12 * np.max(np.abs(tr_n.p))
