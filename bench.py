@@ -174,8 +174,8 @@ def run_reference(args):
 def algorithmic_bytes(phase: str, n: int, cells: int, modes: int, npass: int) -> float:
     if phase == "push":        # read state 32, write state 32 + class 1, force grids 12 per cell
         return n * (32 + 32 + 1) + cells * 12.0
-    if phase == "sort":        # full Morton sort (every 16th step), amortised in the step time
-        return n * (4.0 + npass * 16.0 - 4.0) + n * 64.0
+    if phase == "sort":        # super-tile re-sort in shared memory (every 16th step): read + write state
+        return n * 64.0
     if phase == "bin":         # read class 1 + state 32, write state 32
         return n * 65.0
     if phase == "deposit":     # read positions 16, write delta 4 per cell (face/halo partials are overhead)
@@ -185,7 +185,7 @@ def algorithmic_bytes(phase: str, n: int, cells: int, modes: int, npass: int) ->
     return 0.0
 
 
-PHASES = ["push", "advance", "sort", "bin", "deposit", "r2c", "green", "c2r"]
+PHASES = ["push", "advance", "bin", "sort", "deposit", "r2c", "green", "c2r"]
 
 # DRAM bytes (read + write) per launch from one ncu capture of the plain 256^3 run
 # (profiles/kernels_plain256.md), per particle (per mode for Green), scaled to a launch by the
@@ -294,7 +294,7 @@ def run_ours(args):
                            regroup="Morton radix sort every step" if args.full_sort else
                            "re-binning each step, Morton radix sort every 16th", parallelism=f"replicas x{world}",
                            super_tiles={str(k): v for k, v in sorted(tiles.items())}),
-            "clocks": clocks, "gpu_launches": args.steps * (11 + npass), "roofline": roofline}
+            "clocks": clocks, "gpu_launches": args.steps * (13 + npass), "roofline": roofline}
 
     if rank == 0 and not args.no_plain and args.workload == "batched":
         pr = plain_rate(specs, steps=8, warmup=3, device=local, tiles=tiles)

@@ -103,9 +103,9 @@ int pm_set_particles(pm_engine* e, int peak, const double* x, const double* p, d
 int pm_run(pm_engine* e, int nsteps);
 
 /* pm_run without the graph, with a CUDA event between kernel phases on the engine's stream;
- * adds each phase's device time (ms) into phase_ms[8]: push, advance, sort (with its
- * permutation), re-binning, deposit (with the face fix-up), R2C, Green, C2R.  For per-kernel
- * rooflines. */
+ * adds each phase's device time (ms) into phase_ms[8]: push, energy + clock advance,
+ * re-binning, sorts (priming radix sort with its permutation; super-tile re-sort on refresh
+ * steps), deposit (with the face fix-up), R2C, Green, C2R.  For per-kernel rooflines. */
 int pm_run_timed(pm_engine* e, int nsteps, double* phase_ms);
 /* The engine's CUDA stream (cudaStream_t), for events and stream ordering by callers. */
 void* pm_engine_stream(pm_engine* e);

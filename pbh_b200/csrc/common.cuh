@@ -82,8 +82,8 @@ struct PeakClock {
   int max_steps;   // SCHED_RATIO length
   int sbuf;        // which super-tile start array describes the current grouping
   int dep;         // 1 when this step re-deposits (set by the advance kernel)
-  int sortstep;    // 1 when this step regroups by a full Morton-key sort (else re-binning)
-  int pad2;
+  int sortstep;    // 1 when this step groups by a full Morton-key sort (priming; else re-binning)
+  int refresh;     // 1 when this step re-sorts every super-tile's particles by cell after re-binning
   int has_delta;   // delta/grids hold data
   int stop_on_collapse;  // end the run (finalize) on the step that detects collapse
   double delta_collapse;  // collapse threshold on max delta (<= 0: not tracked)

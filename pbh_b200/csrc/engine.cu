@@ -83,12 +83,14 @@ struct pm_engine {
   double2* eslice = nullptr; // energy slice partials
   u32* ecount = nullptr;     // energy slices done per peak
   u32* sort_gate = nullptr;  // one word: any peak sorts this step
+  u32* refresh_gate = nullptr;  // one word: any peak re-sorts its super-tiles this step
   u32* totals = nullptr;
   long long* face = nullptr;
   long long* halo = nullptr;
   SortPlan sort{};       // Morton-key sort used by priming and every full_every steps
   int sort_result = 0;   // which (keys, vals) pair holds the sorted output
-  cudaGraphExec_t graph = nullptr;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // replayed step without / with the priming sort
+  bool prime_pending = false;  // a peak was (re)loaded: the next step must include the priming sort
   std::vector<char> occupied;  // host view: slots holding a run (dynamic mode FFT extents)
   long long bytes = 0;
 
@@ -122,6 +124,7 @@ struct pm_engine {
     A.far_count = far_count;
     A.far_fill = far_fill;
     A.sort_gate = sort_gate;
+    A.refresh_gate = refresh_gate;
     A.totals = totals;
     A.face = face;
     A.halo = halo;
@@ -168,9 +171,9 @@ struct pm_engine {
   }
 
   // One step for every peak.  With ev != nullptr an event is recorded after each phase and the
-  // phase times (push, advance, sort, re-bin, deposit with its face fix-up, R2C, Green, C2R) are
-  // accumulated.
-  int launch_step(cudaEvent_t* ev = nullptr, double* phase_ms = nullptr) {
+  // phase times (push, energy + advance, re-bin, sorts, deposit with its face fix-up, R2C, Green,
+  // C2R) are accumulated.
+  int launch_step(bool with_sort, cudaEvent_t* ev = nullptr, double* phase_ms = nullptr) {
     const StepArgs A = args();
     int k = 0;
     auto mark = [&]() -> cudaError_t { return ev ? cudaEventRecord(ev[k++], stream) : cudaSuccess; };
@@ -180,12 +183,15 @@ struct pm_engine {
     launch_energy(A, stream);
     launch_advance(A, stream);
     CU(mark());
-    int r = sort_run<u32>(&sort, keys[0], vals[0], keys[1], vals[1], true, true, stream);
-    if (r) return r;
-    launch_permute(A, ntot, stream);
-    launch_st_starts(A, ntot, stream);
-    CU(mark());
     launch_bin(A, nst, stream);
+    CU(mark());
+    int r = 0;
+    if (with_sort) {  // only steps that prime a peak: no launches at all in the steady state
+      if ((r = sort_run<u32>(&sort, keys[0], vals[0], keys[1], vals[1], true, true, stream))) return r;
+      launch_permute(A, ntot, stream);
+      launch_st_starts(A, ntot, stream);
+    }
+    launch_tile_sort(A, nst, stream);
     CU(mark());
     launch_deposit(A, nst, smem_dep, nullptr, stream);
     CU(mark());
@@ -208,21 +214,29 @@ struct pm_engine {
   }
 
   int step() {
+    const bool with_sort = prime_pending;
+    prime_pending = false;
     if ((flags & 2) && !(flags & 4)) {
-      if (!graph) {
+      cudaGraphExec_t& g = graph[with_sort ? 1 : 0];
+      if (!g) {
         cudaGraph_t cg = nullptr;
         CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-        int r = launch_step();
+        int r = launch_step(with_sort);
         cudaError_t ce = cudaStreamEndCapture(stream, &cg);
         if (r) return r;
         CU(ce);
-        CU(cudaGraphInstantiate(&graph, cg, 0));
+        CU(cudaGraphInstantiate(&g, cg, 0));
         cudaGraphDestroy(cg);
       }
-      CU(cudaGraphLaunch(graph, stream));
+      CU(cudaGraphLaunch(g, stream));
       return 0;
     }
-    return launch_step();
+    return launch_step(with_sort);
+  }
+  int step_timed(cudaEvent_t* ev, double* phase_ms) {
+    const bool with_sort = prime_pending;
+    prime_pending = false;
+    return launch_step(with_sort, ev, phase_ms);
   }
 
   int read_clock(int pk, PeakClock* c) {
@@ -231,13 +245,15 @@ struct pm_engine {
     return 0;
   }
   int write_clock(int pk, const PeakClock& c) {
+    if (c.state == PS_PRIME) prime_pending = true;
     CU(cudaMemcpyAsync(d_clocks + pk, &c, sizeof(PeakClock), cudaMemcpyHostToDevice, stream));
     CU(cudaStreamSynchronize(stream));
     return 0;
   }
 
   ~pm_engine() {
-    if (graph) cudaGraphExecDestroy(graph);
+    for (auto g : graph)
+      if (g) cudaGraphExecDestroy(g);
     for (auto& c : classes) {
       if (c.plans) {
         cufftDestroy(c.r2c);
@@ -254,7 +270,7 @@ struct pm_engine {
     sort_plan_destroy(&sort);
     void* bufs[] = {d_peaks, d_clocks, d_stats, d_st_base, d_p_base, d_mode_base, arrive, epart, wpart, eslice, ecount, pos, mom, tpos,
                     tmom, cls, keys[0], keys[1], vals[0], vals[1], sstart[0], sstart[1], counts, lpre, far_count,
-                    far_fill, sort_gate, totals, face, halo};
+                    far_fill, sort_gate, refresh_gate, totals, face, halo};
     for (void* b : bufs) cudaFree(b);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -440,6 +456,7 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   if ((r = E->alloc(&E->eslice, (size_t)npeaks * ENERGY_SLICES * 5))) return r;
   if ((r = E->alloc(&E->ecount, npeaks))) return r;
   if ((r = E->alloc(&E->sort_gate, 1))) return r;
+  if ((r = E->alloc(&E->refresh_gate, 1))) return r;
   if ((r = E->alloc(&E->totals, E->nst))) return r;
   if ((r = E->alloc(&E->face, E->nfc))) return r;
   if ((r = E->alloc(&E->halo, E->nhc))) return r;
@@ -466,6 +483,7 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   CU(cudaMemset(E->wpart, 0, sizeof(double2) * E->nmodeblk));
   CU(cudaMemset(E->ecount, 0, sizeof(u32) * npeaks));
   CU(cudaMemset(E->sort_gate, 0, sizeof(u32)));
+  CU(cudaMemset(E->refresh_gate, 0, sizeof(u32)));
   for (int b = 0; b < 2; ++b) CU(cudaMemset(E->sstart[b], 0, sizeof(u32) * E->nsst));
 
   // Sort plan: one segment per peak over the whole Morton key (sorted at priming and every
@@ -533,6 +551,7 @@ int pm_set_particles(pm_engine* e, int peak, const double* x, const double* p, d
   CU(cudaSetDevice(e->device));
   const StepArgs A = e->args();
   launch_reset_peak(A, peak, a0, mode, param, a_end, max_steps, e->stream);
+  e->prime_pending = true;
   launch_set_particles(A, peak, e->peaks[peak], x, p, e->stream);
   e->occupied[peak] = 1;
   CU(cudaGetLastError());
@@ -556,7 +575,7 @@ int pm_run_timed(pm_engine* e, int nsteps, double* phase_ms) {
   cudaEvent_t ev[10];
   for (int k = 0; k < 10; ++k) CU(cudaEventCreate(&ev[k]));
   int r = 0;
-  for (int s = 0; s < nsteps && !r; ++s) r = e->launch_step(ev, phase_ms);
+  for (int s = 0; s < nsteps && !r; ++s) r = e->step_timed(ev, phase_ms);
   for (int k = 0; k < 10; ++k) cudaEventDestroy(ev[k]);
   return r;
 }

@@ -80,7 +80,7 @@ __device__ __forceinline__ int bin_offset(int d, int NS) { return (NS <= 5 || d 
 // its new super-tile; per-class counts feed the re-binning.
 struct PushCoef {
   float kA, kB, D, gscale;
-  int run, sortnext;
+  int run;
 };
 
 template <int T>
@@ -154,7 +154,6 @@ __device__ __forceinline__ void push_one(const StepArgs& A, const PeakDesc& P, c
   bad |= !(isfinite(px) && isfinite(py) && isfinite(pz));
   A.tpos[j] = make_int4((nx << (2 * l2)) | (ny << l2) | nz, __float_as_int(fx), __float_as_int(fy), __float_as_int(fz));
   A.tmom[j] = make_float4(px, py, pz, m.w);
-  if (K.sortnext) A.keys_push[j] = pm_cell_key(nx, ny, nz);
   // Class of the destination super-tile.
   const int NS = P.NS;
   const int tx = nx >> P.log2TS, ty = ny >> P.log2TS, tz = nz >> P.log2TS;
@@ -264,7 +263,6 @@ __global__ void __launch_bounds__(PUSH_THREADS, 2) k_push(StepArgs A) {
     s_k.D = run ? (float)(da / (amid * amid * amid * pm_hubble(amid)) / P.dx) : 0.f;
     s_k.gscale = (float)(C.a_grid / a);
     s_k.run = run ? 1 : 0;
-    s_k.sortnext = run && ((C.nsteps + 1) % P.full_every == 0) ? 1 : 0;
   }
   __syncthreads();
   const PushCoef K = s_k;
@@ -279,7 +277,7 @@ __global__ void __launch_bounds__(PUSH_THREADS, 2) k_push(StepArgs A) {
 // Clock advance (one thread per peak): applies the step that the push kernel just made,
 // selects the next step size, whether this step regroups by sort, and which peaks re-deposit.
 __global__ void k_advance(StepArgs A) {
-  int any_sort = 0;
+  int any_sort = 0, any_refresh = 0;
   for (int pk = threadIdx.x; pk < A.npeaks; pk += blockDim.x) {
     PeakClock c = A.clocks[pk];
     const PeakDesc& P = A.peaks[pk];
@@ -296,6 +294,7 @@ __global__ void k_advance(StepArgs A) {
       case PS_PRIME:
         dep = 1;
         c.sortstep = 1;
+        c.refresh = 0;
         c.sbuf ^= 1;
         c.kpend = 0.0;
         c.a_grid = c.a;
@@ -308,7 +307,8 @@ __global__ void k_advance(StepArgs A) {
         c.a = an;
         c.a_grid = an;
         c.nsteps += 1;
-        c.sortstep = (c.nsteps % P.full_every) == 0 ? 1 : 0;
+        c.sortstep = 0;
+        c.refresh = (c.nsteps % P.full_every) == 0 ? 1 : 0;
         c.sbuf ^= 1;
         dep = 1;
         if (c.mode == SCHED_RATIO) {
@@ -325,6 +325,7 @@ __global__ void k_advance(StepArgs A) {
       case PS_FINALIZE:
         c.kpend = 0.0;
         c.sortstep = 0;
+        c.refresh = 0;
         c.sbuf ^= 1;
         dep = 1;
         c.state = PS_IDLE;
@@ -336,13 +337,18 @@ __global__ void k_advance(StepArgs A) {
     A.clocks[pk] = c;
     A.sortseg[pk].active = dep && c.sortstep;
     any_sort |= dep && c.sortstep;
+    any_refresh |= dep && c.refresh;
     if (dep) {
       A.stats[pk].max_fix = 0;
       A.stats[pk].mass_defect = 0;
     }
   }
   any_sort = __syncthreads_or(any_sort);
-  if (threadIdx.x == 0) *A.sort_gate = any_sort ? 1u : 0u;
+  any_refresh = __syncthreads_or(any_refresh);
+  if (threadIdx.x == 0) {
+    *A.sort_gate = any_sort ? 1u : 0u;
+    *A.refresh_gate = any_refresh ? 1u : 0u;
+  }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -571,6 +577,133 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_bin_scatter(StepArgs A) {
     }
     A.pos[dest] = ps;
     A.mom[dest] = m;
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Refresh: every full_every steps, after re-binning, each super-tile's particles are re-sorted
+// by cell (local Morton code of the cell inside the super-tile), so the deposit's and the
+// push's warps see neighbouring cells and same-cell runs again.  A counting sort per
+// super-tile: the order inside one cell is not kept (nothing downstream depends on it; the
+// deposit sums integers).  Up to TSORT_CAP particles the super-tile is staged in shared memory
+// and written back in place, coalesced (64 bytes of traffic per particle); denser super-tiles
+// go through the temporary state (push output, free after re-binning) and back.  Persistent
+// grid (one CTA per SM) over the super-tiles; every launch returns at once when no peak
+// refreshes this step.
+template <int TS>
+__device__ __forceinline__ void tile_sort(const StepArgs& A, const PeakDesc& P, const PeakClock& C, u32 st,
+                                          unsigned char* smem) {
+  constexpr int NCELL = TS * TS * TS;
+  u32* hist = (u32*)smem;                                           // [NCELL], then its prefix
+  int4* spos = (int4*)(smem + sizeof(u32) * 16 * 16 * 16);          // [TSORT_CAP]
+  float4* smom = (float4*)(spos + TSORT_CAP);                       // [TSORT_CAP]
+  u32* cr = (u32*)(smom + TSORT_CAP);                               // [TSORT_CAP] cell << 16 | rank
+  unsigned short* inv = (unsigned short*)(cr + TSORT_CAP);          // [TSORT_CAP] slot -> particle
+  __shared__ u32 s_wsum[TSORT_THREADS / 32];
+  const u32* ss = sst(A, C.sbuf) + P.sst_off;
+  const long long b = ss[st], e = ss[st + 1];
+  const int n = (int)(e - b);
+  if (n < 2) return;  // uniform
+  const int N = P.N, l2 = P.log2N;
+  const int sx = pm_compact3(st >> 2), sy = pm_compact3(st >> 1), sz = pm_compact3(st);
+  // Local cell code; masked into the super-tile so a corrupted grouping cannot index outside.
+  auto cell_of = [&](int c) -> u32 {
+    const int ix = c >> (2 * l2), iy = (c >> l2) & (N - 1), iz = c & (N - 1);
+    return pm_morton3((ix - sx * TS) & (TS - 1), (iy - sy * TS) & (TS - 1), (iz - sz * TS) & (TS - 1));
+  };
+  for (int i = threadIdx.x; i < NCELL; i += TSORT_THREADS) hist[i] = 0u;
+  __syncthreads();
+  const bool staged = n <= TSORT_CAP;
+  if (staged) {
+    for (int i = threadIdx.x; i < n; i += TSORT_THREADS) {
+      const int4 p = A.pos[b + i];
+      spos[i] = p;
+      smom[i] = A.mom[b + i];
+      const u32 c = cell_of(p.x);
+      cr[i] = (c << 16) | atomicAdd(&hist[c], 1u);
+    }
+  } else {
+    for (int i = threadIdx.x; i < n; i += TSORT_THREADS) {
+      const u32 c = cell_of(A.pos[b + i].x);
+      A.keys_push[b + i] = atomicAdd(&hist[c], 1u);
+    }
+  }
+  __syncthreads();
+  // Exclusive prefix of the cell counts (NCELL <= 4096 = 4 per thread).
+  {
+    constexpr int PER = (NCELL + TSORT_THREADS - 1) / TSORT_THREADS;
+    u32 v[PER];
+    u32 tot = 0;
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      const int i = threadIdx.x * PER + k;
+      v[k] = i < NCELL ? hist[i] : 0u;
+      tot += v[k];
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    u32 incl = tot;
+    for (int d = 1; d < 32; d <<= 1) {
+      const u32 t = __shfl_up_sync(0xffffffffu, incl, d);
+      if (lane >= d) incl += t;
+    }
+    if (lane == 31) s_wsum[warp] = incl;
+    __syncthreads();
+    u32 off = 0;
+    for (int w = 0; w < warp; ++w) off += s_wsum[w];
+    u32 run = off + incl - tot;
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      const int i = threadIdx.x * PER + k;
+      if (i < NCELL) hist[i] = run;
+      run += v[k];
+    }
+  }
+  __syncthreads();
+  if (staged) {
+    for (int i = threadIdx.x; i < n; i += TSORT_THREADS) {
+      const u32 x = cr[i];
+      inv[hist[x >> 16] + (x & 0xFFFFu)] = (unsigned short)i;
+    }
+    __syncthreads();
+    for (int o = threadIdx.x; o < n; o += TSORT_THREADS) {
+      const int i = inv[o];
+      A.pos[b + o] = spos[i];
+      A.mom[b + o] = smom[i];
+    }
+  } else {
+    for (int i = threadIdx.x; i < n; i += TSORT_THREADS) {
+      const int4 p = A.pos[b + i];
+      const long long d = b + hist[cell_of(p.x)] + A.keys_push[b + i];
+      A.tpos[d] = p;
+      A.tmom[d] = A.mom[b + i];
+    }
+    __syncthreads();  // the block's global writes are visible to the block after the barrier
+    for (int o = threadIdx.x; o < n; o += TSORT_THREADS) {
+      A.pos[b + o] = A.tpos[b + o];
+      A.mom[b + o] = A.tmom[b + o];
+    }
+  }
+  __syncthreads();  // shared arrays are reused by the next super-tile
+}
+
+__global__ void __launch_bounds__(TSORT_THREADS) k_tile_sort(StepArgs A, long long nst) {
+  extern __shared__ __align__(16) unsigned char s_ts[];
+  __shared__ int s_pk;
+  if (*A.refresh_gate == 0u) return;
+  for (long long t = blockIdx.x; t < nst; t += gridDim.x) {
+    if (threadIdx.x == 0) s_pk = pm_find(A.st_base, A.npeaks, t);
+    __syncthreads();
+    const int pk = s_pk;
+    __syncthreads();
+    const PeakClock& C = A.clocks[pk];
+    if (!(C.dep && C.refresh)) continue;
+    const PeakDesc& P = A.peaks[pk];
+    const u32 st = (u32)(t - A.st_base[pk]);
+    switch (P.TS) {
+      case 4: tile_sort<4>(A, P, C, st, s_ts); break;
+      case 8: tile_sort<8>(A, P, C, st, s_ts); break;
+      default: tile_sort<16>(A, P, C, st, s_ts); break;
+    }
   }
 }
 
@@ -987,6 +1120,7 @@ __global__ void k_reset_peak(StepArgs A, int pk, double a0, int mode, double par
   c.has_delta = 0;
   c.dep = 0;
   c.sortstep = 0;
+  c.refresh = 0;
   c.a_collapse = -1.0;
   c.stop_on_collapse = 0;
   if (mode == SCHED_RATIO) c.da = a0 * param;
@@ -1110,9 +1244,15 @@ __global__ void k_interp64(const double* __restrict__ F, const double* __restric
 size_t pm_deposit_smem(int TSmax) { return sizeof(u32) * 2 * (size_t)patch_size(TSmax); }
 size_t pm_push_smem(int TSmax) { return sizeof(float) * 3 * (size_t)patch_size(TSmax); }
 
+size_t pm_tile_sort_smem() {
+  return sizeof(u32) * 16 * 16 * 16 + (size_t)TSORT_CAP * (sizeof(int4) + sizeof(float4) + sizeof(u32) + sizeof(unsigned short));
+}
+
 int pm_kernels_init() {
   cudaError_t e = cudaFuncSetAttribute(k_push, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_deposit, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_tile_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pm_tile_sort_smem());
   return e == cudaSuccess ? 0 : -(int)e;
 }
 
@@ -1142,6 +1282,9 @@ void launch_permute(const StepArgs& A, long long ntot, cudaStream_t s) {
 }
 void launch_st_starts(const StepArgs& A, long long ntot, cudaStream_t s) {
   k_st_starts<<<stride_grid(ntot, PM_THREADS, 8), PM_THREADS, 0, s>>>(A, ntot);
+}
+void launch_tile_sort(const StepArgs& A, long long nst, cudaStream_t s) {
+  k_tile_sort<<<stride_grid(nst, 1, 1), TSORT_THREADS, pm_tile_sort_smem(), s>>>(A, nst);
 }
 void launch_bin(const StepArgs& A, long long nst, cudaStream_t s) {
   k_bin_scan1<<<(unsigned)nst, BIN_CLASSES, 0, s>>>(A);

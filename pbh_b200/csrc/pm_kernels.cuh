@@ -7,9 +7,10 @@
 //              (one of <= 125 neighbours) and counted per class
 //   energy     per peak: momentum, kinetic and potential energy, Layzer-Irvine integral
 //   advance    per peak clock (and which peaks regroup by sort this step)
-//   regroup    re-binning (scan of the class counts, then a scatter into the new grouping) for
-//              most steps; a full Morton-key radix sort plus a permutation every full_every
-//              steps and when particles are first loaded
+//   regroup    re-binning (scan of the class counts, then a scatter into the new grouping);
+//              every full_every steps each super-tile's particles are then re-sorted by cell
+//              (local counting sort); when particles are first loaded, a full Morton-key radix
+//              sort plus a permutation instead
 //   deposit    per super-tile: CIC density of its particles into (TS+1)^3 nodes; interior nodes
 //              final, face and upper-halo nodes as 64-bit partials; the last of the 8 tiles
 //              that feed a super-tile's lower faces finishes them (own partial + neighbours'
@@ -24,6 +25,8 @@
 #define DEP_THREADS 512
 #define GREEN_MODES 4      // modes per thread of the Green kernel (a block covers PM_THREADS * GREEN_MODES)
 #define ENERGY_SLICES 16   // CTAs per peak of the energy reduction
+#define TSORT_THREADS 1024 // super-tile sort (refresh) CTA
+#define TSORT_CAP 5120     // particles of a super-tile sorted in shared memory; denser ones via global
 #define BIN_CLASSES 128   // stride of the per-super-tile class arrays (>= 125)
 #define BIN_FAR 255       // class of a particle that moved more than 2 super-tiles
 
@@ -34,6 +37,7 @@ struct StepArgs {
   PeakStats* stats;
   SortSeg* sortseg;            // sort activity flags, written by the advance kernel
   u32* sort_gate;              // 1 when any peak regroups by sort this step (advance kernel)
+  u32* refresh_gate;           // 1 when any peak re-sorts its super-tiles this step (advance kernel)
   const long long* st_base;    // [npeaks + 1] prefix of super-tiles
   const long long* p_base;     // [npeaks + 1] prefix of particles
   const long long* mode_base;  // [npeaks + 1] prefix of Green blocks
@@ -45,7 +49,8 @@ struct StepArgs {
   int4* tpos;                  // push output (same order as the input), regrouped into pos/mom
   float4* tmom;
   unsigned char* cls;          // per particle: re-binning class or BIN_FAR
-  u32* keys_push;              // Morton keys written by push / set_particles (sort input)
+  u32* keys_push;              // Morton keys written by set_particles / reload (priming sort input);
+                               // per-particle scratch of the super-tile sort on refresh steps
   const u32* keys_sorted;      // sort output keys
   const u32* perm;             // sort output permutation
   u32* sstart[2];              // super-tile starts, two generations (clock.sbuf selects)
@@ -82,6 +87,7 @@ void launch_energy(const StepArgs& A, cudaStream_t s);
 void launch_permute(const StepArgs& A, long long ntot, cudaStream_t s);
 void launch_st_starts(const StepArgs& A, long long ntot, cudaStream_t s);
 void launch_bin(const StepArgs& A, long long nst, cudaStream_t s);
+void launch_tile_sort(const StepArgs& A, long long nst, cudaStream_t s);
 void launch_deposit(const StepArgs& A, long long nst, size_t smem, double* rho64, cudaStream_t s);
 void launch_green(const StepArgs& A, long long nblocks, cudaStream_t s);
 
