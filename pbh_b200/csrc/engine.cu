@@ -77,7 +77,6 @@ struct pm_engine {
   u32* lpre = nullptr;
   u32* far_count = nullptr;
   u32* far_fill = nullptr;
-  u32* arrive = nullptr;     // per super-tile face arrivals of the deposit (0 between steps)
   double2* epart = nullptr;  // push partials of the energy sums
   double2* wpart = nullptr;  // Green partials of the potential energy
   double2* eslice = nullptr; // energy slice partials
@@ -103,7 +102,6 @@ struct pm_engine {
     A.st_base = d_st_base;
     A.p_base = d_p_base;
     A.mode_base = d_mode_base;
-    A.arrive = arrive;
     A.epart = epart;
     A.wpart = wpart;
     A.eslice = eslice;
@@ -194,6 +192,7 @@ struct pm_engine {
     launch_tile_sort(A, nst, stream);
     CU(mark());
     launch_deposit(A, nst, smem_dep, nullptr, stream);
+    launch_fixup(A, nst, nullptr, stream);
     CU(mark());
     if ((r = fft_r2c())) return r;
     CU(mark());
@@ -268,7 +267,7 @@ struct pm_engine {
       cudaFree(c.force);
     }
     sort_plan_destroy(&sort);
-    void* bufs[] = {d_peaks, d_clocks, d_stats, d_st_base, d_p_base, d_mode_base, arrive, epart, wpart, eslice, ecount, pos, mom, tpos,
+    void* bufs[] = {d_peaks, d_clocks, d_stats, d_st_base, d_p_base, d_mode_base, epart, wpart, eslice, ecount, pos, mom, tpos,
                     tmom, cls, keys[0], keys[1], vals[0], vals[1], sstart[0], sstart[1], counts, lpre, far_count,
                     far_fill, sort_gate, refresh_gate, totals, face, halo};
     for (void* b : bufs) cudaFree(b);
@@ -450,7 +449,6 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   if ((r = E->alloc(&E->lpre, E->nst * BIN_CLASSES))) return r;
   if ((r = E->alloc(&E->far_count, E->nst))) return r;
   if ((r = E->alloc(&E->far_fill, E->nst))) return r;
-  if ((r = E->alloc(&E->arrive, E->nst))) return r;
   if ((r = E->alloc(&E->epart, 4 * E->nst))) return r;
   if ((r = E->alloc(&E->wpart, E->nmodeblk))) return r;
   if ((r = E->alloc(&E->eslice, (size_t)npeaks * ENERGY_SLICES * 5))) return r;
@@ -478,7 +476,6 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   CU(cudaMemset(E->tmom, 0, sizeof(float4) * E->ntot));
   CU(cudaMemset(E->far_count, 0, sizeof(u32) * E->nst));
   CU(cudaMemset(E->far_fill, 0, sizeof(u32) * E->nst));
-  CU(cudaMemset(E->arrive, 0, sizeof(u32) * E->nst));
   CU(cudaMemset(E->epart, 0, sizeof(double2) * 4 * E->nst));
   CU(cudaMemset(E->wpart, 0, sizeof(double2) * E->nmodeblk));
   CU(cudaMemset(E->ecount, 0, sizeof(u32) * npeaks));
@@ -714,6 +711,7 @@ int pm_get_counts(pm_engine* e, int peak, double* counts) {
   CU(cudaMemcpy(e->d_stats + peak, &st, sizeof(PeakStats), cudaMemcpyHostToDevice));
   // Same kernels with the extra float64 output; delta is rewritten with identical values.
   launch_deposit(e->args(), e->nst, e->smem_dep, counts, e->stream);
+  launch_fixup(e->args(), e->nst, counts, e->stream);
   CU(cudaGetLastError());
   CU(cudaStreamSynchronize(e->stream));
   CU(cudaMemcpy(e->d_clocks, all.data(), sizeof(PeakClock) * e->npeaks, cudaMemcpyHostToDevice));

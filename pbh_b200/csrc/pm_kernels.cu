@@ -719,11 +719,8 @@ __global__ void __launch_bounds__(TSORT_THREADS) k_tile_sort(StepArgs A, long lo
 // lower faces (which neighbours also reach) and on the upper halo (which belongs to the
 // neighbours) are written as 64-bit partials.
 //
-// Face fix-up in the same launch: super-tile Y's face nodes are complete once Y and its 7 lower
-// neighbours have written their partials.  Every CTA, after its partials, counts itself in at
-// Y = S + o for the 8 offsets o in {0,1}^3 (a bijection per o, so each Y is counted exactly 8
-// times per step); the CTA that arrives 8th finishes Y's faces (own partial + the neighbours'
-// halo partials, still in L2) and clears the counter.  No CTA waits on another.
+// The face fix-up (k_fixup, the next launch) completes the face nodes: own partial plus the
+// lower neighbours' halo partials.
 // Integer sums make the result independent of particle order, bit for bit; no float atomics.
 __device__ __forceinline__ int face_index(int lx, int ly, int lz, int T) {
   if (lx == 0) return ly * T + lz;
@@ -755,7 +752,8 @@ __device__ __forceinline__ void face_coords(int f, int& lx, int& ly, int& lz) {
   }
 }
 
-// Finish the face nodes of super-tile Y (whole CTA).  Adds to the caller's statistics.
+// Finish the face nodes of super-tile Y (whole CTA of FIX_THREADS).  Adds to the caller's
+// statistics.
 template <int TS>
 __device__ __forceinline__ void fixup_faces(const StepArgs& A, const PeakDesc& P, u32 Y, double* rho64,
                                             long long& dsum, long long& smax) {
@@ -767,7 +765,6 @@ __device__ __forceinline__ void fixup_faces(const StepArgs& A, const PeakDesc& P
   __shared__ const long long* s_nb[8];
   const int NS = P.NS, N = P.N;
   const int sx = pm_compact3(Y >> 2), sy = pm_compact3(Y >> 1), sz = pm_compact3(Y);
-  __syncthreads();  // s_nb of a previous call has been read
   if (threadIdx.x < 8) {
     const int o = threadIdx.x, ox = o & 1, oy = (o >> 1) & 1, oz = (o >> 2) & 1;
     const u32 sn = pm_morton3((sx - ox) & (NS - 1), (sy - oy) & (NS - 1), (sz - oz) & (NS - 1));
@@ -775,7 +772,7 @@ __device__ __forceinline__ void fixup_faces(const StepArgs& A, const PeakDesc& P
   }
   __syncthreads();
   const long long* face = A.face + P.face_off + (long long)Y * FC;
-  for (int f = threadIdx.x; f < FC; f += DEP_THREADS) {
+  for (int f = threadIdx.x; f < FC; f += FIX_THREADS) {
     int lx, ly, lz;
     face_coords<TS>(f, lx, ly, lz);
     long long S = __ldcg(face + f);
@@ -815,11 +812,11 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
   u32* acc_lo = smem + SZ;
   __shared__ long long s_red[DEP_THREADS / 32];
   __shared__ long long s_max[DEP_THREADS / 32];
-  __shared__ u32 s_last;
   const int N = P.N, l2 = P.log2N;
   const int sx = pm_compact3(st >> 2), sy = pm_compact3(st >> 1), sz = pm_compact3(st);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int i = threadIdx.x; i < 2 * SZ; i += DEP_THREADS) smem[i] = 0u;
+  static_assert((2 * SZ) % 4 == 0, "accumulators are cleared 16 bytes at a time");
+  for (int i = threadIdx.x; i < 2 * SZ / 4; i += DEP_THREADS) reinterpret_cast<uint4*>(smem)[i] = make_uint4(0u, 0u, 0u, 0u);
   const u32* ss = sst(A, C.sbuf) + P.sst_off;
   const long long b = ss[st], e = ss[st + 1];
   const long long total = e - b;
@@ -951,28 +948,6 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
       }
     }
   }
-  // Count this tile in at the 8 super-tiles whose faces it feeds; finish those it completes.
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) s_last = 0u;
-  __syncthreads();
-  const int NS = P.NS;
-  if (threadIdx.x < 8) {
-    const int o = threadIdx.x;
-    const u32 Y = pm_morton3((sx + (o & 1)) & (NS - 1), (sy + ((o >> 1) & 1)) & (NS - 1), (sz + ((o >> 2) & 1)) & (NS - 1));
-    if (atomicAdd(&A.arrive[P.st_base + Y], 1u) == 7u) atomicOr(&s_last, 1u << o);
-  }
-  __syncthreads();
-  const u32 last = s_last;
-  if (last) {
-    __threadfence();
-    for (int o = 0; o < 8; ++o) {
-      if (!((last >> o) & 1u)) continue;
-      const u32 Y = pm_morton3((sx + (o & 1)) & (NS - 1), (sy + ((o >> 1) & 1)) & (NS - 1), (sz + ((o >> 2) & 1)) & (NS - 1));
-      fixup_faces<TS>(A, P, Y, rho64, dsum, smax);
-      if (threadIdx.x == 0) A.arrive[P.st_base + Y] = 0u;  // all 8 arrivals of this step are in
-    }
-  }
   for (int d = 16; d > 0; d >>= 1) {
     dsum += __shfl_xor_sync(0xffffffffu, dsum, d);
     const long long om = __shfl_xor_sync(0xffffffffu, smax, d);
@@ -1006,6 +981,42 @@ __global__ void __launch_bounds__(DEP_THREADS, 2) k_deposit(StepArgs A, double* 
     case 4: deposit_super<4>(A, P, C, tr.pk, (u32)tr.t, s_dep, rho64); break;
     case 8: deposit_super<8>(A, P, C, tr.pk, (u32)tr.t, s_dep, rho64); break;
     default: deposit_super<16>(A, P, C, tr.pk, (u32)tr.t, s_dep, rho64); break;
+  }
+}
+
+// Face fix-up: one CTA per super-tile whose peak deposited this step.  Small and
+// latency-bound, so many CTAs per SM; the partials are fresh in L2.
+__global__ void __launch_bounds__(FIX_THREADS) k_fixup(StepArgs A, double* rho64) {
+  __shared__ long long s_red[FIX_THREADS / 32];
+  __shared__ long long s_max[FIX_THREADS / 32];
+  const TileRef tr = find_tile(A.st_base, A.npeaks);
+  if (!A.clocks[tr.pk].dep) return;
+  const PeakDesc& P = A.peaks[tr.pk];
+  long long dsum = 0, smax = 0;
+  switch (P.TS) {
+    case 4: fixup_faces<4>(A, P, (u32)tr.t, rho64, dsum, smax); break;
+    case 8: fixup_faces<8>(A, P, (u32)tr.t, rho64, dsum, smax); break;
+    default: fixup_faces<16>(A, P, (u32)tr.t, rho64, dsum, smax); break;
+  }
+  for (int d = 16; d > 0; d >>= 1) {
+    dsum += __shfl_xor_sync(0xffffffffu, dsum, d);
+    const long long om = __shfl_xor_sync(0xffffffffu, smax, d);
+    smax = om > smax ? om : smax;
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    s_red[warp] = dsum;
+    s_max[warp] = smax;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long ts = 0, tm = 0;
+    for (int w = 0; w < FIX_THREADS / 32; ++w) {
+      ts += s_red[w];
+      tm = s_max[w] > tm ? s_max[w] : tm;
+    }
+    atomicAdd((unsigned long long*)&A.stats[tr.pk].mass_defect, (unsigned long long)ts);
+    atomicMax(&A.stats[tr.pk].max_fix, (u64)tm);
   }
 }
 
@@ -1293,6 +1304,9 @@ void launch_bin(const StepArgs& A, long long nst, cudaStream_t s) {
 }
 void launch_deposit(const StepArgs& A, long long nst, size_t smem, double* rho64, cudaStream_t s) {
   k_deposit<<<(unsigned)nst, DEP_THREADS, smem, s>>>(A, rho64);
+}
+void launch_fixup(const StepArgs& A, long long nst, double* rho64, cudaStream_t s) {
+  k_fixup<<<(unsigned)nst, FIX_THREADS, 0, s>>>(A, rho64);
 }
 void launch_green(const StepArgs& A, long long nblocks, cudaStream_t s) {
   k_green<<<(unsigned)nblocks, PM_THREADS, 0, s>>>(A);

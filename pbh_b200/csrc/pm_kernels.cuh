@@ -12,9 +12,8 @@
 //              (local counting sort); when particles are first loaded, a full Morton-key radix
 //              sort plus a permutation instead
 //   deposit    per super-tile: CIC density of its particles into (TS+1)^3 nodes; interior nodes
-//              final, face and upper-halo nodes as 64-bit partials; the last of the 8 tiles
-//              that feed a super-tile's lower faces finishes them (own partial + neighbours'
-//              halo partials) in the same launch
+//              final, face and upper-halo nodes as 64-bit partials
+//   fixup      per super-tile: face nodes = own partial + the lower neighbours' halo partials
 //   R2C, Green, C2R (x3)
 #pragma once
 #include "common.cuh"
@@ -25,6 +24,7 @@
 #define DEP_THREADS 512
 #define GREEN_MODES 4      // modes per thread of the Green kernel (a block covers PM_THREADS * GREEN_MODES)
 #define ENERGY_SLICES 16   // CTAs per peak of the energy reduction
+#define FIX_THREADS 256    // face fix-up CTA
 #define TSORT_THREADS 1024 // super-tile sort (refresh) CTA
 #define TSORT_CAP 5120     // particles of a super-tile sorted in shared memory; denser ones via global
 #define BIN_CLASSES 128   // stride of the per-super-tile class arrays (>= 125)
@@ -41,7 +41,6 @@ struct StepArgs {
   const long long* st_base;    // [npeaks + 1] prefix of super-tiles
   const long long* p_base;     // [npeaks + 1] prefix of particles
   const long long* mode_base;  // [npeaks + 1] prefix of Green blocks
-  u32* arrive;                 // [super-tile] deposits counted in at its faces this step (0..8)
   int npeaks;
   int pad;
   int4* pos;                   // state, grouped by super-tile
@@ -89,6 +88,7 @@ void launch_st_starts(const StepArgs& A, long long ntot, cudaStream_t s);
 void launch_bin(const StepArgs& A, long long nst, cudaStream_t s);
 void launch_tile_sort(const StepArgs& A, long long nst, cudaStream_t s);
 void launch_deposit(const StepArgs& A, long long nst, size_t smem, double* rho64, cudaStream_t s);
+void launch_fixup(const StepArgs& A, long long nst, double* rho64, cudaStream_t s);
 void launch_green(const StepArgs& A, long long nblocks, cudaStream_t s);
 
 // Host-requested per-peak operations.
