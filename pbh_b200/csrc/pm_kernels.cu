@@ -252,7 +252,7 @@ __global__ void __launch_bounds__(PUSH_THREADS, 2) k_push(StepArgs A) {
   const TileRef tr = find_tile(A.st_base, A.npeaks);
   const PeakClock C = A.clocks[tr.pk];
   if (C.state != PS_RUN && C.state != PS_FINALIZE) return;
-  const PeakDesc& P = A.peaks[tr.pk];
+  const PeakDesc P = A.peaks[tr.pk];
   if (threadIdx.x < BIN_CLASSES) s_cnt[threadIdx.x] = 0u;
   if (threadIdx.x == 0) {
     const double a = C.a, da = C.da;
@@ -280,7 +280,7 @@ __global__ void k_advance(StepArgs A) {
   int any_sort = 0, any_refresh = 0;
   for (int pk = threadIdx.x; pk < A.npeaks; pk += blockDim.x) {
     PeakClock c = A.clocks[pk];
-    const PeakDesc& P = A.peaks[pk];
+    const PeakDesc P = A.peaks[pk];
     int dep = 0;
     // Collapse detection on the deposit of the current positions (made by the previous step).
     if (c.has_delta && c.delta_collapse > 0 && c.a_collapse < 0 && c.state != PS_PRIME) {
@@ -362,7 +362,7 @@ __global__ void __launch_bounds__(PM_THREADS) k_energy(StepArgs A) {
   const int pk = blockIdx.y, sl = blockIdx.x;
   const PeakClock C = A.clocks[pk];
   if (C.state != PS_RUN && C.state != PS_FINALIZE) return;
-  const PeakDesc& P = A.peaks[pk];
+  const PeakDesc P = A.peaks[pk];
   __shared__ CSum s_w[PM_THREADS / 32][5];
   __shared__ u32 s_last;
   CSum v[5];
@@ -442,7 +442,7 @@ __global__ void k_permute(StepArgs A, long long ntot) {
   if (*A.sort_gate == 0u) return;
   for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < ntot; j += (long long)gridDim.x * blockDim.x) {
     const int pk = pm_find(A.p_base, A.npeaks, j);
-    const PeakClock& C = A.clocks[pk];
+    const PeakClock C = A.clocks[pk];
     if (!(C.dep && C.sortstep)) continue;
     const u32 q = A.perm[j];
     A.pos[j] = A.tpos[q];
@@ -454,9 +454,9 @@ __global__ void k_st_starts(StepArgs A, long long ntot) {
   if (*A.sort_gate == 0u) return;
   for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < ntot; j += (long long)gridDim.x * blockDim.x) {
     const int pk = pm_find(A.p_base, A.npeaks, j);
-    const PeakClock& C = A.clocks[pk];
+    const PeakClock C = A.clocks[pk];
     if (!(C.dep && C.sortstep)) continue;
-    const PeakDesc& P = A.peaks[pk];
+    const PeakDesc P = A.peaks[pk];
     u32* ss = sst(A, C.sbuf) + P.sst_off;
     const int b = (int)(A.keys_sorted[j] >> P.st_shift);
     const int bprev = j == P.p_off ? -1 : (int)(A.keys_sorted[j - 1] >> P.st_shift);
@@ -473,9 +473,9 @@ __global__ void k_st_starts(StepArgs A, long long ntot) {
 __global__ void __launch_bounds__(BIN_CLASSES) k_bin_scan1(StepArgs A) {
   __shared__ u32 s_w[BIN_CLASSES / 32];
   const TileRef tr = find_tile(A.st_base, A.npeaks);
-  const PeakClock& C = A.clocks[tr.pk];
+  const PeakClock C = A.clocks[tr.pk];
   if (!(C.dep && !C.sortstep)) return;
-  const PeakDesc& P = A.peaks[tr.pk];
+  const PeakDesc P = A.peaks[tr.pk];
   const u32 D = (u32)tr.t;
   const int dx = pm_compact3(D >> 2), dy = pm_compact3(D >> 1), dz = pm_compact3(D);
   const int c = threadIdx.x, lane = c & 31, warp = c >> 5;
@@ -504,9 +504,9 @@ __global__ void __launch_bounds__(1024) k_bin_scan2(StepArgs A) {
   __shared__ u32 s_w[32];
   __shared__ long long s_carry;
   const int pk = blockIdx.x;
-  const PeakClock& C = A.clocks[pk];
+  const PeakClock C = A.clocks[pk];
   if (!(C.dep && !C.sortstep)) return;
-  const PeakDesc& P = A.peaks[pk];
+  const PeakDesc P = A.peaks[pk];
   u32* ss = sst(A, C.sbuf) + P.sst_off;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (threadIdx.x == 0) s_carry = P.p_off;
@@ -539,9 +539,9 @@ __global__ void __launch_bounds__(1024) k_bin_scan2(StepArgs A) {
 __global__ void __launch_bounds__(PUSH_THREADS) k_bin_scatter(StepArgs A) {
   __shared__ u32 s_rank[BIN_CLASSES];
   const TileRef tr = find_tile(A.st_base, A.npeaks);
-  const PeakClock& C = A.clocks[tr.pk];
+  const PeakClock C = A.clocks[tr.pk];
   if (!(C.dep && !C.sortstep)) return;
-  const PeakDesc& P = A.peaks[tr.pk];
+  const PeakDesc P = A.peaks[tr.pk];
   const u32 S = (u32)tr.t;
   const u32* old = sst(A, C.sbuf ^ 1) + P.sst_off;
   const u32* ss = sst(A, C.sbuf) + P.sst_off;
@@ -695,9 +695,9 @@ __global__ void __launch_bounds__(TSORT_THREADS) k_tile_sort(StepArgs A, long lo
     __syncthreads();
     const int pk = s_pk;
     __syncthreads();
-    const PeakClock& C = A.clocks[pk];
+    const PeakClock C = A.clocks[pk];
     if (!(C.dep && C.refresh)) continue;
-    const PeakDesc& P = A.peaks[pk];
+    const PeakDesc P = A.peaks[pk];
     const u32 st = (u32)(t - A.st_base[pk]);
     switch (P.TS) {
       case 4: tile_sort<4>(A, P, C, st, s_ts); break;
@@ -976,7 +976,7 @@ __global__ void __launch_bounds__(DEP_THREADS, 2) k_deposit(StepArgs A, double* 
   const TileRef tr = find_tile(A.st_base, A.npeaks);
   const PeakClock C = A.clocks[tr.pk];
   if (!C.dep) return;
-  const PeakDesc& P = A.peaks[tr.pk];
+  const PeakDesc P = A.peaks[tr.pk];
   switch (P.TS) {
     case 4: deposit_super<4>(A, P, C, tr.pk, (u32)tr.t, s_dep, rho64); break;
     case 8: deposit_super<8>(A, P, C, tr.pk, (u32)tr.t, s_dep, rho64); break;
@@ -991,7 +991,7 @@ __global__ void __launch_bounds__(FIX_THREADS) k_fixup(StepArgs A, double* rho64
   __shared__ long long s_max[FIX_THREADS / 32];
   const TileRef tr = find_tile(A.st_base, A.npeaks);
   if (!A.clocks[tr.pk].dep) return;
-  const PeakDesc& P = A.peaks[tr.pk];
+  const PeakDesc P = A.peaks[tr.pk];
   long long dsum = 0, smax = 0;
   switch (P.TS) {
     case 4: fixup_faces<4>(A, P, (u32)tr.t, rho64, dsum, smax); break;
@@ -1039,46 +1039,49 @@ __device__ __forceinline__ float grad_k(float k, float dx, int mode) {
   return k;
 }
 
-__device__ __forceinline__ double green_mode(const PeakDesc& P, long long m, float s_c) {
-  const int N = P.N, Nh = N / 2 + 1;
+// Per-peak constants of the Green kernel, read once into registers.
+struct GreenCtx {
+  int N, log2N, Nh, gm;
+  long long M;
+  double inv_nh;
+  float kf, dx, sd2, s_c;
+  const float2* spec;
+  float2* out;
+};
+
+__device__ __forceinline__ double green_mode(const GreenCtx& g, long long m, float2 d) {
+  const int N = g.N, Nh = g.Nh;
   // m = row * Nh + kz without an integer division: the double quotient is off by at most one.
-  long long rest = (long long)((double)m * P.inv_nh);
+  long long rest = (long long)((double)m * g.inv_nh);
   if (rest * Nh > m) --rest;
   else if ((rest + 1) * Nh <= m) ++rest;
   const int kz = (int)(m - rest * Nh);
-  const int iy = (int)(rest & (N - 1)), ix = (int)(rest >> P.log2N);
-  const float kf = (float)(kTwoPi / P.L), dx = (float)P.dx;
-  const float kx = kline(ix, N, kf), ky = kline(iy, N, kf), kzv = kf * (float)kz;
+  const int iy = (int)(rest & (N - 1)), ix = (int)(rest >> g.log2N);
+  const float kx = kline(ix, N, g.kf), ky = kline(iy, N, g.kf), kzv = g.kf * (float)kz;
   const float k2 = kx * kx + ky * ky + kzv * kzv;
-  const long long M = P.nmodes;
-  float2* out = P.gspec;
+  const long long M = g.M;
   if (m == 0) {
-    out[0] = out[M] = out[2 * M] = make_float2(0.f, 0.f);
+    g.out[0] = g.out[M] = g.out[2 * M] = make_float2(0.f, 0.f);
     return 0.0;
   }
-  float G = s_c / k2;
-  if (P.smooth > 0) {
-    const float sd = (float)(P.smooth * P.dx);
-    G *= expf(-0.5f * k2 * sd * sd);
-  }
-  const int gm = P.gradient;
-  const float gx = grad_k(kx, dx, gm) * G, gy = grad_k(ky, dx, gm) * G, gz = grad_k(kzv, dx, gm) * G;
-  const float2 d = P.spec[m];
+  float G = g.s_c / k2;
+  if (g.sd2 > 0.f) G *= expf(-0.5f * k2 * g.sd2);
+  const float gx = grad_k(kx, g.dx, g.gm) * G, gy = grad_k(ky, g.dx, g.gm) * G, gz = grad_k(kzv, g.dx, g.gm) * G;
   // -i k G d = (k G d.y, -k G d.x)
   float2 ox = make_float2(gx * d.y, -gx * d.x), oy = make_float2(gy * d.y, -gy * d.x),
          oz = make_float2(gz * d.y, -gz * d.x);
   if (kz == 0 || kz == N / 2) {
     const int px = (-ix) & (N - 1), py = (-iy) & (N - 1);
-    const float2 dp = P.spec[((long long)px * N + py) * Nh + kz];
-    const float hx = grad_k(kline(px, N, kf), dx, gm) * G, hy = grad_k(kline(py, N, kf), dx, gm) * G;
+    const float2 dp = g.spec[((long long)px * N + py) * Nh + kz];
+    const float hx = grad_k(kline(px, N, g.kf), g.dx, g.gm) * G, hy = grad_k(kline(py, N, g.kf), g.dx, g.gm) * G;
     // (v + conj(v_partner)) / 2 with v_partner = (h dp.y, -h dp.x)
     ox = make_float2(0.5f * (ox.x + hx * dp.y), 0.5f * (ox.y + hx * dp.x));
     oy = make_float2(0.5f * (oy.x + hy * dp.y), 0.5f * (oy.y + hy * dp.x));
     oz = make_float2(0.5f * (oz.x + gz * dp.y), 0.5f * (oz.y + gz * dp.x));
   }
-  out[m] = ox;
-  out[M + m] = oy;
-  out[2 * M + m] = oz;
+  g.out[m] = ox;
+  g.out[M + m] = oy;
+  g.out[2 * M + m] = oz;
   // Potential-energy term: sum_x delta Phi = sum_k |delta_k|^2 G_k over the full spectrum; the
   // half spectrum counts each kz in (0, N/2) twice.
   const double wk = (kz == 0 || kz == N / 2) ? 1.0 : 2.0;
@@ -1087,27 +1090,43 @@ __device__ __forceinline__ double green_mode(const PeakDesc& P, long long m, flo
 
 __global__ void __launch_bounds__(PM_THREADS) k_green(StepArgs A) {
   __shared__ int s_pk;
-  __shared__ float s_c;
   __shared__ CSum s_w[PM_THREADS / 32];
-  if (threadIdx.x == 0) {
-    s_pk = pm_find(A.mode_base, A.npeaks, (long long)blockIdx.x);
-    const PeakDesc& P = A.peaks[s_pk];
-    const double n3 = (double)P.N * P.N * P.N;
-    s_c = (float)(-1.5 * PM_H_I * PM_H_I / A.clocks[s_pk].a_grid / n3);
-  }
+  if (threadIdx.x == 0) s_pk = pm_find(A.mode_base, A.npeaks, (long long)blockIdx.x);
   __syncthreads();
   const int pk = s_pk;
-  if (!A.clocks[pk].has_delta) return;
+  const PeakClock& C = A.clocks[pk];
+  if (!C.has_delta) return;
   const PeakDesc& P = A.peaks[pk];
+  GreenCtx g;
+  g.N = P.N;
+  g.log2N = P.log2N;
+  g.Nh = P.N / 2 + 1;
+  g.gm = P.gradient;
+  g.M = P.nmodes;
+  g.inv_nh = P.inv_nh;
+  g.kf = (float)(kTwoPi / P.L);
+  g.dx = (float)P.dx;
+  g.sd2 = P.smooth > 0 ? (float)(P.smooth * P.dx) * (float)(P.smooth * P.dx) : 0.f;
+  g.s_c = (float)(-1.5 * PM_H_I * PM_H_I / C.a_grid / ((double)P.N * P.N * P.N));
+  g.spec = P.spec;
+  g.out = P.gspec;
   const long long m0 = ((long long)blockIdx.x - A.mode_base[pk]) * (PM_THREADS * GREEN_MODES) + threadIdx.x;
+  // All loads of the block's modes first (the stores below could alias them as far as the
+  // compiler knows), then the arithmetic and the stores.
+  float2 d[GREEN_MODES];
+#pragma unroll
+  for (int k = 0; k < GREEN_MODES; ++k) {
+    const long long m = m0 + k * PM_THREADS;
+    d[k] = m < g.M ? __ldg(g.spec + m) : make_float2(0.f, 0.f);
+  }
   double w = 0.0;
 #pragma unroll
   for (int k = 0; k < GREEN_MODES; ++k) {
     const long long m = m0 + k * PM_THREADS;
-    if (m < P.nmodes) w += green_mode(P, m, s_c);
+    if (m < g.M) w += green_mode(g, m, d[k]);
   }
   // Within the block a plain FP64 tree (at most 1024 terms); across blocks the compensated sum.
-  for (int d = 16; d > 0; d >>= 1) w += __shfl_down_sync(0xffffffffu, w, d);
+  for (int dd = 16; dd > 0; dd >>= 1) w += __shfl_down_sync(0xffffffffu, w, dd);
   if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = CSum{w, 0.0};
   __syncthreads();
   if (threadIdx.x == 0) {
