@@ -172,12 +172,12 @@ def run_reference(args):
 # Algorithmic bytes per launch of each kernel phase: n particles, N^3 cells,
 # M modes; fc/hc: face and halo partials.
 def algorithmic_bytes(phase: str, n: int, cells: int, modes: int, npass: int) -> float:
-    if phase == "push":        # read state 32, write state 32 + class 1, force grids 12 per cell
-        return n * (32 + 32 + 1) + cells * 12.0
+    if phase == "push":        # read state 32, write state 32, force grids 12 per cell
+        return n * (32 + 32) + cells * 12.0
     if phase == "sort":        # super-tile re-sort in shared memory (every 16th step): read + write state
         return n * 64.0
-    if phase == "bin":         # read class 1 + state 32, write state 32
-        return n * 65.0
+    if phase == "bin":         # read state 32, write state 32
+        return n * 64.0
     if phase == "deposit":     # read positions 16, write delta 4 per cell (face/halo partials are overhead)
         return n * 16.0 + cells * 4.0
     if phase == "green":       # read the spectrum 8, write three gradient spectra 24 per mode

@@ -69,7 +69,6 @@ struct pm_engine {
   float4* mom = nullptr;
   int4* tpos = nullptr;  // push output / loading area
   float4* tmom = nullptr;
-  unsigned char* cls = nullptr;
   u32* keys[2] = {nullptr, nullptr};
   u32* vals[2] = {nullptr, nullptr};
   u32* sstart[2] = {nullptr, nullptr};
@@ -111,7 +110,6 @@ struct pm_engine {
     A.mom = mom;
     A.tpos = tpos;
     A.tmom = tmom;
-    A.cls = cls;
     A.keys_push = keys[0];
     A.keys_sorted = keys[sort_result];
     A.perm = vals[sort_result];
@@ -268,7 +266,7 @@ struct pm_engine {
     }
     sort_plan_destroy(&sort);
     void* bufs[] = {d_peaks, d_clocks, d_stats, d_st_base, d_p_base, d_mode_base, epart, wpart, eslice, ecount, pos, mom, tpos,
-                    tmom, cls, keys[0], keys[1], vals[0], vals[1], sstart[0], sstart[1], counts, lpre, far_count,
+                    tmom, keys[0], keys[1], vals[0], vals[1], sstart[0], sstart[1], counts, lpre, far_count,
                     far_fill, sort_gate, refresh_gate, totals, face, halo};
     for (void* b : bufs) cudaFree(b);
     if (stream) cudaStreamDestroy(stream);
@@ -439,7 +437,6 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   if ((r = E->alloc(&E->mom, E->ntot))) return r;
   if ((r = E->alloc(&E->tpos, E->ntot))) return r;
   if ((r = E->alloc(&E->tmom, E->ntot))) return r;
-  if ((r = E->alloc(&E->cls, E->ntot))) return r;
   for (int b = 0; b < 2; ++b) {
     if ((r = E->alloc(&E->keys[b], E->ntot))) return r;
     if ((r = E->alloc(&E->vals[b], E->ntot))) return r;

@@ -71,6 +71,19 @@ __device__ __forceinline__ int bin_digit(int u, int NS) {
 }
 __device__ __forceinline__ int bin_offset(int d, int NS) { return (NS <= 5 || d <= 2) ? d : NS - (d - 2); }
 
+// Re-binning class of a particle of super-tile (sx, sy, sz) whose cell is now `cell`: class 0 is
+// "stayed", BIN_FAR "moved more than two super-tiles" (its destination super-tile in *far_st).
+__device__ __forceinline__ int bin_class(int cell, int sx, int sy, int sz, const PeakDesc& P, u32* far_st) {
+  const int l2 = P.log2N, N = P.N, NS = P.NS;
+  const int tx = (cell >> (2 * l2)) >> P.log2TS, ty = ((cell >> l2) & (N - 1)) >> P.log2TS,
+            tz = (cell & (N - 1)) >> P.log2TS;
+  const int dxc = bin_digit((tx - sx) & (NS - 1), NS), dyc = bin_digit((ty - sy) & (NS - 1), NS),
+            dzc = bin_digit((tz - sz) & (NS - 1), NS);
+  if (dxc >= 0 && dyc >= 0 && dzc >= 0) return (dxc * P.W + dyc) * P.W + dzc;
+  *far_st = pm_morton3(tx, ty, tz);
+  return BIN_FAR;
+}
+
 // ------------------------------------------------------------------------------------------
 // Push: CIC gather of the three force grids (pm3d.py:91-99) fused with the pending closing
 // kick of the previous step, the opening kick and the drift of this one (pm3d.py:122-127).
@@ -152,23 +165,20 @@ __device__ __forceinline__ void push_one(const StepArgs& A, const PeakDesc& P, c
 #undef PM_DRIFT
   }
   bad |= !(isfinite(px) && isfinite(py) && isfinite(pz));
-  A.tpos[j] = make_int4((nx << (2 * l2)) | (ny << l2) | nz, __float_as_int(fx), __float_as_int(fy), __float_as_int(fz));
+  const int cell = (nx << (2 * l2)) | (ny << l2) | nz;
+  A.tpos[j] = make_int4(cell, __float_as_int(fx), __float_as_int(fy), __float_as_int(fz));
   A.tmom[j] = make_float4(px, py, pz, m.w);
-  // Class of the destination super-tile.
-  const int NS = P.NS;
-  const int tx = nx >> P.log2TS, ty = ny >> P.log2TS, tz = nz >> P.log2TS;
-  const int dxc = bin_digit((tx - sx) & (NS - 1), NS), dyc = bin_digit((ty - sy) & (NS - 1), NS),
-            dzc = bin_digit((tz - sz) & (NS - 1), NS);
-  int c = BIN_FAR;
-  if (dxc >= 0 && dyc >= 0 && dzc >= 0) c = (dxc * P.W + dyc) * P.W + dzc;
-  A.cls[j] = (unsigned char)c;
-  const u32 am = __activemask();
-  const u32 peers = __match_any_sync(am, c);
-  if (c == BIN_FAR) {
-    // Far movers of one warp can be bound for different super-tiles: count each one at its own.
-    atomicAdd(&A.far_count[P.st_base + pm_morton3(tx, ty, tz)], 1u);
-  } else if ((peers & lanemask_lt()) == 0) {
-    atomicAdd(&s_cnt[c], (u32)__popc(peers));
+  // Class of the destination super-tile (re-derived from the cell by the scatter), counted:
+  // most particles stay (one warp-aggregated add), the few movers add one each.
+  u32 far_st = 0;
+  const int c = bin_class(cell, sx, sy, sz, P, &far_st);
+  const u32 stay = __ballot_sync(__activemask(), c == 0);
+  if (c == 0) {
+    if ((stay & lanemask_lt()) == 0) atomicAdd(&s_cnt[0], (u32)__popc(stay));
+  } else if (c == BIN_FAR) {
+    atomicAdd(&A.far_count[P.st_base + far_st], 1u);  // counted at its own destination
+  } else {
+    atomicAdd(&s_cnt[c], 1u);
   }
 }
 
@@ -550,25 +560,28 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_bin_scatter(StepArgs A) {
   const int sx = pm_compact3(S >> 2), sy = pm_compact3(S >> 1), sz = pm_compact3(S);
   const int NS = P.NS, W = P.W;
   const long long b = old[S], e = old[S + 1];
+  // Run of the stayers (class 0) in this super-tile's own new range.
+  const long long stay0 = (long long)ss[S] + A.lpre[(P.st_base + S) * BIN_CLASSES];
   for (long long j = b + threadIdx.x; j < e; j += PUSH_THREADS) {
-    const int c = A.cls[j];
     const int4 ps = A.tpos[j];
     const float4 m = A.tmom[j];
+    u32 D = 0;
+    const int c = bin_class(ps.x, sx, sy, sz, P, &D);
     long long dest;
-    const u32 am = __activemask();
-    const u32 peers = __match_any_sync(am, c);
-    const int leader = __ffs(peers) - 1;
-    if (c != BIN_FAR) {
+    // Ranks inside a class run: one warp-aggregated add for the stayers, one add per mover.
+    // The order inside a run is arbitrary; nothing downstream depends on it.
+    const u32 stay = __ballot_sync(__activemask(), c == 0);
+    if (c == 0) {
+      const int leader = __ffs(stay) - 1;
       u32 base = 0;
-      if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(&s_rank[c], (u32)__popc(peers));
-      base = __shfl_sync(peers, base, leader);
+      if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(&s_rank[0], (u32)__popc(stay));
+      base = __shfl_sync(stay, base, leader);
+      dest = stay0 + base + __popc(stay & lanemask_lt());
+    } else if (c != BIN_FAR) {
       const int ux = bin_offset(c / (W * W), NS), uy = bin_offset((c / W) % W, NS), uz = bin_offset(c % W, NS);
-      const u32 D = pm_morton3((sx + ux) & (NS - 1), (sy + uy) & (NS - 1), (sz + uz) & (NS - 1));
-      dest = (long long)ss[D] + A.lpre[(P.st_base + S) * BIN_CLASSES + c] + base + __popc(peers & lanemask_lt());
+      D = pm_morton3((sx + ux) & (NS - 1), (sy + uy) & (NS - 1), (sz + uz) & (NS - 1));
+      dest = (long long)ss[D] + A.lpre[(P.st_base + S) * BIN_CLASSES + c] + atomicAdd(&s_rank[c], 1u);
     } else {
-      const int l2 = P.log2N;
-      const u32 D = pm_morton3((ps.x >> (2 * l2)) >> P.log2TS, ((ps.x >> l2) & (P.N - 1)) >> P.log2TS,
-                               (ps.x & (P.N - 1)) >> P.log2TS);
       dest = (long long)ss[D + 1] - A.far_count[P.st_base + D] + atomicAdd(&A.far_fill[P.st_base + D], 1u);
     }
     if (dest < P.p_off || dest >= P.p_off + P.n) {  // counts and classes disagree: never write outside

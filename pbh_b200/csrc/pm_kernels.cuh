@@ -47,7 +47,6 @@ struct StepArgs {
   float4* mom;
   int4* tpos;                  // push output (same order as the input), regrouped into pos/mom
   float4* tmom;
-  unsigned char* cls;          // per particle: re-binning class or BIN_FAR
   u32* keys_push;              // Morton keys written by set_particles / reload (priming sort input);
                                // per-particle scratch of the super-tile sort on refresh steps
   const u32* keys_sorted;      // sort output keys
