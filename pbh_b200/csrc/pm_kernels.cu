@@ -802,6 +802,14 @@ __device__ __forceinline__ void fixup_faces(const StepArgs& A, const PeakDesc& P
   }
 }
 
+// Nearest integer to the exact product a*b for 0 <= a*b < 2^51: one FMA with 2^52 rounds the
+// product to an integer in the mantissa (round half to even), whose low 52 bits are read off.
+// The same rounding as __double2ll_rn of the exact product, on the FP64 pipe instead of the
+// conversion unit.
+__device__ __forceinline__ u64 fix_round(double a, double b) {
+  return (u64)__double_as_longlong(fma(a, b, 4503599627370496.0)) & 0xFFFFFFFFFFFFFull;
+}
+
 // Shared-memory address of node number `node` (z fastest) of a (TS+1)^3 patch.
 template <int TS>
 __device__ __forceinline__ int dep_addr(int node) {
@@ -835,9 +843,9 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
   const long long total = e - b;
   __syncthreads();
   const u32 le = lanemask_le();
-  u64 acc[NPT];  // nodes' sums of the chunks folded so far
-#pragma unroll
-  for (int k = 0; k < NPT; ++k) acc[k] = 0ull;
+  // Nodes' sums of the chunks folded so far (only super-tiles of more than one chunk use it).
+  u64* acc64 = reinterpret_cast<u64*>(smem + 2 * SZ);
+  bool folded = false;
   // Split accumulators.  A weight W (at most 2^38, at least -3 for a remainder corner) goes in as
   // hi = W >> 19 in [-1, 2^19] and lo = W & (2^19 - 1).  A node takes at most one contribution
   // per particle of a chunk, so with CHUNK <= 8191 the low sums stay below 2^32 and the high
@@ -849,14 +857,20 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
   static_assert(PM_FIX_BITS == 38, "the split accumulators assume 38 fractional bits");
   const long long nit = (total + DEP_THREADS - 1) / DEP_THREADS;
   long long j = b + threadIdx.x;
-  int4 ps_n = j < e ? A.pos[j] : make_int4(-1, 0, 0, 0);
+  // Three sweeps' particles in flight.
+  const int4 none = make_int4(-1, 0, 0, 0);
+  int4 pa = j < e ? A.pos[j] : none;
+  int4 pb = j + DEP_THREADS < e ? A.pos[j + DEP_THREADS] : none;
+  int4 pc = j + 2 * DEP_THREADS < e ? A.pos[j + 2 * DEP_THREADS] : none;
   bool bad = false;
   int left = CH_IT;
   for (long long it = 0; it < nit; ++it) {
-    const int4 ps = ps_n;
+    const int4 ps = pa;
     const bool valid = j < e;
+    pa = pb;
+    pb = pc;
+    if (j + 3 * DEP_THREADS < e) pc = A.pos[j + 3 * DEP_THREADS];
     j += DEP_THREADS;
-    if (j < e) ps_n = A.pos[j];  // next sweep's particle, fetched before this one is used
     {
       const int ix = ps.x >> (2 * l2), iy = (ps.x >> l2) & (N - 1), iz = ps.x & (N - 1);
       const int lx = ix - sx * TS, ly = iy - sy * TS, lz = iz - sz * TS;
@@ -868,13 +882,13 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
       const double w00 = gx * gy * one, w01 = gx * fy * one, w10 = fx * gy * one, w11 = fx * fy * one;
       u64 W0 = 0, W1 = 0, W2 = 0, W3 = 0, W4 = 0, W5 = 0, W6 = 0, W7 = 0;
       if (in) {
-        W0 = (u64)__double2ll_rn(w00 * gz);
-        W1 = (u64)__double2ll_rn(w00 * fz);
-        W2 = (u64)__double2ll_rn(w01 * gz);
-        W3 = (u64)__double2ll_rn(w01 * fz);
-        W4 = (u64)__double2ll_rn(w10 * gz);
-        W5 = (u64)__double2ll_rn(w10 * fz);
-        W6 = (u64)__double2ll_rn(w11 * gz);
+        W0 = fix_round(w00, gz);
+        W1 = fix_round(w00, fz);
+        W2 = fix_round(w01, gz);
+        W3 = fix_round(w01, fz);
+        W4 = fix_round(w10, gz);
+        W5 = fix_round(w10, fz);
+        W6 = fix_round(w11, gz);
         W7 = PM_FIX_ONE - (W0 + W1 + W2 + W3 + W4 + W5 + W6);
       }
       // Warp-shuffle segmented scan over runs of the same cell.
@@ -918,19 +932,16 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
 #undef PM_ADD
       }
     }
-    if (--left == 0 && it + 1 < nit) {  // chunk full and more to come: fold it into registers
+    if (--left == 0 && it + 1 < nit) {  // chunk full and more to come: fold it into acc64
       left = CH_IT;
       __syncthreads();
-#pragma unroll
-      for (int q = 0; q < NPT; ++q) {
-        const int node = threadIdx.x + q * DEP_THREADS;
-        if (node < NN) {
-          const int ad = dep_addr<TS>(node);
-          acc[q] += (u64)chunk_sum(acc_hi[ad], acc_lo[ad]);
-          acc_hi[ad] = 0u;
-          acc_lo[ad] = 0u;
-        }
+      for (int node = threadIdx.x; node < NN; node += DEP_THREADS) {
+        const int ad = dep_addr<TS>(node);
+        acc64[ad] = (folded ? acc64[ad] : 0ull) + (u64)chunk_sum(acc_hi[ad], acc_lo[ad]);
+        acc_hi[ad] = 0u;
+        acc_lo[ad] = 0u;
       }
+      folded = true;
       __syncthreads();
     }
   }
@@ -946,7 +957,7 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
     if (node < NN) {
       const int lx = node / (T1 * T1), r = node - lx * (T1 * T1), ly = r / T1, lz = r - ly * T1;
       const int ad = lx * PS + ly * RS + lz;
-      const long long S = (long long)(acc[q] + (u64)chunk_sum(acc_hi[ad], acc_lo[ad]));
+      const long long S = (long long)((folded ? acc64[ad] : 0ull) + (u64)chunk_sum(acc_hi[ad], acc_lo[ad]));
       if (lx == TS || ly == TS || lz == TS) {
         halo[halo_index(lx, ly, lz, TS)] = S;
       } else if (lx == 0 || ly == 0 || lz == 0) {
@@ -1284,7 +1295,7 @@ __global__ void k_interp64(const double* __restrict__ F, const double* __restric
 }  // namespace
 
 // Dynamic shared memory of the largest super-tile in use (the smaller ones fit inside).
-size_t pm_deposit_smem(int TSmax) { return sizeof(u32) * 2 * (size_t)patch_size(TSmax); }
+size_t pm_deposit_smem(int TSmax) { return (sizeof(u32) * 2 + sizeof(u64)) * (size_t)patch_size(TSmax); }
 size_t pm_push_smem(int TSmax) { return sizeof(float) * 3 * (size_t)patch_size(TSmax); }
 
 size_t pm_tile_sort_smem() {
