@@ -193,6 +193,21 @@ PHASES = ["push", "advance", "bin", "sort", "deposit", "r2c", "green", "c2r"]
 NCU_TRAFFIC = {"push": 78.35, "bin": 62.27, "deposit": 22.45, "green_per_mode": 25.77}
 
 
+def replica_throughput(t_local: float, n_local: int, steps: int, dist=None, device="cpu"):
+    """Whole-job particle-steps/s of independent replicas (one ensemble per rank, the same
+    particle count on every rank): the job takes the slowest rank's device time.
+    Returns (max time over ranks, value)."""
+    import torch
+    world = 1
+    t = t_local
+    if dist is not None:
+        world = dist.get_world_size()
+        tt = torch.tensor([t_local], dtype=torch.float64, device=device)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t = float(tt.item())
+    return t, world * n_local * steps / t
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -246,12 +261,8 @@ def run_ours(args):
     if dist:
         dist.barrier()
     clocks = sampler.stop()
-    t = e0.elapsed_time(e1) / 1e3
-    if dist:
-        tt = torch.tensor([t], device=f"cuda:{local}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t = float(tt.item())
-    value = world * n_step * args.steps / t
+    t, value = replica_throughput(e0.elapsed_time(e1) / 1e3, n_step, args.steps, dist,
+                                  device=f"cuda:{local}")
     ms_per_step = t / args.steps * 1e3
 
     # Per-kernel device times: a few ungraphed steps with events between phases, same stream.
