@@ -190,7 +190,7 @@ PHASES = ["push", "advance", "bin", "sort", "deposit", "r2c", "green", "c2r"]
 # DRAM bytes (read + write) per launch from one ncu capture of the plain 256^3 run
 # (profiles/kernels_plain256.md), per particle (per mode for Green), scaled to a launch by the
 # particles (modes) it processes.
-NCU_TRAFFIC = {"push": 78.35, "bin": 62.27, "deposit": 22.45, "green_per_mode": 25.77}
+NCU_TRAFFIC = {"push": 77.17, "bin": 61.18, "deposit": 28.62, "green_per_mode": 25.69}
 
 
 def replica_throughput(t_local: float, n_local: int, steps: int, dist=None, device="cpu"):
