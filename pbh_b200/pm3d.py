@@ -205,6 +205,17 @@ class PM3D:
         self._engine.step_explicit(0, a, da)
         return a + da, self._out(self._engine.delta(0))
 
+    def delta_max(self) -> float:
+        """Max delta of the latest deposit, from the device's own statistics (no grid copy)."""
+        return float(self._engine.stats(0).delta_max)
+
+    def energy(self) -> dict:
+        """The engine's energy check at its last sample: total momentum, K, W and the
+        Layzer-Irvine residual a(K + W) + int K da - a0 (K0 + W0) with its scale a(K + |W|)."""
+        s = self._engine.stats(0)
+        return dict(a=s.a_energy, samples=s.energy_samples, momentum=list(s.momentum), kinetic=s.kinetic,
+                    potential=s.potential, layzer_irvine=s.li_residual, scale=s.li_scale)
+
     def run(self, a_end: float, da_frac: float = 0.02, a: float = 1.0, callback=None, every: int = 0):
         """The driver loop of pbhgr/scripts/pm3d_peak.py:24-33 on the device: da = min(da_frac a,
         a_end - a) until a_end, all steps replayed from one captured graph.  With ``callback``

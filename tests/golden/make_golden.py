@@ -94,6 +94,28 @@ def recipe_case(pm3d, name, N, Np, seed, steps):
           x0=ic["x"], p0=ic["p"], **snaps)
 
 
+def profiles_case(path: str, name="profiles"):
+    """Profile tables (pbhgr/pbhgr/profiles.py) and the driver's LTB units (pbhgr/pbhgr/ltb.py)
+    used by scripts/pm3d_peak.py: spline values and slopes on a radius grid, r_m, t_H, t_C(0)."""
+    sys.path.insert(0, path)
+    from pbhgr import ltb, profiles          # noqa: E402
+    r = np.linspace(0.0, 20.0, 201)
+    out, meta = {}, {}
+    for prof in ("yoo", "ln0.5", "ln0.1", "tophat"):
+        tab = profiles.profile_table(prof)
+        tab["name"] = prof
+        key = prof.replace(".", "p")
+        out[f"{key}_psi"] = tab["spline"](r)
+        out[f"{key}_dpsi"] = tab["spline"].derivative(1)(r)
+        for mu in (0.1, 0.5):
+            ref = ltb.LTBGaussian(mu) if prof == "yoo" else ltb.LTBProfile(mu, tab)
+            tc0 = ref.tC(1e-6)
+            if not np.isfinite(tc0):
+                tc0 = ref.tC(ref.r_m)
+            meta[f"{key}_mu{mu:g}"] = dict(r_m=float(ref.r_m), t_H=float(ref.t_H), tC0=float(tc0))
+    _save(name, dict(units=meta), r=r, **out)
+
+
 def main():
     ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PBH_REFERENCE", "")
     if not ref:
@@ -103,6 +125,7 @@ def main():
     zeta_case(pm3d, profiles, "zeta_16_np8_smooth", 16, 8.0, 8, 1, 2.0, 0.3, 0.0, 0.0, 0.0, 4)
     mesh_case(pm3d, "mesh_8", 8, 1.0, 600, 11)
     recipe_case(pm3d, "recipe_16", 16, 16, 5, 10)
+    profiles_case(ref)
 
 
 if __name__ == "__main__":

@@ -136,3 +136,22 @@ def test_torch64_oracle_matches_numpy_oracle():
         a, _ = tr_t.step(a, 0.05 * a)
     assert np.max(np.abs(tr_t.x.numpy() - tr_n.x)) <= 1e-12
     assert np.max(np.abs(tr_t.p.numpy() - tr_n.p)) <= 1e-12 * np.max(np.abs(tr_n.p))
+
+
+def test_profile_tables_and_units_match_reference(golden):
+    """pbh_b200.profiles (host side of the driver) against the reference's profile tables and
+    LTB units, recorded by tests/golden/make_golden.py."""
+    from pbh_b200 import profiles as P
+    g = golden("profiles")
+    r = g["r"]
+    for name in ("yoo", "ln0.5", "ln0.1", "tophat"):
+        key = name.replace(".", "p")
+        tab = P.profile_table(name)
+        assert np.max(np.abs(tab["spline"](r) - g[f"{key}_psi"])) <= 1e-12
+        assert np.max(np.abs(tab["spline"].derivative(1)(r) - g[f"{key}_dpsi"])) <= 1e-11
+        for mu in (0.1, 0.5):
+            want = g["meta"]["units"][f"{key}_mu{mu:g}"]
+            r_m, t_h, tc0 = P.ltb_units(mu, name, tab)
+            assert r_m == pytest.approx(want["r_m"], rel=1e-12)
+            assert t_h == pytest.approx(want["t_H"], rel=1e-12)
+            assert tc0 == pytest.approx(want["tC0"], rel=1e-9)
