@@ -62,7 +62,8 @@ struct PeakDesc {
   long long halo_off;      // offset of this peak's halo partials (nst * hc)
   long long mode_base;     // first global mode-block of this peak (Green kernel)
   long long nmodes;        // N*N*(N/2+1)
-  double inv_nh;           // 1/(N/2+1)
+  u32 nh_magic;            // m / (N/2+1) = (umulhi(m, nh_magic) + m) >> nh_shift for 32-bit m
+  int nh_shift;
   float* delta;            // N^3 FP32 density contrast (R2C input)
   float2* spec;            // N*N*(N/2+1) complex spectrum (R2C output)
   float2* gspec;           // 3 gradient spectra
@@ -166,3 +167,16 @@ __host__ __device__ __forceinline__ u32 pm_morton3(u32 x, u32 y, u32 z) {
 __host__ __device__ __forceinline__ u32 pm_cell_key(int ix, int iy, int iz) { return pm_morton3(ix, iy, iz); }
 
 __host__ __device__ __forceinline__ double pm_hubble(double a) { return PM_H_I / (a * sqrt(a)); }
+
+// Unsigned division by an invariant divisor d >= 1 (Granlund & Montgomery 1994, the round-up
+// method for 32-bit operands): with l = ceil(log2 d) and magic = floor(2^32 (2^l - d) / d) + 1,
+// n / d = (umulhi(n, magic) + n) >> l for every 32-bit n (the sum is formed in 64 bits).
+inline void pm_div_magic(u32 d, u32* magic, int* shift) {
+  int l = 0;
+  while ((1ull << l) < d) ++l;
+  *magic = (u32)(((1ull << 32) * ((1ull << l) - d)) / d + 1);
+  *shift = l;
+}
+__device__ __forceinline__ u32 pm_div_by(u32 n, u32 magic, int shift) {
+  return (u32)(((unsigned long long)__umulhi(n, magic) + n) >> shift);
+}

@@ -335,7 +335,7 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
     P.face_off = fo;
     P.halo_off = ho;
     P.nmodes = (long long)c.N * c.N * (c.N / 2 + 1);
-    P.inv_nh = 1.0 / (double)(c.N / 2 + 1);
+    pm_div_magic((u32)(c.N / 2 + 1), &P.nh_magic, &P.nh_shift);
     P.mode_base = mb;
     st_base[i] = stb;
     p_base[i] = poff;

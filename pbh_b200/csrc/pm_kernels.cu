@@ -2,6 +2,7 @@
 // clock advance, regrouping (re-binning scatter, or radix-sort permutation), halo-exchange CIC
 // deposit with its face fix-up, Green's function + gradient, and particle I/O.
 #include <algorithm>
+#include <type_traits>
 
 #include "pm_kernels.cuh"
 
@@ -823,6 +824,19 @@ __device__ __forceinline__ long long chunk_sum(u32 hi, u32 lo) {
   return hs * (1LL << 19) + (long long)lo;
 }
 
+// Adds a full chunk's node sums into the fold scratch (first chunk: stores) and clears the
+// chunk accumulators.  Kept out of line: it runs only for super-tiles of more than one chunk.
+template <int TS>
+__device__ __noinline__ void fold_chunk(u64* acc64, u32* acc_hi, u32* acc_lo, bool add) {
+  constexpr int NN = (TS + 1) * (TS + 1) * (TS + 1);
+  for (int node = threadIdx.x; node < NN; node += DEP_THREADS) {
+    const int ad = dep_addr<TS>(node);
+    acc64[node] = (add ? acc64[node] : 0ull) + (u64)chunk_sum(acc_hi[ad], acc_lo[ad]);
+    acc_hi[ad] = 0u;
+    acc_lo[ad] = 0u;
+  }
+}
+
 template <int TS>
 __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc& P, const PeakClock& C, int pk,
                                               u32 st, u32* smem, double* rho64) {
@@ -843,8 +857,10 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
   const long long total = e - b;
   __syncthreads();
   const u32 le = lanemask_le();
-  // Nodes' sums of the chunks folded so far (only super-tiles of more than one chunk use it).
-  u64* acc64 = reinterpret_cast<u64*>(smem + 2 * SZ);
+  // Nodes' sums of the chunks folded so far, only for a super-tile of more than one chunk: kept
+  // in the temporary particle state of its own range (free during the deposit; a range of more
+  // than one chunk of 16-byte entries holds the NN 8-byte sums several times over).
+  static_assert((8191 / DEP_THREADS) * DEP_THREADS * sizeof(int4) >= NN * sizeof(u64), "fold scratch too small");
   bool folded = false;
   // Split accumulators.  A weight W (at most 2^38, at least -3 for a remainder corner) goes in as
   // hi = W >> 19 in [-1, 2^19] and lo = W & (2^19 - 1).  A node takes at most one contribution
@@ -935,12 +951,7 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
     if (--left == 0 && it + 1 < nit) {  // chunk full and more to come: fold it into acc64
       left = CH_IT;
       __syncthreads();
-      for (int node = threadIdx.x; node < NN; node += DEP_THREADS) {
-        const int ad = dep_addr<TS>(node);
-        acc64[ad] = (folded ? acc64[ad] : 0ull) + (u64)chunk_sum(acc_hi[ad], acc_lo[ad]);
-        acc_hi[ad] = 0u;
-        acc_lo[ad] = 0u;
-      }
+      fold_chunk<TS>(reinterpret_cast<u64*>(A.tpos + b), acc_hi, acc_lo, folded);
       folded = true;
       __syncthreads();
     }
@@ -951,27 +962,33 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
   const long long gbase = ((long long)sx * TS * N + (long long)sy * TS) * N + sz * TS;
   long long* face = A.face + P.face_off + (long long)st * P.fc;
   long long* halo = A.halo + P.halo_off + (long long)st * P.hc;
+  // Two copies of the loop: the common single-chunk one carries no load of the fold scratch.
+  auto write_out = [&](auto with_fold) {
 #pragma unroll
-  for (int q = 0; q < NPT; ++q) {
-    const int node = threadIdx.x + q * DEP_THREADS;
-    if (node < NN) {
-      const int lx = node / (T1 * T1), r = node - lx * (T1 * T1), ly = r / T1, lz = r - ly * T1;
-      const int ad = lx * PS + ly * RS + lz;
-      const long long S = (long long)((folded ? acc64[ad] : 0ull) + (u64)chunk_sum(acc_hi[ad], acc_lo[ad]));
-      if (lx == TS || ly == TS || lz == TS) {
-        halo[halo_index(lx, ly, lz, TS)] = S;
-      } else if (lx == 0 || ly == 0 || lz == 0) {
-        face[face_index(lx, ly, lz, TS)] = S;
-      } else {
-        const long long Dv = S - P.n_mean_fix;
-        const long long g = gbase + ((long long)lx * N + ly) * N + lz;
-        P.delta[g] = (float)((double)Dv * P.inv_fix_nmean);
-        if (rho64) rho64[g] = (double)S * (1.0 / (double)PM_FIX_ONE);
-        dsum += Dv;
-        smax = S > smax ? S : smax;
+    for (int q = 0; q < NPT; ++q) {
+      const int node = threadIdx.x + q * DEP_THREADS;
+      if (node < NN) {
+        const int lx = node / (T1 * T1), r = node - lx * (T1 * T1), ly = r / T1, lz = r - ly * T1;
+        const int ad = lx * PS + ly * RS + lz;
+        long long S = chunk_sum(acc_hi[ad], acc_lo[ad]);
+        if (decltype(with_fold)::value) S += (long long)reinterpret_cast<const u64*>(A.tpos + b)[node];
+        if (lx == TS || ly == TS || lz == TS) {
+          halo[halo_index(lx, ly, lz, TS)] = S;
+        } else if (lx == 0 || ly == 0 || lz == 0) {
+          face[face_index(lx, ly, lz, TS)] = S;
+        } else {
+          const long long Dv = S - P.n_mean_fix;
+          const long long g = gbase + ((long long)lx * N + ly) * N + lz;
+          P.delta[g] = (float)((double)Dv * P.inv_fix_nmean);
+          if (rho64) rho64[g] = (double)S * (1.0 / (double)PM_FIX_ONE);
+          dsum += Dv;
+          smax = S > smax ? S : smax;
+        }
       }
     }
-  }
+  };
+  if (folded) write_out(std::true_type{});
+  else write_out(std::false_type{});
   for (int d = 16; d > 0; d >>= 1) {
     dsum += __shfl_xor_sync(0xffffffffu, dsum, d);
     const long long om = __shfl_xor_sync(0xffffffffu, smax, d);
@@ -995,7 +1012,7 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
   }
 }
 
-__global__ void __launch_bounds__(DEP_THREADS, 2) k_deposit(StepArgs A, double* rho64) {
+__global__ void __launch_bounds__(DEP_THREADS, 4) k_deposit(StepArgs A, double* rho64) {
   extern __shared__ __align__(16) u32 s_dep[];
   const TileRef tr = find_tile(A.st_base, A.npeaks);
   const PeakClock C = A.clocks[tr.pk];
@@ -1067,7 +1084,8 @@ __device__ __forceinline__ float grad_k(float k, float dx, int mode) {
 struct GreenCtx {
   int N, log2N, Nh, gm;
   long long M;
-  double inv_nh;
+  u32 nh_magic;
+  int nh_shift;
   float kf, dx, sd2, s_c;
   const float2* spec;
   float2* out;
@@ -1075,11 +1093,9 @@ struct GreenCtx {
 
 __device__ __forceinline__ double green_mode(const GreenCtx& g, long long m, float2 d) {
   const int N = g.N, Nh = g.Nh;
-  // m = row * Nh + kz without an integer division: the double quotient is off by at most one.
-  long long rest = (long long)((double)m * g.inv_nh);
-  if (rest * Nh > m) --rest;
-  else if ((rest + 1) * Nh <= m) ++rest;
-  const int kz = (int)(m - rest * Nh);
+  // m = row * Nh + kz (m < N^2 Nh < 2^32 for N <= 1024): division by the invariant Nh.
+  const u32 rest = pm_div_by((u32)m, g.nh_magic, g.nh_shift);
+  const int kz = (int)((u32)m - rest * (u32)Nh);
   const int iy = (int)(rest & (N - 1)), ix = (int)(rest >> g.log2N);
   const float kx = kline(ix, N, g.kf), ky = kline(iy, N, g.kf), kzv = g.kf * (float)kz;
   const float k2 = kx * kx + ky * ky + kzv * kzv;
@@ -1108,8 +1124,9 @@ __device__ __forceinline__ double green_mode(const GreenCtx& g, long long m, flo
   g.out[2 * M + m] = oz;
   // Potential-energy term: sum_x delta Phi = sum_k |delta_k|^2 G_k over the full spectrum; the
   // half spectrum counts each kz in (0, N/2) twice.
-  const double wk = (kz == 0 || kz == N / 2) ? 1.0 : 2.0;
-  return wk * (double)G * ((double)d.x * d.x + (double)d.y * d.y);
+  // The term in FP32 (relative rounding ~1e-7, independent from mode to mode), summed in FP64.
+  const float wk = (kz == 0 || kz == N / 2) ? 1.0f : 2.0f;
+  return (double)(wk * G * (d.x * d.x + d.y * d.y));
 }
 
 __global__ void __launch_bounds__(PM_THREADS) k_green(StepArgs A) {
@@ -1127,7 +1144,8 @@ __global__ void __launch_bounds__(PM_THREADS) k_green(StepArgs A) {
   g.Nh = P.N / 2 + 1;
   g.gm = P.gradient;
   g.M = P.nmodes;
-  g.inv_nh = P.inv_nh;
+  g.nh_magic = P.nh_magic;
+  g.nh_shift = P.nh_shift;
   g.kf = (float)(kTwoPi / P.L);
   g.dx = (float)P.dx;
   g.sd2 = P.smooth > 0 ? (float)(P.smooth * P.dx) * (float)(P.smooth * P.dx) : 0.f;
@@ -1295,7 +1313,7 @@ __global__ void k_interp64(const double* __restrict__ F, const double* __restric
 }  // namespace
 
 // Dynamic shared memory of the largest super-tile in use (the smaller ones fit inside).
-size_t pm_deposit_smem(int TSmax) { return (sizeof(u32) * 2 + sizeof(u64)) * (size_t)patch_size(TSmax); }
+size_t pm_deposit_smem(int TSmax) { return sizeof(u32) * 2 * (size_t)patch_size(TSmax); }
 size_t pm_push_smem(int TSmax) { return sizeof(float) * 3 * (size_t)patch_size(TSmax); }
 
 size_t pm_tile_sort_smem() {

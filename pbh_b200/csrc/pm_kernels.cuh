@@ -21,7 +21,7 @@
 
 #define PM_THREADS 256
 #define PUSH_THREADS 512
-#define DEP_THREADS 512
+#define DEP_THREADS 256    // deposit CTA (4 per SM)
 #define GREEN_MODES 4      // modes per thread of the Green kernel (a block covers PM_THREADS * GREEN_MODES)
 #define ENERGY_SLICES 16   // CTAs per peak of the energy reduction
 #define FIX_THREADS 256    // face fix-up CTA

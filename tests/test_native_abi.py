@@ -45,3 +45,23 @@ def test_cell_key_layout_host_helper():
     # the top bits are the Morton code of the 16^3 super-tile
     st = (spread(ix.ravel() // 16) << 2) | (spread(iy.ravel() // 16) << 1) | spread(iz.ravel() // 16)
     assert np.array_equal(keys >> np.uint32(12), st.astype(np.uint32))
+
+
+def test_invariant_divisor_magic_numbers():
+    """The Green kernel splits a mode index m = row * (N/2 + 1) + kz with a multiply-high by a
+    magic number (common.cuh pm_div_magic / pm_div_by); the same arithmetic, exactly, for every
+    mesh size on samples that include every multiple of the divisor near the range ends."""
+    import numpy as np
+    rng = np.random.default_rng(0)
+    for N in (8, 16, 32, 64, 128, 256, 512, 1024):
+        d = N // 2 + 1
+        l = 0
+        while (1 << l) < d:
+            l += 1
+        magic = ((1 << 32) * ((1 << l) - d)) // d + 1
+        top = N * N * d
+        n = np.concatenate([np.arange(0, min(top, 200000)), np.arange(max(0, top - 200000), top),
+                            rng.integers(0, top, 200000), (np.arange(1, 2000) * d)[:, None].ravel() - 1])
+        n = n[(n >= 0) & (n < top)].astype(np.uint64)
+        q = (((n * np.uint64(magic)) >> np.uint64(32)) + n) >> np.uint64(l)
+        assert np.array_equal(q, n // np.uint64(d)), N
