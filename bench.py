@@ -213,7 +213,7 @@ def run_ours(args):
     import torch
 
     from pbh_b200 import _lib
-    from pbh_b200.batch import Ensemble, plain_rate
+    from pbh_b200.batch import Ensemble, plain_rate, pm3d_step_rate
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -311,6 +311,10 @@ def run_ours(args):
         pr = plain_rate(specs, steps=8, warmup=3, device=local, tiles=tiles)
         line["plain"] = dict(pr, batched_over_plain=value / world / pr["particle_steps_per_s"],
                              how="each peak alone in a single-peak engine, sequentially, same kernels")
+        ps = pm3d_step_rate(specs, steps=5, warmup=2, device=local)
+        line["plain_pm3d_step"] = dict(ps, batched_over_pm3d_step=value / world / ps["particle_steps_per_s"],
+                                       how="each peak alone through PM3D.step (delta returned to the host "
+                                           "every step, as the reference driver uses it); wall clock")
 
     if not args.no_e2e:
         line["e2e"] = e2e_job(ens, specs, torch, local)

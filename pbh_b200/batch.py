@@ -112,3 +112,33 @@ def plain_rate(specs, steps: int = 8, warmup: int = 3, device: int = 0, tiles=No
         total_t += len(group) * t_step
         ens.close()
     return {"particle_steps_per_s": total_ps / total_t, "step_s_by_mesh": {str(k): v for k, v in per.items()}}
+
+
+def pm3d_step_rate(specs, steps: int = 5, warmup: int = 2, device: int = 0) -> dict:
+    """The drop-in call surface used as the reference's driver uses it: one PM3D per peak,
+    `a, delta = pm.step(a, da)` per step, each step returning the density grid to the host as
+    float64 numpy (pbhgr/pbhgr/pm3d.py:117-129, pbhgr/scripts/pm3d_peak.py:26-28).  Wall clock
+    per step, one peak per mesh size, weighted by the ensemble's composition."""
+    import time
+
+    from .pm3d import PM3D
+    by_n = {}
+    for s in specs:
+        by_n.setdefault(s.N, []).append(s)
+    total_ps, total_t, per = 0.0, 0.0, {}
+    for N, group in sorted(by_n.items()):
+        s = group[0]
+        pm = PM3D(N, s.L, N, seed=s.seed, device=device).make_peak(s.R, s.delta0, s.noise_frac)
+        a = 1.0
+        for _ in range(warmup):
+            a, _ = pm.step(a, a * s.ratio())
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            a, _ = pm.step(a, a * s.ratio())
+        t_step = (time.perf_counter() - t0) / steps
+        per[N] = t_step
+        total_ps += len(group) * s.n
+        total_t += len(group) * t_step
+        pm.close()
+    return {"particle_steps_per_s": total_ps / total_t, "step_s_by_mesh": {str(k): v for k, v in per.items()}}
+

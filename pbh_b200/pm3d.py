@@ -205,6 +205,10 @@ class PM3D:
         self._engine.step_explicit(0, a, da)
         return a + da, self._out(self._engine.delta(0))
 
+    def close(self):
+        """Release the device memory of this run now (it is also released with the object)."""
+        self._engine.close()
+
     def delta_max(self) -> float:
         """Max delta of the latest deposit, from the device's own statistics (no grid copy)."""
         return float(self._engine.stats(0).delta_max)
