@@ -77,7 +77,7 @@ struct pm_engine {
   u32* far_count = nullptr;
   u32* far_fill = nullptr;
   double2* epart = nullptr;  // push partials of the energy sums
-  double2* wpart = nullptr;  // Green partials of the potential energy
+  double* wpart = nullptr;   // Green partials of the potential energy (per warp)
   double2* eslice = nullptr; // energy slice partials
   u32* ecount = nullptr;     // energy slices done per peak
   u32* sort_gate = nullptr;  // one word: any peak sorts this step
@@ -447,7 +447,7 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   if ((r = E->alloc(&E->far_count, E->nst))) return r;
   if ((r = E->alloc(&E->far_fill, E->nst))) return r;
   if ((r = E->alloc(&E->epart, 4 * E->nst))) return r;
-  if ((r = E->alloc(&E->wpart, E->nmodeblk))) return r;
+  if ((r = E->alloc(&E->wpart, E->nmodeblk * (PM_THREADS / 32)))) return r;
   if ((r = E->alloc(&E->eslice, (size_t)npeaks * ENERGY_SLICES * 5))) return r;
   if ((r = E->alloc(&E->ecount, npeaks))) return r;
   if ((r = E->alloc(&E->sort_gate, 1))) return r;
@@ -474,7 +474,7 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   CU(cudaMemset(E->far_count, 0, sizeof(u32) * E->nst));
   CU(cudaMemset(E->far_fill, 0, sizeof(u32) * E->nst));
   CU(cudaMemset(E->epart, 0, sizeof(double2) * 4 * E->nst));
-  CU(cudaMemset(E->wpart, 0, sizeof(double2) * E->nmodeblk));
+  CU(cudaMemset(E->wpart, 0, sizeof(double) * E->nmodeblk * (PM_THREADS / 32)));
   CU(cudaMemset(E->ecount, 0, sizeof(u32) * npeaks));
   CU(cudaMemset(E->sort_gate, 0, sizeof(u32)));
   CU(cudaMemset(E->refresh_gate, 0, sizeof(u32)));

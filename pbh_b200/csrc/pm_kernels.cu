@@ -387,12 +387,11 @@ __global__ void __launch_bounds__(PM_THREADS) k_energy(StepArgs A) {
       csum_merge(v[q], CSum{e.x, e.y});
     }
   }
-  const long long nblk = (P.nmodes + PM_THREADS * GREEN_MODES - 1) / (PM_THREADS * GREEN_MODES);  // Green blocks
-  const long long g0 = nblk * sl / ENERGY_SLICES, g1 = nblk * (sl + 1) / ENERGY_SLICES;
-  for (long long t = g0 + threadIdx.x; t < g1; t += PM_THREADS) {
-    const double2 e = A.wpart[P.mode_base + t];
-    csum_merge(v[4], CSum{e.x, e.y});
-  }
+  // Green partials: one per warp of each Green block of this peak.
+  const long long nw = (P.nmodes + PM_THREADS * GREEN_MODES - 1) / (PM_THREADS * GREEN_MODES) * (PM_THREADS / 32);
+  const long long g0 = nw * sl / ENERGY_SLICES, g1 = nw * (sl + 1) / ENERGY_SLICES;
+  const double* wp = A.wpart + P.mode_base * (PM_THREADS / 32);
+  for (long long t = g0 + threadIdx.x; t < g1; t += PM_THREADS) csum_add(v[4], wp[t]);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int q = 0; q < 5; ++q) {
@@ -1131,7 +1130,6 @@ __device__ __forceinline__ double green_mode(const GreenCtx& g, long long m, flo
 
 __global__ void __launch_bounds__(PM_THREADS) k_green(StepArgs A) {
   __shared__ int s_pk;
-  __shared__ CSum s_w[PM_THREADS / 32];
   if (threadIdx.x == 0) s_pk = pm_find(A.mode_base, A.npeaks, (long long)blockIdx.x);
   __syncthreads();
   const int pk = s_pk;
@@ -1167,15 +1165,10 @@ __global__ void __launch_bounds__(PM_THREADS) k_green(StepArgs A) {
     const long long m = m0 + k * PM_THREADS;
     if (m < g.M) w += green_mode(g, m, d[k]);
   }
-  // Within the block a plain FP64 tree (at most 1024 terms); across blocks the compensated sum.
+  // Within a warp a plain FP64 tree (128 terms); one partial per warp, no block barrier; the
+  // energy kernel merges the partials with the compensated sum.
   for (int dd = 16; dd > 0; dd >>= 1) w += __shfl_down_sync(0xffffffffu, w, dd);
-  if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = CSum{w, 0.0};
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    CSum t = s_w[0];
-    for (int q = 1; q < PM_THREADS / 32; ++q) csum_merge(t, s_w[q]);
-    A.wpart[blockIdx.x] = make_double2(t.s, t.c);
-  }
+  if ((threadIdx.x & 31) == 0) A.wpart[(long long)blockIdx.x * (PM_THREADS / 32) + (threadIdx.x >> 5)] = w;
 }
 
 __global__ void k_reset_peak(StepArgs A, int pk, double a0, int mode, double param, double a_end, int max_steps) {

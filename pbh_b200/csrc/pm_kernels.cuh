@@ -60,7 +60,7 @@ struct StepArgs {
   long long* face;             // face partials
   long long* halo;             // upper-halo partials
   double2* epart;              // [super-tile][4] push partials (sum, compensation): p_x, p_y, p_z, p^2
-  double2* wpart;              // [Green block] partials of sum_k w_k |delta_k|^2 G_k
+  double* wpart;               // [Green block][warp] partials of sum_k w_k |delta_k|^2 G_k
   double2* eslice;             // [peak][ENERGY_SLICES][5] slice partials of the energy kernel
   u32* ecount;                 // [peak] energy slices finished this step (0 between steps)
 };
