@@ -109,6 +109,23 @@ def force_grids(mesh: Mesh, delta: np.ndarray, a: float):
     return [_irfftn(-1j * kc * phik, mesh.N) for kc in (mesh.kx, mesh.ky, mesh.kz)]
 
 
+def force_grids_fd(mesh: Mesh, delta: np.ndarray, a: float, order: int):
+    """-dPhi/dx_i by central differences of the potential in real space, the finite-difference
+    alternative to the spectral gradient of pm3d.py:110-112 (which has no such option): order 2,
+    -(Phi(x+dx) - Phi(x-dx))/(2dx); order 4, -(8[Phi(x+dx) - Phi(x-dx)] - [Phi(x+2dx) -
+    Phi(x-2dx)])/(12dx).  Phi is the reference's potential (pm3d.py:105-109)."""
+    phi = _irfftn(potential_k(mesh, np.fft.rfftn(delta), a), mesh.N)
+    out = []
+    for ax in range(3):
+        d1 = np.roll(phi, -1, axis=ax) - np.roll(phi, 1, axis=ax)
+        if order == 2:
+            out.append(-d1 / (2.0 * mesh.dx))
+        else:
+            d2 = np.roll(phi, -2, axis=ax) - np.roll(phi, 2, axis=ax)
+            out.append(-(8.0 * d1 - d2) / (12.0 * mesh.dx))
+    return out
+
+
 def density_contrast(mesh: Mesh, X: np.ndarray) -> np.ndarray:
     """delta = n/n_mean - 1 from the CIC counts (pm3d.py:103-104)."""
     return deposit(X, mesh.N, mesh.dx) / mesh.n_mean - 1.0

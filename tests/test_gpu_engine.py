@@ -217,3 +217,23 @@ def test_fast_particles_cross_several_super_tiles():
     assert rel(eng.delta(0).cpu().numpy(), O.density_contrast(mesh, xg)) < TOL_DENSITY
     s = eng.stats(0)
     assert s.mass_defect == 0.0 and s.status == 0
+
+
+@pytest.mark.parametrize("gradient,order", [("fd2", 2), ("fd4", 4)])
+def test_finite_difference_gradients(gradient, order):
+    """The engine's finite-difference gradients (transfer functions sin(k dx)/dx and
+    (8 sin(k dx) - sin(2 k dx))/(6 dx) applied in k-space) against central differences of the
+    oracle's potential taken in real space, at the same positions."""
+    N = 32
+    mesh, ic = recipe(N, delta0=0.1, seed=4)
+    eng = engine([dict(N=N, Np=N, L=1.0, gradient=gradient)])
+    eng.set_particles(0, ic["x"], ic["p"], 1.0)
+    eng.run(1)
+    x = eng.particles(0)[0].cpu().numpy()
+    delta = O.density_contrast(mesh, x)
+    grids = O.force_grids_fd(mesh, delta, 1.0, order)
+    ref = np.stack([O.interp(g, x, N, mesh.dx) for g in grids], axis=-1)
+    acc = eng.acc(0, 1.0).cpu().numpy()
+    assert rel(acc, ref) < TOL_FORCE
+    spectral, _ = O.accelerations(mesh, x, 1.0)
+    assert rel(ref, spectral) > 1e-3                      # the stencils differ from the spectral gradient
