@@ -75,7 +75,7 @@ def autotune(sizes, device: int = 0, steps: int = 8, warmup: int = 3, use_cache:
         out[N] = best
         dirty = True
     if dirty and use_cache:
-        tmp = CACHE.with_suffix(".tmp")
+        tmp = CACHE.with_suffix(f".{os.getpid()}.tmp")  # one writer per process (ranks share the file)
         tmp.write_text(json.dumps(cache, indent=1))
         os.replace(tmp, CACHE)
     return out
