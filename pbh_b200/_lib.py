@@ -15,6 +15,7 @@ STATE_IDLE, STATE_PRIME, STATE_RUN, STATE_FINALIZE, STATE_HOLD = 0, 1, 2, 3, 4
 FLAG_BUCKET_SORT = 1
 FLAG_GRAPH = 2
 FLAG_DYNAMIC = 4
+FLAG_NATIVE_FFT = 8
 NOALLOC_MAX_KEYS = 1 << 18          # PM_NOALLOC_MAX_KEYS of include/pmb200.h
 
 
@@ -74,6 +75,8 @@ _SIGS = {
     "pm_interp64": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong, C.c_int, C.c_double, C.c_void_p]),
     "pm_sort_u64": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.c_int,
                               C.c_int]),
+    "pm_rfft3_256": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "pm_irfft3_256": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     "pm_sort_u64_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.c_int, C.c_int,
                                       C.c_void_p]),
     "pm_cell_keys": (C.c_int, [C.c_void_p, C.c_longlong, C.c_int, C.c_int, C.c_void_p]),

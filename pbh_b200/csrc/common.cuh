@@ -52,6 +52,8 @@ struct PeakDesc {
   int fc, hc;              // face nodes (any local coordinate 0) and upper-halo nodes per super-tile
   int gradient;            // 0 spectral (reference), 1 two-point finite difference, 2 four-point
   int full_every;          // a full Morton-key sort every this many steps (re-binning between)
+  int native_fft;          // 1: the native 256^3 transform carries the Green multiply (no k_green)
+  int pad_nf;
   double L, dx, smooth, n_mean, m_part;
   long long n_mean_fix;    // round(n_mean * 2^38)
   double inv_fix_nmean;    // 2^-38 / n_mean

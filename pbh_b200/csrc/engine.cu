@@ -44,6 +44,9 @@ struct MeshClass {
   // Dynamic mode: plans for every batch size 1..B over the leading slots, one shared work area.
   std::vector<cufftHandle> r2c_b, c2r_b;
   void* work = nullptr;
+  // The native 256^3 transform (fft256.cu) instead of cuFFT, Green multiply fused into it.
+  bool native = false;
+  int* slot_peak = nullptr;  // device: peak index of each slot
 };
 
 }  // namespace
@@ -145,7 +148,10 @@ struct pm_engine {
   }
   int fft_r2c() {
     for (auto& c : classes) {
-      if (flags & 4) {
+      if (c.native) {
+        const int x = (flags & 4) ? extent(c) : (int)c.peaks.size();
+        if (int r = fft256_r2c(c.delta, c.spec, x, stream)) return r;
+      } else if (flags & 4) {
         const int x = extent(c);
         if (x) CF(cufftExecR2C(c.r2c_b[x - 1], c.delta, (cufftComplex*)c.spec));
       } else {
@@ -155,8 +161,12 @@ struct pm_engine {
     return 0;
   }
   int fft_c2r() {
+    const StepArgs A = args();
     for (auto& c : classes) {
-      if (flags & 4) {
+      if (c.native) {
+        const int x = (flags & 4) ? extent(c) : (int)c.peaks.size();
+        if (int r = fft256_green_c2r(c.spec, c.gspec, c.force, A, c.slot_peak, x, stream)) return r;
+      } else if (flags & 4) {
         const int x = extent(c);
         if (x) CF(cufftExecC2R(c.c2r_b[x - 1], (cufftComplex*)c.gspec, c.force));
       } else {
@@ -263,6 +273,7 @@ struct pm_engine {
       cudaFree(c.spec);
       cudaFree(c.gspec);
       cudaFree(c.force);
+      cudaFree(c.slot_peak);
     }
     sort_plan_destroy(&sort);
     void* bufs[] = {d_peaks, d_clocks, d_stats, d_st_base, d_p_base, d_mode_base, epart, wpart, eslice, ecount, pos, mom, tpos,
@@ -389,7 +400,13 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
       P.force = mc.force + 3 * k * N3;
     }
     int n[3] = {(int)N, (int)N, (int)N};
-    if (E->flags & 4) {
+    if ((E->flags & 8) && N == 256) {
+      mc.native = true;
+      if ((r = E->alloc(&mc.slot_peak, (size_t)B))) return r;
+      CU(cudaMemcpy(mc.slot_peak, mc.peaks.data(), sizeof(int) * B, cudaMemcpyHostToDevice));
+      for (int k = 0; k < B; ++k) E->peaks[mc.peaks[k]].native_fft = 1;
+      if ((r = fft256_init())) return r;
+    } else if (E->flags & 4) {
       // Dynamic mode: a plan per batch size, all sharing the largest work area, so a step
       // transforms only the slots up to the highest one in use.
       size_t wmax = 0;

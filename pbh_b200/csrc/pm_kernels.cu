@@ -1136,6 +1136,7 @@ __global__ void __launch_bounds__(PM_THREADS) k_green(StepArgs A) {
   const PeakClock& C = A.clocks[pk];
   if (!C.has_delta) return;
   const PeakDesc& P = A.peaks[pk];
+  if (P.native_fft) return;  // the native transform applies the Green multiply itself
   GreenCtx g;
   g.N = P.N;
   g.log2N = P.log2N;

@@ -1,0 +1,69 @@
+"""The native 256^3 real FFT (pm_rfft3_256 / pm_irfft3_256) against torch's cuFFT in float64,
+and the engine's native-transform step (Green multiply fused into the inverse) against its
+cuFFT step on the same particles."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+N = 256
+
+
+def _rel(a, b):
+    return float((a - b).abs().pow(2).sum().sqrt() / b.abs().pow(2).sum().sqrt())
+
+
+def test_forward_and_inverse_match_cufft():
+    import torch
+    from pbh_b200 import _lib
+    lib = _lib.load()
+    g = torch.Generator(device="cuda").manual_seed(3)
+    x = torch.randn((2, N, N, N), device="cuda", generator=g, dtype=torch.float32)
+    spec = torch.empty((2, N // 2 + 1, N, N), dtype=torch.complex64, device="cuda")
+    torch.cuda.synchronize()
+    _lib.check(lib.pm_rfft3_256(x.data_ptr(), spec.data_ptr(), 2, None), "pm_rfft3_256")
+    torch.cuda.synchronize()
+    ref = torch.fft.rfftn(x.double(), dim=(1, 2, 3)).permute(0, 3, 1, 2)      # [f][kz][kx][ky]
+    assert _rel(spec.to(torch.complex128), ref) < 2e-6
+    work = torch.empty_like(spec)
+    back = torch.empty_like(x)
+    _lib.check(lib.pm_irfft3_256(spec.data_ptr(), work.data_ptr(), back.data_ptr(), 2, None), "pm_irfft3_256")
+    torch.cuda.synchronize()
+    assert _rel(back.double() / N ** 3, x.double()) < 2e-6
+    # an arbitrary (not Hermitian-consistent) spectrum: the inverse equals irfftn's (which uses
+    # the real parts of the kz = 0 and N/2 lines after the x-y inverse, like any C2R)
+    s2 = torch.randn((1, N // 2 + 1, N, N), dtype=torch.complex64, device="cuda", generator=g)
+    out = torch.empty((1, N, N, N), dtype=torch.float32, device="cuda")
+    _lib.check(lib.pm_irfft3_256(s2.data_ptr(), work.data_ptr(), out.data_ptr(), 1, None), "pm_irfft3_256")
+    torch.cuda.synchronize()
+    full = s2.to(torch.complex128).permute(0, 2, 3, 1)                      # [f][kx][ky][kz]
+    t = torch.fft.ifft(torch.fft.ifft(full, dim=1), dim=2) * (N * N)        # x-y inverse, unnormalised
+    t[..., 0] = t[..., 0].real.to(torch.complex128)
+    t[..., N // 2] = t[..., N // 2].real.to(torch.complex128)
+    ref2 = torch.fft.irfft(t, n=N, dim=3) * N
+    assert _rel(out.double(), ref2) < 2e-6
+
+
+def test_engine_native_transform_matches_cufft_step():
+    import torch
+    from pbh_b200 import recipe
+    from pbh_b200.engine import Engine, PeakConfig
+    from pbh_b200.ic import recipe_particles
+    spec = recipe.single_peak(N=N, steps=20, seed=9)
+    x, p = recipe_particles(spec, device=0, device_noise=True)
+    res = []
+    for native in (False, True):
+        eng = Engine([PeakConfig(N=N, Np=N, L=1.0)], native_fft=native)
+        eng.set_particles(0, x, p, 1.0, mode=0, param=spec.ratio(), max_steps=20)
+        eng.run(1)                                   # prime: deposit and forces at the loaded positions
+        r = dict(delta=eng.delta(0).double(), acc=eng.acc(0, 1.0).double())
+        eng.run(3)                                   # three pushes with these forces and their successors
+        r.update(pos=eng.particles(0)[0], st=eng.stats(0))
+        res.append(r)
+        eng.close()
+    a, b = res
+    assert torch.equal(a["delta"], b["delta"])       # same positions: the deposit does not involve the FFT
+    assert _rel(b["acc"], a["acc"]) < 1e-5
+    # after a few steps the two runs differ by the FP32 rounding of their forces only
+    assert float((b["pos"] - a["pos"]).abs().max()) * N < 1e-5   # in cells
+    assert b["st"].potential == pytest.approx(a["st"].potential, rel=1e-5)
+    assert b["st"].status == 0
