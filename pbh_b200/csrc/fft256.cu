@@ -6,18 +6,26 @@
 //   spectrum        s[kz][kx][ky]       129 x 256 x 256 complex ("plane-major")
 // numpy's rfftn(r)[kx][ky][kz] is s[kz][kx][ky]: the same transform, stored with kz outermost.
 //
-// Forward (R2C).  Pass Z: a real FFT along z of 32 (x, y) lines per CTA -- a complex FFT of the
-// 128 packed (even, odd) pairs, then the split into 129 outputs -- written transposed into the
-// kz planes.  Pass XY: a 2D complex FFT of every kz plane by a cluster of 4 CTAs: CTA c holds
-// the rows x = 4 x1 + c (64 rows, 128 KB of shared memory), transforms them along y and then
-// along x1, and the final 4-point combination reads the other CTAs' rows through distributed
-// shared memory and writes each output row exactly once.
+// Every 1D transform is a two-factor (Cooley-Tukey "four-step") transform held in registers:
+// a line of length L = 16 T is owned by T threads, thread t holding the 16 elements
+// n = T n1 + t, n1 = 0..15.  Each thread runs a 16-point DFT over n1 in registers and scales by
+// W_L^{t k1}; one shared-memory exchange hands every thread the T values of its k1 for the
+// T-point DFTs of the second factor; output k = k1 + 16 k2.  Register DFTs are radix-2
+// decimation in frequency, so their outputs sit in bit-reversed register order (compile-time).
+// Exchange layouts are XOR-swizzled so that both the write and the read side of every exchange
+// hit distinct shared-memory banks within each half-warp.
+//
+// Forward (R2C).  Pass Z: a real FFT along z of 32 (x, y) lines per CTA -- a complex 128-point
+// FFT of the packed (even, odd) pairs, then the split into 129 outputs -- written transposed into
+// the kz planes.  Pass XY: a 2D complex FFT of every kz plane by a cluster of XC CTAs: each
+// CTA transforms 256/XC rows along y, the cluster transposes through distributed shared
+// memory, and each CTA transforms 256/XC columns along x and writes them.
 // Inverse (C2R).  Pass XY with the Green multiply on load (-i k_i G(k) delta_k / N^3, the
 // Hermitian projection of the kz = 0, N/2 planes, the potential-energy partials), one cluster
-// per plane and gradient component; pass Z, the real inverse along z, written as force rows.
-// The 1D transforms are in-place radix-4 decimation in frequency (radix 2 first for length
-// 128), so their outputs sit in digit-reversed order and are read back through the reversal.
-// Twiddles come from a 256-entry table computed in double precision on the host.
+// per plane and gradient component (the three components of a plane adjacent in the grid, so
+// the spectrum is read from HBM once); pass Z, the real inverse along z, written as force rows.
+// Twiddles come from a 256-entry table computed in double precision on the host; the register
+// DFTs use the exact constants cos(pi/8), cos(pi/4), cos(3 pi/8).
 // Transforms are unnormalised like cuFFT's; the Green factor carries numpy's 1/N^3.
 #include <cooperative_groups.h>
 
@@ -27,20 +35,25 @@
 
 namespace cg = cooperative_groups;
 
+#ifndef PM_FFT_XC
+#define PM_FFT_XC 8  // CTAs per plane cluster (4 or 8)
+#endif
+
 namespace {
 
 constexpr int FN = 256;            // mesh side
 constexpr int FNH = FN / 2 + 1;    // kz planes
 constexpr int FM = FN / 2;         // packed complex length of a z line
-constexpr int XR = FN / 4;         // plane rows per CTA of a cluster
-constexpr int XS = FN + 1;         // padded row stride (float2) of a plane slice
-constexpr int ZT = 32;             // z lines per CTA in the Z passes
-constexpr int ZS = FM + 8;         // stride of a packed z line (two 64-halves + pad)
-constexpr int TT = ZT + 1;         // padded stride of the transposed kz tile
-constexpr int FT = 256;            // threads per CTA of the Z passes
-constexpr int XT = 1024;           // threads per CTA of the plane (XY) pass
+constexpr int ZL = 32;             // z lines per CTA in the Z passes
+constexpr int ZTH = ZL * 8;        // threads of a Z-pass CTA (8 per line)
+constexpr int ZX = FM + 8;         // row stride (float2) of a z line in shared memory, = 8 mod 16
+constexpr int ZC = ZL + 2;         // stride of the kz-major input tile of the inverse, = 2 mod 16
+constexpr int XC = PM_FFT_XC;      // CTAs per plane cluster
+constexpr int XR = FN / XC;        // plane rows (and columns) per CTA
+constexpr int XT = 16 * XR;        // threads of a plane CTA (16 per row)
 constexpr long long N2 = (long long)FN * FN;
 constexpr long long N3 = N2 * FN;
+static_assert(XC == 4 || XC == 8, "cluster size");
 
 __device__ float2 g_tw[FN];        // exp(-2 pi i k / 256) of this device
 
@@ -52,146 +65,160 @@ __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2
 // times W_4 = -i (forward) or +i (inverse)
 template <bool INV>
 __device__ __forceinline__ float2 mul_w4(float2 a) { return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x); }
-// W_256^e (forward) or its conjugate
+
+__host__ __device__ constexpr int brev(int p, int bits) {
+  int r = 0;
+  for (int i = 0; i < bits; ++i) r |= ((p >> i) & 1) << (bits - 1 - i);
+  return r;
+}
+
+// x W_16^e (conjugate twiddle for the inverse).  e is a compile-time constant wherever this is
+// called from the unrolled register DFTs, so the branches and constants fold away.
 template <bool INV>
-__device__ __forceinline__ float2 w256(const float2* t, int e) {
-  const float2 v = t[e & (FN - 1)];
-  return INV ? cconj(v) : v;
+__device__ __forceinline__ float2 mul_w16(float2 x, int e) {
+  e &= 15;
+  if (e == 0) return x;
+  if (e == 8) return make_float2(-x.x, -x.y);
+  if (e == 4) return mul_w4<INV>(x);
+  if (e == 12) return mul_w4<!INV>(x);
+  constexpr float C1 = 0.923879532511286756f, C2 = 0.707106781186547524f, C3 = 0.382683432365089772f;
+  const int q = e >> 2, r = e & 3;
+  const float cb = r == 1 ? C1 : (r == 2 ? C2 : C3), sb = r == 1 ? C3 : (r == 2 ? C2 : C1);
+  // (cos, sin) of 2 pi e / 16: the base angle r pi / 8 turned by q quarter turns
+  const float c = q == 0 ? cb : (q == 1 ? -sb : (q == 2 ? -cb : sb));
+  const float s = q == 0 ? sb : (q == 1 ? cb : (q == 2 ? -sb : -cb));
+  return cmul(x, make_float2(c, INV ? s : -s));
 }
 
-__device__ __forceinline__ int rev4_3(int p) { return ((p & 3) << 4) | (p & 12) | ((p >> 4) & 3); }
-__device__ __forceinline__ int rev4_4(int p) {
-  return ((p & 3) << 6) | (((p >> 2) & 3) << 4) | (((p >> 4) & 3) << 2) | ((p >> 6) & 3);
-}
-// Where output k of the 128-point transform (radix 2, then radix 4 x 3) sits.
-__device__ __forceinline__ int pos128(int k) { return ((k & 1) << 6) | rev4_3(k >> 1); }
-
-// Radix-4 DIF stages with sub-lengths LS, LS/4, ..., 4 on nseq sequences of length L whose
-// element i sits at buf[base(seq) + i * es], by NT threads.  All divisors are compile-time
-// powers of two.  SEQ_FAST: consecutive threads take consecutive sequences (for sequences
-// that run across rows); otherwise consecutive butterflies of one sequence.  Ends with a barrier.
-template <bool INV, int L, int LS, int NT, bool SEQ_FAST, class Base>
-__device__ __forceinline__ void dif4(float2* buf, int nseq, Base base, int es, const float2* t) {
-  constexpr int q = LS / 4, step = FN / LS, BPS = L / 4;
-  const int nb = nseq * BPS;
-  for (int b = threadIdx.x; b < nb; b += NT) {
-    int seq, r;
-    if (SEQ_FAST) {
-      seq = b % nseq;
-      r = b / nseq;
-    } else {
-      seq = b / BPS;
-      r = b % BPS;
+// Radix-2 DIF DFT of length L on v[OFF .. OFF + L - 1] in registers: afterwards v[OFF + p] holds
+// output brev(p, log2 L).
+template <bool INV, int L, int OFF, int NV>
+__device__ __forceinline__ void dft_reg(float2 (&v)[NV]) {
+  if constexpr (L > 1) {
+#pragma unroll
+    for (int j = 0; j < L / 2; ++j) {
+      const float2 a = v[OFF + j], b = v[OFF + j + L / 2];
+      v[OFF + j] = cadd(a, b);
+      v[OFF + j + L / 2] = mul_w16<INV>(csub(a, b), j * (16 / L));
     }
-    const int blk = r / q, j = r % q;
-    float2* p = buf + base(seq) + (blk * LS + j) * es;
-    const int qs = q * es;
-    const float2 x0 = p[0], x1 = p[qs], x2 = p[2 * qs], x3 = p[3 * qs];
-    const float2 a = cadd(x0, x2), c = csub(x0, x2), s = cadd(x1, x3), d = mul_w4<INV>(csub(x1, x3));
-    // y_r = sum_q x_q W_4^{q r}; quarter r takes y_r W_LS^{j r}
-    p[0] = cadd(a, s);
-    p[qs] = cmul(cadd(c, d), w256<INV>(t, j * step));
-    p[2 * qs] = cmul(csub(a, s), w256<INV>(t, 2 * j * step));
-    p[3 * qs] = cmul(csub(c, d), w256<INV>(t, 3 * j * step));
+    dft_reg<INV, L / 2, OFF, NV>(v);
+    dft_reg<INV, L / 2, OFF + L / 2, NV>(v);
   }
-  __syncthreads();
-  if constexpr (LS > 4) dif4<INV, L, LS / 4, NT, SEQ_FAST>(buf, nseq, base, es, t);
-}
-
-// 128-point transforms of nseq sequences at buf[seq * ZS + i]: radix 2, then radix 4 on the two
-// 64-point halves.
-template <bool INV, int NT>
-__device__ __forceinline__ void fft128(float2* buf, int nseq, const float2* t) {
-  for (int b = threadIdx.x; b < nseq * 64; b += NT) {
-    const int seq = b >> 6, j = b & 63;
-    float2* p = buf + seq * ZS + j;
-    const float2 a = p[0], c = p[64];
-    p[0] = cadd(a, c);
-    p[64] = cmul(csub(a, c), w256<INV>(t, 2 * j));  // W_128^j
-  }
-  __syncthreads();
-  dif4<INV, 64, 64, NT, false>(buf, 2 * nseq, [](int h) { return (h >> 1) * ZS + (h & 1) * 64; }, 1, t);
 }
 
 __device__ __forceinline__ void cpa8(void* dst, const void* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
                : "memory");
 }
-__device__ __forceinline__ void cpa16(void* dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
-               : "memory");
-}
 __device__ __forceinline__ void cpa_wait() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-template <int NT>
-__device__ __forceinline__ void load_tw(float2* t) {
-  for (int i = threadIdx.x; i < FN; i += NT) t[i] = g_tw[i];
+// Shared twiddle tables of the Z passes: tw[e] = W_256^e, t8[k1 * 8 + t] = W_128^{t k1}
+// (conjugated for the inverse).
+template <bool INV>
+__device__ __forceinline__ void load_ztw(float2* tw, float2* t8) {
+  for (int i = threadIdx.x; i < FN; i += ZTH) {
+    const float2 w = g_tw[i];
+    tw[i] = INV ? cconj(w) : w;
+  }
+  for (int i = threadIdx.x; i < FM; i += ZTH) {
+    const float2 w = g_tw[(2 * (i >> 3) * (i & 7)) & (FN - 1)];
+    t8[i] = INV ? cconj(w) : w;
+  }
 }
 
-// Pass Z forward: fields in[f][x][y][z] -> planes out[f][kz][x][y].  grid (FN/ZT, FN, nf).
-__global__ void __launch_bounds__(FT) k_fft_z_r2c(const float* __restrict__ in, float2* __restrict__ out) {
-  extern __shared__ __align__(16) float2 zs[];
-  float2* t = zs;                  // [FN]
-  float2* buf = t + FN;            // [ZT][ZS]
-  float2* T = buf + ZT * ZS;       // [FNH][TT]
-  load_tw<FT>(t);
-  const int y0 = blockIdx.x * ZT, x = blockIdx.y, f = blockIdx.z;
-  const float2* src = reinterpret_cast<const float2*>(in + (long long)f * N3 + ((long long)x * FN + y0) * FN);
-  for (int e = threadIdx.x; e < ZT * FM / 2; e += FT) {  // two packed pairs (16 bytes) per copy
-    const int yl = e / (FM / 2), n = 2 * (e - yl * (FM / 2));
-    cpa16(buf + yl * ZS + n, src + (long long)yl * FM + n);  // (r[2n], r[2n+1]) packed as one complex
+// The 128-point transform of one packed z line shared by 8 threads (thread t holds v[n1] =
+// element 8 n1 + t): returns u[8 s + q] = element k1 + 16 brev(q, 3) of the transform, k1 = t + 8 s.
+// row: this line's exchange row in shared memory.  Ends after the exchange has been read: the
+// caller must barrier before it writes the row again.
+template <bool INV>
+__device__ __forceinline__ void fft128_line(float2 (&v)[16], float2 (&u)[16], float2* row, const float2* t8, int t) {
+  dft_reg<INV, 16, 0, 16>(v);
+#pragma unroll
+  for (int p = 0; p < 16; ++p) {
+    const int k1 = brev(p, 4);
+    row[k1 * 8 + (t ^ (k1 & 7))] = k1 ? cmul(v[p], t8[k1 * 8 + t]) : v[p];
   }
-  cpa_wait();
   __syncthreads();
-  fft128<false, FT>(buf, ZT, t);
+#pragma unroll
+  for (int s = 0; s < 2; ++s)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) u[8 * s + j] = row[(t + 8 * s) * 8 + (j ^ t)];
+  dft_reg<INV, 8, 0, 16>(u);
+  dft_reg<INV, 8, 8, 16>(u);
+}
+
+// Pass Z forward: fields in[f][x][y][z] -> planes out[f][kz][x][y].  grid (FN/ZL, FN, nf).
+__global__ void __launch_bounds__(ZTH, 4) k_fft_z_r2c(const float* __restrict__ in, float2* __restrict__ out) {
+  __shared__ float2 tw[FN], t8[FM];
+  __shared__ __align__(16) float2 xb[ZL * ZX];
+  load_ztw<false>(tw, t8);
+  const int t = threadIdx.x & 7, l = threadIdx.x >> 3;
+  const int y0 = blockIdx.x * ZL, x = blockIdx.y, f = blockIdx.z;
+  const float2* src = reinterpret_cast<const float2*>(in + (long long)f * N3 + ((long long)x * FN + y0 + l) * FN);
+  float2 v[16], u[16];
+#pragma unroll
+  for (int n1 = 0; n1 < 16; ++n1) v[n1] = __ldg(src + 8 * n1 + t);  // (r[2n], r[2n+1]), n = 8 n1 + t
+  __syncthreads();  // tables
+  float2* row = xb + l * ZX;
+  fft128_line<false>(v, u, row, t8, t);
+  __syncthreads();
+  // Z_k into the line's row in natural order, swizzled so that the column reads below are
+  // conflict-free: Z_k at row[k ^ sw(l)].
+  const int sw = (l >> 1) & 7;
+#pragma unroll
+  for (int s = 0; s < 2; ++s)
+#pragma unroll
+    for (int q = 0; q < 8; ++q) row[(t + 8 * s + 16 * brev(q, 3)) ^ sw] = u[8 * s + q];
+  __syncthreads();
   // X_k = E_k + W_256^k O_k with E = (Z_k + conj Z_{M-k})/2, O = -i (Z_k - conj Z_{M-k})/2
-  for (int e = threadIdx.x; e < FNH * ZT; e += FT) {
-    const int k = e / ZT, yl = e - k * ZT;
-    const float2 zk = buf[yl * ZS + pos128(k & (FM - 1))];
-    const float2 zm = cconj(buf[yl * ZS + pos128((FM - k) & (FM - 1))]);
+  float2* dst = out + (long long)f * FNH * N2 + (long long)x * FN + y0;
+  for (int e = threadIdx.x; e < FNH * ZL; e += ZTH) {
+    const int k = e / ZL, ll = e - k * ZL, sl = (ll >> 1) & 7;
+    const float2* zr = xb + ll * ZX;
+    const float2 zk = zr[(k & (FM - 1)) ^ sl];
+    const float2 zm = cconj(zr[((FM - k) & (FM - 1)) ^ sl]);
     const float2 E = cscale(cadd(zk, zm), 0.5f);
     const float2 O = cscale(mul_w4<false>(csub(zk, zm)), 0.5f);
-    T[k * TT + yl] = cadd(E, cmul(w256<false>(t, k), O));
-  }
-  __syncthreads();
-  float2* dst = out + (long long)f * FNH * N2 + (long long)x * FN + y0;
-  for (int e = threadIdx.x; e < FNH * ZT; e += FT) {
-    const int k = e / ZT, yl = e - k * ZT;
-    dst[(long long)k * N2 + yl] = T[k * TT + yl];
+    dst[(long long)k * N2 + ll] = cadd(E, cmul(tw[k], O));
   }
 }
 
-// Pass Z inverse: planes in[f][kz][x][y] -> fields out[f][x][y][z].  grid (FN/ZT, FN, nf).
-__global__ void __launch_bounds__(FT) k_fft_z_c2r(const float2* __restrict__ in, float* __restrict__ out) {
-  extern __shared__ __align__(16) float2 zs[];
-  float2* t = zs;
-  float2* buf = t + FN;
-  float2* T = buf + ZT * ZS;
-  load_tw<FT>(t);
-  const int y0 = blockIdx.x * ZT, x = blockIdx.y, f = blockIdx.z;
+// Pass Z inverse: planes in[f][kz][x][y] -> fields out[f][x][y][z].  grid (FN/ZL, FN, nf).
+__global__ void __launch_bounds__(ZTH, 4) k_fft_z_c2r(const float2* __restrict__ in, float* __restrict__ out) {
+  __shared__ float2 tw[FN], t8[FM];
+  __shared__ __align__(16) float2 xb[FNH * ZC];  // the kz-major tile, later the exchange rows
+  static_assert(FNH * ZC >= ZL * ZX, "exchange rows fit in the tile");
+  const int y0 = blockIdx.x * ZL, x = blockIdx.y, f = blockIdx.z;
   const float2* src = in + (long long)f * FNH * N2 + (long long)x * FN + y0;
-  for (int e = threadIdx.x; e < FNH * ZT; e += FT) {
-    const int k = e / ZT, yl = e - k * ZT;
-    cpa8(T + k * TT + yl, src + (long long)k * N2 + yl);
+  for (int e = threadIdx.x; e < FNH * ZL; e += ZTH) {
+    const int k = e / ZL, ll = e - k * ZL;
+    cpa8(xb + k * ZC + ll, src + (long long)k * N2 + ll);
   }
+  load_ztw<true>(tw, t8);
   cpa_wait();
   __syncthreads();
-  if (threadIdx.x < 2 * ZT) T[(threadIdx.x < ZT ? 0 : FM) * TT + (threadIdx.x & (ZT - 1))].y = 0.f;  // C2R reads
-  __syncthreads();                                                                                  // only Re of DC, Nyquist
-  // Z_k = E_k + i O_k with E = X_k + conj X_{M-k}, O = (X_k - conj X_{M-k}) W_256^{-k}
-  for (int e = threadIdx.x; e < ZT * FM; e += FT) {
-    const int yl = e / FM, k = e - yl * FM;
-    const float2 xk = T[k * TT + yl], xm = cconj(T[(FM - k) * TT + yl]);
-    const float2 O = cmul(csub(xk, xm), w256<true>(t, k));
-    buf[yl * ZS + k] = cadd(cadd(xk, xm), make_float2(-O.y, O.x));
+  const int t = threadIdx.x & 7, l = threadIdx.x >> 3;
+  // Z_n = E_n + i O_n with E = X_n + conj X_{M-n}, O = (X_n - conj X_{M-n}) W_256^{-n}; a C2R
+  // reads only the real parts of X_0 and X_M.
+  float2 v[16], u[16];
+#pragma unroll
+  for (int n1 = 0; n1 < 16; ++n1) {
+    const int n = 8 * n1 + t;
+    float2 xk = xb[n * ZC + l], xm = cconj(xb[(FM - n) * ZC + l]);
+    if (n == 0) {
+      xk.y = 0.f;
+      xm.y = 0.f;
+    }
+    const float2 O = cmul(csub(xk, xm), tw[n]);
+    v[n1] = cadd(cadd(xk, xm), make_float2(-O.y, O.x));
   }
-  __syncthreads();
-  fft128<true, FT>(buf, ZT, t);
-  float2* dst = reinterpret_cast<float2*>(out + (long long)f * N3 + ((long long)x * FN + y0) * FN);
-  for (int e = threadIdx.x; e < ZT * FM; e += FT) {
-    const int yl = e / FM, n = e - yl * FM;
-    dst[(long long)yl * FM + n] = buf[yl * ZS + pos128(n)];  // (r[2n], r[2n+1])
-  }
+  __syncthreads();  // the tile is read; its memory becomes the exchange rows
+  fft128_line<true>(v, u, xb + l * ZX, t8, t);
+  float2* dst = reinterpret_cast<float2*>(out + (long long)f * N3 + ((long long)x * FN + y0 + l) * FN);
+#pragma unroll
+  for (int s = 0; s < 2; ++s)
+#pragma unroll
+    for (int q = 0; q < 8; ++q) dst[t + 8 * s + 16 * brev(q, 3)] = u[8 * s + q];  // (r[2n], r[2n+1])
 }
 
 // Green's-function multiply of one spectral value (the per-mode work of k_green).
@@ -205,21 +232,50 @@ __device__ __forceinline__ float gk(float k, float dx, int mode) {
   if (mode == 2) return (8.0f * sinf(k * dx) - sinf(2.0f * k * dx)) / (6.0f * dx);
   return k;
 }
+// -i g_comp(k) G(k) delta_k at mode (x, y, kz) of a plane whose values start at plane; adds the
+// mode's weight in the potential energy to w (component 0).
+__device__ __forceinline__ float2 green_mode(float2 v, int x, int y, int kz, int comp, const GreenPlane& gp,
+                                             const float2* plane, double& w) {
+  const float kx = kl(x, gp.kf), ky = kl(y, gp.kf), kzv = gp.kf * (float)kz;
+  const float k2 = kx * kx + ky * ky + kzv * kzv;
+  if (x == 0 && y == 0 && kz == 0) return make_float2(0.f, 0.f);
+  float G = gp.s_c / k2;
+  if (gp.sd2 > 0.f) G *= expf(-0.5f * k2 * gp.sd2);
+  const float kc = comp == 0 ? kx : (comp == 1 ? ky : kzv);
+  const float g = gk(kc, gp.dx, gp.gm) * G;
+  if (comp == 0) w += (double)(((kz == 0 || kz == FM) ? 1.0f : 2.0f) * G * (v.x * v.x + v.y * v.y));
+  float2 o = make_float2(g * v.y, -g * v.x);  // -i g v
+  if (kz == 0 || kz == FM) {  // (o + conj(o at -k)) / 2: numpy's C2R sees this plane's Hermitian part
+    const int px = (-x) & (FN - 1), py = (-y) & (FN - 1);
+    const float2 dp = plane[(long long)px * FN + py];
+    const float kpc = comp == 0 ? kl(px, gp.kf) : (comp == 1 ? kl(py, gp.kf) : kzv);
+    const float h = gk(kpc, gp.dx, gp.gm) * G;
+    o = make_float2(0.5f * (o.x + h * dp.y), 0.5f * (o.y + h * dp.x));
+  }
+  return o;
+}
 
-// Pass XY: 2D FFT of every kz plane, one cluster of 4 CTAs per plane (and component).
-// Forward: in = out = planes[slot][kz][x][y] (in place).  Inverse with GREEN: in = spectrum
-// planes[slot][kz][kx][ky], out = planes[slot][comp][kz][x][y], comp = blockIdx.y, the
-// multiply applied on load; slot_peak maps a slot to its peak.  Inverse without GREEN:
-// in = out layout [f][kz][.][.].  grid (4 * nslots * FNH, ncomp), cluster (4, 1, 1).
+// Pass XY: 2D FFT of every kz plane by a cluster of XC CTAs.  CTA c transforms the rows
+// x = XR c + r along y, the cluster transposes through distributed shared memory (CTA m takes
+// the columns ky = XR m + j of all 256 rows, each value crossing between SMs once), and CTA m
+// transforms its columns along x and writes them.  Forward: in = out = planes[slot][kz][x][y]
+// (in place: every load precedes the first cluster barrier).  Inverse with GREEN: in =
+// spectrum planes[slot][kz][kx][ky], out = planes[slot][comp][kz][x][y], the multiply applied
+// on load; slot_peak maps a slot to its peak.  Inverse without GREEN: in = out layout
+// [f][kz][.][.].  grid (XC * nslots * FNH * ncomp): cluster index (slot * FNH + kz) * ncomp + comp.
 template <bool INV, bool GREEN>
-__global__ void __launch_bounds__(XT, 1) k_fft_xy(const float2* in, float2* out, StepArgs A, const int* slot_peak) {
+__global__ void __launch_bounds__(XT, XC == 4 ? 1 : 2) k_fft_xy(const float2* in, float2* out, StepArgs A,
+                                                                 const int* slot_peak, int ncomp) {
   extern __shared__ __align__(16) float2 xs[];
-  float2* t = xs;              // [FN]
-  float2* buf = t + FN;        // [XR][XS]
+  float2* ty = xs;             // [16 * 16]  W_256^{t k1} at k1 * 16 + t (conjugated for the inverse)
+  float2* buf = ty + FN;       // [XR][FN]: the y-transformed rows, then the x exchange
+  for (int i = threadIdx.x; i < FN; i += XT) {
+    const float2 b = g_tw[((i >> 4) * (i & 15)) & (FN - 1)];
+    ty[i] = INV ? cconj(b) : b;
+  }
   cg::cluster_group cluster = cg::this_cluster();
   const int c = (int)cluster.block_rank();
-  const int pl = blockIdx.x >> 2, slot = pl / FNH, kz = pl - slot * FNH;
-  const int comp = blockIdx.y, ncomp = gridDim.y;
+  const int cl = blockIdx.x / XC, comp = cl % ncomp, pl = cl / ncomp, slot = pl / FNH, kz = pl - slot * FNH;
   GreenPlane gp{};
   int pk = 0;
   if (GREEN) {
@@ -232,114 +288,80 @@ __global__ void __launch_bounds__(XT, 1) k_fft_xy(const float2* in, float2* out,
     gp.sd2 = P.smooth > 0 ? (float)(P.smooth * P.dx) * (float)(P.smooth * P.dx) : 0.f;
     gp.gm = P.gradient;
   }
-  load_tw<XT>(t);
-  const float2* src = in + (long long)pl * N2;
-  double w = 0.0;  // potential-energy partial (component 0 of the Green pass)
-  constexpr int PER = XR * FN / XT;  // elements per thread
-  float2 vin[PER];
+  // Along y: row r (x = XR c + r) by 16 threads, thread t holding y = 16 n1 + t.
+  const int t = threadIdx.x & 15, r = threadIdx.x >> 4, x = XR * c + r;
+  const float2* plane = in + (long long)pl * N2;
+  float2 v[16], u[16];
+#pragma unroll
+  for (int n1 = 0; n1 < 16; ++n1) v[n1] = plane[(long long)x * FN + 16 * n1 + t];
   if (GREEN) {
+    double w = 0.0;  // potential-energy partial (component 0)
 #pragma unroll
-    for (int i = 0; i < PER; ++i) {  // all loads in flight before any is used
-      const int e = threadIdx.x + i * XT, x1 = e / FN, y = e - x1 * FN;
-      vin[i] = src[(long long)(4 * x1 + c) * FN + y];
+    for (int n1 = 0; n1 < 16; ++n1) v[n1] = green_mode(v[n1], x, 16 * n1 + t, kz, comp, gp, plane, w);
+    if (comp == 0) {
+      for (int d = 16; d > 0; d >>= 1) w += __shfl_down_sync(0xffffffffu, w, d);
+      if ((threadIdx.x & 31) == 0)
+        A.wpart[A.peaks[pk].mode_base * (PM_THREADS / 32) + ((long long)kz * XC + c) * (XT / 32) + (threadIdx.x >> 5)] = w;
     }
-  } else {
-    for (int e = threadIdx.x; e < XR * FN; e += XT) {
-      const int x1 = e / FN, y = e - x1 * FN;
-      cpa8(buf + x1 * XS + y, src + (long long)(4 * x1 + c) * FN + y);
-    }
-    cpa_wait();
   }
+  __syncthreads();  // table
+  float2* row = buf + r * FN;
+  dft_reg<INV, 16, 0, 16>(v);
 #pragma unroll
-  for (int i = 0; i < (GREEN ? PER : 0); ++i) {
-    const int e = threadIdx.x + i * XT;
-    const int x1 = e / FN, y = e - x1 * FN, x = 4 * x1 + c;
-    float2 v = vin[i];
-    {
-      const float kx = kl(x, gp.kf), ky = kl(y, gp.kf), kzv = gp.kf * (float)kz;
-      const float k2 = kx * kx + ky * ky + kzv * kzv;
-      if (x == 0 && y == 0 && kz == 0) {
-        v = make_float2(0.f, 0.f);
-      } else {
-        float G = gp.s_c / k2;
-        if (gp.sd2 > 0.f) G *= expf(-0.5f * k2 * gp.sd2);
-        const float kc = comp == 0 ? kx : (comp == 1 ? ky : kzv);
-        const float g = gk(kc, gp.dx, gp.gm) * G;
-        if (comp == 0) w += (double)(((kz == 0 || kz == FM) ? 1.0f : 2.0f) * G * (v.x * v.x + v.y * v.y));
-        float2 o = make_float2(g * v.y, -g * v.x);  // -i g v
-        if (kz == 0 || kz == FM) {  // (o + conj(o at -k)) / 2: numpy's C2R sees this plane's Hermitian part
-          const int px = (-x) & (FN - 1), py = (-y) & (FN - 1);
-          const float2 dp = src[(long long)px * FN + py];
-          const float kpc = comp == 0 ? kl(px, gp.kf) : (comp == 1 ? kl(py, gp.kf) : kzv);
-          const float h = gk(kpc, gp.dx, gp.gm) * G;
-          o = make_float2(0.5f * (o.x + h * dp.y), 0.5f * (o.y + h * dp.x));
-        }
-        v = o;
-      }
-    }
-    buf[x1 * XS + y] = v;
-  }
-  if (GREEN && comp == 0) {
-    for (int d = 16; d > 0; d >>= 1) w += __shfl_down_sync(0xffffffffu, w, d);
-    if ((threadIdx.x & 31) == 0)
-      A.wpart[A.peaks[pk].mode_base * (PM_THREADS / 32) + ((long long)kz * 4 + c) * (XT / 32) + (threadIdx.x >> 5)] = w;
+  for (int p = 0; p < 16; ++p) {
+    const int k1 = brev(p, 4);
+    row[k1 * 16 + (t ^ k1)] = k1 ? cmul(v[p], ty[k1 * 16 + t]) : v[p];
   }
   __syncthreads();
-  dif4<INV, FN, FN, XT, false>(buf, XR, [](int s) { return s * XS; }, 1, t);   // along y, 64 rows
-  dif4<INV, XR, XR, XT, true>(buf, FN, [](int s) { return s; }, XS, t);        // along x1, 256 columns
-  // Undo the digit reversal along y in place (an involution: swap each pair once), so the
-  // cross-CTA reads below run along consecutive addresses.
-  for (int e = threadIdx.x; e < XR * FN; e += XT) {
-    const int row = e / FN, y = e - row * FN, ry = rev4_4(y);
-    if (y < ry) {
-      float2* r = buf + row * XS;
-      const float2 v = r[y];
-      r[y] = r[ry];
-      r[ry] = v;
-    }
-  }
+#pragma unroll
+  for (int j = 0; j < 16; ++j) u[j] = row[t * 16 + (j ^ t)];
+  dft_reg<INV, 16, 0, 16>(u);  // u[p] = row spectrum at ky = t + 16 brev(p)
+  __syncthreads();
+#pragma unroll
+  for (int p = 0; p < 16; ++p) row[t + 16 * brev(p, 4)] = u[p];
   cluster.sync();
-  // out[k1 + 64 c][y] = sum_cc W_256^{cc k1} W_4^{cc c} F_cc[k1][y]
-  float2* dst = out + ((long long)(slot * ncomp + comp) * FNH + kz) * N2;
-  const float2* rbs[4];
+  // Along x: column ky = XR c + j by 16 threads, thread tx holding x = 16 n1 + tx, which is row
+  // (16 n1) % XR + tx of CTA (16 n1) / XR.
+  const int j = threadIdx.x % XR, tx = threadIdx.x / XR, ky = XR * c + j;
 #pragma unroll
-  for (int cc = 0; cc < 4; ++cc) rbs[cc] = cluster.map_shared_rank(buf, cc);
-  for (int e = threadIdx.x; e < XR * FN; e += XT) {
-    const int k1 = e / FN, yn = e - k1 * FN;
-    const int at = rev4_3(k1) * XS + yn;
-    float2 acc = make_float2(0.f, 0.f);
-#pragma unroll
-    for (int cc = 0; cc < 4; ++cc) {
-      const float2 f = cmul(rbs[cc][at], w256<INV>(t, cc * k1));
-      // W_4^{cc c}: 1, -i, -1, +i (forward; conjugate for the inverse)
-      const int m = (cc * c) & 3;
-      const float2 r = m == 0 ? f : (m == 2 ? make_float2(-f.x, -f.y) : (m == 1 ? mul_w4<INV>(f) : mul_w4<!INV>(f)));
-      acc = cadd(acc, r);
-    }
-    dst[(long long)(k1 + XR * c) * FN + yn] = acc;
+  for (int n1 = 0; n1 < 16; ++n1) {
+    const float2* src = cluster.map_shared_rank(buf, (16 * n1) / XR);
+    v[n1] = src[((16 * n1) % XR + tx) * FN + ky];
   }
-  cluster.sync();  // the other CTAs have finished reading this CTA's rows
+  cluster.sync();  // every CTA has read its columns: the buffers are free again
+  dft_reg<INV, 16, 0, 16>(v);
+#pragma unroll
+  for (int p = 0; p < 16; ++p) {
+    const int k1 = brev(p, 4);
+    buf[(k1 * 16 + tx) * XR + j] = k1 ? cmul(v[p], ty[k1 * 16 + tx]) : v[p];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < 16; ++i) u[i] = buf[(tx * 16 + i) * XR + j];
+  dft_reg<INV, 16, 0, 16>(u);  // u[p] = column spectrum at kx = tx + 16 brev(p)
+  float2* dst = out + ((long long)(slot * ncomp + comp) * FNH + kz) * N2 + ky;
+#pragma unroll
+  for (int p = 0; p < 16; ++p) dst[(long long)(tx + 16 * brev(p, 4)) * FN] = u[p];
 }
 
-constexpr size_t kZSmem = sizeof(float2) * (FN + ZT * ZS + FNH * TT);
-constexpr size_t kXYSmem = sizeof(float2) * (FN + XR * XS);
+constexpr size_t kXYSmem = sizeof(float2) * (FN + XR * FN);
 
 template <bool INV, bool GREEN>
 cudaError_t launch_xy(const float2* in, float2* out, const StepArgs& A, const int* slot_peak, int nslots, int ncomp,
                       cudaStream_t s) {
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(4u * (unsigned)nslots * FNH, (unsigned)ncomp, 1);
+  cfg.gridDim = dim3((unsigned)XC * (unsigned)nslots * FNH * (unsigned)ncomp, 1, 1);
   cfg.blockDim = dim3(XT, 1, 1);
   cfg.dynamicSmemBytes = kXYSmem;
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = 4;
+  attr[0].val.clusterDim.x = XC;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_fft_xy<INV, GREEN>, in, out, A, slot_peak);
+  return cudaLaunchKernelEx(&cfg, k_fft_xy<INV, GREEN>, in, out, A, slot_peak, ncomp);
 }
 
 }  // namespace
@@ -352,8 +374,6 @@ int fft256_init() {
     h[k] = make_float2((float)cos(a), (float)sin(a));
   }
   cudaError_t e = cudaMemcpyToSymbol(g_tw, h, sizeof(h));
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fft_z_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kZSmem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fft_z_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kZSmem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_fft_xy<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kXYSmem);
   if (e == cudaSuccess)
@@ -366,7 +386,7 @@ int fft256_init() {
 // delta fields [slot][x][y][z] -> spectra [slot][kz][kx][ky]
 int fft256_r2c(const float* delta, float2* spec, int nslots, cudaStream_t s) {
   if (nslots <= 0) return 0;
-  k_fft_z_r2c<<<dim3(FN / ZT, FN, nslots), FT, kZSmem, s>>>(delta, spec);
+  k_fft_z_r2c<<<dim3(FN / ZL, FN, nslots), ZTH, 0, s>>>(delta, spec);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = launch_xy<false, false>(spec, spec, StepArgs{}, nullptr, nslots, 1, s);
   return e == cudaSuccess ? 0 : -(int)e;
@@ -379,7 +399,7 @@ int fft256_green_c2r(const float2* spec, float2* gwork, float* force, const Step
   if (nslots <= 0) return 0;
   cudaError_t e = launch_xy<true, true>(spec, gwork, A, slot_peak, nslots, 3, s);
   if (e == cudaSuccess) {
-    k_fft_z_c2r<<<dim3(FN / ZT, FN, 3 * nslots), FT, kZSmem, s>>>(gwork, force);
+    k_fft_z_c2r<<<dim3(FN / ZL, FN, 3 * nslots), ZTH, 0, s>>>(gwork, force);
     e = cudaGetLastError();
   }
   return e == cudaSuccess ? 0 : -(int)e;
@@ -390,7 +410,7 @@ int fft256_c2r(const float2* spec, float2* gwork, float* out, int nfields, cudaS
   if (nfields <= 0) return 0;
   cudaError_t e = launch_xy<true, false>(spec, gwork, StepArgs{}, nullptr, nfields, 1, s);
   if (e == cudaSuccess) {
-    k_fft_z_c2r<<<dim3(FN / ZT, FN, nfields), FT, kZSmem, s>>>(gwork, out);
+    k_fft_z_c2r<<<dim3(FN / ZL, FN, nfields), ZTH, 0, s>>>(gwork, out);
     e = cudaGetLastError();
   }
   return e == cudaSuccess ? 0 : -(int)e;
