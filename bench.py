@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="arrival window of the served stream")
     ap.add_argument("--serve-rate", type=float, default=20.0, help="mean request arrivals per second")
     ap.add_argument("--tiles", default="auto", help="super-tile side: 'auto' (autotuned per mesh size) or 4/8/16")
+    ap.add_argument("--fft", choices=["cufft", "native"], default="cufft",
+                    help="256^3 transforms: cuFFT, or the native kernels with the Green multiply fused")
     return ap.parse_args()
 
 
@@ -235,7 +237,11 @@ def run_ours(args):
         tiles = autotune({s.N for s in specs} | ({64, 128, 256} if not args.no_serve else set()), device=local)
     else:
         tiles = {s.N: min(int(args.tiles), s.N) for s in specs}
-    ens = Ensemble(specs, device=local, bucket_sort=not args.full_sort, tiles=tiles)
+    ens = Ensemble(specs, device=local, bucket_sort=not args.full_sort, tiles=tiles, native_fft=args.fft == "native")
+    # the native 256^3 transform: 4 launches a step (2 passes each way), and no Green launch
+    # when every mesh is 256^3
+    has256 = args.fft == "native" and any(s.N == 256 for s in specs)
+    native_launches = (4 - (1 if all(s.N == 256 for s in specs) else 0)) if has256 else 0
     lib = _lib.load()
     info = (np.zeros(6, dtype=np.int64))
     lib.pm_engine_info(ens.engine._h, info.ctypes.data)
@@ -304,8 +310,9 @@ def run_ours(args):
             "config": dict(desc, particles_per_gpu=n_step, peaks=len(specs), l2="inputs larger than L2 (126 MB)",
                            regroup="Morton radix sort every step" if args.full_sort else
                            "re-binning each step, Morton radix sort every 16th", parallelism=f"replicas x{world}",
-                           super_tiles={str(k): v for k, v in sorted(tiles.items())}),
-            "clocks": clocks, "gpu_launches": args.steps * (13 + npass), "roofline": roofline}
+                           super_tiles={str(k): v for k, v in sorted(tiles.items())},
+                           fft_256="native (Green fused into the inverse)" if args.fft == "native" else "cuFFT"),
+            "clocks": clocks, "gpu_launches": args.steps * (13 + npass + native_launches), "roofline": roofline}
 
     if rank == 0 and not args.no_plain and args.workload == "batched":
         pr = plain_rate(specs, steps=8, warmup=3, device=local, tiles=tiles)

@@ -19,7 +19,7 @@ from .ic import recipe_particles
 
 class Ensemble:
     def __init__(self, specs, device: int = 0, graph: bool = True, bucket_sort: bool = True, tiles=None,
-                 delta_collapse: float = 0.0):
+                 delta_collapse: float = 0.0, native_fft: bool = False):
         self.specs = list(specs)
         if tiles == "auto":                      # per mesh size, timed on this GPU (pbh_b200.tune)
             from .tune import autotune
@@ -27,7 +27,7 @@ class Ensemble:
         tiles = tiles or {}
         self.tiles = {int(k): int(v) for k, v in tiles.items()}
         self.cfgs = [PeakConfig(N=s.N, Np=s.N, L=s.L, tile=int(tiles.get(s.N, 0))) for s in self.specs]
-        self.engine = Engine(self.cfgs, device=device, bucket_sort=bucket_sort, graph=graph)
+        self.engine = Engine(self.cfgs, device=device, bucket_sort=bucket_sort, graph=graph, native_fft=native_fft)
         self.device = device
         self.delta_collapse = float(delta_collapse)
         self.n = np.array([s.n for s in self.specs], dtype=np.int64)

@@ -204,7 +204,9 @@ struct pm_engine {
     CU(mark());
     if ((r = fft_r2c())) return r;
     CU(mark());
-    launch_green(A, nmodeblk, stream);
+    bool any_cufft = false;  // the native transform carries the Green multiply of its classes
+    for (const auto& c : classes) any_cufft = any_cufft || !c.native;
+    if (any_cufft) launch_green(A, nmodeblk, stream);
     CU(mark());
     if ((r = fft_c2r())) return r;
     CU(mark());

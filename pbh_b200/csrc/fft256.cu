@@ -53,7 +53,7 @@ constexpr int XR = FN / XC;        // plane rows (and columns) per CTA
 constexpr int XT = 16 * XR;        // threads of a plane CTA (16 per row)
 constexpr long long N2 = (long long)FN * FN;
 constexpr long long N3 = N2 * FN;
-static_assert(XC == 4 || XC == 8, "cluster size");
+static_assert(XC == 4 || XC == 8 || XC == 16, "cluster size");
 
 __device__ float2 g_tw[FN];        // exp(-2 pi i k / 256) of this device
 
@@ -264,7 +264,7 @@ __device__ __forceinline__ float2 green_mode(float2 v, int x, int y, int kz, int
 // on load; slot_peak maps a slot to its peak.  Inverse without GREEN: in = out layout
 // [f][kz][.][.].  grid (XC * nslots * FNH * ncomp): cluster index (slot * FNH + kz) * ncomp + comp.
 template <bool INV, bool GREEN>
-__global__ void __launch_bounds__(XT, XC == 4 ? 1 : 2) k_fft_xy(const float2* in, float2* out, StepArgs A,
+__global__ void __launch_bounds__(XT, 1024 / XT) k_fft_xy(const float2* in, float2* out, StepArgs A,
                                                                  const int* slot_peak, int ncomp) {
   extern __shared__ __align__(16) float2 xs[];
   float2* ty = xs;             // [16 * 16]  W_256^{t k1} at k1 * 16 + t (conjugated for the inverse)
@@ -361,6 +361,10 @@ cudaError_t launch_xy(const float2* in, float2* out, const StepArgs& A, const in
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
+  if (XC > 8) {
+    const cudaError_t e = cudaFuncSetAttribute(k_fft_xy<INV, GREEN>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) return e;
+  }
   return cudaLaunchKernelEx(&cfg, k_fft_xy<INV, GREEN>, in, out, A, slot_peak, ncomp);
 }
 
