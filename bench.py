@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="arrival window of the served stream")
     ap.add_argument("--serve-rate", type=float, default=20.0, help="mean request arrivals per second")
     ap.add_argument("--tiles", default="auto", help="super-tile side: 'auto' (autotuned per mesh size) or 4/8/16")
-    ap.add_argument("--fft", choices=["cufft", "native"], default="cufft",
+    ap.add_argument("--fft", choices=["cufft", "native"], default="native",
                     help="256^3 transforms: cuFFT, or the native kernels with the Green multiply fused")
     return ap.parse_args()
 

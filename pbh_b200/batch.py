@@ -19,7 +19,7 @@ from .ic import recipe_particles
 
 class Ensemble:
     def __init__(self, specs, device: int = 0, graph: bool = True, bucket_sort: bool = True, tiles=None,
-                 delta_collapse: float = 0.0, native_fft: bool = False):
+                 delta_collapse: float = 0.0, native_fft: bool = True):
         self.specs = list(specs)
         if tiles == "auto":                      # per mesh size, timed on this GPU (pbh_b200.tune)
             from .tune import autotune

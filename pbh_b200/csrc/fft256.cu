@@ -295,9 +295,17 @@ __global__ void __launch_bounds__(XT, 1024 / XT) k_fft_xy(const float2* in, floa
 #pragma unroll
   for (int n1 = 0; n1 < 16; ++n1) v[n1] = plane[(long long)x * FN + 16 * n1 + t];
   if (GREEN) {
-    double w = 0.0;  // potential-energy partial (component 0)
+    // The multiply in a rolled loop over this thread's slots of its row in shared memory (one
+    // copy of its code keeps the kernel within the instruction cache); no other thread touches
+    // these slots before the barrier below.
+    float2* own = buf + r * FN + t;
 #pragma unroll
-    for (int n1 = 0; n1 < 16; ++n1) v[n1] = green_mode(v[n1], x, 16 * n1 + t, kz, comp, gp, plane, w);
+    for (int n1 = 0; n1 < 16; ++n1) own[16 * n1] = v[n1];
+    double w = 0.0;  // potential-energy partial (component 0)
+#pragma unroll 1
+    for (int n1 = 0; n1 < 16; ++n1) own[16 * n1] = green_mode(own[16 * n1], x, 16 * n1 + t, kz, comp, gp, plane, w);
+#pragma unroll
+    for (int n1 = 0; n1 < 16; ++n1) v[n1] = own[16 * n1];
     if (comp == 0) {
       for (int d = 16; d > 0; d >>= 1) w += __shfl_down_sync(0xffffffffu, w, d);
       if ((threadIdx.x & 31) == 0)
