@@ -30,6 +30,7 @@
 #include <cooperative_groups.h>
 
 #include <cmath>
+#include <cstdint>
 
 #include "pm_kernels.cuh"
 
@@ -294,6 +295,7 @@ __global__ void __launch_bounds__(XT, 1024 / XT) k_fft_xy(const float2* in, floa
   float2 v[16], u[16];
 #pragma unroll
   for (int n1 = 0; n1 < 16; ++n1) v[n1] = plane[(long long)x * FN + 16 * n1 + t];
+  double w = 0.0;  // potential-energy partial (component 0 of the Green pass), stored at the end
   if (GREEN) {
     // The multiply in a rolled loop over this thread's slots of its row in shared memory (one
     // copy of its code keeps the kernel within the instruction cache); no other thread touches
@@ -301,16 +303,12 @@ __global__ void __launch_bounds__(XT, 1024 / XT) k_fft_xy(const float2* in, floa
     float2* own = buf + r * FN + t;
 #pragma unroll
     for (int n1 = 0; n1 < 16; ++n1) own[16 * n1] = v[n1];
-    double w = 0.0;  // potential-energy partial (component 0)
 #pragma unroll 1
     for (int n1 = 0; n1 < 16; ++n1) own[16 * n1] = green_mode(own[16 * n1], x, 16 * n1 + t, kz, comp, gp, plane, w);
 #pragma unroll
     for (int n1 = 0; n1 < 16; ++n1) v[n1] = own[16 * n1];
-    if (comp == 0) {
+    if (comp == 0)
       for (int d = 16; d > 0; d >>= 1) w += __shfl_down_sync(0xffffffffu, w, d);
-      if ((threadIdx.x & 31) == 0)
-        A.wpart[A.peaks[pk].mode_base * (PM_THREADS / 32) + ((long long)kz * XC + c) * (XT / 32) + (threadIdx.x >> 5)] = w;
-    }
   }
   __syncthreads();  // table
   float2* row = buf + r * FN;
@@ -350,6 +348,8 @@ __global__ void __launch_bounds__(XT, 1024 / XT) k_fft_xy(const float2* in, floa
   float2* dst = out + ((long long)(slot * ncomp + comp) * FNH + kz) * N2 + ky;
 #pragma unroll
   for (int p = 0; p < 16; ++p) dst[(long long)(tx + 16 * brev(p, 4)) * FN] = u[p];
+  if (GREEN && comp == 0 && (threadIdx.x & 31) == 0)
+    A.wpart[A.peaks[pk].mode_base * (PM_THREADS / 32) + ((long long)kz * XC + c) * (XT / 32) + (threadIdx.x >> 5)] = w;
 }
 
 constexpr size_t kXYSmem = sizeof(float2) * (FN + XR * FN);
@@ -445,12 +445,14 @@ int ensure_fft256_init() {
 
 extern "C" int pm_rfft3_256(const float* x, void* spec, int nfields, void* stream) {
   if (!x || !spec || nfields < 0) return -2000;
+  if (((uintptr_t)x | (uintptr_t)spec) & 7) return -2001;  // float2 accesses
   if (int r = ensure_fft256_init()) return r;
   return fft256_r2c(x, (float2*)spec, nfields, (cudaStream_t)stream);
 }
 
 extern "C" int pm_irfft3_256(const void* spec, void* work, float* x, int nfields, void* stream) {
   if (!spec || !work || !x || nfields < 0) return -2000;
+  if (((uintptr_t)x | (uintptr_t)spec | (uintptr_t)work) & 7) return -2001;
   if (int r = ensure_fft256_init()) return r;
   return fft256_c2r((const float2*)spec, (float2*)work, x, nfields, (cudaStream_t)stream);
 }
