@@ -67,3 +67,29 @@ def test_engine_native_transform_matches_cufft_step():
     assert float((b["pos"] - a["pos"]).abs().max()) * N < 1e-5   # in cells
     assert b["st"].potential == pytest.approx(a["st"].potential, rel=1e-5)
     assert b["st"].status == 0
+
+
+def test_native_transform_in_a_mixed_served_engine():
+    """Served (dynamic) mode with meshes of two sizes and an idle 256^3 slot below an occupied
+    one: the native transform's slot mapping and Green partials against cuFFT's."""
+    import torch
+    from pbh_b200 import recipe
+    from pbh_b200.engine import Engine, PeakConfig
+    from pbh_b200.ic import recipe_particles
+    cfgs = [PeakConfig(N=32, Np=32, L=1.0), PeakConfig(N=N, Np=N, L=1.0), PeakConfig(N=N, Np=N, L=1.0)]
+    loads = {0: recipe.single_peak(N=32, steps=20, seed=5), 2: recipe.single_peak(N=N, steps=20, seed=6)}
+    res = []
+    for native in (False, True):
+        eng = Engine(cfgs, graph=False, dynamic=True, native_fft=native)
+        for i, spec in loads.items():
+            x, p = recipe_particles(spec, device=0, device_noise=True)
+            eng.set_particles(i, x, p, 1.0, mode=0, param=spec.ratio(), max_steps=20)
+            del x, p
+        eng.run(1)
+        res.append({i: (eng.acc(i, 1.0).double(), eng.stats(i)) for i in loads})
+        eng.close()
+    for i in loads:
+        (a_cu, s_cu), (a_na, s_na) = res[0][i], res[1][i]
+        assert _rel(a_na, a_cu) < 1e-5
+        assert s_na.potential == pytest.approx(s_cu.potential, rel=1e-5)
+        assert s_na.status == 0
