@@ -171,7 +171,7 @@ def run_reference(args):
 
 
 # ------------------------------------------------------------------------------ GPU side
-# Algorithmic bytes per launch of each kernel phase (see DESIGN.md): n particles, N^3 cells,
+# Algorithmic bytes per launch of each kernel phase: n particles, N^3 cells,
 # M modes; fc/hc: face and halo partials.
 def algorithmic_bytes(phase: str, n: int, cells: int, modes: int, npass: int) -> float:
     if phase == "push":        # read state 32, write state 32, force grids 12 per cell
