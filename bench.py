@@ -239,10 +239,10 @@ def run_ours(args):
         tiles = {s.N: min(int(args.tiles), s.N) for s in specs}
     ens = Ensemble(specs, device=local, bucket_sort=not args.full_sort, tiles=tiles, native_fft=args.fft == "native")
     # Our launches per timed step: push, energy, advance, 3 re-bin, super-tile sort, deposit,
-    # fix-up, Green (10); the native 256^3 transform adds 4 (2 passes each way) and drops the
+    # fix-up, Green (10); the native 256^3 transform adds 6 (3 passes each way) and drops the
     # Green launch when every mesh is 256^3.  The radix sort runs only when a peak is primed.
     has256 = args.fft == "native" and any(s.N == 256 for s in specs)
-    native_launches = (4 - (1 if all(s.N == 256 for s in specs) else 0)) if has256 else 0
+    native_launches = (6 - (1 if all(s.N == 256 for s in specs) else 0)) if has256 else 0
     lib = _lib.load()
     info = (np.zeros(6, dtype=np.int64))
     lib.pm_engine_info(ens.engine._h, info.ctypes.data)

@@ -1,5 +1,5 @@
-// Native 3D real FFT for the 256^3 mesh (sm_100a), two passes over HBM per direction, with the
-// Green's-function gradient (pm3d.py:105-112) fused into the inverse.
+// Native 3D real FFT for the 256^3 mesh (sm_100a), with the Green's-function gradient
+// (pm3d.py:105-112) fused into the inverse.
 //
 // Layouts (one field; fields of a batch are consecutive):
 //   real field      r[x][y][z]          256^3 float (the deposit's delta, the force grids)
@@ -12,33 +12,27 @@
 // W_L^{t k1}; one shared-memory exchange hands every thread the T values of its k1 for the
 // T-point DFTs of the second factor; output k = k1 + 16 k2.  Register DFTs are radix-2
 // decimation in frequency, so their outputs sit in bit-reversed register order (compile-time).
-// Exchange layouts are XOR-swizzled so that both the write and the read side of every exchange
-// hit distinct shared-memory banks within each half-warp.
+// Exchange layouts are laid out (XOR-swizzled where needed) so that both the write and the
+// read side of every exchange hit distinct shared-memory banks within each half-warp.
 //
-// Forward (R2C).  Pass Z: a real FFT along z of 32 (x, y) lines per CTA -- a complex 128-point
-// FFT of the packed (even, odd) pairs, then the split into 129 outputs -- written transposed into
-// the kz planes.  Pass XY: a 2D complex FFT of every kz plane by a cluster of XC CTAs: each
-// CTA transforms 256/XC rows along y, the cluster transposes through distributed shared
-// memory, and each CTA transforms 256/XC columns along x and writes them.
-// Inverse (C2R).  Pass XY with the Green multiply on load (-i k_i G(k) delta_k / N^3, the
-// Hermitian projection of the kz = 0, N/2 planes, the potential-energy partials), one cluster
-// per plane and gradient component (the three components of a plane adjacent in the grid, so
-// the spectrum is read from HBM once); pass Z, the real inverse along z, written as force rows.
+// Forward (R2C), three passes over HBM.  Pass Z: a real FFT along z of 32 (x, y) lines per CTA
+// -- a complex 128-point FFT of the packed (even, odd) pairs, then the split into 129 outputs --
+// written transposed into the kz planes.  Pass Y: 16 rows of a kz plane per CTA, in place.
+// Pass X: 16 columns of a kz plane per CTA (128-byte row segments), in place.  Every pass is
+// 256 threads and 34-38 KB of shared memory, 4 CTAs per SM, with no inter-CTA communication.
+// Inverse (C2R).  Pass Y with the Green multiply on load (-i k_i G(k) delta_k / N^3, the
+// Hermitian projection of the kz = 0, N/2 planes, the potential-energy partials), one CTA per
+// row block and gradient component (the three components of a row block adjacent in the grid,
+// so the spectrum is read from HBM once); pass X in place; pass Z, the real inverse along z,
+// written as force rows.
 // Twiddles come from a 256-entry table computed in double precision on the host; the register
 // DFTs use the exact constants cos(pi/8), cos(pi/4), cos(3 pi/8).
 // Transforms are unnormalised like cuFFT's; the Green factor carries numpy's 1/N^3.
-#include <cooperative_groups.h>
-
 #include <cmath>
 #include <cstdint>
 
 #include "pm_kernels.cuh"
 
-namespace cg = cooperative_groups;
-
-#ifndef PM_FFT_XC
-#define PM_FFT_XC 8  // CTAs per plane cluster (4 or 8)
-#endif
 
 namespace {
 
@@ -49,12 +43,8 @@ constexpr int ZL = 32;             // z lines per CTA in the Z passes
 constexpr int ZTH = ZL * 8;        // threads of a Z-pass CTA (8 per line)
 constexpr int ZX = FM + 8;         // row stride (float2) of a z line in shared memory, = 8 mod 16
 constexpr int ZC = ZL + 2;         // stride of the kz-major input tile of the inverse, = 2 mod 16
-constexpr int XC = PM_FFT_XC;      // CTAs per plane cluster
-constexpr int XR = FN / XC;        // plane rows (and columns) per CTA
-constexpr int XT = 16 * XR;        // threads of a plane CTA (16 per row)
 constexpr long long N2 = (long long)FN * FN;
 constexpr long long N3 = N2 * FN;
-static_assert(XC == 4 || XC == 8 || XC == 16, "cluster size");
 
 __device__ float2 g_tw[FN];        // exp(-2 pi i k / 256) of this device
 
@@ -256,32 +246,31 @@ __device__ __forceinline__ float2 green_mode(float2 v, int x, int y, int kz, int
   return o;
 }
 
-// Pass XY: 2D FFT of every kz plane by a cluster of XC CTAs.  CTA c transforms the rows
-// x = XR c + r along y, the cluster transposes through distributed shared memory (CTA m takes
-// the columns ky = XR m + j of all 256 rows, each value crossing between SMs once), and CTA m
-// transforms its columns along x and writes them.  Forward: in = out = planes[slot][kz][x][y]
-// (in place: every load precedes the first cluster barrier).  Inverse with GREEN: in =
-// spectrum planes[slot][kz][kx][ky], out = planes[slot][comp][kz][x][y], the multiply applied
-// on load; slot_peak maps a slot to its peak.  Inverse without GREEN: in = out layout
-// [f][kz][.][.].  grid (XC * nslots * FNH * ncomp): cluster index (slot * FNH + kz) * ncomp + comp.
+constexpr int RB = 16;        // lines per CTA of the plane passes
+constexpr int RT = RB * 16;   // threads (16 per line)
+
+// Pass Y: rows x = RB rb + r of one kz plane, 16 threads per row.  Forward: in = out =
+// planes[slot][kz][x][y] (in place: a CTA reads its rows before it writes them).  Inverse with
+// GREEN: in = spectrum planes[slot][kz][kx][ky], out = planes[slot][comp][kz][kx][y], the
+// multiply applied on load; slot_peak maps a slot to its peak.  Inverse without GREEN: in and
+// out [f][kz][.][.].  grid (FN/RB * nslots * FNH * ncomp), block index
+// ((slot * FNH + kz) * (FN/RB) + rb) * ncomp + comp (the components of a row block adjacent).
 template <bool INV, bool GREEN>
-__global__ void __launch_bounds__(XT, 1024 / XT) k_fft_xy(const float2* in, float2* out, StepArgs A,
-                                                                 const int* slot_peak, int ncomp) {
-  extern __shared__ __align__(16) float2 xs[];
-  float2* ty = xs;             // [16 * 16]  W_256^{t k1} at k1 * 16 + t (conjugated for the inverse)
-  float2* buf = ty + FN;       // [XR][FN]: the y-transformed rows, then the x exchange
-  for (int i = threadIdx.x; i < FN; i += XT) {
+__global__ void __launch_bounds__(RT, 4) k_fft_rows(const float2* in, float2* out, StepArgs A, const int* slot_peak,
+                                                     int ncomp) {
+  __shared__ float2 ty[FN];
+  __shared__ __align__(16) float2 buf[RB * FN];
+  for (int i = threadIdx.x; i < FN; i += RT) {
     const float2 b = g_tw[((i >> 4) * (i & 15)) & (FN - 1)];
     ty[i] = INV ? cconj(b) : b;
   }
-  cg::cluster_group cluster = cg::this_cluster();
-  const int c = (int)cluster.block_rank();
-  const int cl = blockIdx.x / XC, comp = cl % ncomp, pl = cl / ncomp, slot = pl / FNH, kz = pl - slot * FNH;
+  const int bi = blockIdx.x, comp = bi % ncomp, q = bi / ncomp, rb = q % (FN / RB), pl = q / (FN / RB);
+  const int slot = pl / FNH, kz = pl - slot * FNH;
   GreenPlane gp{};
   int pk = 0;
   if (GREEN) {
     pk = slot_peak[slot];
-    if (!A.clocks[pk].has_delta) return;  // uniform over the cluster: nobody reaches a barrier
+    if (!A.clocks[pk].has_delta) return;
     const PeakDesc& P = A.peaks[pk];
     gp.s_c = (float)(-1.5 * PM_H_I * PM_H_I / A.clocks[pk].a_grid / (double)N3);
     gp.kf = (float)(2.0 * M_PI / P.L);
@@ -289,18 +278,15 @@ __global__ void __launch_bounds__(XT, 1024 / XT) k_fft_xy(const float2* in, floa
     gp.sd2 = P.smooth > 0 ? (float)(P.smooth * P.dx) * (float)(P.smooth * P.dx) : 0.f;
     gp.gm = P.gradient;
   }
-  // Along y: row r (x = XR c + r) by 16 threads, thread t holding y = 16 n1 + t.
-  const int t = threadIdx.x & 15, r = threadIdx.x >> 4, x = XR * c + r;
+  const int t = threadIdx.x & 15, r = threadIdx.x >> 4, x = RB * rb + r;
   const float2* plane = in + (long long)pl * N2;
   float2 v[16], u[16];
 #pragma unroll
   for (int n1 = 0; n1 < 16; ++n1) v[n1] = plane[(long long)x * FN + 16 * n1 + t];
-  double w = 0.0;  // potential-energy partial (component 0 of the Green pass), stored at the end
+  float2* row = buf + r * FN;
+  double w = 0.0;
   if (GREEN) {
-    // The multiply in a rolled loop over this thread's slots of its row in shared memory (one
-    // copy of its code keeps the kernel within the instruction cache); no other thread touches
-    // these slots before the barrier below.
-    float2* own = buf + r * FN + t;
+    float2* own = row + t;
 #pragma unroll
     for (int n1 = 0; n1 < 16; ++n1) own[16 * n1] = v[n1];
 #pragma unroll 1
@@ -310,8 +296,7 @@ __global__ void __launch_bounds__(XT, 1024 / XT) k_fft_xy(const float2* in, floa
     if (comp == 0)
       for (int d = 16; d > 0; d >>= 1) w += __shfl_down_sync(0xffffffffu, w, d);
   }
-  __syncthreads();  // table
-  float2* row = buf + r * FN;
+  __syncthreads();
   dft_reg<INV, 16, 0, 16>(v);
 #pragma unroll
   for (int p = 0; p < 16; ++p) {
@@ -321,64 +306,48 @@ __global__ void __launch_bounds__(XT, 1024 / XT) k_fft_xy(const float2* in, floa
   __syncthreads();
 #pragma unroll
   for (int j = 0; j < 16; ++j) u[j] = row[t * 16 + (j ^ t)];
-  dft_reg<INV, 16, 0, 16>(u);  // u[p] = row spectrum at ky = t + 16 brev(p)
-  __syncthreads();
+  dft_reg<INV, 16, 0, 16>(u);
+  float2* dst = out + ((long long)(slot * ncomp + comp) * FNH + kz) * N2 + (long long)x * FN;
 #pragma unroll
-  for (int p = 0; p < 16; ++p) row[t + 16 * brev(p, 4)] = u[p];
-  cluster.sync();
-  // Along x: column ky = XR c + j by 16 threads, thread tx holding x = 16 n1 + tx, which is row
-  // (16 n1) % XR + tx of CTA (16 n1) / XR.
-  const int j = threadIdx.x % XR, tx = threadIdx.x / XR, ky = XR * c + j;
-#pragma unroll
-  for (int n1 = 0; n1 < 16; ++n1) {
-    const float2* src = cluster.map_shared_rank(buf, (16 * n1) / XR);
-    v[n1] = src[((16 * n1) % XR + tx) * FN + ky];
+  for (int p = 0; p < 16; ++p) dst[t + 16 * brev(p, 4)] = u[p];
+  if (GREEN && comp == 0 && (threadIdx.x & 31) == 0)
+    A.wpart[A.peaks[pk].mode_base * (PM_THREADS / 32) + ((long long)kz * (FN / RB) + rb) * (RT / 32) + (threadIdx.x >> 5)] = w;
+}
+
+// Pass X, in place: columns ky = RB cb + j of one kz plane, 16 threads per column (a warp reads
+// and writes 128-byte segments of two rows).  grid (FN/RB * nplanes).
+template <bool INV>
+__global__ void __launch_bounds__(RT, 4) k_fft_cols(float2* io) {
+  __shared__ float2 ty[FN];
+  __shared__ __align__(16) float2 buf[RB * FN];  // [k1][t][j]
+  for (int i = threadIdx.x; i < FN; i += RT) {
+    const float2 b = g_tw[((i >> 4) * (i & 15)) & (FN - 1)];
+    ty[i] = INV ? cconj(b) : b;
   }
-  cluster.sync();  // every CTA has read its columns: the buffers are free again
+  const int cb = blockIdx.x % (FN / RB), pl = blockIdx.x / (FN / RB);
+  const int j = threadIdx.x & 15, t = threadIdx.x >> 4, ky = RB * cb + j;
+  float2* plane = io + (long long)pl * N2 + ky;
+  float2 v[16], u[16];
+#pragma unroll
+  for (int n1 = 0; n1 < 16; ++n1) v[n1] = plane[(long long)(16 * n1 + t) * FN];
+  __syncthreads();
   dft_reg<INV, 16, 0, 16>(v);
 #pragma unroll
   for (int p = 0; p < 16; ++p) {
     const int k1 = brev(p, 4);
-    buf[(k1 * 16 + tx) * XR + j] = k1 ? cmul(v[p], ty[k1 * 16 + tx]) : v[p];
+    buf[(k1 * 16 + t) * RB + j] = k1 ? cmul(v[p], ty[k1 * 16 + t]) : v[p];
   }
   __syncthreads();
 #pragma unroll
-  for (int i = 0; i < 16; ++i) u[i] = buf[(tx * 16 + i) * XR + j];
-  dft_reg<INV, 16, 0, 16>(u);  // u[p] = column spectrum at kx = tx + 16 brev(p)
-  float2* dst = out + ((long long)(slot * ncomp + comp) * FNH + kz) * N2 + ky;
+  for (int i = 0; i < 16; ++i) u[i] = buf[(t * 16 + i) * RB + j];
+  dft_reg<INV, 16, 0, 16>(u);
 #pragma unroll
-  for (int p = 0; p < 16; ++p) dst[(long long)(tx + 16 * brev(p, 4)) * FN] = u[p];
-  if (GREEN && comp == 0 && (threadIdx.x & 31) == 0)
-    A.wpart[A.peaks[pk].mode_base * (PM_THREADS / 32) + ((long long)kz * XC + c) * (XT / 32) + (threadIdx.x >> 5)] = w;
-}
-
-constexpr size_t kXYSmem = sizeof(float2) * (FN + XR * FN);
-
-template <bool INV, bool GREEN>
-cudaError_t launch_xy(const float2* in, float2* out, const StepArgs& A, const int* slot_peak, int nslots, int ncomp,
-                      cudaStream_t s) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)XC * (unsigned)nslots * FNH * (unsigned)ncomp, 1, 1);
-  cfg.blockDim = dim3(XT, 1, 1);
-  cfg.dynamicSmemBytes = kXYSmem;
-  cfg.stream = s;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = XC;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  if (XC > 8) {
-    const cudaError_t e = cudaFuncSetAttribute(k_fft_xy<INV, GREEN>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-    if (e != cudaSuccess) return e;
-  }
-  return cudaLaunchKernelEx(&cfg, k_fft_xy<INV, GREEN>, in, out, A, slot_peak, ncomp);
+  for (int p = 0; p < 16; ++p) plane[(long long)(t + 16 * brev(p, 4)) * FN] = u[p];
 }
 
 }  // namespace
 
-// Per-device set-up: twiddle table and shared-memory limits.  Call with the device current.
+// Per-device set-up: the twiddle table.  Call with the device current.
 int fft256_init() {
   float2 h[FN];
   for (int k = 0; k < FN; ++k) {
@@ -386,12 +355,6 @@ int fft256_init() {
     h[k] = make_float2((float)cos(a), (float)sin(a));
   }
   cudaError_t e = cudaMemcpyToSymbol(g_tw, h, sizeof(h));
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_fft_xy<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kXYSmem);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_fft_xy<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kXYSmem);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_fft_xy<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kXYSmem);
   return e == cudaSuccess ? 0 : -(int)e;
 }
 
@@ -400,7 +363,11 @@ int fft256_r2c(const float* delta, float2* spec, int nslots, cudaStream_t s) {
   if (nslots <= 0) return 0;
   k_fft_z_r2c<<<dim3(FN / ZL, FN, nslots), ZTH, 0, s>>>(delta, spec);
   cudaError_t e = cudaGetLastError();
-  if (e == cudaSuccess) e = launch_xy<false, false>(spec, spec, StepArgs{}, nullptr, nslots, 1, s);
+  if (e == cudaSuccess) {
+    k_fft_rows<false, false><<<(unsigned)((FN / RB) * nslots * FNH), RT, 0, s>>>(spec, spec, StepArgs{}, nullptr, 1);
+    k_fft_cols<false><<<(unsigned)((FN / RB) * nslots * FNH), RT, 0, s>>>(spec);
+    e = cudaGetLastError();
+  }
   return e == cudaSuccess ? 0 : -(int)e;
 }
 
@@ -409,7 +376,9 @@ int fft256_r2c(const float* delta, float2* spec, int nslots, cudaStream_t s) {
 int fft256_green_c2r(const float2* spec, float2* gwork, float* force, const StepArgs& A, const int* slot_peak,
                      int nslots, cudaStream_t s) {
   if (nslots <= 0) return 0;
-  cudaError_t e = launch_xy<true, true>(spec, gwork, A, slot_peak, nslots, 3, s);
+  k_fft_rows<true, true><<<(unsigned)((FN / RB) * nslots * FNH * 3), RT, 0, s>>>(spec, gwork, A, slot_peak, 3);
+  k_fft_cols<true><<<(unsigned)((FN / RB) * nslots * FNH * 3), RT, 0, s>>>(gwork);
+  cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) {
     k_fft_z_c2r<<<dim3(FN / ZL, FN, 3 * nslots), ZTH, 0, s>>>(gwork, force);
     e = cudaGetLastError();
@@ -420,7 +389,9 @@ int fft256_green_c2r(const float2* spec, float2* gwork, float* force, const Step
 // Plain unnormalised inverse: spectra [f][kz][kx][ky] -> fields [f][x][y][z]; gwork as spec.
 int fft256_c2r(const float2* spec, float2* gwork, float* out, int nfields, cudaStream_t s) {
   if (nfields <= 0) return 0;
-  cudaError_t e = launch_xy<true, false>(spec, gwork, StepArgs{}, nullptr, nfields, 1, s);
+  k_fft_rows<true, false><<<(unsigned)((FN / RB) * nfields * FNH), RT, 0, s>>>(spec, gwork, StepArgs{}, nullptr, 1);
+  k_fft_cols<true><<<(unsigned)((FN / RB) * nfields * FNH), RT, 0, s>>>(gwork);
+  cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) {
     k_fft_z_c2r<<<dim3(FN / ZL, FN, nfields), ZTH, 0, s>>>(gwork, out);
     e = cudaGetLastError();
