@@ -190,8 +190,8 @@ int pm_analyse_partials(const double* x, int Np, double L, const double* A, cons
  * x: nfields fields [f][x][y][z] float.  spec: [f][kz][kx][ky] complex (kz = 0..128; numpy's
  * rfftn(x)[kx][ky][kz] is spec[kz][kx][ky]).  Both directions are unnormalised (the inverse is
  * 256^3 times numpy's irfftn).  work: caller scratch of the spectrum's size.  Device pointers,
- * 8-byte aligned (-2001 otherwise); asynchronous on `stream`; the first call on a device sets up
- * its twiddle table. */
+ * 16-byte aligned (-2001 otherwise); asynchronous on `stream`; the first call on a device sets
+ * up its twiddle table. */
 int pm_rfft3_256(const float* x, void* spec, int nfields, void* stream);
 int pm_irfft3_256(const void* spec, void* work, float* x, int nfields, void* stream);
 

@@ -97,8 +97,8 @@ __device__ __forceinline__ void dft_reg(float2 (&v)[NV]) {
   }
 }
 
-__device__ __forceinline__ void cpa8(void* dst, const void* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+__device__ __forceinline__ void cpa16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
                : "memory");
 }
 __device__ __forceinline__ void cpa_wait() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
@@ -181,9 +181,9 @@ __global__ void __launch_bounds__(ZTH, 4) k_fft_z_c2r(const float2* __restrict__
   static_assert(FNH * ZC >= ZL * ZX, "exchange rows fit in the tile");
   const int y0 = blockIdx.x * ZL, x = blockIdx.y, f = blockIdx.z;
   const float2* src = in + (long long)f * FNH * N2 + (long long)x * FN + y0;
-  for (int e = threadIdx.x; e < FNH * ZL; e += ZTH) {
-    const int k = e / ZL, ll = e - k * ZL;
-    cpa8(xb + k * ZC + ll, src + (long long)k * N2 + ll);
+  for (int e = threadIdx.x; e < FNH * ZL / 2; e += ZTH) {  // two complex values (16 bytes) per copy
+    const int k = e / (ZL / 2), ll = 2 * (e - k * (ZL / 2));
+    cpa16(xb + k * ZC + ll, src + (long long)k * N2 + ll);
   }
   load_ztw<true>(tw, t8);
   cpa_wait();
@@ -286,13 +286,32 @@ __global__ void __launch_bounds__(RT, 4) k_fft_rows(const float2* in, float2* ou
   float2* row = buf + r * FN;
   double w = 0.0;
   if (GREEN) {
-    float2* own = row + t;
+    if (kz != 0 && kz != FM && (gp.gm == 0 || comp != 1)) {
+      // Interior planes (no Hermitian partner, k != 0), with the gradient factor constant along
+      // the row (components x and z) or the spectral ky (component y): unrolled, in registers.
+      const float kx = kl(x, gp.kf), kzv = gp.kf * (float)kz, a = kx * kx + kzv * kzv;
+      const float gc = gk(comp == 0 ? kx : kzv, gp.dx, gp.gm);
 #pragma unroll
-    for (int n1 = 0; n1 < 16; ++n1) own[16 * n1] = v[n1];
+      for (int n1 = 0; n1 < 16; ++n1) {
+        const float ky = kl(16 * n1 + t, gp.kf), k2 = a + ky * ky;
+        float G = gp.s_c / k2;
+        if (gp.sd2 > 0.f) G *= expf(-0.5f * k2 * gp.sd2);
+        const float g = (comp == 1 ? ky : gc) * G;
+        const float2 d = v[n1];
+        if (comp == 0) w += (double)(2.0f * G * (d.x * d.x + d.y * d.y));
+        v[n1] = make_float2(g * d.y, -g * d.x);  // -i g d
+      }
+    } else {
+      // The general multiply in a rolled loop over this thread's slots of its row in shared
+      // memory (one copy of its code keeps the kernel within the instruction cache).
+      float2* own = row + t;
+#pragma unroll
+      for (int n1 = 0; n1 < 16; ++n1) own[16 * n1] = v[n1];
 #pragma unroll 1
-    for (int n1 = 0; n1 < 16; ++n1) own[16 * n1] = green_mode(own[16 * n1], x, 16 * n1 + t, kz, comp, gp, plane, w);
+      for (int n1 = 0; n1 < 16; ++n1) own[16 * n1] = green_mode(own[16 * n1], x, 16 * n1 + t, kz, comp, gp, plane, w);
 #pragma unroll
-    for (int n1 = 0; n1 < 16; ++n1) v[n1] = own[16 * n1];
+      for (int n1 = 0; n1 < 16; ++n1) v[n1] = own[16 * n1];
+    }
     if (comp == 0)
       for (int d = 16; d > 0; d >>= 1) w += __shfl_down_sync(0xffffffffu, w, d);
   }
@@ -416,14 +435,14 @@ int ensure_fft256_init() {
 
 extern "C" int pm_rfft3_256(const float* x, void* spec, int nfields, void* stream) {
   if (!x || !spec || nfields < 0) return -2000;
-  if (((uintptr_t)x | (uintptr_t)spec) & 7) return -2001;  // float2 accesses
+  if (((uintptr_t)x | (uintptr_t)spec) & 15) return -2001;  // 16-byte copies
   if (int r = ensure_fft256_init()) return r;
   return fft256_r2c(x, (float2*)spec, nfields, (cudaStream_t)stream);
 }
 
 extern "C" int pm_irfft3_256(const void* spec, void* work, float* x, int nfields, void* stream) {
   if (!spec || !work || !x || nfields < 0) return -2000;
-  if (((uintptr_t)x | (uintptr_t)spec | (uintptr_t)work) & 7) return -2001;
+  if (((uintptr_t)x | (uintptr_t)spec | (uintptr_t)work) & 15) return -2001;
   if (int r = ensure_fft256_init()) return r;
   return fft256_c2r((const float2*)spec, (float2*)work, x, nfields, (cudaStream_t)stream);
 }
