@@ -68,6 +68,10 @@ struct pm_engine {
   long long* d_st_base = nullptr;
   long long* d_p_base = nullptr;
   long long* d_mode_base = nullptr;
+  long long* d_green_base = nullptr;  // Green blocks of the peaks that k_green serves
+  int* d_green_peak = nullptr;
+  int ngreen = 0;
+  long long ngreenblk = 0;
   int4* pos = nullptr;   // state, grouped by super-tile
   float4* mom = nullptr;
   int4* tpos = nullptr;  // push output / loading area
@@ -104,6 +108,9 @@ struct pm_engine {
     A.st_base = d_st_base;
     A.p_base = d_p_base;
     A.mode_base = d_mode_base;
+    A.green_base = d_green_base;
+    A.green_peak = d_green_peak;
+    A.ngreen = ngreen;
     A.epart = epart;
     A.wpart = wpart;
     A.eslice = eslice;
@@ -204,9 +211,7 @@ struct pm_engine {
     CU(mark());
     if ((r = fft_r2c())) return r;
     CU(mark());
-    bool any_cufft = false;  // the native transform carries the Green multiply of its classes
-    for (const auto& c : classes) any_cufft = any_cufft || !c.native;
-    if (any_cufft) launch_green(A, nmodeblk, stream);
+    if (ngreenblk) launch_green(A, ngreenblk, stream);  // the native transform does its own
     CU(mark());
     if ((r = fft_c2r())) return r;
     CU(mark());
@@ -278,7 +283,8 @@ struct pm_engine {
       cudaFree(c.slot_peak);
     }
     sort_plan_destroy(&sort);
-    void* bufs[] = {d_peaks, d_clocks, d_stats, d_st_base, d_p_base, d_mode_base, epart, wpart, eslice, ecount, pos, mom, tpos,
+    void* bufs[] = {d_peaks, d_clocks, d_stats, d_st_base, d_p_base, d_mode_base, d_green_base, d_green_peak, epart,
+                    wpart, eslice, ecount, pos, mom, tpos,
                     tmom, keys[0], keys[1], vals[0], vals[1], sstart[0], sstart[1], counts, lpre, far_count,
                     far_fill, sort_gate, refresh_gate, totals, face, halo};
     for (void* b : bufs) cudaFree(b);
@@ -452,6 +458,21 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   if ((r = E->alloc(&E->d_st_base, npeaks + 1))) return r;
   if ((r = E->alloc(&E->d_p_base, npeaks + 1))) return r;
   if ((r = E->alloc(&E->d_mode_base, npeaks + 1))) return r;
+  // The Green kernel's grid covers only the peaks without the native transform.
+  std::vector<long long> green_base(1, 0);
+  std::vector<int> green_peak;
+  for (int i = 0; i < npeaks; ++i)
+    if (!E->peaks[i].native_fft) {
+      green_peak.push_back(i);
+      green_base.push_back(green_base.back() + (mode_base[i + 1] - mode_base[i]));
+    }
+  E->ngreen = (int)green_peak.size();
+  E->ngreenblk = green_base.back();
+  if ((r = E->alloc(&E->d_green_base, green_base.size()))) return r;
+  if ((r = E->alloc(&E->d_green_peak, green_peak.size()))) return r;
+  CU(cudaMemcpy(E->d_green_base, green_base.data(), sizeof(long long) * green_base.size(), cudaMemcpyHostToDevice));
+  if (E->ngreen)
+    CU(cudaMemcpy(E->d_green_peak, green_peak.data(), sizeof(int) * green_peak.size(), cudaMemcpyHostToDevice));
   if ((r = E->alloc(&E->pos, E->ntot))) return r;
   if ((r = E->alloc(&E->mom, E->ntot))) return r;
   if ((r = E->alloc(&E->tpos, E->ntot))) return r;

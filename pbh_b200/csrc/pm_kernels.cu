@@ -1128,15 +1128,21 @@ __device__ __forceinline__ double green_mode(const GreenCtx& g, long long m, flo
   return (double)(wk * G * (d.x * d.x + d.y * d.y));
 }
 
+// Grid: the Green blocks of the peaks in A.green_peak (those without the native transform).
 __global__ void __launch_bounds__(PM_THREADS) k_green(StepArgs A) {
   __shared__ int s_pk;
-  if (threadIdx.x == 0) s_pk = pm_find(A.mode_base, A.npeaks, (long long)blockIdx.x);
+  __shared__ long long s_lb;
+  if (threadIdx.x == 0) {
+    const int gi = pm_find(A.green_base, A.ngreen, (long long)blockIdx.x);
+    s_pk = A.green_peak[gi];
+    s_lb = (long long)blockIdx.x - A.green_base[gi];
+  }
   __syncthreads();
   const int pk = s_pk;
+  const long long lb = s_lb;  // block within the peak
   const PeakClock& C = A.clocks[pk];
   if (!C.has_delta) return;
   const PeakDesc& P = A.peaks[pk];
-  if (P.native_fft) return;  // the native transform applies the Green multiply itself
   GreenCtx g;
   g.N = P.N;
   g.log2N = P.log2N;
@@ -1151,7 +1157,7 @@ __global__ void __launch_bounds__(PM_THREADS) k_green(StepArgs A) {
   g.s_c = (float)(-1.5 * PM_H_I * PM_H_I / C.a_grid / ((double)P.N * P.N * P.N));
   g.spec = P.spec;
   g.out = P.gspec;
-  const long long m0 = ((long long)blockIdx.x - A.mode_base[pk]) * (PM_THREADS * GREEN_MODES) + threadIdx.x;
+  const long long m0 = lb * (PM_THREADS * GREEN_MODES) + threadIdx.x;
   // All loads of the block's modes first (the stores below could alias them as far as the
   // compiler knows), then the arithmetic and the stores.
   float2 d[GREEN_MODES];
@@ -1169,7 +1175,7 @@ __global__ void __launch_bounds__(PM_THREADS) k_green(StepArgs A) {
   // Within a warp a plain FP64 tree (128 terms); one partial per warp, no block barrier; the
   // energy kernel merges the partials with the compensated sum.
   for (int dd = 16; dd > 0; dd >>= 1) w += __shfl_down_sync(0xffffffffu, w, dd);
-  if ((threadIdx.x & 31) == 0) A.wpart[(long long)blockIdx.x * (PM_THREADS / 32) + (threadIdx.x >> 5)] = w;
+  if ((threadIdx.x & 31) == 0) A.wpart[(P.mode_base + lb) * (PM_THREADS / 32) + (threadIdx.x >> 5)] = w;
 }
 
 __global__ void k_reset_peak(StepArgs A, int pk, double a0, int mode, double param, double a_end, int max_steps) {

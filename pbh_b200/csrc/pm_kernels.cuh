@@ -41,8 +41,10 @@ struct StepArgs {
   const long long* st_base;    // [npeaks + 1] prefix of super-tiles
   const long long* p_base;     // [npeaks + 1] prefix of particles
   const long long* mode_base;  // [npeaks + 1] prefix of Green blocks
+  const long long* green_base; // [ngreen + 1] prefix of Green blocks over the peaks k_green serves
+  const int* green_peak;       // [ngreen] those peaks (the others use the native transform)
   int npeaks;
-  int pad;
+  int ngreen;
   int4* pos;                   // state, grouped by super-tile
   float4* mom;
   int4* tpos;                  // push output (same order as the input), regrouped into pos/mom
