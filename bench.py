@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--serve-rate", type=float, default=20.0, help="mean request arrivals per second")
     ap.add_argument("--tiles", default="auto", help="super-tile side: 'auto' (autotuned per mesh size) or 4/8/16")
     ap.add_argument("--fft", choices=["cufft", "native"], default="native",
-                    help="256^3 transforms: cuFFT, or the native kernels with the Green multiply fused")
+                    help="256^3 and 512^3 transforms: cuFFT, or the native kernels with the Green multiply fused")
     return ap.parse_args()
 
 
@@ -188,6 +188,7 @@ def algorithmic_bytes(phase: str, n: int, cells: int, modes: int, npass: int) ->
 
 
 PHASES = ["push", "advance", "bin", "sort", "deposit", "r2c", "green", "c2r"]
+NATIVE_FFT_SIZES = (256, 512)     # meshes the native transform serves (the others use cuFFT)
 
 # DRAM bytes (read + write) per launch from one ncu capture of the plain 256^3 run
 # (profiles/kernels_plain256.md), per particle (per mode for Green), scaled to a launch by the
@@ -239,10 +240,12 @@ def run_ours(args):
         tiles = {s.N: min(int(args.tiles), s.N) for s in specs}
     ens = Ensemble(specs, device=local, bucket_sort=not args.full_sort, tiles=tiles, native_fft=args.fft == "native")
     # Our launches per timed step: push, energy, advance, 3 re-bin, super-tile sort, deposit,
-    # fix-up, Green (10); the native 256^3 transform adds 6 (3 passes each way) and drops the
-    # Green launch when every mesh is 256^3.  The radix sort runs only when a peak is primed.
-    has256 = args.fft == "native" and any(s.N == 256 for s in specs)
-    native_launches = (6 - (1 if all(s.N == 256 for s in specs) else 0)) if has256 else 0
+    # fix-up, Green (10); the native transform adds 6 per mesh size it serves (3 passes each way)
+    # and drops the Green launch when it serves every mesh.  The radix sort runs only when a peak
+    # is primed.
+    native = args.fft == "native"
+    n_native = len({s.N for s in specs if native and s.N in NATIVE_FFT_SIZES})
+    native_launches = 6 * n_native - (1 if n_native and all(s.N in NATIVE_FFT_SIZES for s in specs) else 0)
     lib = _lib.load()
     info = (np.zeros(6, dtype=np.int64))
     lib.pm_engine_info(ens.engine._h, info.ctypes.data)
@@ -276,7 +279,7 @@ def run_ours(args):
     ph = ens.timed_phases(16)                     # one sort step and fifteen re-binning steps
     cells = sum(s.N ** 3 for s in specs)
     # modes the Green kernel handles (the native 256^3 transform applies its own multiply)
-    modes = sum(s.N * s.N * (s.N // 2 + 1) for s in specs if not (args.fft == "native" and s.N == 256))
+    modes = sum(s.N * s.N * (s.N // 2 + 1) for s in specs if not (args.fft == "native" and s.N in NATIVE_FFT_SIZES))
     kern = {}
     for k, name in enumerate(PHASES):
         b = algorithmic_bytes(name, n_step, cells, modes, npass)
@@ -313,7 +316,7 @@ def run_ours(args):
                            regroup="Morton radix sort every step" if args.full_sort else
                            "re-binning each step, Morton radix sort every 16th", parallelism=f"replicas x{world}",
                            super_tiles={str(k): v for k, v in sorted(tiles.items())},
-                           fft_256="native (Green fused into the inverse)" if args.fft == "native" else "cuFFT"),
+                           fft_256_512="native (Green fused into the inverse)" if args.fft == "native" else "cuFFT"),
             "clocks": clocks, "gpu_launches": args.steps * (10 + native_launches), "roofline": roofline}
 
     if rank == 0 and not args.no_plain and args.workload == "batched":

@@ -44,7 +44,7 @@ struct MeshClass {
   // Dynamic mode: plans for every batch size 1..B over the leading slots, one shared work area.
   std::vector<cufftHandle> r2c_b, c2r_b;
   void* work = nullptr;
-  // The native 256^3 transform (fft256.cu) instead of cuFFT, Green multiply fused into it.
+  // The native transform (native_fft.cu) instead of cuFFT, Green multiply fused into it.
   bool native = false;
   int* slot_peak = nullptr;  // device: peak index of each slot
 };
@@ -157,7 +157,7 @@ struct pm_engine {
     for (auto& c : classes) {
       if (c.native) {
         const int x = (flags & 4) ? extent(c) : (int)c.peaks.size();
-        if (int r = fft256_r2c(c.delta, c.spec, x, stream)) return r;
+        if (int r = fft_native_r2c(c.N, c.delta, c.spec, x, stream)) return r;
       } else if (flags & 4) {
         const int x = extent(c);
         if (x) CF(cufftExecR2C(c.r2c_b[x - 1], c.delta, (cufftComplex*)c.spec));
@@ -172,7 +172,7 @@ struct pm_engine {
     for (auto& c : classes) {
       if (c.native) {
         const int x = (flags & 4) ? extent(c) : (int)c.peaks.size();
-        if (int r = fft256_green_c2r(c.spec, c.gspec, c.force, A, c.slot_peak, x, stream)) return r;
+        if (int r = fft_native_green_c2r(c.N, c.spec, c.gspec, c.force, A, c.slot_peak, x, stream)) return r;
       } else if (flags & 4) {
         const int x = extent(c);
         if (x) CF(cufftExecC2R(c.c2r_b[x - 1], (cufftComplex*)c.gspec, c.force));
@@ -408,12 +408,12 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
       P.force = mc.force + 3 * k * N3;
     }
     int n[3] = {(int)N, (int)N, (int)N};
-    if ((E->flags & 8) && N == 256) {
+    if ((E->flags & 8) && fft_native_size((int)N)) {
       mc.native = true;
       if ((r = E->alloc(&mc.slot_peak, (size_t)B))) return r;
       CU(cudaMemcpy(mc.slot_peak, mc.peaks.data(), sizeof(int) * B, cudaMemcpyHostToDevice));
       for (int k = 0; k < B; ++k) E->peaks[mc.peaks[k]].native_fft = 1;
-      if ((r = fft256_init())) return r;
+      if ((r = fft_native_init())) return r;
     } else if (E->flags & 4) {
       // Dynamic mode: a plan per batch size, all sharing the largest work area, so a step
       // transforms only the slots up to the highest one in use.

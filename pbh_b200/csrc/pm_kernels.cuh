@@ -92,12 +92,14 @@ void launch_deposit(const StepArgs& A, long long nst, size_t smem, double* rho64
 void launch_fixup(const StepArgs& A, long long nst, double* rho64, cudaStream_t s);
 void launch_green(const StepArgs& A, long long nblocks, cudaStream_t s);
 
-// Native 256^3 real FFT (fft256.cu).  fft256_init: once per device before use.
-int fft256_init();
-int fft256_r2c(const float* delta, float2* spec, int nslots, cudaStream_t s);
-int fft256_green_c2r(const float2* spec, float2* gwork, float* force, const StepArgs& A, const int* slot_peak,
-                     int nslots, cudaStream_t s);
-int fft256_c2r(const float2* spec, float2* gwork, float* out, int nfields, cudaStream_t s);
+// Native real FFT of 256^3 and 512^3 meshes (native_fft.cu).  fft_native_init: once per device
+// before use.
+bool fft_native_size(int N);
+int fft_native_init();
+int fft_native_r2c(int N, const float* delta, float2* spec, int nslots, cudaStream_t s);
+int fft_native_green_c2r(int N, const float2* spec, float2* gwork, float* force, const StepArgs& A,
+                         const int* slot_peak, int nslots, cudaStream_t s);
+int fft_native_c2r(int N, const float2* spec, float2* gwork, float* out, int nfields, cudaStream_t s);
 
 // Host-requested per-peak operations.
 void launch_reset_peak(const StepArgs& A, int pk, double a0, int mode, double param, double a_end,

@@ -1,6 +1,6 @@
-"""The native 256^3 real FFT (pm_rfft3_256 / pm_irfft3_256) against torch's cuFFT in float64,
-and the engine's native-transform step (Green multiply fused into the inverse) against its
-cuFFT step on the same particles."""
+"""The native 256^3 and 512^3 real FFT (pm_rfft3_native / pm_irfft3_native) against torch's cuFFT
+in float64, and the engine's native-transform step (Green multiply fused into the inverse)
+against its cuFFT step on the same particles."""
 import numpy as np
 import pytest
 
@@ -12,35 +12,44 @@ def _rel(a, b):
     return float((a - b).abs().pow(2).sum().sqrt() / b.abs().pow(2).sum().sqrt())
 
 
-def test_forward_and_inverse_match_cufft():
+@pytest.mark.parametrize("n,nf", [(256, 2), (512, 1)])
+def test_forward_and_inverse_match_cufft(n, nf):
     import torch
     from pbh_b200 import _lib
     lib = _lib.load()
     g = torch.Generator(device="cuda").manual_seed(3)
-    x = torch.randn((2, N, N, N), device="cuda", generator=g, dtype=torch.float32)
-    spec = torch.empty((2, N // 2 + 1, N, N), dtype=torch.complex64, device="cuda")
+    x = torch.randn((nf, n, n, n), device="cuda", generator=g, dtype=torch.float32)
+    spec = torch.empty((nf, n // 2 + 1, n, n), dtype=torch.complex64, device="cuda")
     torch.cuda.synchronize()
-    _lib.check(lib.pm_rfft3_256(x.data_ptr(), spec.data_ptr(), 2, None), "pm_rfft3_256")
+    _lib.check(lib.pm_rfft3_native(n, x.data_ptr(), spec.data_ptr(), nf, None), "pm_rfft3_native")
     torch.cuda.synchronize()
-    ref = torch.fft.rfftn(x.double(), dim=(1, 2, 3)).permute(0, 3, 1, 2)      # [f][kz][kx][ky]
-    assert _rel(spec.to(torch.complex128), ref) < 2e-6
+    for f in range(nf):                                                     # [kz][kx][ky]
+        ref = torch.fft.rfftn(x[f].double()).permute(2, 0, 1)
+        assert _rel(spec[f].to(torch.complex128), ref) < 2e-6
+        del ref
     work = torch.empty_like(spec)
     back = torch.empty_like(x)
-    _lib.check(lib.pm_irfft3_256(spec.data_ptr(), work.data_ptr(), back.data_ptr(), 2, None), "pm_irfft3_256")
+    _lib.check(lib.pm_irfft3_native(n, spec.data_ptr(), work.data_ptr(), back.data_ptr(), nf, None), "pm_irfft3_native")
     torch.cuda.synchronize()
-    assert _rel(back.double() / N ** 3, x.double()) < 2e-6
+    assert _rel(back.double() / n ** 3, x.double()) < 2e-6
+    if n == N:
+        # the n = 256 forms give the same bits
+        spec2 = torch.empty_like(spec)
+        _lib.check(lib.pm_rfft3_256(x.data_ptr(), spec2.data_ptr(), nf, None), "pm_rfft3_256")
+        torch.cuda.synchronize()
+        assert torch.equal(spec2, spec)
     # an arbitrary (not Hermitian-consistent) spectrum: the inverse equals irfftn's (which uses
-    # the real parts of the kz = 0 and N/2 lines after the x-y inverse, like any C2R)
-    s2 = torch.randn((1, N // 2 + 1, N, N), dtype=torch.complex64, device="cuda", generator=g)
-    out = torch.empty((1, N, N, N), dtype=torch.float32, device="cuda")
-    _lib.check(lib.pm_irfft3_256(s2.data_ptr(), work.data_ptr(), out.data_ptr(), 1, None), "pm_irfft3_256")
+    # the real parts of the kz = 0 and n/2 lines after the x-y inverse, like any C2R)
+    s2 = torch.randn((1, n // 2 + 1, n, n), dtype=torch.complex64, device="cuda", generator=g)
+    out = torch.empty((1, n, n, n), dtype=torch.float32, device="cuda")
+    _lib.check(lib.pm_irfft3_native(n, s2.data_ptr(), work.data_ptr(), out.data_ptr(), 1, None), "pm_irfft3_native")
     torch.cuda.synchronize()
-    full = s2.to(torch.complex128).permute(0, 2, 3, 1)                      # [f][kx][ky][kz]
-    t = torch.fft.ifft(torch.fft.ifft(full, dim=1), dim=2) * (N * N)        # x-y inverse, unnormalised
+    full = s2[0].to(torch.complex128).permute(1, 2, 0)                      # [kx][ky][kz]
+    t = torch.fft.ifft(torch.fft.ifft(full, dim=0), dim=1) * (n * n)        # x-y inverse, unnormalised
     t[..., 0] = t[..., 0].real.to(torch.complex128)
-    t[..., N // 2] = t[..., N // 2].real.to(torch.complex128)
-    ref2 = torch.fft.irfft(t, n=N, dim=3) * N
-    assert _rel(out.double(), ref2) < 2e-6
+    t[..., n // 2] = t[..., n // 2].real.to(torch.complex128)
+    ref2 = torch.fft.irfft(t, n=n, dim=2) * n
+    assert _rel(out[0].double(), ref2) < 2e-6
 
 
 def test_engine_native_transform_matches_cufft_step():

@@ -65,3 +65,13 @@ def test_invariant_divisor_magic_numbers():
         n = n[(n >= 0) & (n < top)].astype(np.uint64)
         q = (((n * np.uint64(magic)) >> np.uint64(32)) + n) >> np.uint64(l)
         assert np.array_equal(q, n // np.uint64(d)), N
+
+
+def test_native_fft_rejects_other_sizes_before_touching_the_device():
+    """Only 256^3 and 512^3 have a native transform; other sizes are refused with the
+    invalid-argument code for the size, before any pointer is used or any CUDA call is made."""
+    from pbh_b200 import _lib
+    lib = _lib.load()
+    assert lib.pm_rfft3_native(128, 16, 16, 1, None) == -2000
+    assert lib.pm_irfft3_native(1024, 16, 16, 16, 1, None) == -2000
+    assert lib.pm_rfft3_native(300, 16, 16, 1, None) == -2000
