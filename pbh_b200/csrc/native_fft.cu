@@ -377,9 +377,9 @@ __global__ void __launch_bounds__(CTA, 4) k_fft_rows(const float2* in, float2* o
     A.wpart[A.peaks[pk].mode_base * (PM_THREADS / 32) + ((long long)kz * (N / B) + rb) * (CTA / 32) + (threadIdx.x >> 5)] = w;
 }
 
-// Pass X, in place: columns ky = B cb + j of one kz plane, T threads per column (consecutive
-// lanes hold consecutive columns, so a warp reads and writes 8 B segments of B columns of
-// 32/B rows).  grid (N/B * nplanes).
+// Pass X, in place: columns ky = B cb + j of one kz plane, T threads per column.  Consecutive
+// lanes hold consecutive columns, so each warp access covers 32/B rows, B columns (8 B bytes)
+// of each.  grid (N/B * nplanes).
 template <int N, bool INV>
 __global__ void __launch_bounds__(CTA, 4) k_fft_cols(float2* io) {
   using G = PGeo<N>;
