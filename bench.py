@@ -190,6 +190,15 @@ def algorithmic_bytes(phase: str, n: int, cells: int, modes: int, npass: int) ->
 PHASES = ["push", "advance", "bin", "sort", "deposit", "r2c", "green", "c2r"]
 NATIVE_FFT_SIZES = (256, 512)     # meshes the native transform serves (the others use cuFFT)
 
+
+def launches_per_step(sizes, fft: str) -> int:
+    """Our kernel launches in one steady (non-priming) step of an ensemble with these mesh sizes:
+    push, energy, advance, 3 re-bin, super-tile sort, deposit, fix-up and Green (10); the native
+    transform adds 6 per mesh size it serves (3 passes each way) and drops the Green launch when
+    it serves every mesh.  The radix sort runs only in steps that prime a peak."""
+    native = {n for n in sizes if fft == "native" and n in NATIVE_FFT_SIZES}
+    return 10 + 6 * len(native) - (1 if native and all(n in native for n in sizes) else 0)
+
 # DRAM bytes (read + write) per launch from one ncu capture of the plain 256^3 run
 # (profiles/kernels_plain256.md), per particle (per mode for Green), scaled to a launch by the
 # particles (modes) it processes.
@@ -239,13 +248,7 @@ def run_ours(args):
     else:
         tiles = {s.N: min(int(args.tiles), s.N) for s in specs}
     ens = Ensemble(specs, device=local, bucket_sort=not args.full_sort, tiles=tiles, native_fft=args.fft == "native")
-    # Our launches per timed step: push, energy, advance, 3 re-bin, super-tile sort, deposit,
-    # fix-up, Green (10); the native transform adds 6 per mesh size it serves (3 passes each way)
-    # and drops the Green launch when it serves every mesh.  The radix sort runs only when a peak
-    # is primed.
-    native = args.fft == "native"
-    n_native = len({s.N for s in specs if native and s.N in NATIVE_FFT_SIZES})
-    native_launches = 6 * n_native - (1 if n_native and all(s.N in NATIVE_FFT_SIZES for s in specs) else 0)
+
     lib = _lib.load()
     info = (np.zeros(6, dtype=np.int64))
     lib.pm_engine_info(ens.engine._h, info.ctypes.data)
@@ -317,7 +320,8 @@ def run_ours(args):
                            "re-binning each step, Morton radix sort every 16th", parallelism=f"replicas x{world}",
                            super_tiles={str(k): v for k, v in sorted(tiles.items())},
                            fft_256_512="native (Green fused into the inverse)" if args.fft == "native" else "cuFFT"),
-            "clocks": clocks, "gpu_launches": args.steps * (10 + native_launches), "roofline": roofline}
+            "clocks": clocks, "gpu_launches": args.steps * launches_per_step([sp.N for sp in specs], args.fft),
+            "roofline": roofline}
 
     if rank == 0 and not args.no_plain and args.workload == "batched":
         pr = plain_rate(specs, steps=8, warmup=3, device=local, tiles=tiles)

@@ -1,0 +1,117 @@
+"""Host-side logic that needs no GPU: the benchmark recipes, the served stream's arrivals,
+latency summary and slot budget, the benchmark's launch and byte accounting, and the error
+mapping of the C ABI's return codes."""
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+sys.path.insert(0, str(ROOT))
+
+
+def test_zeldovich_axes_and_implied_ep_invert_each_other():
+    from pbh_b200 import recipe
+    for e, p in [(0.0, 0.0), (0.2, 0.0), (0.3, 0.1), (0.1, -0.05)]:
+        A = recipe.zeldovich_axes(e, p)
+        assert np.prod(A) == pytest.approx(1.0, rel=1e-12)
+        lam = np.array([1 + 3 * e + p, 1 - 2 * p, 1 - 3 * e + p]) / 3.0     # pm3d.py:20-23
+        assert A == pytest.approx(lam ** -0.5 / np.prod(lam ** -0.5) ** (1 / 3), rel=1e-12)
+        e2, p2 = recipe.implied_ep(A)
+        assert (e2, p2) == pytest.approx((e, p), abs=1e-12)
+
+
+def test_step_ratio_spans_a_factor_100():
+    from pbh_b200 import recipe
+    for steps in (50, 100, 150, 300):
+        spec = recipe.single_peak(N=32, steps=steps)
+        assert (1.0 + spec.ratio()) ** steps == pytest.approx(100.0, rel=1e-12)
+
+
+def test_spherical_delta0_is_the_linear_threshold():
+    from pbh_b200 import recipe
+    # e = p = 0: the first axis collapses with the sphere, delta_lin(a_c) = 1.686
+    assert recipe.first_axis_ratio(0.0, 0.0) == pytest.approx(1.0)
+    for a_c in (0.3, 0.5, 0.8, 1.0):
+        d0 = recipe.delta0_for_collapse(a_c, 0.0, 0.0)
+        assert d0 * a_c / recipe.A_START_CFG == pytest.approx(recipe.DELTA_C, rel=1e-12)
+    # an ellipsoid's first axis collapses earlier, so it needs less initial overdensity
+    assert recipe.delta0_for_collapse(0.8, 0.3, 0.1) < recipe.delta0_for_collapse(0.8, 0.0, 0.0)
+
+
+def test_ensemble_is_seeded_and_within_its_ranges():
+    from pbh_b200 import recipe
+    a = recipe.ensemble(npeaks=64, seed=1234)
+    b = recipe.ensemble(npeaks=64, seed=1234)
+    assert [(s.N, s.e, s.p, s.delta0, s.seed) for s in a] == [(s.N, s.e, s.p, s.delta0, s.seed) for s in b]
+    assert {s.N for s in a} <= {32, 64, 128, 256}
+    assert all(0.0 <= s.e <= 0.3 and -0.1 <= s.p <= 0.1 and 0.3 <= s.a_collapse_cfg <= 1.0 for s in a)
+    assert [s.seed for s in a] == list(range(1234, 1234 + 64))
+    assert sum(s.n for s in a) >= 1e8
+
+
+def test_poisson_arrivals_are_seeded_and_ordered():
+    from pbh_b200.serve import poisson_arrivals
+    a = poisson_arrivals(rate=20.0, duration=10.0, seed=3)
+    b = poisson_arrivals(rate=20.0, duration=10.0, seed=3)
+    assert [(t, s.N, s.seed) for t, s in a] == [(t, s.N, s.seed) for t, s in b]
+    times = [t for t, _ in a]
+    assert times == sorted(times) and 0.0 < times[0] and times[-1] <= 10.0
+    assert 120 <= len(a) <= 280                      # 200 expected
+    assert {s.N for _, s in a} <= {64, 128, 256}
+    assert len(poisson_arrivals(rate=20.0, duration=10.0, seed=3, npeaks_max=5)) == 5
+
+
+def test_latency_summary():
+    from pbh_b200.serve import Request, latency_summary
+    done = []
+    for i, lat in enumerate(np.linspace(1.0, 2.0, 101)):
+        r = Request(rid=i, spec=None, t_arrival=10.0)
+        r.t_done = 10.0 + lat
+        done.append(r)
+    s = latency_summary(done)
+    assert s["completed"] == 101
+    assert s["p50_s"] == pytest.approx(1.5) and s["max_s"] == pytest.approx(2.0)
+    assert s["p99_s"] == pytest.approx(1.99)
+    assert latency_summary([]) == {"completed": 0}
+
+
+def test_served_slot_pool_fits_the_budget():
+    from pbh_b200.serve import slot_bytes
+    sizes = [slot_bytes(n) for n in (64, 128, 256)]
+    assert sizes == sorted(sizes)
+    assert slot_bytes(256) == pytest.approx(8 * slot_bytes(128), rel=0.01)   # per particle
+    pool = 32 * slot_bytes(64) + 32 * slot_bytes(128) + 24 * slot_bytes(256)  # the served benchmark's pool
+    assert pool <= 150e9
+
+
+def test_launch_accounting():
+    import bench
+    assert bench.launches_per_step([32, 64], "native") == 10          # cuFFT sizes only
+    assert bench.launches_per_step([256], "cufft") == 10
+    assert bench.launches_per_step([256], "native") == 15             # + 6, no Green launch
+    assert bench.launches_per_step([512], "native") == 15
+    assert bench.launches_per_step([32, 256, 256], "native") == 16    # Green still runs for 32^3
+    assert bench.launches_per_step([256, 512], "native") == 21
+
+
+def test_algorithmic_bytes_per_phase():
+    import bench
+    n, cells, modes = 1000, 1000, 600
+    assert bench.algorithmic_bytes("push", n, cells, modes, 3) == n * 64 + cells * 12
+    assert bench.algorithmic_bytes("bin", n, cells, modes, 3) == n * 64
+    assert bench.algorithmic_bytes("deposit", n, cells, modes, 3) == n * 16 + cells * 4
+    assert bench.algorithmic_bytes("green", n, cells, modes, 3) == modes * 32
+    assert bench.algorithmic_bytes("r2c", n, cells, modes, 3) == 0.0
+
+
+def test_return_code_mapping():
+    from pbh_b200 import _lib
+    assert _lib.check(0, "x") == 0 and _lib.check(3, "x") == 3        # >0: flagged items
+    with pytest.raises(_lib.PMError, match="CUDA error 2"):
+        _lib.check(-2, "x")
+    with pytest.raises(_lib.PMError, match="cuFFT error 5"):
+        _lib.check(-1005, "x")
+    with pytest.raises(_lib.PMError, match="invalid argument"):
+        _lib.check(-2003, "x")
