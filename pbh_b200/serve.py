@@ -44,12 +44,16 @@ class Request:
         return self.t_done - self.t_arrival
 
 
-def slot_bytes(N: int) -> int:
+NATIVE_FFT_SIZES = (256, 512)   # meshes the engine transforms natively (no cuFFT work area)
+
+
+def slot_bytes(N: int, native_fft: bool = True) -> int:
     """Device bytes one slot of mesh N holds in the engine (particles = cells)."""
     n = N ** 3
     per_particle = 2 * 16 + 2 * 16 + 2 * 4 + 2 * 4 + 4      # state x2, keys x2, values x2, bucket starts
     per_cell = 4 + 8 * (N // 2 + 1) / N * 4 + 12            # delta, 4 spectra, 3 force grids
-    fft_work = 4 * 12 * n                                   # shared cuFFT work area, per slot of the batch
+    native = native_fft and N in NATIVE_FFT_SIZES
+    fft_work = 0 if native else 4 * 12 * n                  # shared cuFFT work area, per slot of the batch
     return int(n * per_particle + n * per_cell + fft_work)
 
 
