@@ -61,3 +61,18 @@ def test_admission_waits_for_free_slots():
             assert b.t_admit >= a.t_done - 1e-9
     s = latency_summary(done)
     assert s["completed"] == 5 and s["p99_s"] >= s["p50_s"] > 0
+
+
+@pytest.mark.parametrize("sizes", [[64, 64, 64], [128, 128], [256]])
+def test_slot_footprint_matches_the_engine_allocation(sizes):
+    """The admission budget counts serve.slot_bytes per slot; the served engine's own device
+    allocation (dynamic mode, native transform where it applies) stays within 5 % of it."""
+    from pbh_b200.engine import Engine, PeakConfig
+    from pbh_b200.serve import slot_bytes
+    eng = Engine([PeakConfig(N=n, Np=n, L=1.0) for n in sizes], graph=False, dynamic=True)
+    try:
+        got = eng.device_bytes
+    finally:
+        eng.close()
+    est = sum(slot_bytes(n) for n in sizes)
+    assert 0.95 * est <= got <= 1.05 * est, (got, est)
