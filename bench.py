@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--serve-rate", type=float, default=20.0, help="mean request arrivals per second")
     ap.add_argument("--tiles", default="auto", help="super-tile side: 'auto' (autotuned per mesh size) or 4/8/16")
     ap.add_argument("--fft", choices=["cufft", "native"], default="native",
-                    help="256^3 and 512^3 transforms: cuFFT, or the native kernels with the Green multiply fused")
+                    help="64^3-512^3 transforms: cuFFT, or the native kernels with the Green multiply fused")
     return ap.parse_args()
 
 
@@ -188,7 +188,7 @@ def algorithmic_bytes(phase: str, n: int, cells: int, modes: int, npass: int) ->
 
 
 PHASES = ["push", "advance", "bin", "sort", "deposit", "r2c", "green", "c2r"]
-NATIVE_FFT_SIZES = (256, 512)     # meshes the native transform serves (the others use cuFFT)
+NATIVE_FFT_SIZES = (64, 128, 256, 512)   # meshes the native transform serves (the others use cuFFT)
 
 
 def launches_per_step(sizes, fft: str) -> int:
@@ -319,7 +319,7 @@ def run_ours(args):
                            regroup="Morton radix sort every step" if args.full_sort else
                            "re-binning each step, Morton radix sort every 16th", parallelism=f"replicas x{world}",
                            super_tiles={str(k): v for k, v in sorted(tiles.items())},
-                           fft_256_512="native (Green fused into the inverse)" if args.fft == "native" else "cuFFT"),
+                           fft_64_to_512="native (Green fused into the inverse)" if args.fft == "native" else "cuFFT"),
             "clocks": clocks, "gpu_launches": args.steps * launches_per_step([sp.N for sp in specs], args.fft),
             "roofline": roofline}
 

@@ -87,7 +87,7 @@ typedef struct {
  * graph; bit 2 = dynamic mode for served runs: no graph, and each step's FFTs cover only the
  * slots up to the highest one in use in each mesh size (slots are the peaks of one size, in
  * order); bit 3 = the native transform with the Green multiply fused (pm_rfft3_native) for
- * 256^3 and 512^3 meshes instead of cuFFT. */
+ * meshes 64^3-512^3 instead of cuFFT. */
 int pm_engine_create(const pm_peak_cfg* cfg, int npeaks, int device, int flags, pm_engine** out);
 int pm_engine_destroy(pm_engine* e);
 int pm_engine_sync(pm_engine* e);
@@ -185,7 +185,7 @@ int pm_sort_u64(const unsigned long long* keys, unsigned long long* keys_out, un
 int pm_rell_keys(int Np, double L, const double* A, unsigned long long* keys);
 int pm_analyse_partials(const double* x, int Np, double L, const double* A, const double* centre,
                         const double* set_radii, const double* radii, int nblocks, double* partials);
-/* Native 3D real FFT of n^3 fields, n = 256 or 512 (the transform the engine uses for those mesh
+/* Native 3D real FFT of n^3 fields, n = 64, 128, 256 or 512 (the transform the engine uses for those mesh
  * sizes; replaces np.fft.rfftn of pbhgr/pbhgr/pm3d.py:105 and np.fft.irfftn of pm3d.py:112).
  * x: nfields fields [f][x][y][z] float.  spec: [f][kz][kx][ky] complex (kz = 0..n/2; numpy's
  * rfftn(x)[kx][ky][kz] is spec[kz][kx][ky]).  Both directions are unnormalised (the inverse is

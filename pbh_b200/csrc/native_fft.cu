@@ -1,7 +1,7 @@
-// Native 3D real FFT for 256^3 and 512^3 meshes (sm_100a), with the Green's-function gradient
+// Native 3D real FFT for meshes of 64^3 to 512^3 (sm_100a), with the Green's-function gradient
 // (pm3d.py:105-112) fused into the inverse.
 //
-// Layouts (one field; fields of a batch are consecutive), N = 256 or 512:
+// Layouts (one field; fields of a batch are consecutive), N = 64, 128, 256 or 512:
 //   real field      r[x][y][z]          N^3 float (the deposit's delta, the force grids)
 //   spectrum        s[kz][kx][ky]       (N/2+1) x N x N complex ("plane-major")
 // numpy's rfftn(r)[kx][ky][kz] is s[kz][kx][ky]: the same transform, stored with kz outermost.
@@ -10,17 +10,19 @@
 // a line of length L = 16 T is owned by T threads, thread t holding the 16 elements
 // n = T n1 + t, n1 = 0..15.  Each thread runs a 16-point DFT over n1 in registers and scales by
 // W_L^{t k1}; one shared-memory exchange hands the threads the T values of each k1 for the
-// T-point DFTs of the second factor; output k = k1 + 16 k2.  For T = 8 a thread does two 8-point
-// DFTs, for T = 16 one 16-point DFT, for T = 32 a pair of threads shares each 32-point DFT (two
-// 16-point halves and a radix-2 step across the pair by warp shuffle).  Register DFTs are radix-2
+// T-point DFTs of the second factor; output k = k1 + 16 k2.  For T <= 16 a thread does 16/T
+// DFTs of T points; for T = 32 a pair of threads shares each 32-point DFT (two 16-point halves
+// and a radix-2 step across the pair by warp shuffle).  Register DFTs are radix-2
 // decimation in frequency, so their outputs sit in bit-reversed register order (compile-time).
-// Exchange layouts are XOR-swizzled so that both the write and the read side of every exchange
-// hit distinct shared-memory banks within each half-warp.
+// Exchange layouts are XOR-swizzled and rows padded so that both the write and the read side of
+// every exchange hit distinct shared-memory banks within each half-warp (for the 64^3 Z pass,
+// at most two-way).
 //
-// Forward (R2C), three passes over HBM.  Pass Z: a real FFT along z of 256/T (x, y) lines per CTA
-// (T = N/32) -- a complex FFT of the N/2 packed (even, odd) pairs, then the split into N/2+1
-// outputs -- written transposed into the kz planes.  Pass Y: 256/(N/16) rows of a kz plane per
-// CTA, in place.  Pass X: the same number of columns of a kz plane per CTA, in place.  Every
+// Forward (R2C), three passes over HBM.  Pass Z: a real FFT along z of 256/T consecutive (x, y)
+// lines per CTA (T = N/32) -- a complex FFT of the N/2 packed (even, odd) pairs, then the split
+// into N/2+1 outputs -- written transposed into the kz planes.  Pass Y: 256/(N/16) rows of a kz
+// plane per CTA, in place.  Pass X: the same number of columns of a kz plane per CTA, in place.
+// Every
 // kernel: 256 threads, at most 43 KB of static shared memory, 64 registers, 4 CTAs per SM, no
 // inter-CTA communication.
 // Inverse (C2R).  Pass Y with the Green multiply on load (-i k_i G(k) delta_k / N^3, the
@@ -99,19 +101,30 @@ __device__ __forceinline__ void dft_reg(float2 (&v)[NV]) {
   }
 }
 
-// Output element held in u[p] by thread t of a line of T threads after line_fft.
+template <int T>
+__host__ __device__ constexpr int log2i() { return T <= 1 ? 0 : 1 + log2i<T / 2>(); }
+
+// T-point DFTs of the 16 / T consecutive groups of u.
+template <bool INV, int T, int S = 0>
+__device__ __forceinline__ void dft_groups(float2 (&u)[16]) {
+  if constexpr (S < 16 / T) {
+    dft_reg<INV, T, T * S, 16>(u);
+    dft_groups<INV, T, S + 1>(u);
+  }
+}
+
+// Output element held in u[p] by thread t of a line of T threads after line_fft: for T <= 16
+// group s = p / T of the thread's 16 / T groups, element q = p % T of its T-point DFT.
 template <int T>
 __device__ __forceinline__ int line_k(int t, int p) {
-  if constexpr (T == 8) return t + 8 * (p >> 3) + 16 * brev(p & 7, 3);
-  else if constexpr (T == 16) return t + 16 * brev(p, 4);
+  if constexpr (T <= 16) return t + T * (p / T) + 16 * brev(p % T, log2i<T>());
   else return (t >> 1) + 16 * brev(p, 4) + 256 * (t & 1);
 }
 
 // Swizzled position of Y[k1][t] in a line's exchange row.
 template <int T>
 __device__ __forceinline__ int line_slot(int k1, int t) {
-  if constexpr (T == 8) return k1 * 8 + (t ^ (k1 & 7));
-  else if constexpr (T == 16) return k1 * 16 + (t ^ k1);
+  if constexpr (T <= 16) return k1 * T + (t ^ (k1 & (T - 1)));
   else return k1 * 32 + (t ^ (2 * k1));
 }
 
@@ -129,17 +142,13 @@ __device__ __forceinline__ void line_fft(float2 (&v)[16], float2 (&u)[16], float
     row[line_slot<T>(k1, t)] = k1 ? cmul(v[p], tl[k1 * T + t]) : v[p];
   }
   __syncthreads();
-  if constexpr (T == 8) {
+  if constexpr (T <= 16) {
+    // this thread's k1 = t + T s, s < 16 / T: one T-point DFT each
 #pragma unroll
-    for (int s = 0; s < 2; ++s)
+    for (int s = 0; s < 16 / T; ++s)
 #pragma unroll
-      for (int j = 0; j < 8; ++j) u[8 * s + j] = row[line_slot<8>(t + 8 * s, j)];
-    dft_reg<INV, 8, 0, 16>(u);
-    dft_reg<INV, 8, 8, 16>(u);
-  } else if constexpr (T == 16) {
-#pragma unroll
-    for (int j = 0; j < 16; ++j) u[j] = row[line_slot<16>(t, j)];
-    dft_reg<INV, 16, 0, 16>(u);
+      for (int j = 0; j < T; ++j) u[T * s + j] = row[line_slot<T>(t + T * s, j)];
+    dft_groups<INV, T>(u);
   } else {
     // k1 = t / 2; this thread's half t0 = t & 1 of the 32 values: Y[k1][2 t1 + t0], t1 = 0..15
     const int k1 = t >> 1, t0 = t & 1;
@@ -160,9 +169,15 @@ __device__ __forceinline__ void line_fft(float2 (&v)[16], float2 (&u)[16], float
 template <int N>
 struct ZGeo {
   static constexpr int M = N / 2, NH = N / 2 + 1, T = M / 16, L = CTA / T;  // L lines per CTA
-  static constexpr int X = M + 8;       // row stride (float2) of a line in shared memory, = 8 mod 16
+  // Row stride (float2) of a line in shared memory and the swizzle of its natural-order row,
+  // chosen so that the exchange, the row writes and the column reads of the split are free of
+  // bank conflicts (T = 2: at most two-way).
+  static constexpr int X = M + (T >= 8 ? 8 : T);
   static constexpr int C = L + 2;       // stride of the kz-major input tile of the inverse
+  static constexpr int TILE = (NH * C > L * X) ? NH * C : L * X;
   static constexpr long long N2 = (long long)N * N, N3 = N2 * N;
+  static_assert(L <= N * N, "lines per CTA");
+  __device__ static int sw(int l) { return T >= 8 ? (l >> 1) & 7 : (l & 15); }
 };
 
 // Shared twiddle tables of the Z passes: tw[e] = W_N^e (e <= N/2), tl[k1 * T + t] = W_M^{t k1}.
@@ -179,7 +194,8 @@ __device__ __forceinline__ void cpa16(void* dst, const void* src) {
 }
 __device__ __forceinline__ void cpa_wait() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-// Pass Z forward: fields in[f][x][y][z] -> planes out[f][kz][x][y].  grid (N/L, N, nf).
+// Pass Z forward: fields in[f][x][y][z] -> planes out[f][kz][x][y].  A CTA takes L consecutive
+// (x, y) lines.  grid (N^2/L, nf).
 template <int N>
 __global__ void __launch_bounds__(CTA, 4) k_fft_z_r2c(const float* __restrict__ in, float2* __restrict__ out) {
   using G = ZGeo<N>;
@@ -187,8 +203,9 @@ __global__ void __launch_bounds__(CTA, 4) k_fft_z_r2c(const float* __restrict__ 
   __shared__ __align__(16) float2 xb[G::L * G::X];
   load_ztw<false, N>(tw, tl);
   const int t = threadIdx.x % G::T, l = threadIdx.x / G::T;
-  const int y0 = blockIdx.x * G::L, x = blockIdx.y, f = blockIdx.z;
-  const float2* src = reinterpret_cast<const float2*>(in + (long long)f * G::N3 + ((long long)x * N + y0 + l) * N);
+  const long long g0 = (long long)blockIdx.x * G::L;  // first line (x N + y) of this CTA
+  const int f = blockIdx.y;
+  const float2* src = reinterpret_cast<const float2*>(in + (long long)f * G::N3 + (g0 + l) * N);
   float2 v[16], u[16];
 #pragma unroll
   for (int n1 = 0; n1 < 16; ++n1) v[n1] = __ldg(src + G::T * n1 + t);  // (r[2n], r[2n+1]), n = T n1 + t
@@ -198,14 +215,14 @@ __global__ void __launch_bounds__(CTA, 4) k_fft_z_r2c(const float* __restrict__ 
   __syncthreads();
   // Z_k into the line's row in natural order, swizzled so that the column reads below are
   // conflict-free: Z_k at row[k ^ sw(l)].
-  const int sw = (l >> 1) & 7;
+  const int sw = G::sw(l);
 #pragma unroll
   for (int p = 0; p < 16; ++p) row[line_k<G::T>(t, p) ^ sw] = u[p];
   __syncthreads();
   // X_k = E_k + W_N^k O_k with E = (Z_k + conj Z_{M-k})/2, O = -i (Z_k - conj Z_{M-k})/2
-  float2* dst = out + (long long)f * G::NH * G::N2 + (long long)x * N + y0;
+  float2* dst = out + (long long)f * G::NH * G::N2 + g0;
   for (int e = threadIdx.x; e < G::NH * G::L; e += CTA) {
-    const int k = e / G::L, ll = e - k * G::L, sl = (ll >> 1) & 7;
+    const int k = e / G::L, ll = e - k * G::L, sl = G::sw(ll);
     const float2* zr = xb + ll * G::X;
     const float2 zk = zr[(k & (G::M - 1)) ^ sl];
     const float2 zm = cconj(zr[((G::M - k) & (G::M - 1)) ^ sl]);
@@ -215,15 +232,16 @@ __global__ void __launch_bounds__(CTA, 4) k_fft_z_r2c(const float* __restrict__ 
   }
 }
 
-// Pass Z inverse: planes in[f][kz][x][y] -> fields out[f][x][y][z].  grid (N/L, N, nf).
+// Pass Z inverse: planes in[f][kz][x][y] -> fields out[f][x][y][z].  A CTA takes L consecutive
+// (x, y) lines.  grid (N^2/L, nf).
 template <int N>
 __global__ void __launch_bounds__(CTA, 4) k_fft_z_c2r(const float2* __restrict__ in, float* __restrict__ out) {
   using G = ZGeo<N>;
   __shared__ float2 tw[G::M + 1], tl[16 * G::T];
-  __shared__ __align__(16) float2 xb[G::NH * G::C];  // the kz-major tile, later the exchange rows
-  static_assert(G::NH * G::C >= G::L * G::X, "exchange rows fit in the tile");
-  const int y0 = blockIdx.x * G::L, x = blockIdx.y, f = blockIdx.z;
-  const float2* src = in + (long long)f * G::NH * G::N2 + (long long)x * N + y0;
+  __shared__ __align__(16) float2 xb[G::TILE];  // the kz-major tile, later the exchange rows
+  const long long g0 = (long long)blockIdx.x * G::L;
+  const int f = blockIdx.y;
+  const float2* src = in + (long long)f * G::NH * G::N2 + g0;
   for (int e = threadIdx.x; e < G::NH * G::L / 2; e += CTA) {  // two complex values (16 bytes) per copy
     const int k = e / (G::L / 2), ll = 2 * (e - k * (G::L / 2));
     cpa16(xb + k * G::C + ll, src + (long long)k * G::N2 + ll);
@@ -248,7 +266,7 @@ __global__ void __launch_bounds__(CTA, 4) k_fft_z_c2r(const float2* __restrict__
   }
   __syncthreads();  // the tile is read; its memory becomes the exchange rows
   line_fft<true, G::T>(v, u, xb + l * G::X, tl, t);
-  float2* dst = reinterpret_cast<float2*>(out + (long long)f * G::N3 + ((long long)x * N + y0 + l) * N);
+  float2* dst = reinterpret_cast<float2*>(out + (long long)f * G::N3 + (g0 + l) * N);
 #pragma unroll
   for (int p = 0; p < 16; ++p) dst[line_k<G::T>(t, p)] = u[p];  // (r[2n], r[2n+1])
 }
@@ -294,7 +312,9 @@ __device__ __forceinline__ float2 green_mode(float2 v, int x, int y, int kz, int
 template <int N>
 struct PGeo {
   static constexpr int T = N / 16, B = CTA / T, NH = N / 2 + 1;
+  static constexpr int RS = N + (T <= 8 ? T : 0);  // row stride in shared memory (bank-conflict free)
   static constexpr long long N2 = (long long)N * N, N3 = N2 * N;
+  static_assert(B <= N, "a CTA's rows (columns) lie in one plane");
 };
 
 template <bool INV, int N>
@@ -315,7 +335,7 @@ __global__ void __launch_bounds__(CTA, 4) k_fft_rows(const float2* in, float2* o
   using G = PGeo<N>;
   constexpr int T = G::T, B = G::B;
   __shared__ float2 tl[16 * T];
-  __shared__ __align__(16) float2 buf[B * N];
+  __shared__ __align__(16) float2 buf[B * G::RS];
   load_ptw<INV, N>(tl);
   const int bi = blockIdx.x, comp = bi % ncomp, q = bi / ncomp, rb = q % (N / B), pl = q / (N / B);
   const int slot = pl / G::NH, kz = pl - slot * G::NH;
@@ -336,7 +356,7 @@ __global__ void __launch_bounds__(CTA, 4) k_fft_rows(const float2* in, float2* o
   float2 v[16], u[16];
 #pragma unroll
   for (int n1 = 0; n1 < 16; ++n1) v[n1] = plane[(long long)x * N + T * n1 + t];
-  float2* row = buf + r * N;
+  float2* row = buf + r * G::RS;
   double w = 0.0;
   if (GREEN) {
     if (kz != 0 && kz != N / 2 && (gp.gm == 0 || comp != 1)) {
@@ -401,12 +421,15 @@ __global__ void __launch_bounds__(CTA, 4) k_fft_cols(float2* io) {
     buf[(k1 * T + t) * B + j] = k1 ? cmul(v[p], tl[k1 * T + t]) : v[p];
   }
   __syncthreads();
-  if constexpr (T == 16) {
+  if constexpr (T <= 16) {
+    // this thread's k1 = t + T s, s < 16 / T: one T-point DFT each
 #pragma unroll
-    for (int i = 0; i < 16; ++i) u[i] = buf[(t * 16 + i) * B + j];
-    dft_reg<INV, 16, 0, 16>(u);
+    for (int s = 0; s < 16 / T; ++s)
+#pragma unroll
+      for (int i = 0; i < T; ++i) u[T * s + i] = buf[((t + T * s) * T + i) * B + j];
+    dft_groups<INV, T>(u);
   } else {
-    static_assert(T == 32, "column pass for N = 256 or 512");
+    static_assert(T == 32, "column pass for N <= 512");
     const int k1 = t >> 1, t0 = t & 1;
 #pragma unroll
     for (int i = 0; i < 16; ++i) u[i] = buf[(k1 * 32 + 2 * i + t0) * B + j];
@@ -428,7 +451,7 @@ int r2c_n(const float* delta, float2* spec, int nslots, cudaStream_t s) {
   using Z = ZGeo<N>;
   using G = PGeo<N>;
   const unsigned planes = (unsigned)(nslots * G::NH), blocks = (unsigned)(N / G::B) * planes;
-  k_fft_z_r2c<N><<<dim3(N / Z::L, N, nslots), CTA, 0, s>>>(delta, spec);
+  k_fft_z_r2c<N><<<dim3((unsigned)(Z::N2 / Z::L), nslots), CTA, 0, s>>>(delta, spec);
   k_fft_rows<N, false, false><<<blocks, CTA, 0, s>>>(spec, spec, StepArgs{}, nullptr, 1);
   k_fft_cols<N, false><<<blocks, CTA, 0, s>>>(spec);
   const cudaError_t e = cudaGetLastError();
@@ -443,7 +466,7 @@ int green_c2r_n(const float2* spec, float2* gwork, float* force, const StepArgs&
   const unsigned blocks = (unsigned)(N / G::B) * (unsigned)(nslots * G::NH) * 3u;
   k_fft_rows<N, true, true><<<blocks, CTA, 0, s>>>(spec, gwork, A, slot_peak, 3);
   k_fft_cols<N, true><<<blocks, CTA, 0, s>>>(gwork);
-  k_fft_z_c2r<N><<<dim3(N / Z::L, N, 3 * nslots), CTA, 0, s>>>(gwork, force);
+  k_fft_z_c2r<N><<<dim3((unsigned)(Z::N2 / Z::L), 3 * nslots), CTA, 0, s>>>(gwork, force);
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? 0 : -(int)e;
 }
@@ -455,14 +478,14 @@ int c2r_n(const float2* spec, float2* gwork, float* out, int nfields, cudaStream
   const unsigned blocks = (unsigned)(N / G::B) * (unsigned)(nfields * G::NH);
   k_fft_rows<N, true, false><<<blocks, CTA, 0, s>>>(spec, gwork, StepArgs{}, nullptr, 1);
   k_fft_cols<N, true><<<blocks, CTA, 0, s>>>(gwork);
-  k_fft_z_c2r<N><<<dim3(N / Z::L, N, nfields), CTA, 0, s>>>(gwork, out);
+  k_fft_z_c2r<N><<<dim3((unsigned)(Z::N2 / Z::L), nfields), CTA, 0, s>>>(gwork, out);
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? 0 : -(int)e;
 }
 
 }  // namespace
 
-bool fft_native_size(int N) { return N == 256 || N == 512; }
+bool fft_native_size(int N) { return N == 64 || N == 128 || N == 256 || N == 512; }
 
 // Per-device set-up: the twiddle table.  Call with the device current.
 int fft_native_init() {
@@ -478,7 +501,13 @@ int fft_native_init() {
 // delta fields [slot][x][y][z] -> spectra [slot][kz][kx][ky]
 int fft_native_r2c(int N, const float* delta, float2* spec, int nslots, cudaStream_t s) {
   if (nslots <= 0) return 0;
-  return N == 512 ? r2c_n<512>(delta, spec, nslots, s) : r2c_n<256>(delta, spec, nslots, s);
+  switch (N) {
+    case 64: return r2c_n<64>(delta, spec, nslots, s);
+    case 128: return r2c_n<128>(delta, spec, nslots, s);
+    case 256: return r2c_n<256>(delta, spec, nslots, s);
+    case 512: return r2c_n<512>(delta, spec, nslots, s);
+    default: return -2000;
+  }
 }
 
 // spectra [slot][kz][kx][ky] -> 3 force grids per slot [slot][comp][x][y][z] through the
@@ -486,14 +515,25 @@ int fft_native_r2c(int N, const float* delta, float2* spec, int nslots, cudaStre
 int fft_native_green_c2r(int N, const float2* spec, float2* gwork, float* force, const StepArgs& A,
                          const int* slot_peak, int nslots, cudaStream_t s) {
   if (nslots <= 0) return 0;
-  return N == 512 ? green_c2r_n<512>(spec, gwork, force, A, slot_peak, nslots, s)
-                  : green_c2r_n<256>(spec, gwork, force, A, slot_peak, nslots, s);
+  switch (N) {
+    case 64: return green_c2r_n<64>(spec, gwork, force, A, slot_peak, nslots, s);
+    case 128: return green_c2r_n<128>(spec, gwork, force, A, slot_peak, nslots, s);
+    case 256: return green_c2r_n<256>(spec, gwork, force, A, slot_peak, nslots, s);
+    case 512: return green_c2r_n<512>(spec, gwork, force, A, slot_peak, nslots, s);
+    default: return -2000;
+  }
 }
 
 // Plain unnormalised inverse: spectra [f][kz][kx][ky] -> fields [f][x][y][z]; gwork as spec.
 int fft_native_c2r(int N, const float2* spec, float2* gwork, float* out, int nfields, cudaStream_t s) {
   if (nfields <= 0) return 0;
-  return N == 512 ? c2r_n<512>(spec, gwork, out, nfields, s) : c2r_n<256>(spec, gwork, out, nfields, s);
+  switch (N) {
+    case 64: return c2r_n<64>(spec, gwork, out, nfields, s);
+    case 128: return c2r_n<128>(spec, gwork, out, nfields, s);
+    case 256: return c2r_n<256>(spec, gwork, out, nfields, s);
+    case 512: return c2r_n<512>(spec, gwork, out, nfields, s);
+    default: return -2000;
+  }
 }
 
 namespace {

@@ -56,8 +56,8 @@ class Engine:
         # `full_every` steps each super-tile is re-sorted by cell (bucket_sort=False: every step).
         # Results do not depend on the choice: the deposit is order-independent bit for bit.
         # dynamic: served runs; no graph, and each step's FFTs cover only the slots in use.
-        # native_fft: 256^3 and 512^3 meshes use the native transform with the Green multiply
-        # fused (False: cuFFT and the separate Green kernel, as for every other mesh size).
+        # native_fft: 64^3-512^3 meshes use the native transform with the Green multiply fused
+        # (False: cuFFT and the separate Green kernel, as for every other mesh size).
         every = int(full_every) if bucket_sort else 1
         flags = ((max(1, min(every, 255)) & 0xFF) << 8) | (_lib.FLAG_GRAPH if graph else 0) | \
                 (_lib.FLAG_DYNAMIC if dynamic else 0) | (_lib.FLAG_NATIVE_FFT if native_fft else 0)

@@ -44,7 +44,7 @@ class Request:
         return self.t_done - self.t_arrival
 
 
-NATIVE_FFT_SIZES = (256, 512)   # meshes the engine transforms natively (no cuFFT work area)
+NATIVE_FFT_SIZES = (64, 128, 256, 512)   # meshes the engine transforms natively (no cuFFT work area)
 
 
 def slot_bytes(N: int, native_fft: bool = True) -> int:

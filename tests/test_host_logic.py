@@ -81,16 +81,19 @@ def test_served_slot_pool_fits_the_budget():
     from pbh_b200.serve import slot_bytes
     sizes = [slot_bytes(n) for n in (64, 128, 256)]
     assert sizes == sorted(sizes)
-    # per particle the same, less the cuFFT work area that the native 256^3 transform does not use
-    assert slot_bytes(256, native_fft=False) == pytest.approx(8 * slot_bytes(128), rel=0.01)
+    # per particle the same, less the cuFFT work area that the native transform does not use
+    assert slot_bytes(256) == pytest.approx(8 * slot_bytes(128), rel=0.01)
     assert slot_bytes(256) == slot_bytes(256, native_fft=False) - 16 * 256 ** 3
+    assert slot_bytes(32) == slot_bytes(32, native_fft=False)            # cuFFT at 32^3 either way
     pool = 32 * slot_bytes(64) + 32 * slot_bytes(128) + 24 * slot_bytes(256)  # the served benchmark's pool
     assert pool <= 150e9
 
 
 def test_launch_accounting():
     import bench
-    assert bench.launches_per_step([32, 64], "native") == 10          # cuFFT sizes only
+    assert bench.launches_per_step([32], "native") == 10              # cuFFT size only
+    assert bench.launches_per_step([32, 64], "native") == 16          # 64^3 native, Green for 32^3
+    assert bench.launches_per_step([32, 64, 128, 256], "native") == 28  # the batched ensemble
     assert bench.launches_per_step([256], "cufft") == 10
     assert bench.launches_per_step([256], "native") == 15             # + 6, no Green launch
     assert bench.launches_per_step([512], "native") == 15

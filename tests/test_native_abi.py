@@ -68,10 +68,10 @@ def test_invariant_divisor_magic_numbers():
 
 
 def test_native_fft_rejects_other_sizes_before_touching_the_device():
-    """Only 256^3 and 512^3 have a native transform; other sizes are refused with the
+    """Only 64^3 to 512^3 have a native transform; other sizes are refused with the
     invalid-argument code for the size, before any pointer is used or any CUDA call is made."""
     from pbh_b200 import _lib
     lib = _lib.load()
-    assert lib.pm_rfft3_native(128, 16, 16, 1, None) == -2000
+    assert lib.pm_rfft3_native(32, 16, 16, 1, None) == -2000
     assert lib.pm_irfft3_native(1024, 16, 16, 16, 1, None) == -2000
     assert lib.pm_rfft3_native(300, 16, 16, 1, None) == -2000
