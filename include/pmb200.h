@@ -207,10 +207,12 @@ int pm_irfft3_256(const void* spec, void* work, float* x, int nfields, void* str
  * until the process exits; it calls no allocating routine.  n must not exceed
  * PM_NOALLOC_MAX_KEYS (larger n returns -2003 and touches nothing).  The first call on a device
  * looks up the array's device address for that device (cudaGetSymbolAddress, with that device
- * current), so make that first call before any stream capture.  Every call shares the array:
- * calls that overlap on the GPU (from several streams or threads) race, and must be serialized
- * by the caller.  Runs on `stream` (a cudaStream_t, NULL for the default stream) and returns
- * after the sort has finished: 0, 1 if a bounded look-back wait gave up, < 0 on error. */
+ * current) and keeps it for the life of the process, so make that first call before any stream
+ * capture, and do not reset the device (cudaDeviceReset) after it.  Every call shares the
+ * array: calls that overlap on the GPU (from several streams or threads) race, and must be
+ * serialized by the caller.  Runs on `stream` (a cudaStream_t, NULL for the default stream);
+ * each call copies the sort's error word back to the host and waits for `stream` before it
+ * returns: 0, 1 if a bounded look-back wait gave up, < 0 on error. */
 #define PM_NOALLOC_MAX_KEYS (1LL << 18)
 #define PM_NOALLOC_SCRATCH_BYTES (3670016)
 int pm_sort_u64_noalloc(const unsigned long long* keys, unsigned long long* keys_out, unsigned int* perm_out,

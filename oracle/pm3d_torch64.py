@@ -68,23 +68,39 @@ class TorchMesh:
             out += flat_f[flat] * w
         return out
 
+    def potential_k(self, delta, a: float):
+        """Phi_k = -(3/2) H_i^2 delta_k /(a k^2), optional Gaussian smoothing, zero mode
+        removed (pm3d.py:105-109)."""
+        phik = (-1.5 * H_I ** 2 / a) * torch.fft.rfftn(delta) / self.k2
+        if self.smooth > 0:
+            phik = phik * torch.exp(-0.5 * self.k2 * (self.smooth * self.dx) ** 2)
+        phik[0, 0, 0] = 0.0
+        return phik
+
     def forces(self, X, a: float):
         """(-grad Phi at the particles, delta) of ``PM3D.forces`` (pm3d.py:101-114); numpy's
         irfftn convention (Hermitian part of the kz = 0, N/2 planes) is what torch's irfftn
         computes as well."""
         N = self.N
         delta = self.deposit(X) / self.n_mean - 1.0
-        dk = torch.fft.rfftn(delta)
-        phik = (-1.5 * H_I ** 2 / a) * dk / self.k2
-        if self.smooth > 0:
-            phik = phik * torch.exp(-0.5 * self.k2 * (self.smooth * self.dx) ** 2)
-        phik[0, 0, 0] = 0.0
+        phik = self.potential_k(delta, a)
         acc = []
         for kc in (self.kx, self.ky, self.kz):
             g = torch.fft.irfftn(-1j * kc * phik, s=(N, N, N))
             acc.append(self.interp(g, X))
             del g
         return torch.stack(acc, dim=-1), delta
+
+    def energies(self, X, P, a: float):
+        """(m_p sum p, K, W) at expansion factor a, as ``oracle.pm3d_oracle.energies``: K =
+        m_p/(2 a^2) sum p^2 and W = (1/2) rho_b a^3 dx^3 sum_nodes delta Phi, from pm3d's
+        equations of motion (pm3d.py:3-6) and its mesh potential (pm3d.py:103-109)."""
+        mom = self.m_part * P.sum(dim=0)
+        kin = self.m_part / (2.0 * a * a) * float((P * P).sum())
+        delta = self.deposit(X) / self.n_mean - 1.0
+        phi = torch.fft.irfftn(self.potential_k(delta, a), s=(self.N,) * 3)
+        pot = 0.5 * RHO_A3 * self.dx ** 3 * float((delta * phi).sum())
+        return mom, kin, pot
 
 
 def hubble(a: float) -> float:

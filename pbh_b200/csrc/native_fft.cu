@@ -36,6 +36,8 @@
 #include <cmath>
 #include <cstdint>
 
+#include <mutex>
+
 #include "pm_kernels.cuh"
 
 namespace {
@@ -537,12 +539,16 @@ int fft_native_c2r(int N, const float2* spec, float2* gwork, float* out, int nfi
 }
 
 namespace {
+// Per-device set-up of the twiddle table, once per device; the lock keeps two host threads that
+// make their first call on one device at the same time from racing on it.
+std::mutex g_init_mu;
 int ensure_native_init() {
   static int done[64] = {};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return -(int)e;
   if (dev < 0 || dev >= 64) return -2004;
+  std::lock_guard<std::mutex> lock(g_init_mu);
   if (!done[dev]) {
     if (int r = fft_native_init()) return r;
     done[dev] = 1;

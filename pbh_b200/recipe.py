@@ -51,36 +51,68 @@ def _shape_coeffs(R):
                      2.0 / 3.0 * pr * elliprd(x[0], x[1], x[2])]) - 2.0 / 3.0
 
 
-@functools.lru_cache(maxsize=4096)
-def _first_axis_time(e: float, p: float, delta_i: float = 1e-2, f_freeze: float = 0.01) -> float:
-    """Time (units of t_i, EdS, G = 1) at which the first axis of a homogeneous ellipsoid with
-    Zel'dovich eigenvalues delta_i (1+3e+p, 1-2p, 1-3e+p)/3 falls to f_freeze of its initial
-    size, with the external tide in linear theory."""
+def collapse_times(e: float, p: float, delta_i: float = 1e-2, f_freeze: float = 0.01,
+                   max_step: float = 50.0) -> np.ndarray:
+    """Bond & Myers (1996) collapse times t1 <= t2 <= t3 (units of t_i; EdS, G = 1) of the three
+    axes of a homogeneous ellipsoid with Zel'dovich eigenvalues delta_i (1+3e+p, 1-2p, 1-3e+p)/3
+    and the external tide in linear theory: the model of pbhgr/scripts/ellipsoidal_collapse.py:
+    14-54, pinned against it by tests/golden/collapse_times.npz.
+
+    The axes obey R_i'' = -4 pi rho_b R_i [(1 + delta)/3 + b_i delta/2 + (lambda_i - delta_i/3) a]
+    with a = t^(2/3), rho_b = 1/(6 pi t^2), delta = a^3/(R1 R2 R3) - 1 and the interior shape
+    coefficients b_i (Carlson's R_D).  The run is integrated in segments, one per freeze: an
+    axis freezes (its size held, its velocity zeroed) when it falls to f_freeze of its largest
+    size as known at the start of the segment, and the largest sizes are updated from the state
+    at the end of each segment.  max_step bounds the integrator's step; the reference bounds it
+    by 0.02 t_segment, which changes the times by less than 1e-6 relative (the fixture test)."""
     from scipy.integrate import solve_ivp
     lam = delta_i * np.array([1 + 3 * e + p, 1 - 2 * p, 1 - 3 * e + p]) / 3.0
-    R0 = 1.0 - lam
-    V0 = (2.0 / 3.0) * (1.0 - 2.0 * lam)
+    frozen = np.zeros(3, dtype=bool)
+    r_hold = np.zeros(3)
+    t_col = np.full(3, np.nan)
+    r_top = 1.0 - lam
+    t, y = 1.0, np.concatenate([1.0 - lam, (2.0 / 3.0) * (1.0 - 2.0 * lam)])
+    t_end = 1e5
 
-    def rhs(t, y):
-        R = np.maximum(y[:3], 1e-9)
-        a = t ** (2.0 / 3.0)
-        rho_b = 1.0 / (6.0 * math.pi * t * t)
+    def rhs(tt, yy):
+        R = np.where(frozen, r_hold, np.maximum(yy[:3], 1e-9))
+        a = tt ** (2.0 / 3.0)
+        rho_b = 1.0 / (6.0 * math.pi * tt * tt)
         delta = a ** 3 / np.prod(R) - 1.0
         acc = -4.0 * math.pi * rho_b * R * ((1.0 + delta) / 3.0 + 0.5 * _shape_coeffs(R) * delta
                                            + (lam - delta_i / 3.0) * a)
-        return np.concatenate([y[3:], acc])
+        return np.concatenate([np.where(frozen, 0.0, yy[3:]), np.where(frozen, 0.0, acc)])
 
-    def ev(t, y):
-        return float(np.min(y[:3] - f_freeze * R0))
-    ev.terminal = True
-    ev.direction = -1
-    sol = solve_ivp(rhs, (1.0, 1e5), np.concatenate([R0, V0]), events=ev, rtol=1e-8, atol=1e-12,
-                    method="DOP853", max_step=50.0)
-    return float(sol.t_events[0][0]) if sol.t_events[0].size else float("nan")
+    while t < t_end and not frozen.all():
+        floor = f_freeze * r_top.copy()
+        live = np.flatnonzero(~frozen)
+
+        def hit(tt, yy, live=live, floor=floor):
+            return float(np.min(yy[live] - floor[live]))
+        hit.terminal = True
+        hit.direction = -1
+        sol = solve_ivp(rhs, (t, t_end), y, events=hit, rtol=1e-8, atol=1e-12, method="DOP853",
+                        max_step=max_step)
+        t, y = float(sol.t[-1]), sol.y[:, -1].copy()
+        r_top = np.maximum(r_top, y[:3])
+        if sol.status != 1:
+            break
+        gap = np.where(frozen, np.inf, y[:3] - f_freeze * r_top)
+        i = int(np.argmin(gap))
+        frozen[i] = True
+        r_hold[i] = y[i]
+        t_col[i] = t
+    return t_col
+
+
+@functools.lru_cache(maxsize=4096)
+def _first_axis_time(e: float, p: float) -> float:
+    return float(collapse_times(e, p)[0])
 
 
 def first_axis_ratio(e: float, p: float) -> float:
-    """t1/t_sph for Zel'dovich ellipticity e and prolateness p (rounded to 1e-4 for caching)."""
+    """t1/t_sph for Zel'dovich ellipticity e and prolateness p (rounded to 1e-4 for caching):
+    the first axis's collapse time over the spherical (e = p = 0) one."""
     e, p = round(float(e), 4), round(float(p), 4)
     return _first_axis_time(e, p) / _first_axis_time(0.0, 0.0)
 

@@ -1,10 +1,11 @@
 """Generate the golden fixtures by running the unmodified reference pm3d.
 
 Usage (in a container that has the reference checkout):
-    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py /root/reference/pbhgr
+    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py <checkout>/pbhgr [pm3d|profiles|collapse ...]
 
-The reference package directory is given on the command line (or through
-PBH_REFERENCE); nothing at test time reads it.  Each case is a small run of
+The reference package directory (the one holding pbhgr/ and scripts/ of the reference
+checkout) is given on the command line (or through PBH_REFERENCE); the optional names pick
+which fixtures to regenerate.  Nothing at test time reads the checkout.  Each case is a small run of
 ``pbhgr.pm3d`` whose inputs and outputs are saved as float64 ``.npz`` files
 (plus ``analyse`` output as JSON), with the numpy version recorded.
 """
@@ -116,16 +117,44 @@ def profiles_case(path: str, name="profiles"):
     _save(name, dict(units=meta), r=r, **out)
 
 
+COLLAPSE_POINTS = ((0.0, 0.0), (0.05, 0.0), (0.1, -0.05), (0.15, 0.05), (0.2, 0.0), (0.3, 0.1), (0.3, -0.1))
+
+
+def collapse_case(path: str, name="collapse_times"):
+    """Bond-Myers collapse times t1 <= t2 <= t3 of scripts/ellipsoidal_collapse.py (its
+    collapse_times, lines 14-54) at a few (e, p) points.  The script runs a scan when it is
+    imported, so only its text up to the scan is executed, with the script's default
+    arguments (nu = 4, f_freeze = 0.01)."""
+    src = Path(path) / "scripts" / "ellipsoidal_collapse.py"
+    text = src.read_text()
+    head = text[:text.index("\nt_sph = collapse_times")]
+    ns = {"__name__": "ellipsoidal_collapse_defs"}
+    argv = sys.argv
+    sys.argv = [str(src)]
+    try:
+        exec(compile(head, str(src), "exec"), ns)
+    finally:
+        sys.argv = argv
+    times = np.array([ns["collapse_times"](e, p) for e, p in COLLAPSE_POINTS])
+    _save(name, dict(f_freeze=ns["f_freeze"], delta_i=1e-2, points=[list(q) for q in COLLAPSE_POINTS]),
+          ep=np.array(COLLAPSE_POINTS), times=times)
+
+
 def main():
     ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PBH_REFERENCE", "")
     if not ref:
         raise SystemExit("give the reference package directory (the one holding pbhgr/)")
-    pm3d, profiles = _load_reference(ref)
-    zeta_case(pm3d, profiles, "zeta_16", 16, 8.0, 16, 7, 0.0, 0.1, 0.15, 0.05, 0.05, 3)
-    zeta_case(pm3d, profiles, "zeta_16_np8_smooth", 16, 8.0, 8, 1, 2.0, 0.3, 0.0, 0.0, 0.0, 4)
-    mesh_case(pm3d, "mesh_8", 8, 1.0, 600, 11)
-    recipe_case(pm3d, "recipe_16", 16, 16, 5, 10)
-    profiles_case(ref)
+    only = sys.argv[2:]
+    if not only or "pm3d" in only:
+        pm3d, profiles = _load_reference(ref)
+        zeta_case(pm3d, profiles, "zeta_16", 16, 8.0, 16, 7, 0.0, 0.1, 0.15, 0.05, 0.05, 3)
+        zeta_case(pm3d, profiles, "zeta_16_np8_smooth", 16, 8.0, 8, 1, 2.0, 0.3, 0.0, 0.0, 0.0, 4)
+        mesh_case(pm3d, "mesh_8", 8, 1.0, 600, 11)
+        recipe_case(pm3d, "recipe_16", 16, 16, 5, 10)
+    if not only or "profiles" in only:
+        profiles_case(ref)
+    if not only or "collapse" in only:
+        collapse_case(ref)
 
 
 if __name__ == "__main__":

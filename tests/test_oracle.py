@@ -136,6 +136,11 @@ def test_torch64_oracle_matches_numpy_oracle():
         a, _ = tr_t.step(a, 0.05 * a)
     assert np.max(np.abs(tr_t.x.numpy() - tr_n.x)) <= 1e-12
     assert np.max(np.abs(tr_t.p.numpy() - tr_n.p)) <= 1e-12 * np.max(np.abs(tr_n.p))
+    m_t, k_t, w_t = tm.energies(tr_t.x, tr_t.p, a)
+    m_n, k_n, w_n = O.energies(mesh, tr_n.x, tr_n.p, a)
+    assert np.max(np.abs(m_t.numpy() - m_n)) <= 1e-12 * mesh.m_part * mesh.Np ** 3 * np.max(np.abs(tr_n.p))
+    assert k_t == pytest.approx(k_n, rel=1e-12)
+    assert w_t == pytest.approx(w_n, rel=1e-11)
 
 
 def test_profile_tables_and_units_match_reference(golden):
@@ -155,3 +160,18 @@ def test_profile_tables_and_units_match_reference(golden):
             assert r_m == pytest.approx(want["r_m"], rel=1e-12)
             assert t_h == pytest.approx(want["t_H"], rel=1e-12)
             assert tc0 == pytest.approx(want["tC0"], rel=1e-9)
+
+
+def test_bond_myers_collapse_times_match_reference(golden):
+    """pbh_b200.recipe.collapse_times (the Bond-Myers model behind every recipe's delta0)
+    against the reference's own collapse_times (pbhgr/scripts/ellipsoidal_collapse.py:22-54),
+    run by tests/golden/make_golden.py.  The reference bounds the integrator's step by 0.02 t;
+    the restatement's larger step changes the times by ~1e-7 relative."""
+    from pbh_b200 import recipe
+    g = golden("collapse_times")
+    t_sph_ref = g["times"][0][2]                       # the reference's t_sph: collapse_times(0, 0)[2]
+    for (e, p), want in zip(g["ep"], g["times"]):
+        got = recipe.collapse_times(float(e), float(p))
+        assert np.all(np.abs(got - want) <= 5e-7 * want), (e, p, got, want)
+        ratio = recipe.first_axis_ratio(float(e), float(p))
+        assert abs(ratio - want[0] / t_sph_ref) <= 1e-7 * ratio, (e, p)
