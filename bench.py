@@ -42,6 +42,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-errors", action="store_true", help="skip the per-output errors against the float64 oracle")
     ap.add_argument("--full-sort", action="store_true", help="sort the whole cell key every step")
     ap.add_argument("--no-serve", action="store_true", help="skip the served-stream latency run")
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="arrival window of the served stream")
@@ -68,6 +69,12 @@ def workload_specs(name: str, npeaks: int, seed: int, rank: int):
         specs = [recipe.large_peak(N=512, steps=300, seed=seed + rank)]
         desc = {"workload": "large single run: 512^3 mesh and particles, e=0.3, p=0.1, collapse a_cfg=0.5, 300 steps"}
     return specs, desc
+
+
+def workload_config(desc: dict, specs, gpus: int) -> dict:
+    """The `config` of both arms: the workload only (its engine settings go under `engine`)."""
+    return dict(desc, particles_per_gpu=int(sum(s.n for s in specs)), peaks=len(specs),
+                l2="inputs larger than L2 (126 MB)", parallelism=f"replicas x{gpus}")
 
 
 # ------------------------------------------------------------------------------ clocks
@@ -149,8 +156,11 @@ def cpu_rate(specs, steps: int, warmup: int, max_mesh: int, workers: int | None 
     tmax = max(t for _, t in res)
     import platform
     return {"value": ps / tmax, "unit": UNIT, "cores": len(tasks), "kind": "port",
-            "sample": f"{len(tasks)} peaks (one per core) with meshes {sorted({t[0] for t in tasks})}^3 from the "
-                      f"same recipe, {steps} timed KDK steps each after {warmup} untimed, float64 numpy oracle",
+            "sample": f"{len(tasks)} peaks of the workload (one per core) with meshes "
+                      f"{sorted({t[0] for t in tasks})}^3, {steps} timed KDK steps each after {warmup} untimed, "
+                      f"float64 numpy restatement of pm3d; meshes above {max_mesh}^3 are left out of the sample "
+                      f"(one float64 step of a 256^3 peak takes ~12 s on one core), and the per-core rate falls "
+                      f"slowly with mesh size, so the sample's rate is, if anything, above the full mix's",
             "host_cpus": cores, "cpu": platform.processor() or platform.machine(), "wall_s": wall}
 
 
@@ -163,8 +173,8 @@ def run_reference(args):
     cb = cpu_rate(specs, args.steps, args.warmup, max_mesh)
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(desc, sample_meshes_max=max_mesh),
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (recipe peaks, seeded numpy noise)",
+            "config": workload_config(desc, specs, args.gpus),
             "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -199,9 +209,9 @@ def launches_per_step(sizes, fft: str) -> int:
     native = {n for n in sizes if fft == "native" and n in NATIVE_FFT_SIZES}
     return 10 + 6 * len(native) - (1 if native and all(n in native for n in sizes) else 0)
 
-# DRAM bytes (read + write) per launch from one ncu capture of the plain 256^3 run
-# (profiles/kernels_plain256.md), per particle (per mode for Green), scaled to a launch by the
-# particles (modes) it processes.
+# DRAM bytes (read + write) per launch from single-kernel ncu captures of a 128^3 run (the
+# summaries under profiles/ give the commands), per particle (per mode for Green), scaled to a
+# launch by the particles (modes) it processes.
 NCU_TRAFFIC = {"push": 77.17, "bin": 61.18, "deposit": 28.62, "green_per_mode": 25.69}
 
 
@@ -218,6 +228,65 @@ def replica_throughput(t_local: float, n_local: int, steps: int, dist=None, devi
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         t = float(tt.item())
     return t, world * n_local * steps / t
+
+
+def oracle_errors(specs, tiles, device: int, nsteps: int = 50) -> dict:
+    """Per-output errors of the engine against the float64 oracle -- the checker, run outside
+    every timed region.  For one seeded peak of each mesh size of the workload: nsteps KDK
+    steps of the peak's own schedule from the engine's loaded particles, on the engine and on
+    the float64 torch restatement of pm3d (oracle/pm3d_torch64.py, pinned to the numpy oracle);
+    positions after nsteps (max, in cells), then the oracle's density and forces at the
+    engine's final positions (relative L2).  Tolerances: density 1e-6, forces 1e-5, positions
+    1e-5 cell."""
+    import torch
+
+    from oracle.pm3d_torch64 import TorchMesh, TorchTrajectory
+    from pbh_b200 import _lib
+    from pbh_b200.engine import Engine, PeakConfig
+    from pbh_b200.ic import recipe_particles
+    out = {}
+    for N in sorted({s.N for s in specs}):
+        sp = next(s for s in specs if s.N == N)
+        eng = Engine([PeakConfig(N=N, Np=N, L=sp.L, tile=int(tiles.get(N, 0)))], device=device)
+        x, p = recipe_particles(sp, device=device)
+        eng.set_particles(0, x, p, 1.0, mode=_lib.SCHED_RATIO, param=sp.ratio(), max_steps=nsteps)
+        del x, p
+        x0, p0 = eng.particles(0)
+        eng.run(nsteps + 2)
+        c = eng.clock(0)
+        x = eng.particles(0)[0]
+        delta = eng.delta(0).double()
+        acc = eng.acc(0, c.a)
+        eng.close()
+        tm = TorchMesh(N, sp.L, N, device=f"cuda:{device}")
+        acc_ref, delta_ref = tm.forces(x, c.a)
+        rel = lambda a, b: float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+        e = {"density_rel_l2": rel(delta, delta_ref), "forces_rel_l2": rel(acc, acc_ref)}
+        del acc_ref, delta_ref, acc, delta
+        tr = TorchTrajectory(tm, x0, p0)
+        a = 1.0
+        for _ in range(nsteps):
+            a, _ = tr.step(a, a * sp.ratio())
+        d = x - tr.x
+        d = d - sp.L * torch.round(d / sp.L)
+        e["positions_cells"] = float(d.abs().max()) / tm.dx
+        e["seed"] = sp.seed
+        out[str(N)] = e
+        del tr, x, x0, p0, tm
+        torch.cuda.empty_cache()
+    worst = {k: max(v[k] for v in out.values()) for k in ("density_rel_l2", "forces_rel_l2", "positions_cells")}
+    return {"vs": "float64 pm3d restatement on the same initial particles (same positions for density and forces)",
+            "steps": nsteps, "by_mesh": out, "max": worst,
+            "tolerance": {"density_rel_l2": 1e-6, "forces_rel_l2": 1e-5, "positions_cells": 1e-5},
+            "within": bool(worst["density_rel_l2"] <= 1e-6 and worst["forces_rel_l2"] <= 1e-5
+                           and worst["positions_cells"] <= 1e-5)}
+
+
+# Ideal HBM bytes of a whole step: 176 per particle outside the transforms (push 64, regroup 64,
+# deposit 16 + 4 per cell ... per particle = cell) and 24 per cell for the transforms (R2C reads
+# delta and writes the half spectrum, C2R reads it and writes three force grids).
+IDEAL_BYTES_PER_PARTICLE = 176.0
+IDEAL_FFT_BYTES_PER_CELL = 24.0
 
 
 def run_ours(args):
@@ -280,6 +349,24 @@ def run_ours(args):
 
     # Per-kernel device times: a few ungraphed steps with events between phases, same stream.
     ph = ens.timed_phases(16)                     # one sort step and fifteen re-binning steps
+    # A second device-timed window late in the run (past the collapse of the early peaks).
+    late = None
+    run_len = min(sp.steps for sp in specs)
+    done_steps = args.warmup + args.steps + 16
+    if run_len >= 140 and done_steps <= 120:
+        ens.step(120 - done_steps)
+        n_late = ens.active_particles()
+        ens.engine.sync()
+        l0, l1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0.record(stream)
+        ens.step(20)
+        l1.record(stream)
+        l1.synchronize()
+        t_late = l0.elapsed_time(l1) / 1e3
+        a_cfg = ens.clocks()[0].a / 100.0
+        late = {"steps": [121, 140], "ms_per_step": t_late / 20 * 1e3, "value": n_late * 20 / t_late, "unit": UNIT,
+                "a_cfg_end": a_cfg,
+                "peaks_past_design_collapse": int(sum(1 for sp in specs if sp.a_collapse_cfg <= a_cfg))}
     cells = sum(s.N ** 3 for s in specs)
     # modes the Green kernel handles (the native 256^3 transform applies its own multiply)
     modes = sum(s.N * s.N * (s.N // 2 + 1) for s in specs if not (args.fft == "native" and s.N in NATIVE_FFT_SIZES))
@@ -315,18 +402,31 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 (fields, offsets, momenta; i32 cells; i64 fixed-point density sums)",
             "data": "synthetic (recipe peaks, seeded numpy noise)",
-            "config": dict(desc, particles_per_gpu=n_step, peaks=len(specs), l2="inputs larger than L2 (126 MB)",
-                           regroup="Morton radix sort every step" if args.full_sort else
-                           "re-binning each step, Morton radix sort every 16th", parallelism=f"replicas x{world}",
-                           super_tiles={str(k): v for k, v in sorted(tiles.items())},
-                           fft_64_to_512="native (Green fused into the inverse)" if args.fft == "native" else "cuFFT"),
+            "config": workload_config(desc, specs, world),
+            "engine": {"regroup": "Morton radix sort every step" if args.full_sort else
+                       "re-binning each step, super-tile re-sort every 16th", "timed_steps": [1 + args.warmup,
+                                                                                       args.warmup + args.steps],
+                       "super_tiles": {str(k): v for k, v in sorted(tiles.items())},
+                       "fft_64_to_512": "native (Green fused into the inverse)" if args.fft == "native" else "cuFFT"},
             "clocks": clocks, "gpu_launches": args.steps * launches_per_step([sp.N for sp in specs], args.fft),
             "roofline": roofline}
+    if late is not None:
+        line["late_window"] = late
 
     if rank == 0 and not args.no_plain and args.workload == "batched":
         pr = plain_rate(specs, steps=8, warmup=3, device=local, tiles=tiles)
+        # Upper bound of batched/plain: the plain runs' summed step time over the time of the
+        # whole ensemble's step at the HBM roofline (every byte moved once at the measured peak).
+        plain_ms = sum(pr["step_s_by_mesh"][str(sp.N)] for sp in specs) * 1e3
+        ideal_ms = sum(IDEAL_BYTES_PER_PARTICLE * sp.n + IDEAL_FFT_BYTES_PER_CELL * sp.N ** 3
+                       for sp in specs) / (hbm * 1e9) * 1e3
         line["plain"] = dict(pr, batched_over_plain=value / world / pr["particle_steps_per_s"],
-                             how="each peak alone in a single-peak engine, sequentially, same kernels")
+                             how="each peak alone in a single-peak engine, sequentially, same kernels",
+                             bound={"plain_ms_per_ensemble_step": plain_ms, "roofline_ms_per_ensemble_step": ideal_ms,
+                                    "batched_ms_per_step": ms_per_step,
+                                    "max_batched_over_plain": plain_ms / ideal_ms,
+                                    "how": "sum of the plain per-peak step times / the ensemble step at the HBM "
+                                           "roofline (176 B per particle + 24 B per cell at the measured peak)"})
         ps = pm3d_step_rate(specs, steps=5, warmup=2, device=local)
         line["plain_pm3d_step"] = dict(ps, batched_over_pm3d_step=value / world / ps["particle_steps_per_s"],
                                        how="each peak alone through PM3D.step (delta returned to the host "
@@ -336,10 +436,12 @@ def run_ours(args):
         line["e2e"] = e2e_job(ens, specs, torch, local)
     ens.close()
     del ens
+    if rank == 0 and not args.no_errors:
+        line["errors"] = oracle_errors(specs, tiles, local)
     if rank == 0 and not args.no_serve:
         line["served"] = served_stream(args, local, tiles)
     if rank == 0 and world == 1 and not args.no_cpu:
-        cb = cpu_rate(specs, steps=2, warmup=1, max_mesh=128 if args.workload == "batched" else 64)
+        cb = cpu_rate(specs, steps=4, warmup=1, max_mesh=128 if args.workload == "batched" else 64)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
     if dist:
         dist.barrier()
@@ -351,8 +453,13 @@ def run_ours(args):
 def e2e_job(ens, specs, torch, device):
     """The whole job through the public batch API: per-peak noise fields start in pinned host
     memory, are copied to the device, turned into particles (device IC), then every step runs
-    and its per-peak statistics are read back to the host."""
+    with its per-peak statistics read back to the host, and at the end every peak's final
+    density grid comes back to the host (the job's result)."""
+    import ctypes
+
     import numpy as np
+
+    from pbh_b200 import _lib
     noises = []
     for s in specs:
         h = torch.empty((s.N,) * 3, dtype=torch.float64).pin_memory()
@@ -368,15 +475,20 @@ def e2e_job(ens, specs, torch, device):
     for _ in range(steps + 2):                   # prime + steps + closing kick
         ens.step(1)
         st = ens.stats()
-        stats_bytes += len(st) * 32
+        stats_bytes += len(st) * ctypes.sizeof(_lib.StatsInfo)
         done += 1
+    finals = ens.deltas()                        # the job's result: every peak's final delta
     torch.cuda.synchronize()
     t = time.perf_counter() - t0
     del noises
+    result_bytes = sum(int(f.nbytes) for f in finals)
+    assert all(np.isfinite(f).all() for f in finals)
     ps = sum(s.n for s in specs) * steps
-    return {"value": ps / t, "unit": UNIT, "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step": stats_bytes / done,
-            "job_steps": steps, "seconds": t,
-            "how": "public Ensemble API: pinned host noise -> device IC -> all steps, per-step stats to host; wall clock"}
+    return {"value": ps / t, "unit": UNIT, "h2d_bytes_per_step": h2d / steps,
+            "d2h_bytes_per_step": (stats_bytes + result_bytes) / steps,
+            "job_steps": steps, "seconds": t, "result_bytes": result_bytes,
+            "how": "public Ensemble API: pinned host noise -> device IC -> all steps with per-step stats to the "
+                   "host -> every peak's final delta to the host; wall clock"}
 
 
 def served_stream(args, device, tiles=None):

@@ -129,10 +129,43 @@ int pm_get_delta(pm_engine* e, int peak, float* delta);
 int pm_get_counts(pm_engine* e, int peak, double* counts);
 /* Collapse time tracking: the first a at which max delta of the peak's deposit reaches
  * delta_collapse is recorded on the device (pm_clock_info.a_collapse); <= 0 disables.  With
- * stop != 0 the run ends there (the peak finalizes and goes idle). */
+ * stop != 0 the run ends there: the step on which the crossing is detected (the one after the
+ * deposit that crossed) completes, the next applies its closing kick, and the peak goes idle at
+ * the a that step reached. */
 int pm_set_collapse_threshold(pm_engine* e, int peak, double delta_collapse, int stop);
-/* Free a peak's slot: it goes idle, its mesh is no longer transformed (dynamic mode). */
+/* Free a peak's slot: it goes idle, its mesh is no longer transformed (dynamic mode).  Ordered
+ * on the engine's stream after the work queued so far; returns without waiting. */
 int pm_release(pm_engine* e, int peak);
+
+/* Entry points of a request loop that never waits on the device between steps (the served form
+ * of north_star; no counterpart in pm3d.py, whose driver runs one peak at a time,
+ * pbhgr/scripts/pm3d_peak.py:24-33).  Each is ordered on the engine's stream and returns without
+ * waiting.
+ *
+ * pm_load_peak: pm_set_particles plus pm_set_collapse_threshold in one call, after the engine's
+ * stream has waited for wait_event (a cudaEvent_t recorded where x and p were produced, or NULL).
+ * x and p must stay valid until the engine's stream has passed this point (record an event on
+ * pm_engine_stream after the call). */
+int pm_load_peak(pm_engine* e, int peak, const double* x, const double* p, double a0, int mode, double param,
+                 double a_end, int max_steps, double delta_collapse, int stop, void* wait_event);
+/* pm_snapshot: queue a copy of every peak's clock and statistics, as they stand after the work
+ * queued so far, into the engine's host buffer `slot` (0 or 1).  pm_snapshot_read decodes that
+ * buffer into host arrays of npeaks entries (either may be NULL) as pm_get_clocks_all and
+ * pm_get_stats_all would: with wait = 0 it returns 1 at once if the copy has not finished,
+ * with wait != 0 it waits for the copy (only); 0 once decoded. */
+int pm_snapshot(pm_engine* e, int slot);
+int pm_snapshot_read(pm_engine* e, int slot, int wait, pm_clock_info* clocks, pm_stats_info* stats);
+/* pm_get_delta without waiting: the N^3 float32 delta of the peak's last deposit into dst
+ * (device memory, or page-locked host memory for a direct copy to the host). */
+int pm_get_delta_async(pm_engine* e, int peak, void* dst);
+
+/* Test hook of the failure path: from the next sort on, the look-back words of the first tile
+ * of `peak`'s segment are never published in the first digit pass, so the bounded wait of the
+ * tile after it runs out after spin_limit polls; the sort then proceeds with that tile counted
+ * as empty (every write stays inside the peak's range, the peak's result is wrong) and the
+ * peak's status gets bit 1.  peak < 0 or spin_limit <= 0 restores the normal sort.  The peak
+ * needs more than one sort tile (2048 particles); synchronizes the engine's stream. */
+int pm_debug_sort_stall(pm_engine* e, int peak, int spin_limit);
 int pm_get_clock(pm_engine* e, int peak, pm_clock_info* out);   /* host struct */
 int pm_get_stats(pm_engine* e, int peak, pm_stats_info* out);   /* host struct */
 /* All peaks at once (host arrays of npeaks); the return value counts flagged peaks. */
@@ -164,8 +197,14 @@ typedef struct {
                                    * device (Philox4x32-10 + Box-Muller) instead of numpy's stream */
 } pm_ic_params;
 int pm_make_ic(const pm_ic_params* prm, double* x_out, double* p_out, double* delta_lin_out, double* noise_rms_out);
-/* pm_make_ic keeps its float64 work buffers and cuFFT plans per (device, N) after the first call;
- * this frees them. */
+/* pm_make_ic for the recipe peak (kind 1, noise from a device array or noise_seed) ordered on
+ * `stream` (a cudaStream_t): returns without waiting, allocates nothing after its first call
+ * for a mesh size (its work area is separate from pm_make_ic's), and reports no noise rms.  The
+ * same inputs give the same bits as pm_make_ic.  Calls for one mesh size share the work area:
+ * issue them on one stream.  kind 0 returns -2003. */
+int pm_make_ic_async(const pm_ic_params* prm, double* x_out, double* p_out, void* stream);
+/* pm_make_ic and pm_make_ic_async keep their float64 work buffers and cuFFT plans per (device,
+ * N) after the first call; this frees them. */
 int pm_ic_release_cache(void);
 
 /* Stateless helpers. */

@@ -65,9 +65,16 @@ _SIGS = {
     "pm_get_counts": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "pm_set_collapse_threshold": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int]),
     "pm_release": (C.c_int, [C.c_void_p, C.c_int]),
+    "pm_load_peak": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_int, C.c_double,
+                               C.c_double, C.c_int, C.c_double, C.c_int, C.c_void_p]),
+    "pm_snapshot": (C.c_int, [C.c_void_p, C.c_int]),
+    "pm_snapshot_read": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
+    "pm_get_delta_async": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "pm_debug_sort_stall": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "pm_get_clock": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(ClockInfo)]),
     "pm_get_stats": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(StatsInfo)]),
     "pm_make_ic": (C.c_int, [C.POINTER(ICParams), C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]),
+    "pm_make_ic_async": (C.c_int, [C.POINTER(ICParams), C.c_void_p, C.c_void_p, C.c_void_p]),
     "pm_rell_keys": (C.c_int, [C.c_int, C.c_double, C.c_void_p, C.c_void_p]),
     "pm_analyse_partials": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_int, C.c_void_p]),

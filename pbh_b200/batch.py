@@ -61,6 +61,20 @@ class Ensemble:
         _lib.check(rc, "pm_get_stats_all")
         return list(arr)
 
+    def deltas(self):
+        """Every peak's density contrast of its last deposit (N^3 float32) on the host: one
+        asynchronous copy per peak into page-locked memory behind the engine's work, then one
+        wait.  Returns a list of numpy arrays (views of the page-locked buffers)."""
+        torch = _lib.require_cuda()
+        lib = _lib.load()
+        outs = []
+        for i, s in enumerate(self.specs):
+            buf = torch.empty((s.N,) * 3, dtype=torch.float32, pin_memory=True)
+            _lib.check(lib.pm_get_delta_async(self.engine._h, i, buf.data_ptr()), "pm_get_delta_async")
+            outs.append(buf)
+        self.engine.sync()
+        return [b.numpy() for b in outs]
+
     def active_particles(self) -> int:
         return int(sum(n for n, c in zip(self.n, self.clocks()) if c.state == _lib.STATE_RUN))
 

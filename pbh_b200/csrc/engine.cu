@@ -98,6 +98,16 @@ struct pm_engine {
   bool prime_pending = false;  // a peak was (re)loaded: the next step must include the priming sort
   std::vector<char> occupied;  // host view: slots holding a run (dynamic mode FFT extents)
   long long bytes = 0;
+  int* sort_dbg = nullptr;     // device {spin limit, silent tile} of the sort plan (test hook)
+  // Host snapshots of the clocks and statistics (pm_snapshot): two pinned buffers, each with the
+  // event recorded after its copy.
+  struct Snapshot {
+    PeakClock* clocks = nullptr;
+    PeakStats* stats = nullptr;
+    int* err = nullptr;
+    cudaEvent_t done = nullptr;
+    bool queued = false;
+  } snap[2];
 
   StepArgs args() const {
     StepArgs A{};
@@ -134,6 +144,7 @@ struct pm_engine {
     A.totals = totals;
     A.face = face;
     A.halo = halo;
+    A.sort_err = sort.err;
     return A;
   }
 
@@ -283,6 +294,13 @@ struct pm_engine {
       cudaFree(c.slot_peak);
     }
     sort_plan_destroy(&sort);
+    for (auto& sn : snap) {
+      if (sn.clocks) cudaFreeHost(sn.clocks);
+      if (sn.stats) cudaFreeHost(sn.stats);
+      if (sn.err) cudaFreeHost(sn.err);
+      if (sn.done) cudaEventDestroy(sn.done);
+    }
+    cudaFree(sort_dbg);
     void* bufs[] = {d_peaks, d_clocks, d_stats, d_st_base, d_p_base, d_mode_base, d_green_base, d_green_peak, epart,
                     wpart, eslice, ecount, pos, mom, tpos,
                     tmom, keys[0], keys[1], vals[0], vals[1], sstart[0], sstart[1], counts, lpre, far_count,
@@ -294,6 +312,8 @@ struct pm_engine {
 
 namespace {
 
+void fill_stats(const PeakDesc& P, const PeakStats& s, int sort_err, pm_stats_info* o);
+
 void fill_energy(const PeakStats& s, pm_stats_info* o) {
   o->energy_samples = (int)s.nsamples;
   o->a_energy = s.nsamples ? s.a_e : 0.0;
@@ -302,6 +322,27 @@ void fill_energy(const PeakStats& s, pm_stats_info* o) {
   o->potential = s.nsamples ? s.pot : 0.0;
   o->li_residual = s.nsamples ? s.a_e * (s.kin + s.pot) + s.li_int - s.li_e0 : 0.0;
   o->li_scale = s.nsamples ? s.a_e * (s.kin + fabs(s.pot)) : 0.0;
+}
+
+void fill_stats(const PeakDesc& P, const PeakStats& s, int sort_err, pm_stats_info* o) {
+  o->rho_max_over_mean = (double)s.max_fix / (double)PM_FIX_ONE / P.n_mean;
+  o->delta_max = o->rho_max_over_mean - 1.0;
+  o->mass_defect = (double)s.mass_defect / (double)PM_FIX_ONE;
+  o->status = s.status | (sort_err ? 2u : 0u);
+  fill_energy(s, o);
+}
+
+void fill_clock(const PeakClock& c, pm_clock_info* o) {
+  o->a = c.a;
+  o->da = c.da;
+  o->a_end = c.a_end;
+  o->kpend = c.kpend;
+  o->a_grid = c.a_grid;
+  o->mode = c.mode;
+  o->state = c.state;
+  o->nsteps = c.nsteps;
+  o->max_steps = c.max_steps;
+  o->a_collapse = c.a_collapse;
 }
 
 int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
@@ -531,6 +572,22 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   if ((r = sort_plan_create(&E->sort, segs.data(), npeaks, np, max_bits))) return r;
   E->sort.gate = E->sort_gate;
   E->bytes += (long long)E->sort.ntiles * 8 * (1LL << E->sort.bits);
+  if ((r = E->alloc(&E->sort_dbg, 2))) return r;
+  const int dbg0[2] = {SORT_SPIN_LIMIT, -1};
+  CU(cudaMemcpy(E->sort_dbg, dbg0, sizeof(dbg0), cudaMemcpyHostToDevice));
+  E->sort.dbg = E->sort_dbg;
+  // The sorted key and value buffers start defined, so a sort that fails can only leave
+  // values that were once valid for this engine behind.
+  for (int b = 0; b < 2; ++b) {
+    CU(cudaMemset(E->keys[b], 0, sizeof(u32) * E->ntot));
+    CU(cudaMemset(E->vals[b], 0, sizeof(u32) * E->ntot));
+  }
+  for (auto& sn : E->snap) {
+    CU(cudaMallocHost((void**)&sn.clocks, sizeof(PeakClock) * npeaks));
+    CU(cudaMallocHost((void**)&sn.stats, sizeof(PeakStats) * npeaks));
+    CU(cudaMallocHost((void**)&sn.err, sizeof(int) * npeaks));
+    CU(cudaEventCreateWithFlags(&sn.done, cudaEventDisableTiming));
+  }
   E->sort_result = np & 1;
   CU(cudaDeviceSynchronize());
   return 0;
@@ -584,7 +641,7 @@ int pm_set_particles(pm_engine* e, int peak, const double* x, const double* p, d
   if (!(a0 > 0) || mode < 0 || mode > 2) return -2001;
   CU(cudaSetDevice(e->device));
   const StepArgs A = e->args();
-  launch_reset_peak(A, peak, a0, mode, param, a_end, max_steps, e->stream);
+  launch_reset_peak(A, peak, a0, mode, param, a_end, max_steps, 0, 0.0, 0, e->stream);
   e->prime_pending = true;
   launch_set_particles(A, peak, e->peaks[peak], x, p, e->stream);
   e->occupied[peak] = 1;
@@ -631,18 +688,13 @@ int pm_get_stats_all(pm_engine* e, pm_stats_info* out) {
   if (!e || !out) return -2000;
   CU(cudaSetDevice(e->device));
   std::vector<PeakStats> s(e->npeaks);
-  int err = 0;
+  std::vector<int> err(e->npeaks);
   CU(cudaMemcpyAsync(s.data(), e->d_stats, sizeof(PeakStats) * e->npeaks, cudaMemcpyDeviceToHost, e->stream));
-  CU(cudaMemcpyAsync(&err, e->sort.err, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+  CU(cudaMemcpyAsync(err.data(), e->sort.err, sizeof(int) * e->npeaks, cudaMemcpyDeviceToHost, e->stream));
   CU(cudaStreamSynchronize(e->stream));
   int flagged = 0;
   for (int i = 0; i < e->npeaks; ++i) {
-    const PeakDesc& P = e->peaks[i];
-    out[i].rho_max_over_mean = (double)s[i].max_fix / (double)PM_FIX_ONE / P.n_mean;
-    out[i].delta_max = out[i].rho_max_over_mean - 1.0;
-    out[i].mass_defect = (double)s[i].mass_defect / (double)PM_FIX_ONE;
-    out[i].status = s[i].status | (err ? 2u : 0u);
-    fill_energy(s[i], &out[i]);
+    fill_stats(e->peaks[i], s[i], err[i], &out[i]);
     flagged += out[i].status != 0;
   }
   return flagged;
@@ -654,18 +706,7 @@ int pm_get_clocks_all(pm_engine* e, pm_clock_info* out) {
   std::vector<PeakClock> c(e->npeaks);
   CU(cudaMemcpyAsync(c.data(), e->d_clocks, sizeof(PeakClock) * e->npeaks, cudaMemcpyDeviceToHost, e->stream));
   CU(cudaStreamSynchronize(e->stream));
-  for (int i = 0; i < e->npeaks; ++i) {
-    out[i].a = c[i].a;
-    out[i].da = c[i].da;
-    out[i].a_end = c[i].a_end;
-    out[i].kpend = c[i].kpend;
-    out[i].a_grid = c[i].a_grid;
-    out[i].mode = c[i].mode;
-    out[i].state = c[i].state;
-    out[i].nsteps = c[i].nsteps;
-    out[i].max_steps = c[i].max_steps;
-    out[i].a_collapse = c[i].a_collapse;
-  }
+  for (int i = 0; i < e->npeaks; ++i) fill_clock(c[i], &out[i]);
   return 0;
 }
 
@@ -769,15 +810,80 @@ int pm_set_collapse_threshold(pm_engine* e, int peak, double delta_collapse, int
 int pm_release(pm_engine* e, int peak) {
   if (!e || peak < 0 || peak >= e->npeaks) return -2000;
   CU(cudaSetDevice(e->device));
-  PeakClock c;
-  int r;
-  if ((r = e->read_clock(peak, &c))) return r;
-  c.state = PS_IDLE;
-  c.has_delta = 0;
-  c.dep = 0;
-  c.kpend = 0.0;
-  if ((r = e->write_clock(peak, c))) return r;
+  launch_release_peak(e->args(), peak, e->stream);
+  CU(cudaGetLastError());
   e->occupied[peak] = 0;
+  return 0;
+}
+
+int pm_load_peak(pm_engine* e, int peak, const double* x, const double* p, double a0, int mode, double param,
+                 double a_end, int max_steps, double delta_collapse, int stop, void* wait_event) {
+  if (!e || peak < 0 || peak >= e->npeaks || !x || !p) return -2000;
+  if (!(a0 > 0) || mode < 0 || mode > 2) return -2001;
+  CU(cudaSetDevice(e->device));
+  if (wait_event) CU(cudaStreamWaitEvent(e->stream, (cudaEvent_t)wait_event, 0));
+  const StepArgs A = e->args();
+  launch_reset_peak(A, peak, a0, mode, param, a_end, max_steps, 1, delta_collapse, stop, e->stream);
+  launch_set_particles(A, peak, e->peaks[peak], x, p, e->stream);
+  CU(cudaGetLastError());
+  e->prime_pending = true;
+  e->occupied[peak] = 1;
+  return 0;
+}
+
+int pm_snapshot(pm_engine* e, int slot) {
+  if (!e || slot < 0 || slot > 1) return -2000;
+  CU(cudaSetDevice(e->device));
+  auto& sn = e->snap[slot];
+  const int n = e->npeaks;
+  CU(cudaMemcpyAsync(sn.clocks, e->d_clocks, sizeof(PeakClock) * n, cudaMemcpyDeviceToHost, e->stream));
+  CU(cudaMemcpyAsync(sn.stats, e->d_stats, sizeof(PeakStats) * n, cudaMemcpyDeviceToHost, e->stream));
+  CU(cudaMemcpyAsync(sn.err, e->sort.err, sizeof(int) * n, cudaMemcpyDeviceToHost, e->stream));
+  CU(cudaEventRecord(sn.done, e->stream));
+  sn.queued = true;
+  return 0;
+}
+
+int pm_snapshot_read(pm_engine* e, int slot, int wait, pm_clock_info* clocks, pm_stats_info* stats) {
+  if (!e || slot < 0 || slot > 1) return -2000;
+  auto& sn = e->snap[slot];
+  if (!sn.queued) return -2001;
+  CU(cudaSetDevice(e->device));
+  if (!wait) {
+    const cudaError_t q = cudaEventQuery(sn.done);
+    if (q == cudaErrorNotReady) return 1;
+    if (q != cudaSuccess) return -(int)q;
+  } else {
+    CU(cudaEventSynchronize(sn.done));
+  }
+  for (int i = 0; i < e->npeaks; ++i) {
+    if (clocks) fill_clock(sn.clocks[i], &clocks[i]);
+    if (stats) fill_stats(e->peaks[i], sn.stats[i], sn.err[i], &stats[i]);
+  }
+  return 0;
+}
+
+int pm_get_delta_async(pm_engine* e, int peak, void* dst) {
+  if (!e || peak < 0 || peak >= e->npeaks || !dst) return -2000;
+  CU(cudaSetDevice(e->device));
+  const PeakDesc& P = e->peaks[peak];
+  CU(cudaMemcpyAsync(dst, P.delta, sizeof(float) * (size_t)P.N * P.N * P.N, cudaMemcpyDefault, e->stream));
+  return 0;
+}
+
+int pm_debug_sort_stall(pm_engine* e, int peak, int spin_limit) {
+  if (!e || peak >= e->npeaks) return -2000;
+  CU(cudaSetDevice(e->device));
+  int v[2] = {SORT_SPIN_LIMIT, -1};
+  if (peak >= 0 && spin_limit > 0) {
+    long long tile = 0;  // the first tile of the peak's segment (segments in peak order)
+    for (int i = 0; i < peak; ++i) tile += (e->peaks[i].n + SORT_TILE - 1) / SORT_TILE;
+    if (e->peaks[peak].n <= SORT_TILE) return -2001;  // no successor tile waits on the first one
+    v[0] = spin_limit;
+    v[1] = (int)tile;
+  }
+  CU(cudaMemcpyAsync(e->sort_dbg, v, sizeof(v), cudaMemcpyHostToDevice, e->stream));
+  CU(cudaStreamSynchronize(e->stream));
   return 0;
 }
 
@@ -787,16 +893,7 @@ int pm_get_clock(pm_engine* e, int peak, pm_clock_info* out) {
   PeakClock c;
   int r = e->read_clock(peak, &c);
   if (r) return r;
-  out->a = c.a;
-  out->da = c.da;
-  out->a_end = c.a_end;
-  out->kpend = c.kpend;
-  out->a_grid = c.a_grid;
-  out->mode = c.mode;
-  out->state = c.state;
-  out->nsteps = c.nsteps;
-  out->max_steps = c.max_steps;
-  out->a_collapse = c.a_collapse;
+  fill_clock(c, out);
   return 0;
 }
 
@@ -806,14 +903,9 @@ int pm_get_stats(pm_engine* e, int peak, pm_stats_info* out) {
   PeakStats s;
   int err = 0;
   CU(cudaMemcpyAsync(&s, e->d_stats + peak, sizeof(PeakStats), cudaMemcpyDeviceToHost, e->stream));
-  CU(cudaMemcpyAsync(&err, e->sort.err, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+  CU(cudaMemcpyAsync(&err, e->sort.err + peak, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
   CU(cudaStreamSynchronize(e->stream));
-  const PeakDesc& P = e->peaks[peak];
-  out->rho_max_over_mean = (double)s.max_fix / (double)PM_FIX_ONE / P.n_mean;
-  out->delta_max = out->rho_max_over_mean - 1.0;
-  out->mass_defect = (double)s.mass_defect / (double)PM_FIX_ONE;
-  out->status = s.status | (err ? 2u : 0u);
-  fill_energy(s, out);
+  fill_stats(e->peaks[peak], s, err, out);
   return (int)(out->status != 0);
 }
 

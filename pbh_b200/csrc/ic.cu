@@ -7,6 +7,7 @@
 #include <cmath>
 #include <map>
 #include <mutex>
+#include <tuple>
 #include <utility>
 #include <vector>
 
@@ -131,10 +132,14 @@ __global__ void k_philox_normal(double* __restrict__ out, long long n, unsigned 
     if (4 * q + k < n) out[4 * q + k] = z[k];
 }
 
-__global__ void k_axpy_spec(cufftDoubleComplex* __restrict__ y, const cufftDoubleComplex* __restrict__ x, double a,
-                            long long M) {
+// y += a x with a = 1 (kind 0: make_ic's tail noise is already at its amplitude) or
+// a = noise_frac * amp / rms (kind 1: the recipe's noise scaled to noise_frac of the peak), rms
+// read from stat[1] on the device.
+__global__ void k_axpy_spec(cufftDoubleComplex* __restrict__ y, const cufftDoubleComplex* __restrict__ x,
+                            const double* __restrict__ stat, int kind, double noise_frac, double amp, long long M) {
   const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= M) return;
+  const double a = kind == 0 ? 1.0 : noise_frac * amp / stat[1];
   y[m].x += a * x[m].x;
   y[m].y += a * x[m].y;
 }
@@ -233,8 +238,11 @@ __global__ void k_lattice(int N, int Np, double L, const double* __restrict__ ps
 }
 
 // Block partial sums of x and (x - mean)^2 for numpy's std (mean first, then the spread).
-__global__ void k_partial(const double* __restrict__ v, long long n, double mean, int squares, double* __restrict__ part) {
+// Block partials of sum v (squares = 0) or of sum (v - stat[0])^2 (squares = 1).
+__global__ void k_partial(const double* __restrict__ v, long long n, const double* __restrict__ stat, int squares,
+                          double* __restrict__ part) {
   __shared__ double sh[kThreads];
+  const double mean = squares ? stat[0] : 0.0;
   double s = 0.0;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const double d = squares ? v[i] - mean : v[i];
@@ -249,24 +257,24 @@ __global__ void k_partial(const double* __restrict__ v, long long n, double mean
   if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
 }
 
-int grid_std(const double* v, long long n, double* out) {
-  const int nb = 1024;
-  double* part = nullptr;
-  std::vector<double> h(nb);
-  double mean = 0.0, var = 0.0;
-  int rc = 0;
-  CU(cudaMalloc(&part, sizeof(double) * nb));
-  k_partial<<<nb, kThreads>>>(v, n, 0.0, 0, part);
-  CU(cudaMemcpy(h.data(), part, sizeof(double) * nb, cudaMemcpyDeviceToHost));
-  for (double d : h) mean += d;
-  mean /= (double)n;
-  k_partial<<<nb, kThreads>>>(v, n, mean, 1, part);
-  CU(cudaMemcpy(h.data(), part, sizeof(double) * nb, cudaMemcpyDeviceToHost));
-  for (double d : h) var += d;
-  *out = std::sqrt(var / (double)n);
-done:
-  cudaFree(part);
-  return rc;
+// The partials summed in block order by one thread: stat[0] = mean (squares = 0), or stat[1] =
+// rms / N3 of the unnormalised inverse transform (squares = 1), the noise field's rms.
+__global__ void k_reduce_partials(const double* __restrict__ part, int nb, long long n, long long N3, int squares,
+                                  double* __restrict__ stat) {
+  double t = 0.0;
+  for (int b = 0; b < nb; ++b) t += part[b];
+  if (!squares) stat[0] = t / (double)n;
+  else stat[1] = sqrt(t / (double)n) / (double)N3;
+}
+
+constexpr int kStdBlocks = 1024;
+
+// Standard deviation of v (two passes, fixed order) into stat[1], divided by N3; on stream s.
+void grid_std(const double* v, long long n, long long N3, double* part, double* stat, cudaStream_t s) {
+  k_partial<<<kStdBlocks, kThreads, 0, s>>>(v, n, stat, 0, part);
+  k_reduce_partials<<<1, 1, 0, s>>>(part, kStdBlocks, n, N3, 0, stat);
+  k_partial<<<kStdBlocks, kThreads, 0, s>>>(v, n, stat, 1, part);
+  k_reduce_partials<<<1, 1, 0, s>>>(part, kStdBlocks, n, N3, 1, stat);
 }
 
 unsigned nblk(long long n) { return (unsigned)((n + kThreads - 1) / kThreads); }
@@ -276,15 +284,18 @@ unsigned nblk(long long n) { return (unsigned)((n + kThreads - 1) / kThreads); }
 struct ICWork {
   double *field = nullptr, *real4 = nullptr, *tmp_real = nullptr, *noise = nullptr;
   cufftDoubleComplex *spec = nullptr, *nspec = nullptr, *spec4 = nullptr, *tmp_spec = nullptr;
+  double* part = nullptr;  // kStdBlocks partials, then stat[2] (mean, noise rms)
   cufftHandle d2z = 0, z2d = 0, z2d4 = 0;
   bool ok = false;
 };
 std::mutex g_ic_mu;
-std::map<std::pair<int, int>, ICWork> g_ic;
+// Keyed by (device, N, path): the synchronous pm_make_ic and the stream-ordered
+// pm_make_ic_async keep separate work areas, so the two never share buffers in flight.
+std::map<std::tuple<int, int, int>, ICWork> g_ic;
 
-int ic_work(int device, int N, ICWork** out) {
+int ic_work(int device, int N, int path, ICWork** out) {
   std::lock_guard<std::mutex> lock(g_ic_mu);
-  ICWork& w = g_ic[{device, N}];
+  ICWork& w = g_ic[{device, N, path}];
   if (!w.ok) {
     const long long N3 = (long long)N * N * N, M = (long long)N * N * (N / 2 + 1);
     int rc = 0;
@@ -297,13 +308,14 @@ int ic_work(int device, int N, ICWork** out) {
     CU(cudaMalloc(&w.nspec, sizeof(cufftDoubleComplex) * M));
     CU(cudaMalloc(&w.spec4, sizeof(cufftDoubleComplex) * 4 * M));
     CU(cudaMalloc(&w.tmp_spec, sizeof(cufftDoubleComplex) * M));
+    CU(cudaMalloc(&w.part, sizeof(double) * (kStdBlocks + 2)));
     CF(cufftPlan3d(&w.d2z, N, N, N, CUFFT_D2Z));
     CF(cufftPlan3d(&w.z2d, N, N, N, CUFFT_Z2D));
     CF(cufftPlanMany(&w.z2d4, 3, n3, nullptr, 1, 0, nullptr, 1, 0, CUFFT_Z2D, 4));
     w.ok = true;
   done:
     if (rc) {
-      g_ic.erase({device, N});
+      g_ic.erase({device, N, path});
       return rc;
     }
   }
@@ -317,7 +329,7 @@ extern "C" int pm_ic_release_cache(void) {
   std::lock_guard<std::mutex> lock(g_ic_mu);
   for (auto& kv : g_ic) {
     ICWork& w = kv.second;
-    cudaSetDevice(kv.first.first);
+    cudaSetDevice(std::get<0>(kv.first));
     cudaFree(w.field);
     cudaFree(w.real4);
     cudaFree(w.tmp_real);
@@ -326,6 +338,7 @@ extern "C" int pm_ic_release_cache(void) {
     cudaFree(w.nspec);
     cudaFree(w.spec4);
     cudaFree(w.tmp_spec);
+    cudaFree(w.part);
     if (w.ok) {
       cufftDestroy(w.d2z);
       cufftDestroy(w.z2d);
@@ -336,23 +349,72 @@ extern "C" int pm_ic_release_cache(void) {
   return 0;
 }
 
-extern "C" int pm_make_ic(const pm_ic_params* prm, double* x_out, double* p_out, double* delta_lin_out,
-                          double* noise_rms_out) {
+namespace {
+
+int check_params(const pm_ic_params* prm, const double* x_out, const double* p_out) {
   if (!prm || !x_out || !p_out) return -2000;
   const int N = prm->N, Np = prm->Np;
   if (N < 4 || (N & (N - 1)) || Np < 1 || !(prm->L > 0)) return -2001;
   if (prm->kind == 0 && (!prm->spline_x || !prm->spline_c || prm->spline_m < 1)) return -2002;
   if (prm->kind != 0 && prm->kind != 1) return -2003;
+  return 0;
+}
+
+// The IC pipeline on stream s with work area w (spline arrays xs, cs on the device for kind 0).
+// The noise rms is left in w->part[kStdBlocks + 1].
+int make_ic_on(const pm_ic_params* prm, double* x_out, double* p_out, double* delta_lin_out, const double* xs,
+               const double* cs, ICWork* w, cudaStream_t s) {
+  const int N = prm->N, Np = prm->Np;
   const long long N3 = (long long)N * N * N, M = (long long)N * N * (N / 2 + 1);
   const double L = prm->L;
-  int rc = 0, device = 0;
-  double *xs = nullptr, *cs = nullptr;
-  double noise_rms = 0.0;
+  int rc = 0;
+  double* stat = w->part + kStdBlocks;
   const bool want_noise = (prm->kind == 0 && prm->tail_rms > 0) || (prm->kind == 1 && prm->noise_frac > 0);
   const bool noisy = want_noise && (prm->noise || prm->noise_seed);
+  CF(cufftSetStream(w->d2z, s));
+  CF(cufftSetStream(w->z2d, s));
+  CF(cufftSetStream(w->z2d4, s));
+  CU(cudaMemsetAsync(stat, 0, sizeof(double) * 2, s));
+  k_field<<<nblk(N3), kThreads, 0, s>>>(N, L, prm->kind, prm->amp, prm->axes[0], prm->axes[1], prm->axes[2], xs, cs,
+                                        prm->kind == 0 ? prm->spline_m : 0, w->field);
+  CU(cudaGetLastError());
+  CF(cufftExecD2Z(w->d2z, w->field, w->spec));
+  if (noisy) {
+    if (!prm->noise) {  // seeded device noise
+      k_philox_normal<<<nblk((N3 + 3) / 4), kThreads, 0, s>>>(w->noise, N3, prm->noise_seed);
+      CU(cudaGetLastError());
+    }
+    CF(cufftExecD2Z(w->d2z, prm->noise ? (double*)prm->noise : w->noise, w->nspec));
+    k_shape<<<nblk(M), kThreads, 0, s>>>(w->nspec, N, L, prm->kind, prm->tail_rms, prm->k1, prm->k2);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(w->tmp_spec, w->nspec, sizeof(cufftDoubleComplex) * M, cudaMemcpyDeviceToDevice, s));
+    CF(cufftExecZ2D(w->z2d, w->tmp_spec, w->tmp_real));  // unnormalised inverse; numpy divides by N^3
+    grid_std(w->tmp_real, N3, N3, w->part, stat, s);
+    k_axpy_spec<<<nblk(M), kThreads, 0, s>>>(w->spec, w->nspec, stat, prm->kind, prm->noise_frac, prm->amp, M);
+    CU(cudaGetLastError());
+  }
+  k_disp_spectra<<<nblk(M), kThreads, 0, s>>>(w->spec, N, L, prm->kind, w->spec4);
+  CU(cudaGetLastError());
+  CF(cufftExecZ2D(w->z2d4, w->spec4, w->real4));
+  k_lattice<<<nblk((long long)Np * Np * Np), kThreads, 0, s>>>(N, Np, L, w->real4, x_out, p_out);
+  CU(cudaGetLastError());
+  if (delta_lin_out)
+    CU(cudaMemcpyAsync(delta_lin_out, w->real4, sizeof(double) * N3, cudaMemcpyDeviceToDevice, s));
+done:
+  return rc;
+}
+
+}  // namespace
+
+extern "C" int pm_make_ic(const pm_ic_params* prm, double* x_out, double* p_out, double* delta_lin_out,
+                          double* noise_rms_out) {
+  if (int r = check_params(prm, x_out, p_out)) return r;
+  int rc = 0, device = 0;
+  double *xs = nullptr, *cs = nullptr;
+  double stat[2] = {0.0, 0.0};
   ICWork* w = nullptr;
   CU(cudaGetDevice(&device));
-  rc = ic_work(device, N, &w);
+  rc = ic_work(device, prm->N, 0, &w);
   if (rc) return rc;
   if (prm->kind == 0) {
     const int m = prm->spline_m;
@@ -361,37 +423,24 @@ extern "C" int pm_make_ic(const pm_ic_params* prm, double* x_out, double* p_out,
     CU(cudaMemcpy(xs, prm->spline_x, sizeof(double) * (m + 1), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(cs, prm->spline_c, sizeof(double) * 4 * m, cudaMemcpyHostToDevice));
   }
-  k_field<<<nblk(N3), kThreads>>>(N, L, prm->kind, prm->amp, prm->axes[0], prm->axes[1], prm->axes[2], xs, cs,
-                                  prm->kind == 0 ? prm->spline_m : 0, w->field);
-  CU(cudaGetLastError());
-  CF(cufftExecD2Z(w->d2z, w->field, w->spec));
-  if (noisy) {
-    if (!prm->noise) {  // seeded device noise
-      k_philox_normal<<<nblk((N3 + 3) / 4), kThreads>>>(w->noise, N3, prm->noise_seed);
-      CU(cudaGetLastError());
-    }
-    CF(cufftExecD2Z(w->d2z, prm->noise ? (double*)prm->noise : w->noise, w->nspec));
-    k_shape<<<nblk(M), kThreads>>>(w->nspec, N, L, prm->kind, prm->tail_rms, prm->k1, prm->k2);
-    CU(cudaGetLastError());
-    CU(cudaMemcpy(w->tmp_spec, w->nspec, sizeof(cufftDoubleComplex) * M, cudaMemcpyDeviceToDevice));
-    CF(cufftExecZ2D(w->z2d, w->tmp_spec, w->tmp_real));  // unnormalised inverse; numpy divides by N^3
-    rc = grid_std(w->tmp_real, N3, &noise_rms);
-    if (rc) goto done;
-    noise_rms /= (double)N3;
-    const double scale = prm->kind == 0 ? 1.0 : prm->noise_frac * prm->amp / noise_rms;
-    k_axpy_spec<<<nblk(M), kThreads>>>(w->spec, w->nspec, scale, M);
-    CU(cudaGetLastError());
-  }
-  k_disp_spectra<<<nblk(M), kThreads>>>(w->spec, N, L, prm->kind, w->spec4);
-  CU(cudaGetLastError());
-  CF(cufftExecZ2D(w->z2d4, w->spec4, w->real4));
-  k_lattice<<<nblk((long long)Np * Np * Np), kThreads>>>(N, Np, L, w->real4, x_out, p_out);
-  CU(cudaGetLastError());
-  if (delta_lin_out) CU(cudaMemcpy(delta_lin_out, w->real4, sizeof(double) * N3, cudaMemcpyDeviceToDevice));
+  rc = make_ic_on(prm, x_out, p_out, delta_lin_out, xs, cs, w, 0);
+  if (rc) goto done;
+  CU(cudaMemcpy(stat, w->part + kStdBlocks, sizeof(stat), cudaMemcpyDeviceToHost));
   CU(cudaDeviceSynchronize());
-  if (noise_rms_out) *noise_rms_out = noise_rms;
+  if (noise_rms_out) *noise_rms_out = stat[1];
 done:
   cudaFree(xs);
   cudaFree(cs);
   return rc;
+}
+
+extern "C" int pm_make_ic_async(const pm_ic_params* prm, double* x_out, double* p_out, void* stream) {
+  if (int r = check_params(prm, x_out, p_out)) return r;
+  if (prm->kind != 1) return -2003;  // the curvature-profile ICs copy a host spline: pm_make_ic
+  int device = 0;
+  const cudaError_t e = cudaGetDevice(&device);
+  if (e != cudaSuccess) return -(int)e;
+  ICWork* w = nullptr;
+  if (int r = ic_work(device, prm->N, 1, &w)) return r;
+  return make_ic_on(prm, x_out, p_out, nullptr, nullptr, nullptr, w, (cudaStream_t)stream);
 }

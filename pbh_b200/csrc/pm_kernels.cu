@@ -6,6 +6,12 @@
 
 #include "pm_kernels.cuh"
 
+// Segmented sums over same-cell runs in the deposit when a warp holds fewer than this many runs
+// (0: never; every particle then adds its own eight corners).
+#ifndef PM_DEP_SCAN
+#define PM_DEP_SCAN 24
+#endif
+
 namespace {
 
 constexpr double kTwoPi = 6.283185307179586476925286766559;
@@ -144,7 +150,8 @@ __device__ __forceinline__ void push_one(const StepArgs& A, const PeakDesc& P, c
     acc_e = t;
   }
   int nx = ix, ny = iy, nz = iz;
-  if (K.run) {
+  const bool finite = isfinite(px) && isfinite(py) && isfinite(pz);
+  if (K.run && finite) {  // a non-finite particle stays where it is (the peak is flagged below)
     px += K.kB * ax;
     py += K.kB * ay;
     pz += K.kB * az;
@@ -165,7 +172,7 @@ __device__ __forceinline__ void push_one(const StepArgs& A, const PeakDesc& P, c
     PM_DRIFT(fz, pz, nz)
 #undef PM_DRIFT
   }
-  bad |= !(isfinite(px) && isfinite(py) && isfinite(pz));
+  bad |= !(finite && isfinite(px) && isfinite(py) && isfinite(pz));
   const int cell = (nx << (2 * l2)) | (ny << l2) | nz;
   A.tpos[j] = make_int4(cell, __float_as_int(fx), __float_as_int(fy), __float_as_int(fz));
   A.tmom[j] = make_float4(px, py, pz, m.w);
@@ -293,12 +300,15 @@ __global__ void k_advance(StepArgs A) {
     PeakClock c = A.clocks[pk];
     const PeakDesc P = A.peaks[pk];
     int dep = 0;
-    // Collapse detection on the deposit of the current positions (made by the previous step).
+    // Collapse detection on the deposit made by the previous step, i.e. of the positions at c.a.
+    // This step's push has already moved a running peak on to c.a + c.da, so a stop takes
+    // effect after the step is booked below: the next step applies its closing kick and ends.
+    bool stop_now = false;
     if (c.has_delta && c.delta_collapse > 0 && c.a_collapse < 0 && c.state != PS_PRIME) {
       const double dmax = (double)A.stats[pk].max_fix / (double)PM_FIX_ONE / P.n_mean - 1.0;
       if (dmax >= c.delta_collapse) {
         c.a_collapse = c.a;
-        if (c.stop_on_collapse && c.state == PS_RUN) c.state = PS_FINALIZE;
+        stop_now = c.stop_on_collapse && c.state == PS_RUN;
       }
     }
     switch (c.state) {
@@ -331,6 +341,7 @@ __global__ void k_advance(StepArgs A) {
         } else {
           c.state = PS_HOLD;
         }
+        if (stop_now && c.state == PS_RUN) c.state = PS_FINALIZE;
         break;
       }
       case PS_FINALIZE:
@@ -455,6 +466,11 @@ __global__ void k_permute(StepArgs A, long long ntot) {
     const PeakClock C = A.clocks[pk];
     if (!(C.dep && C.sortstep)) continue;
     const u32 q = A.perm[j];
+    const PeakDesc& P = A.peaks[pk];
+    if ((long long)q < P.p_off || (long long)q >= P.p_off + P.n) {  // a failed sort: never read outside
+      atomicOr(&A.stats[pk].status, 2u);
+      continue;
+    }
     A.pos[j] = A.tpos[q];
     A.mom[j] = A.tmom[q];
   }
@@ -468,8 +484,12 @@ __global__ void k_st_starts(StepArgs A, long long ntot) {
     if (!(C.dep && C.sortstep)) continue;
     const PeakDesc P = A.peaks[pk];
     u32* ss = sst(A, C.sbuf) + P.sst_off;
-    const int b = (int)(A.keys_sorted[j] >> P.st_shift);
-    const int bprev = j == P.p_off ? -1 : (int)(A.keys_sorted[j - 1] >> P.st_shift);
+    // Super-tile of each sorted key; a key outside the peak's key range (a failed sort) is
+    // clamped, so no start is ever written outside the peak's table.
+    const u32 kb = A.keys_sorted[j] >> P.st_shift;
+    if (kb >= (u32)P.nst) atomicOr(&A.stats[pk].status, 2u);
+    const int b = (int)min(kb, (u32)(P.nst - 1));
+    const int bprev = j == P.p_off ? -1 : (int)min(A.keys_sorted[j - 1] >> P.st_shift, (u32)(P.nst - 1));
     for (int bb = bprev + 1; bb <= b; ++bb) ss[bb] = (u32)j;
     if (j == P.p_off + P.n - 1)
       for (int bb = b + 1; bb <= P.nst; ++bb) ss[bb] = (u32)(P.p_off + P.n);
@@ -765,25 +785,17 @@ __device__ __forceinline__ void face_coords(int f, int& lx, int& ly, int& lz) {
   }
 }
 
-// Finish the face nodes of super-tile Y (whole CTA of FIX_THREADS).  Adds to the caller's
-// statistics.
+// Finish the face nodes of super-tile Y (whole CTA of FIX_THREADS): each face node's own
+// partial plus the halo partials of the lower neighbours Y - o, o = (ox, oy, oz) in {0,1}^3 \ 0,
+// that reach it (node (lx + TS ox, ...) of the neighbour, which lies on its upper halo, for a
+// face node with (lx, ly, lz) zero where o is one).  nb[o]: the neighbours' halo partials.
+// Adds to the caller's statistics.
 template <int TS>
-__device__ __forceinline__ void fixup_faces(const StepArgs& A, const PeakDesc& P, u32 Y, double* rho64,
-                                            long long& dsum, long long& smax) {
+__device__ __forceinline__ void fixup_faces(const StepArgs& A, const PeakDesc& P, u32 Y, const long long* const* nb,
+                                            double* rho64, long long& dsum, long long& smax) {
   constexpr int FC = TS * TS * TS - (TS - 1) * (TS - 1) * (TS - 1);
-  constexpr int HC = (TS + 1) * (TS + 1) * (TS + 1) - TS * TS * TS;
-  // Halo partials of the lower neighbour Y - o, o = (ox, oy, oz) in {0,1}^3 \ 0, seen from Y's
-  // face node (lx, ly, lz) with (lx, ly, lz) zero where o is one: node (lx + TS ox, ...) of the
-  // neighbour, which lies on its upper halo.
-  __shared__ const long long* s_nb[8];
-  const int NS = P.NS, N = P.N;
+  const int N = P.N;
   const int sx = pm_compact3(Y >> 2), sy = pm_compact3(Y >> 1), sz = pm_compact3(Y);
-  if (threadIdx.x < 8) {
-    const int o = threadIdx.x, ox = o & 1, oy = (o >> 1) & 1, oz = (o >> 2) & 1;
-    const u32 sn = pm_morton3((sx - ox) & (NS - 1), (sy - oy) & (NS - 1), (sz - oz) & (NS - 1));
-    s_nb[o] = A.halo + P.halo_off + (long long)sn * HC;
-  }
-  __syncthreads();
   const long long* face = A.face + P.face_off + (long long)Y * FC;
   for (int f = threadIdx.x; f < FC; f += FIX_THREADS) {
     int lx, ly, lz;
@@ -791,7 +803,7 @@ __device__ __forceinline__ void fixup_faces(const StepArgs& A, const PeakDesc& P
     long long S = __ldcg(face + f);
     const int zmask = (lx == 0 ? 1 : 0) | (ly == 0 ? 2 : 0) | (lz == 0 ? 4 : 0);
     for (int o = zmask; o; o = (o - 1) & zmask) {  // non-empty subsets of zmask
-      S += __ldcg(s_nb[o] + halo_index(lx + TS * (o & 1), ly + TS * ((o >> 1) & 1), lz + TS * (o >> 2), TS));
+      S += __ldcg(nb[o] + halo_index(lx + TS * (o & 1), ly + TS * ((o >> 1) & 1), lz + TS * (o >> 2), TS));
     }
     const long long Dv = S - P.n_mean_fix;
     const long long node = ((long long)(sx * TS + lx) * N + (sy * TS + ly)) * N + (sz * TS + lz);
@@ -836,12 +848,27 @@ __device__ __noinline__ void fold_chunk(u64* acc64, u32* acc_hi, u32* acc_lo, bo
   }
 }
 
+// One corner weight W (a nearest integer of a product in units of 2^-38, 0 <= W < 2^39, see
+// fix_round) split for the two accumulator words: hi = W >> 19, lo = W & (2^19 - 1).  The FMA's
+// result has the bits 0x4330000000000000 + W, so hi is one funnel shift of its two words (the
+// exponent bits shift out of the 32-bit result) and lo one mask of the low word.
+struct Split {
+  u32 hi, lo;
+};
+__device__ __forceinline__ Split fix_split(double a, double b) {
+  const double r = fma(a, b, 4503599627370496.0);
+  const u32 wl = (u32)__double2loint(r), wh = (u32)__double2hiint(r);
+  return Split{__funnelshift_r(wl, wh, 19), wl & 0x7FFFFu};
+}
+
 template <int TS>
 __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc& P, const PeakClock& C, int pk,
                                               u32 st, u32* smem, double* rho64) {
   constexpr int T1 = TS + 1, NN = T1 * T1 * T1;
   constexpr int RS = patch_rs(TS), PS = patch_ps(TS), SZ = patch_size(TS);
-  constexpr int NPT = (NN + DEP_THREADS - 1) / DEP_THREADS;  // nodes per thread
+  constexpr int NG = TS / 4 + 1;        // 4-node groups per patch row (the last holds the upper halo node)
+  constexpr int FC = TS * TS * TS - (TS - 1) * (TS - 1) * (TS - 1);
+  static_assert(RS % 4 == 0 && PS % 4 == 0 && RS >= 4 * NG, "patch rows are read 16 bytes at a time");
   u32* acc_hi = smem;
   u32* acc_lo = smem + SZ;
   __shared__ long long s_red[DEP_THREADS / 32];
@@ -854,6 +881,10 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
   const u32* ss = sst(A, C.sbuf) + P.sst_off;
   const long long b = ss[st], e = ss[st + 1];
   const long long total = e - b;
+  // A cell index belongs to this super-tile iff its bits outside the local ones equal the
+  // super-tile's: one mask and one compare (negative or out-of-mesh values never match).
+  const int local = ((TS - 1) << (2 * l2)) | ((TS - 1) << l2) | (TS - 1);
+  const int tile_bits = ((sx * TS) << (2 * l2)) | ((sy * TS) << l2) | (sz * TS);
   __syncthreads();
   const u32 le = lanemask_le();
   // Nodes' sums of the chunks folded so far, only for a super-tile of more than one chunk: kept
@@ -861,8 +892,8 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
   // than one chunk of 16-byte entries holds the NN 8-byte sums several times over).
   static_assert((8191 / DEP_THREADS) * DEP_THREADS * sizeof(int4) >= NN * sizeof(u64), "fold scratch too small");
   bool folded = false;
-  // Split accumulators.  A weight W (at most 2^38, at least -3 for a remainder corner) goes in as
-  // hi = W >> 19 in [-1, 2^19] and lo = W & (2^19 - 1).  A node takes at most one contribution
+  // Split accumulators.  A weight W (at most 2^38, at least -3 for the remainder corner) goes in
+  // as hi = W >> 19 in [-1, 2^19] and lo = W & (2^19 - 1).  A node takes at most one contribution
   // per particle of a chunk, so with CHUNK <= 8191 the low sums stay below 2^32 and the high
   // sums lie in [-CHUNK, CHUNK * 2^19], an interval shorter than 2^32 - 8192: kept modulo 2^32
   // in a u32, a value at or above 2^32 - 8192 is the negative one.  Both are exact.  A typical
@@ -872,79 +903,63 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
   static_assert(PM_FIX_BITS == 38, "the split accumulators assume 38 fractional bits");
   const long long nit = (total + DEP_THREADS - 1) / DEP_THREADS;
   long long j = b + threadIdx.x;
-  // Three sweeps' particles in flight.
-  const int4 none = make_int4(-1, 0, 0, 0);
-  int4 pa = j < e ? A.pos[j] : none;
-  int4 pb = j + DEP_THREADS < e ? A.pos[j + DEP_THREADS] : none;
-  int4 pc = j + 2 * DEP_THREADS < e ? A.pos[j + 2 * DEP_THREADS] : none;
+  int4 pn = j < e ? A.pos[j] : make_int4(-1, 0, 0, 0);  // the next sweep's particle, in flight
   bool bad = false;
   int left = CH_IT;
   for (long long it = 0; it < nit; ++it) {
-    const int4 ps = pa;
+    const int4 ps = pn;
     const bool valid = j < e;
-    pa = pb;
-    pb = pc;
-    if (j + 3 * DEP_THREADS < e) pc = A.pos[j + 3 * DEP_THREADS];
+    if (j + DEP_THREADS < e) pn = A.pos[j + DEP_THREADS];
     j += DEP_THREADS;
     {
-      const int ix = ps.x >> (2 * l2), iy = (ps.x >> l2) & (N - 1), iz = ps.x & (N - 1);
-      const int lx = ix - sx * TS, ly = iy - sy * TS, lz = iz - sz * TS;
-      const bool in = valid && (unsigned)lx < (unsigned)TS && (unsigned)ly < (unsigned)TS && (unsigned)lz < (unsigned)TS;
+      const int c = ps.x;
+      const bool in = valid && (c & ~local) == tile_bits;
       bad |= valid && !in;
-      const double fx = __int_as_float(ps.y), fy = __int_as_float(ps.z), fz = __int_as_float(ps.w);
-      const double gx = 1.0 - fx, gy = 1.0 - fy, gz = 1.0 - fz;
       const double one = (double)PM_FIX_ONE;
-      const double w00 = gx * gy * one, w01 = gx * fy * one, w10 = fx * gy * one, w11 = fx * fy * one;
-      u64 W0 = 0, W1 = 0, W2 = 0, W3 = 0, W4 = 0, W5 = 0, W6 = 0, W7 = 0;
-      if (in) {
-        W0 = fix_round(w00, gz);
-        W1 = fix_round(w00, fz);
-        W2 = fix_round(w01, gz);
-        W3 = fix_round(w01, fz);
-        W4 = fix_round(w10, gz);
-        W5 = fix_round(w10, fz);
-        W6 = fix_round(w11, gz);
-        W7 = PM_FIX_ONE - (W0 + W1 + W2 + W3 + W4 + W5 + W6);
-      }
-      // Warp-shuffle segmented scan over runs of the same cell.
-      const int key = in ? ps.x : -1 - lane;
+      const double fx = __int_as_float(ps.y), fy = __int_as_float(ps.z), fz = __int_as_float(ps.w);
+      const double Fx = fx * one, Gx = one - Fx;   // exact: fx has 24 significant bits
+      const double gy = 1.0 - fy, gz = 1.0 - fz;
+      const double w00 = Gx * gy, w01 = Gx * fy, w10 = Fx * gy, w11 = Fx * fy;
+      // Seven corners rounded to integers in units of 2^-38; the eighth takes the remainder so
+      // the particle deposits exactly 2^38 (hi/lo of 2^38 - sum, with lo in [0, 2^19)).
+      const Split c0 = fix_split(w00, gz), c1 = fix_split(w00, fz), c2 = fix_split(w01, gz), c3 = fix_split(w01, fz),
+                  c4 = fix_split(w10, gz), c5 = fix_split(w10, fz), c6 = fix_split(w11, gz);
+      const u32 shi = c0.hi + c1.hi + c2.hi + c3.hi + c4.hi + c5.hi + c6.hi;
+      const u32 slo = c0.lo + c1.lo + c2.lo + c3.lo + c4.lo + c5.lo + c6.lo;
+      const Split c7{(1u << 19) - shi - ((slo + 0x7FFFFu) >> 19), (0u - slo) & 0x7FFFFu};
+      bool tail = true;
+      Split w[8] = {c0, c1, c2, c3, c4, c5, c6, c7};
+#if PM_DEP_SCAN
+      // Warp-shuffle segmented sums over runs of the same cell (long runs: collapsed regions).
+      const int key = in ? c : -1 - lane;
       const int prev = __shfl_up_sync(0xffffffffu, key, 1);
       const bool head = lane == 0 || prev != key;
       const u32 heads = __ballot_sync(0xffffffffu, head);
-      bool tail = true;
-      // A few same-cell neighbours cost a few serialised shared-memory atomics; the scan (about
-      // 250 instructions per lane) pays only when runs are long, as in collapsed regions.
-      if (__popc(heads) < 24) {
+      if (__popc(heads) < PM_DEP_SCAN) {
         const int sstart = 31 - __clz(heads & le);
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
           const bool take = lane - d >= sstart;
-#define PM_SEG(W)                     \
-  {                                   \
-    const u64 v_ = shfl_up_u64(W, d); \
-    if (take) W += v_;                \
-  }
-          PM_SEG(W0) PM_SEG(W1) PM_SEG(W2) PM_SEG(W3) PM_SEG(W4) PM_SEG(W5) PM_SEG(W6) PM_SEG(W7)
-#undef PM_SEG
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const u32 vh = __shfl_up_sync(0xffffffffu, w[q].hi, d), vl = __shfl_up_sync(0xffffffffu, w[q].lo, d);
+            if (take) {
+              w[q].hi += vh;
+              w[q].lo += vl;
+            }
+          }
         }
         tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
       }
+#endif
       if (in && tail) {
-        const int nb = lx * PS + ly * RS + lz;
-#define PM_ADD(off, W)                                                   \
-  {                                                                      \
-    atomicAdd(&acc_hi[nb + (off)], (u32)(int)((long long)(W) >> 19));   \
-    atomicAdd(&acc_lo[nb + (off)], (u32)((W) & 0x7FFFFu));              \
-  }
-        PM_ADD(0, W0)
-        PM_ADD(1, W1)
-        PM_ADD(RS, W2)
-        PM_ADD(RS + 1, W3)
-        PM_ADD(PS, W4)
-        PM_ADD(PS + 1, W5)
-        PM_ADD(PS + RS, W6)
-        PM_ADD(PS + RS + 1, W7)
-#undef PM_ADD
+        const int nb = ((c >> (2 * l2)) & (TS - 1)) * PS + ((c >> l2) & (TS - 1)) * RS + (c & (TS - 1));
+        const int off[8] = {0, 1, RS, RS + 1, PS, PS + 1, PS + RS, PS + RS + 1};
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          atomicAdd(&acc_hi[nb + off[q]], w[q].hi);
+          atomicAdd(&acc_lo[nb + off[q]], w[q].lo);
+        }
       }
     }
     if (--left == 0 && it + 1 < nit) {  // chunk full and more to come: fold it into acc64
@@ -956,38 +971,63 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
     }
   }
   if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&A.stats[pk].status, 1u);
-  // Last chunk folded straight into the output: interior nodes final, the rest as partials.
+  // Write-out of the last chunk (plus the folded ones), four nodes of a patch row at a time:
+  // interior nodes final as FP32 delta (16-byte stores; the first node of an interior row is a
+  // face node, stored here from this super-tile's own sum and completed by k_fixup), nodes on
+  // the lower faces and on the upper halo as 64-bit partials.
   long long dsum = 0, smax = 0;
   const long long gbase = ((long long)sx * TS * N + (long long)sy * TS) * N + sz * TS;
-  long long* face = A.face + P.face_off + (long long)st * P.fc;
+  long long* face = A.face + P.face_off + (long long)st * FC;
   long long* halo = A.halo + P.halo_off + (long long)st * P.hc;
-  // Two copies of the loop: the common single-chunk one carries no load of the fold scratch.
-  auto write_out = [&](auto with_fold) {
+  const u64* fold = reinterpret_cast<const u64*>(A.tpos + b);
+  const long long nmf = P.n_mean_fix;
+  const double inv = P.inv_fix_nmean;
+  for (int item = threadIdx.x; item < T1 * T1 * NG; item += DEP_THREADS) {
+    const int row = item / NG, g = item - row * NG;
+    const int lx = row / T1, ly = row - lx * T1;
+    const int ad = lx * PS + ly * RS + 4 * g;
+    const uint4 h = *reinterpret_cast<const uint4*>(acc_hi + ad);
+    const uint4 l = *reinterpret_cast<const uint4*>(acc_lo + ad);
+    long long S[4] = {chunk_sum(h.x, l.x), chunk_sum(h.y, l.y), chunk_sum(h.z, l.z), chunk_sum(h.w, l.w)};
+    const int nbase = row * T1 + 4 * g;  // dense node number of the group's first node
+    if (folded) {
 #pragma unroll
-    for (int q = 0; q < NPT; ++q) {
-      const int node = threadIdx.x + q * DEP_THREADS;
-      if (node < NN) {
-        const int lx = node / (T1 * T1), r = node - lx * (T1 * T1), ly = r / T1, lz = r - ly * T1;
-        const int ad = lx * PS + ly * RS + lz;
-        long long S = chunk_sum(acc_hi[ad], acc_lo[ad]);
-        if (decltype(with_fold)::value) S += (long long)reinterpret_cast<const u64*>(A.tpos + b)[node];
-        if (lx == TS || ly == TS || lz == TS) {
-          halo[halo_index(lx, ly, lz, TS)] = S;
-        } else if (lx == 0 || ly == 0 || lz == 0) {
-          face[face_index(lx, ly, lz, TS)] = S;
-        } else {
-          const long long Dv = S - P.n_mean_fix;
-          const long long g = gbase + ((long long)lx * N + ly) * N + lz;
-          P.delta[g] = (float)((double)Dv * P.inv_fix_nmean);
-          if (rho64) rho64[g] = (double)S * (1.0 / (double)PM_FIX_ONE);
-          dsum += Dv;
-          smax = S > smax ? S : smax;
+      for (int k = 0; k < 4; ++k)
+        if (4 * g + k <= TS) S[k] += (long long)fold[nbase + k];
+    }
+    if (lx == TS || ly == TS) {  // a row of the upper halo
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int lz = 4 * g + k;
+        if (lz <= TS) halo[halo_index(lx, ly, lz, TS)] = S[k];
+      }
+    } else if (g == NG - 1) {    // the row's upper-halo node
+      halo[halo_index(lx, ly, TS, TS)] = S[0];
+    } else if (lx == 0 || ly == 0) {  // a row of a lower face
+#pragma unroll
+      for (int k = 0; k < 4; ++k) face[face_index(lx, ly, 4 * g + k, TS)] = S[k];
+    } else {                     // interior nodes (and the row's lz = 0 face node)
+      if (g == 0) face[face_index(lx, ly, 0, TS)] = S[0];
+      float4 d;
+      float* dv = &d.x;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const long long D = S[k] - nmf;
+        dv[k] = (float)((double)D * inv);
+        if (g > 0 || k > 0) {
+          dsum += D;
+          smax = S[k] > smax ? S[k] : smax;
         }
       }
+      const long long gi = gbase + ((long long)lx * N + ly) * N + 4 * g;
+      *reinterpret_cast<float4*>(P.delta + gi) = d;
+      if (rho64) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          if (g > 0 || k > 0) rho64[gi + k] = (double)S[k] * (1.0 / (double)PM_FIX_ONE);
+      }
     }
-  };
-  if (folded) write_out(std::true_type{});
-  else write_out(std::false_type{});
+  }
   for (int d = 16; d > 0; d >>= 1) {
     dsum += __shfl_xor_sync(0xffffffffu, dsum, d);
     const long long om = __shfl_xor_sync(0xffffffffu, smax, d);
@@ -1024,39 +1064,68 @@ __global__ void __launch_bounds__(DEP_THREADS, 4) k_deposit(StepArgs A, double* 
   }
 }
 
-// Face fix-up: one CTA per super-tile whose peak deposited this step.  Small and
-// latency-bound, so many CTAs per SM; the partials are fresh in L2.
-__global__ void __launch_bounds__(FIX_THREADS) k_fixup(StepArgs A, double* rho64) {
-  __shared__ long long s_red[FIX_THREADS / 32];
-  __shared__ long long s_max[FIX_THREADS / 32];
-  const TileRef tr = find_tile(A.st_base, A.npeaks);
-  if (!A.clocks[tr.pk].dep) return;
-  const PeakDesc P = A.peaks[tr.pk];
-  long long dsum = 0, smax = 0;
-  switch (P.TS) {
-    case 4: fixup_faces<4>(A, P, (u32)tr.t, rho64, dsum, smax); break;
-    case 8: fixup_faces<8>(A, P, (u32)tr.t, rho64, dsum, smax); break;
-    default: fixup_faces<16>(A, P, (u32)tr.t, rho64, dsum, smax); break;
-  }
-  for (int d = 16; d > 0; d >>= 1) {
-    dsum += __shfl_xor_sync(0xffffffffu, dsum, d);
-    const long long om = __shfl_xor_sync(0xffffffffu, smax, d);
-    smax = om > smax ? om : smax;
-  }
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0) {
-    s_red[warp] = dsum;
-    s_max[warp] = smax;
+// Face fix-up: FIX_ST consecutive super-tiles per CTA (those whose peak deposited this step).
+// Small and latency-bound: the partials are fresh in L2; the neighbours' halo pointers are
+// found once per CTA, the statistics reduced once per super-tile.
+__global__ void __launch_bounds__(FIX_THREADS) k_fixup(StepArgs A, double* rho64, long long nst) {
+  __shared__ const long long* s_nb[FIX_ST][8];
+  __shared__ int s_pk[FIX_ST];
+  __shared__ long long s_red[FIX_ST][FIX_THREADS / 32];
+  __shared__ long long s_max[FIX_ST][FIX_THREADS / 32];
+  const long long t0 = (long long)blockIdx.x * FIX_ST;
+  if (threadIdx.x < FIX_ST * 8) {
+    const int k = threadIdx.x >> 3, o = threadIdx.x & 7;
+    const long long t = t0 + k;
+    int pk = -1;
+    const long long* nbp = nullptr;
+    if (t < nst) {
+      pk = pm_find(A.st_base, A.npeaks, t);
+      const PeakDesc& P = A.peaks[pk];
+      const u32 Y = (u32)(t - A.st_base[pk]);
+      const int NS = P.NS, ox = o & 1, oy = (o >> 1) & 1, oz = (o >> 2) & 1;
+      const u32 sn = pm_morton3((pm_compact3(Y >> 2) - ox) & (NS - 1), (pm_compact3(Y >> 1) - oy) & (NS - 1),
+                                (pm_compact3(Y) - oz) & (NS - 1));
+      nbp = A.halo + P.halo_off + (long long)sn * P.hc;
+      if (!A.clocks[pk].dep) pk = -1;
+    }
+    s_nb[k][o] = nbp;
+    if (o == 0) s_pk[k] = pk;
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll 1
+  for (int k = 0; k < FIX_ST; ++k) {
+    const int pk = s_pk[k];
+    long long dsum = 0, smax = 0;
+    if (pk >= 0) {
+      const PeakDesc& P = A.peaks[pk];
+      const u32 Y = (u32)(t0 + k - A.st_base[pk]);
+      switch (P.TS) {
+        case 4: fixup_faces<4>(A, P, Y, s_nb[k], rho64, dsum, smax); break;
+        case 8: fixup_faces<8>(A, P, Y, s_nb[k], rho64, dsum, smax); break;
+        default: fixup_faces<16>(A, P, Y, s_nb[k], rho64, dsum, smax); break;
+      }
+    }
+    for (int d = 16; d > 0; d >>= 1) {
+      dsum += __shfl_xor_sync(0xffffffffu, dsum, d);
+      const long long om = __shfl_xor_sync(0xffffffffu, smax, d);
+      smax = om > smax ? om : smax;
+    }
+    if (lane == 0) {
+      s_red[k][warp] = dsum;
+      s_max[k][warp] = smax;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < FIX_ST && s_pk[threadIdx.x] >= 0) {
+    const int k = threadIdx.x;
     long long ts = 0, tm = 0;
     for (int w = 0; w < FIX_THREADS / 32; ++w) {
-      ts += s_red[w];
-      tm = s_max[w] > tm ? s_max[w] : tm;
+      ts += s_red[k][w];
+      tm = s_max[k][w] > tm ? s_max[k][w] : tm;
     }
-    atomicAdd((unsigned long long*)&A.stats[tr.pk].mass_defect, (unsigned long long)ts);
-    atomicMax(&A.stats[tr.pk].max_fix, (u64)tm);
+    atomicAdd((unsigned long long*)&A.stats[s_pk[k]].mass_defect, (unsigned long long)ts);
+    atomicMax(&A.stats[s_pk[k]].max_fix, (u64)tm);
   }
 }
 
@@ -1178,7 +1247,8 @@ __global__ void __launch_bounds__(PM_THREADS) k_green(StepArgs A) {
   if ((threadIdx.x & 31) == 0) A.wpart[(P.mode_base + lb) * (PM_THREADS / 32) + (threadIdx.x >> 5)] = w;
 }
 
-__global__ void k_reset_peak(StepArgs A, int pk, double a0, int mode, double param, double a_end, int max_steps) {
+__global__ void k_reset_peak(StepArgs A, int pk, double a0, int mode, double param, double a_end, int max_steps,
+                             int set_thr, double delta_collapse, int stop) {
   PeakClock c = A.clocks[pk];
   c.a = a0;
   c.a_grid = a0;
@@ -1194,13 +1264,24 @@ __global__ void k_reset_peak(StepArgs A, int pk, double a0, int mode, double par
   c.sortstep = 0;
   c.refresh = 0;
   c.a_collapse = -1.0;
-  c.stop_on_collapse = 0;
+  c.stop_on_collapse = set_thr ? (stop ? 1 : 0) : 0;
+  if (set_thr) c.delta_collapse = delta_collapse;
   if (mode == SCHED_RATIO) c.da = a0 * param;
   else if (mode == SCHED_FRAC) c.da = fmin(param * a0, a_end - a0);
   else c.da = 0.0;
   A.clocks[pk] = c;
   A.stats[pk].status = 0;
   A.stats[pk].nsamples = 0;
+  A.sort_err[pk] = 0;
+}
+
+__global__ void k_release_peak(StepArgs A, int pk) {
+  PeakClock c = A.clocks[pk];
+  c.state = PS_IDLE;
+  c.has_delta = 0;
+  c.dep = 0;
+  c.kpend = 0.0;
+  A.clocks[pk] = c;
 }
 
 // Particles (n,3) float64 in lattice order -> split state + cell keys (pm3d.py:76-79 convention).
@@ -1367,15 +1448,16 @@ void launch_deposit(const StepArgs& A, long long nst, size_t smem, double* rho64
   k_deposit<<<(unsigned)nst, DEP_THREADS, smem, s>>>(A, rho64);
 }
 void launch_fixup(const StepArgs& A, long long nst, double* rho64, cudaStream_t s) {
-  k_fixup<<<(unsigned)nst, FIX_THREADS, 0, s>>>(A, rho64);
+  k_fixup<<<nb(nst, FIX_ST), FIX_THREADS, 0, s>>>(A, rho64, nst);
 }
 void launch_green(const StepArgs& A, long long nblocks, cudaStream_t s) {
   k_green<<<(unsigned)nblocks, PM_THREADS, 0, s>>>(A);
 }
-void launch_reset_peak(const StepArgs& A, int pk, double a0, int mode, double param, double a_end, int max_steps,
-                       cudaStream_t s) {
-  k_reset_peak<<<1, 1, 0, s>>>(A, pk, a0, mode, param, a_end, max_steps);
+void launch_reset_peak(const StepArgs& A, int pk, double a0, int mode, double param, double a_end,
+                       int max_steps, int set_thr, double delta_collapse, int stop, cudaStream_t s) {
+  k_reset_peak<<<1, 1, 0, s>>>(A, pk, a0, mode, param, a_end, max_steps, set_thr, delta_collapse, stop);
 }
+void launch_release_peak(const StepArgs& A, int pk, cudaStream_t s) { k_release_peak<<<1, 1, 0, s>>>(A, pk); }
 void launch_set_particles(const StepArgs& A, int pk, const PeakDesc& P, const double* x, const double* p,
                           cudaStream_t s) {
   k_set_particles<<<nb(P.n, PM_THREADS), PM_THREADS, 0, s>>>(A, pk, P, x, p);

@@ -25,6 +25,7 @@
 #define GREEN_MODES 4      // modes per thread of the Green kernel (a block covers PM_THREADS * GREEN_MODES)
 #define ENERGY_SLICES 16   // CTAs per peak of the energy reduction
 #define FIX_THREADS 256    // face fix-up CTA
+#define FIX_ST 4           // super-tiles per face fix-up CTA
 #define TSORT_THREADS 1024 // super-tile sort (refresh) CTA
 #define TSORT_CAP 5120     // particles of a super-tile sorted in shared memory; denser ones via global
 #define BIN_CLASSES 128   // stride of the per-super-tile class arrays (>= 125)
@@ -65,6 +66,7 @@ struct StepArgs {
   double* wpart;               // [Green block][warp] partials of sum_k w_k |delta_k|^2 G_k
   double2* eslice;             // [peak][ENERGY_SLICES][5] slice partials of the energy kernel
   u32* ecount;                 // [peak] energy slices finished this step (0 between steps)
+  int* sort_err;               // [peak] the priming sort's bounded look-back gave up (sort plan)
 };
 
 // Binary search: largest i in [0, n) with base[i] <= v.
@@ -101,9 +103,12 @@ int fft_native_green_c2r(int N, const float2* spec, float2* gwork, float* force,
                          const int* slot_peak, int nslots, cudaStream_t s);
 int fft_native_c2r(int N, const float2* spec, float2* gwork, float* out, int nfields, cudaStream_t s);
 
-// Host-requested per-peak operations.
+// Host-requested per-peak operations.  reset: new schedule from a0, status and sort error
+// cleared; set_thr = 1 also sets the collapse threshold and its stop flag (else they are kept).
 void launch_reset_peak(const StepArgs& A, int pk, double a0, int mode, double param, double a_end,
-                       int max_steps, cudaStream_t s);
+                       int max_steps, int set_thr, double delta_collapse, int stop, cudaStream_t s);
+// release: the peak goes idle (no pending kick, no grids), on the stream, without a host round trip.
+void launch_release_peak(const StepArgs& A, int pk, cudaStream_t s);
 void launch_set_particles(const StepArgs& A, int pk, const PeakDesc& P, const double* x, const double* p,
                           cudaStream_t s);
 void launch_reload(const StepArgs& A, const PeakDesc& P, cudaStream_t s);  // state -> loading area + keys

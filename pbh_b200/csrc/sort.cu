@@ -6,8 +6,6 @@
 
 namespace {
 
-constexpr int kSpinLimit = 1 << 22;
-
 __device__ __forceinline__ u32 lanemask_lt() {
   u32 m;
   asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
@@ -100,6 +98,8 @@ __global__ void __launch_bounds__(SORT_THREADS, 3) k_sort_pass(SortPlan P, int p
   __shared__ u32 whist[SORT_WARPS][RADIX];
   __shared__ long long s_gbase[RADIX];
   if (gate_closed(P)) return;
+  const int spin_limit = P.dbg ? P.dbg[0] : SORT_SPIN_LIMIT;
+  const int silent_tile = (P.dbg && pass == 0) ? P.dbg[1] : -1;
   for (;;) {
     __syncthreads();  // the previous tile's readers of s_tile, whist and s_gbase are done
     if (threadIdx.x == 0) s_tile = atomicAdd(&P.counters[pass], 1u);
@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(SORT_THREADS, 3) k_sort_pass(SortPlan P, int p
       }
       run[q] = r;
       // Publish this tile's own count first, so successors can look past it at once.
-      st[(size_t)t * RADIX + d] = tag | ((P.tile_first[t] ? 2ull : 1ull) << 32) | r;
+      if (t != silent_tile) st[(size_t)t * RADIX + d] = tag | ((P.tile_first[t] ? 2ull : 1ull) << 32) | r;
     }
     // Look back over the predecessors of this segment, LB words per round trip: the loads of a
     // window are independent, so the walk costs one memory latency per LB tiles.
@@ -180,8 +180,8 @@ __global__ void __launch_bounds__(SORT_THREADS, 3) k_sort_pass(SortPlan P, int p
             if (done || p - i < S.first_tile) continue;
             u64 v = w[i];
             while ((v >> 34) != (u64)ep || ((u32)(v >> 32) & 3u) == 0) {
-              if (++spins > kSpinLimit) {
-                atomicExch(P.err, 1);
+              if (++spins > spin_limit) {
+                atomicExch(&P.err[seg], 1);
                 v = tag | (2ull << 32);  // give up: treat as a zero inclusive prefix
                 break;
               }
@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(SORT_THREADS, 3) k_sort_pass(SortPlan P, int p
           p -= LB;
           if (p < S.first_tile) done = true;
         }
-        st[(size_t)t * RADIX + d] = tag | (2ull << 32) | (excl + run[q]);
+        if (t != silent_tile) st[(size_t)t * RADIX + d] = tag | (2ull << 32) | (excl + run[q]);
       }
       s_gbase[d] = P.base[((size_t)seg * SORT_MAX_PASSES + pass) * RADIX + d] + excl;
     }
@@ -250,7 +250,7 @@ int sort_plan_create(SortPlan* P, const SortSeg* segs, int nseg, int npass, int 
   PM_CHECK(cudaMalloc(&P->base, sizeof(long long) * nseg * SORT_MAX_PASSES * radix));
   PM_CHECK(cudaMalloc(&P->status, sizeof(u64) * nt * radix));
   PM_CHECK(cudaMalloc(&P->counters, sizeof(u32) * (SORT_MAX_PASSES + 1)));
-  PM_CHECK(cudaMalloc(&P->err, sizeof(int)));
+  PM_CHECK(cudaMalloc(&P->err, sizeof(int) * nseg));
   PM_CHECK(cudaMemcpy(P->seg, sg.data(), sizeof(SortSeg) * nseg, cudaMemcpyHostToDevice));
   if (!tseg.empty()) {
     PM_CHECK(cudaMemcpy(P->tile_seg, tseg.data(), sizeof(int) * nt, cudaMemcpyHostToDevice));
@@ -260,7 +260,7 @@ int sort_plan_create(SortPlan* P, const SortSeg* segs, int nseg, int npass, int 
   PM_CHECK(cudaMemset(P->hist, 0, sizeof(u32) * nseg * SORT_MAX_PASSES * radix));
   PM_CHECK(cudaMemset(P->status, 0, sizeof(u64) * nt * radix));
   PM_CHECK(cudaMemset(P->counters, 0, sizeof(u32) * (SORT_MAX_PASSES + 1)));
-  PM_CHECK(cudaMemset(P->err, 0, sizeof(int)));
+  PM_CHECK(cudaMemset(P->err, 0, sizeof(int) * nseg));
   return 0;
 }
 

@@ -6,7 +6,8 @@
 // its global offsets by decoupled look-back over the preceding tiles of the same segment, so
 // every pass reads and writes each key once.  Claiming in order guarantees that every tile a
 // CTA waits on is held by a running CTA that waits only on earlier tiles.  Waits are bounded:
-// a CTA that gives up sets the error word and proceeds.  A plan may carry a device gate word:
+// a CTA that gives up sets its segment's error word, counts the tile it waited on as empty
+// (every position it then writes stays inside the segment) and proceeds.  A plan may carry a device gate word:
 // when it reads 0 (no segment active this step) every launch returns at once, so a sort
 // captured in a graph costs a few microseconds on the steps that do not need it.
 //
@@ -48,9 +49,15 @@ struct SortPlan {
   long long* base;       // [nseg][SORT_MAX_PASSES][radix]
   u64* status;           // [ntiles][radix] look-back words: epoch<<34 | flag<<32 | count
   u32* counters;         // [SORT_MAX_PASSES] tile claims, then the epoch word
-  int* err;              // nonzero after a bounded wait gave up
+  int* err;              // [nseg] nonzero after a bounded wait of that segment gave up
   const u32* gate;       // optional (device): when *gate == 0 every launch of the sort returns at once
+  const int* dbg;        // optional (device): {spin limit of the look-back waits, tile whose look-back
+                         // words the first pass never publishes (-1: none)}, read when the sort runs;
+                         // nullptr: SORT_SPIN_LIMIT and no such tile.  A test hook: the waits on an
+                         // unpublished tile run out, so the bounded-wait path can be exercised.
 };
+
+#define SORT_SPIN_LIMIT (1 << 22)
 
 // Host side (sort.cu).  `segs` is a host array.  The digit width is the smallest of 8..10 bits
 // that covers `span` key bits in `npass` passes (npass = 0: as few passes as 10-bit digits allow).

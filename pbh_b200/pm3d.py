@@ -35,6 +35,42 @@ def zeldovich_axes(e: float, p: float):
     return ax / np.prod(ax) ** (1.0 / 3.0)
 
 
+class StateArray(np.ndarray):
+    """Host copy of a PM3D's particle state (``pm.x`` or ``pm.p``), float64 in lattice order.
+
+    The reference's ``x`` and ``p`` are plain arrays a caller may write into
+    (pbhgr/pbhgr/pm3d.py:67-68); here the state lives on the GPU, so writing into this copy
+    (item assignment, in-place arithmetic, ufuncs with ``out=``, through views too) marks it
+    changed, and the owning PM3D loads it into the engine before its next device operation.
+    A copy taken before the state changed on the device is stale, as an array the reference
+    has rebound is: writing into it changes nothing."""
+
+    def __array_finalize__(self, obj):
+        self._owner = getattr(obj, "_owner", None)
+        self._gen = getattr(obj, "_gen", -1)
+
+    def _touch(self):
+        o = self._owner
+        if o is not None and o._host_gen == self._gen:
+            o._host_dirty = True
+
+    def __setitem__(self, key, value):
+        super().__setitem__(key, value)
+        self._touch()
+
+    def __array_ufunc__(self, ufunc, method, *inputs, out=None, **kwargs):
+        args = [i.view(np.ndarray) if isinstance(i, StateArray) else i for i in inputs]
+        if out is not None:
+            for o in out:
+                if isinstance(o, StateArray):
+                    o._touch()
+            kwargs["out"] = tuple(o.view(np.ndarray) if isinstance(o, StateArray) else o for o in out)
+        res = getattr(ufunc, method)(*args, **kwargs)
+        if out is not None:
+            return out[0] if len(out) == 1 else out
+        return res
+
+
 def _lattice(Np: int, L: float) -> np.ndarray:
     q1 = (np.arange(Np) + 0.5) * (L / Np) - L / 2
     return np.stack(np.meshgrid(q1, q1, q1, indexing="ij"), axis=-1).reshape(-1, 3)
@@ -61,6 +97,9 @@ class PM3D:
         self.A = None
         self._delta_lin = None
         self.tail_rms_grid = 0.0
+        self._host = None          # cached StateArray copies of x and p
+        self._host_gen = 0
+        self._host_dirty = False
 
     # ------------------------------------------------------------------ k-grids (pm3d.py:31-35)
     def _k(self):
@@ -85,6 +124,7 @@ class PM3D:
                                        device=self.device, delta_lin=True)
         self._engine.set_particles(0, x, p, 1.0)
         self._loaded = True
+        self._stale()
         self._delta_lin = dl
         self._ic_xp = (x, p) if getattr(self, "keep_ic", False) else None
         self.A = np.asarray(axes, dtype=np.float64)
@@ -128,26 +168,52 @@ class PM3D:
 
     def _prime(self):
         self._require()
+        self._flush()
         if self._engine.clock(0).state == _lib.STATE_PRIME:
             self._engine.run(1)
 
+    # Host copies of x and p: made on first access after the device state changed, loaded back
+    # into the engine before the next device operation if they were written into.
+    def _stale(self):
+        self._host = None
+        self._host_gen += 1
+        self._host_dirty = False
+
+    def _flush(self):
+        if self._host is not None and self._host_dirty:
+            x, p = self._host
+            self._host_dirty = False
+            self._assign(x=np.asarray(x), p=np.asarray(p))
+
+    def _host_state(self):
+        self._require()
+        if self._host is None:
+            xd, pd = self._engine.particles(0)
+            arrs = []
+            for t in (xd, pd):
+                a = t.cpu().numpy().view(StateArray)
+                a._owner, a._gen = self, self._host_gen
+                arrs.append(a)
+            self._host = tuple(arrs)
+        return self._host
+
     @property
     def x(self):
-        self._require()
-        return self._engine.particles(0)[0].cpu().numpy()
+        return self._host_state()[0]
 
     @x.setter
     def x(self, value):
-        self._assign(x=value)
+        self._flush()
+        self._assign(x=np.asarray(value, dtype=np.float64))
 
     @property
     def p(self):
-        self._require()
-        return self._engine.particles(0)[1].cpu().numpy()
+        return self._host_state()[1]
 
     @p.setter
     def p(self, value):
-        self._assign(p=value)
+        self._flush()
+        self._assign(p=np.asarray(value, dtype=np.float64))
 
     def _assign(self, x=None, p=None):
         n = self.Np ** 3
@@ -160,6 +226,7 @@ class PM3D:
             cx, cp = z, z
         self._engine.set_particles(0, cx if x is None else x, cp if p is None else p, a0)
         self._loaded = True
+        self._stale()
 
     @property
     def _acc_a(self):
@@ -168,6 +235,7 @@ class PM3D:
 
     @property
     def _acc(self):
+        self._flush()
         a = self._acc_a
         return None if a is None else self._engine.acc(0, a).cpu().numpy()
 
@@ -211,7 +279,9 @@ class PM3D:
     def step(self, a, da):
         """KDK step in a (pm3d.py:117-129); returns (a + da, delta at a + da)."""
         self._require()
+        self._flush()
         self._engine.step_explicit(0, a, da)
+        self._stale()
         return a + da, self._out(self._engine.delta(0))
 
     def close(self):
@@ -234,9 +304,11 @@ class PM3D:
         a_end - a) until a_end, all steps replayed from one captured graph.  With ``callback``
         and ``every`` > 0 the loop pauses every ``every`` steps and calls callback(self, a, step)."""
         self._require()
+        self._flush()
         eng = self._engine
         xd, pd = eng.particles(0)
         eng.set_particles(0, xd, pd, a, mode=_lib.SCHED_FRAC, param=da_frac, a_end=a_end)
+        self._stale()
         eng.run(1)
         while True:
             c = eng.clock(0)
@@ -246,9 +318,12 @@ class PM3D:
             eng.run(k)
             c = eng.clock(0)
             if callback and every > 0:
-                callback(self, c.a, c.nsteps)
+                self._stale()
+            callback(self, c.a, c.nsteps)
+            self._flush()
         if eng.clock(0).state == _lib.STATE_FINALIZE:
             eng.run(1)
+        self._stale()
         return eng.clock(0).a
 
 
@@ -268,6 +343,7 @@ def analyse(pm: PM3D, a: float, fracs=(0.1, 0.2, 0.3), radii_cells=(1.0, 2.0, 4.
         from .engine import sort_u64
         _, perm = sort_u64(keys.cpu().numpy().view(np.uint64), 0, 64)
         pm._core_ids = perm[:30].astype(np.int64)
+    pm._flush()
     x, _ = pm._engine.particles(0)
     core = np.sort(pm._core_ids[:27])
     xc = x[torch.as_tensor(core, device=dev)].cpu().numpy()

@@ -237,3 +237,37 @@ def test_finite_difference_gradients(gradient, order):
     assert rel(acc, ref) < TOL_FORCE
     spectral, _ = O.accelerations(mesh, x, 1.0)
     assert rel(ref, spectral) > 1e-3                      # the stencils differ from the spectral gradient
+
+
+def test_batched_mix_of_benchmark_sizes_equals_alone():
+    """The batched ensemble's own mesh sizes (32^3-256^3, two peaks of the smallest sizes so
+    their classes are batched transforms, super-tiles as the bench picks them) against every
+    peak alone: positions, momenta and density identical, bit for bit, over 20 steps (one
+    refresh of the super-tile order included)."""
+    from pbh_b200 import recipe
+    from pbh_b200.batch import Ensemble
+    tiles = {32: 8, 64: 8, 128: 16, 256: 16}
+    pool = recipe.ensemble(npeaks=24, sizes=(32, 64, 128, 256), steps=150, seed=77)
+    want = {32: 2, 64: 2, 128: 1, 256: 1}
+    specs = []
+    for s in pool:
+        if want.get(s.N, 0):
+            specs.append(s)
+            want[s.N] -= 1
+    assert not any(want.values())
+    mix = Ensemble(specs, tiles=tiles)
+    mix.load()
+    mix.step(21)
+    got = [(*[t.cpu().numpy() for t in mix.engine.particles(i)], mix.engine.delta(i).cpu().numpy())
+           for i in range(len(specs))]
+    assert all(s.status == 0 and s.mass_defect == 0.0 for s in mix.stats())
+    mix.close()
+    for i, s in enumerate(specs):
+        alone = Ensemble([s], tiles=tiles)
+        alone.load()
+        alone.step(21)
+        xa, pa = [t.cpu().numpy() for t in alone.engine.particles(0)]
+        da = alone.engine.delta(0).cpu().numpy()
+        alone.close()
+        assert np.array_equal(xa, got[i][0]) and np.array_equal(pa, got[i][1]), (i, s.N)
+        assert np.array_equal(da, got[i][2]), (i, s.N)

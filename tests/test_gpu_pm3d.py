@@ -113,3 +113,31 @@ def test_run_loop_matches_explicit_steps():
     assert abs(ab - a) < 1e-12
     assert np.max(np.abs(wrap(pa.x - pb.x, 1.0))) < 1e-12
     assert rel(pa.p, pb.p) < 1e-6
+
+
+def test_writing_into_x_and_p_changes_the_run():
+    """pm.x / pm.p are plain arrays in the reference (pm3d.py:67-68); writing into them must
+    change the next step here too, exactly as assigning the modified arrays does."""
+    from pbh_b200.pm3d import PM3D
+    N = 16
+    pa = PM3D(N, 1.0, N, seed=5).make_peak((0.1, 0.09, 0.08), 0.05)
+    pb = PM3D(N, 1.0, N, seed=5).make_peak((0.1, 0.09, 0.08), 0.05)
+    a, _ = pa.step(1.0, 0.05)
+    pb.step(1.0, 0.05)
+    pa.p[:, 0] *= 2.0                                    # in place, through the property
+    pa.x[7] = (0.5, 0.25, 0.125)
+    p_new, x_new = pb.p.copy(), pb.x.copy()
+    p_new[:, 0] *= 2.0
+    x_new[7] = (0.5, 0.25, 0.125)
+    pb.p = p_new                                         # assignment
+    pb.x = x_new
+    assert np.array_equal(pa.x, pb.x) and np.array_equal(pa.p, pb.p)
+    ra = pa.step(a, 0.05)[1]
+    rb = pb.step(a, 0.05)[1]
+    assert np.array_equal(ra, rb)
+    assert np.array_equal(pa.x, pb.x) and np.array_equal(pa.p, pb.p)
+    assert abs(pa.x[7, 0] - 0.5) > 0.0                   # it moved from the written position
+    stale = pa.x
+    pa.step(a + 0.05, 0.05)
+    stale[0] = 0.0                                       # a copy from before the step: no effect
+    assert not np.array_equal(pa.x[0], np.zeros(3))

@@ -43,7 +43,28 @@ def test_served_results_equal_alone():
         m = done[i]
         assert m.steps == r.steps, i
         assert m.a_collapse_cfg == r.a_collapse_cfg, i
-        assert rel(m.delta, r.delta) <= TOL_DENSITY, i
+        assert np.array_equal(m.delta, r.delta), i      # the deposit sums integers: same bits
+
+
+def test_served_benchmark_sizes_equal_alone():
+    """The served stream's own mesh sizes (64^3-256^3): six requests arriving while others run,
+    each result (steps, collapse a, final density) identical to the same request served alone."""
+    from pbh_b200 import recipe
+    from pbh_b200.serve import Server, ServerConfig
+    sp = recipe.ensemble(npeaks=6, sizes=(64, 128, 256), steps=40, seed=29, a_range=(0.03, 0.06))
+    cfg = ServerConfig(slots={64: 2, 128: 2, 256: 1}, budget_bytes=60e9, delta_collapse=2.0)
+    srv = Server(cfg)
+    arrivals = [(0.02 * i, s) for i, s in enumerate(sp)]
+    done = {r.rid: r for r in srv.serve(arrivals)}
+    srv.close()
+    assert len(done) == len(sp) and all(r.ok for r in done.values())
+    for i, s in enumerate(sp):
+        alone = Server(ServerConfig(slots={s.N: 1}, budget_bytes=60e9, delta_collapse=2.0))
+        r = alone.serve([(0.0, s)])[0]
+        alone.close()
+        m = done[i]
+        assert m.steps == r.steps and m.a_collapse_cfg == r.a_collapse_cfg, (i, s.N)
+        assert np.array_equal(m.delta, r.delta), (i, s.N)
 
 
 def test_admission_waits_for_free_slots():

@@ -74,7 +74,13 @@ def test_latency_summary():
     assert s["completed"] == 101
     assert s["p50_s"] == pytest.approx(1.5) and s["max_s"] == pytest.approx(2.0)
     assert s["p99_s"] == pytest.approx(1.99)
-    assert latency_summary([]) == {"completed": 0}
+    assert s["failed"] == 0
+    assert latency_summary([]) == {"completed": 0, "failed": 0}
+    # refused, cancelled and failed requests are counted apart, not in the latencies
+    bad = Request(rid=999, spec=None, t_arrival=0.0, ok=False, error="cancelled")
+    bad.t_done = 1e6
+    s2 = latency_summary(done + [bad])
+    assert s2["completed"] == 101 and s2["failed"] == 1 and s2["max_s"] == pytest.approx(2.0)
 
 
 def test_served_slot_pool_fits_the_budget():
@@ -120,3 +126,58 @@ def test_return_code_mapping():
         _lib.check(-1005, "x")
     with pytest.raises(_lib.PMError, match="invalid argument"):
         _lib.check(-2003, "x")
+
+
+def test_served_requests_are_refused_for_the_right_reasons():
+    import dataclasses
+
+    from pbh_b200 import recipe
+    from pbh_b200.serve import ServerConfig, refusal_reason
+    cfg = ServerConfig(slots={64: 2, 128: 1}, budget_bytes=150e9)
+    ok = recipe.ensemble(npeaks=1, sizes=(64,), seed=3)[0]
+    assert refusal_reason(ok, cfg) == ""
+    cases = {"no slots": dataclasses.replace(ok, N=256),
+             "non-finite": dataclasses.replace(ok, delta0=float("nan")),
+             "positive": dataclasses.replace(ok, delta0=-0.01)}
+    for why, spec in cases.items():
+        assert why in refusal_reason(spec, cfg), why
+    assert "positive" in refusal_reason(dataclasses.replace(ok, R=(0.1, 0.0, 0.1)), cfg)
+    assert "positive" in refusal_reason(dataclasses.replace(ok, steps=0), cfg)
+    tiny = ServerConfig(slots={64: 1}, budget_bytes=1e6)
+    assert "budget" in refusal_reason(ok, tiny)
+
+
+def test_state_arrays_track_writes_like_the_references_plain_arrays():
+    """PM3D.x / PM3D.p are host copies of device state: writing into them (items, slices,
+    in-place arithmetic, ufunc out=, through views) must mark them for loading back, and a copy
+    from before the device state changed must not."""
+    from types import SimpleNamespace
+
+    from pbh_b200.pm3d import StateArray
+    owner = SimpleNamespace(_host_gen=3, _host_dirty=False)
+
+    def fresh(gen=3):
+        a = np.zeros((10, 3)).view(StateArray)
+        a._owner, a._gen = owner, gen
+        owner._host_dirty = False
+        return a
+
+    a = fresh()
+    a[2] = 1.0
+    assert owner._host_dirty and a[2, 1] == 1.0
+    a = fresh()
+    a[:, 0] *= 2.0                                   # __setitem__ of the augmented assignment
+    assert owner._host_dirty
+    a = fresh()
+    np.add(a, 1.0, out=a)
+    assert owner._host_dirty and np.all(a == 1.0)
+    a = fresh()
+    v = a[3:5]
+    v[0, 0] = 7.0                                    # a view writes through and marks the owner
+    assert owner._host_dirty and a[3, 0] == 7.0
+    a = fresh()
+    b = a + 1.0                                      # a new array is not the state
+    assert not owner._host_dirty and isinstance(b, np.ndarray)
+    s = fresh(gen=2)                                 # stale copy from an earlier state
+    s[0] = 5.0
+    assert not owner._host_dirty
