@@ -210,6 +210,11 @@ int pm_ic_release_cache(void);
 /* Stateless helpers. */
 /* PM3D.interp(F, X) (pm3d.py:91-99) in float64: F (N^3), X (n,3) -> out (n). */
 int pm_interp64(const double* F, const double* X, long long n, int N, double L, double* out);
+/* PM3D.deposit(X) (pm3d.py:81-89) of arbitrary float64 positions X (n,3) without an engine:
+ * counts (N^3 float64), each particle's eight corner weights rounded to 2^-39 in 64-bit fixed
+ * point with integer sums (the result does not depend on the order of X).  work: caller scratch
+ * of N^3 unsigned 64-bit words.  Synchronizes the device. */
+int pm_deposit64(const double* X, long long n, int N, double L, unsigned long long* work, double* counts);
 /* Stable sort of n 64-bit keys over bits [lo, hi): keys_out, perm_out (original indices).
  * tmp_keys/tmp_vals are caller scratch of n entries each. */
 int pm_sort_u64(const unsigned long long* keys, unsigned long long* keys_out, unsigned int* perm_out,

@@ -80,6 +80,7 @@ _SIGS = {
                                       C.c_void_p, C.c_int, C.c_void_p]),
     "pm_ic_release_cache": (C.c_int, []),
     "pm_interp64": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong, C.c_int, C.c_double, C.c_void_p]),
+    "pm_deposit64": (C.c_int, [C.c_void_p, C.c_longlong, C.c_int, C.c_double, C.c_void_p, C.c_void_p]),
     "pm_sort_u64": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.c_int,
                               C.c_int]),
     "pm_rfft3_native": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),

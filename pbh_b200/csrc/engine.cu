@@ -918,6 +918,14 @@ int pm_interp64(const double* F, const double* X, long long n, int N, double L, 
   return 0;
 }
 
+int pm_deposit64(const double* X, long long n, int N, double L, unsigned long long* work, double* counts) {
+  if (!X || !work || !counts || n < 0 || N < 1 || !(L > 0)) return -2000;
+  launch_deposit64(X, n, N, L / N, (u64*)work, counts, 0);
+  CU(cudaGetLastError());
+  CU(cudaDeviceSynchronize());
+  return 0;
+}
+
 int pm_sort_u64(const unsigned long long* keys, unsigned long long* keys_out, unsigned int* perm_out,
                 unsigned long long* tmp_keys, unsigned int* tmp_vals, long long n, int lo, int hi) {
   if (!keys || !keys_out || !perm_out || !tmp_keys || !tmp_vals || n < 0) return -2000;

@@ -150,12 +150,13 @@ __device__ __forceinline__ void push_one(const StepArgs& A, const PeakDesc& P, c
     acc_e = t;
   }
   int nx = ix, ny = iy, nz = iz;
+  int mx = 0, my = 0, mz = 0;  // cells moved along each axis
   const bool finite = isfinite(px) && isfinite(py) && isfinite(pz);
   if (K.run && finite) {  // a non-finite particle stays where it is (the peak is flagged below)
     px += K.kB * ax;
     py += K.kB * ay;
     pz += K.kB * az;
-#define PM_DRIFT(f, p, i)       \
+#define PM_DRIFT(f, p, i, m)    \
   {                             \
     float fn = f + K.D * p;     \
     float c = floorf(fn);       \
@@ -165,11 +166,12 @@ __device__ __forceinline__ void push_one(const StepArgs& A, const PeakDesc& P, c
       c += 1.0f;                \
     }                           \
     f = fn;                     \
-    i = (i + (int)c) & (N - 1); \
+    m = (int)c;                 \
+    i = (i + m) & (N - 1);      \
   }
-    PM_DRIFT(fx, px, nx)
-    PM_DRIFT(fy, py, ny)
-    PM_DRIFT(fz, pz, nz)
+    PM_DRIFT(fx, px, nx, mx)
+    PM_DRIFT(fy, py, ny, my)
+    PM_DRIFT(fz, pz, nz, mz)
 #undef PM_DRIFT
   }
   bad |= !(finite && isfinite(px) && isfinite(py) && isfinite(pz));
@@ -177,9 +179,19 @@ __device__ __forceinline__ void push_one(const StepArgs& A, const PeakDesc& P, c
   A.tpos[j] = make_int4(cell, __float_as_int(fx), __float_as_int(fy), __float_as_int(fz));
   A.tmom[j] = make_float4(px, py, pz, m.w);
   // Class of the destination super-tile (re-derived from the cell by the scatter), counted:
-  // most particles stay (one warp-aggregated add), the few movers add one each.
+  // most particles stay (one warp-aggregated add), the few movers add one each.  With more than
+  // five super-tiles per axis the class follows from the local cell and the cells moved
+  // (super-tile offsets -2..2 per axis, the same class bin_class gives); anything else, and
+  // smaller meshes, go through bin_class.  The sums are formed modulo 2^32: a saturated move of
+  // a runaway particle stays far outside -2..2.
   u32 far_st = 0;
-  const int c = bin_class(cell, sx, sy, sz, P, &far_st);
+  int c;
+  const int ox = (int)((u32)lx + (u32)mx) >> P.log2TS, oy = (int)((u32)ly + (u32)my) >> P.log2TS,
+            oz = (int)((u32)lz + (u32)mz) >> P.log2TS;
+  if (P.NS > 5 && (unsigned)(ox + 2) <= 4u && (unsigned)(oy + 2) <= 4u && (unsigned)(oz + 2) <= 4u)
+    c = ((ox >= 0 ? ox : 2 - ox) * 5 + (oy >= 0 ? oy : 2 - oy)) * 5 + (oz >= 0 ? oz : 2 - oz);
+  else
+    c = bin_class(cell, sx, sy, sz, P, &far_st);
   const u32 stay = __ballot_sync(__activemask(), c == 0);
   if (c == 0) {
     if ((stay & lanemask_lt()) == 0) atomicAdd(&s_cnt[0], (u32)__popc(stay));
@@ -205,15 +217,17 @@ __device__ __forceinline__ void push_super(const StepArgs& A, const PeakDesc& P,
     // z0 = sz*T is a multiple of 4 and the grids are 256-byte aligned).
     const unsigned sbase = (unsigned)__cvta_generic_to_shared(s_f);
     const int z0 = sz * T, zl = (sz * T + T) & (N - 1);
-    for (int i = threadIdx.x; i < 3 * T1 * T1 * CH; i += PUSH_THREADS) {
-      const int row = i / CH, part = i - row * CH;
+    // One patch row (T/4 copies of 16 bytes, then the wrapped last node) per thread and pass:
+    // the row's source and destination are found once, not per copy.
+    for (int row = threadIdx.x; row < 3 * T1 * T1; row += PUSH_THREADS) {
       const int comp = row / (T1 * T1), r = row - comp * (T1 * T1);
       const int lx = r / T1, ly = r - lx * T1;
       const int gx = (sx * T + lx) & (N - 1), gy = (sy * T + ly) & (N - 1);
       const float* src = P.force + comp * N3 + ((long long)gx * N + gy) * N;
-      const unsigned dst = sbase + 4u * (unsigned)(comp * CS + lx * PS + ly * RS + part * 4);
-      if (part < T / 4) cp_async16(dst, src + z0 + part * 4);
-      else cp_async4(dst, src + zl);
+      const unsigned dst = sbase + 4u * (unsigned)(comp * CS + lx * PS + ly * RS);
+#pragma unroll
+      for (int part = 0; part < CH - 1; ++part) cp_async16(dst + 16u * part, src + z0 + part * 4);
+      cp_async4(dst + 16u * (CH - 1), src + zl);
     }
     cp_async_wait_all();
   }
@@ -1391,6 +1405,44 @@ __global__ void k_interp64(const double* __restrict__ F, const double* __restric
   out[i] = s;
 }
 
+// CIC counts of arbitrary float64 positions (pm3d.py:81-89) without an engine: per particle the
+// eight corner weights in 64-bit fixed point (38 fractional bits, the eighth corner taking the
+// remainder, as in the engine's deposit) added with integer atomics, so the sums do not depend
+// on the order; then k_fix_counts turns them into float64 counts.
+__global__ void k_deposit64(const double* __restrict__ X, long long n, int N, double dx, u64* __restrict__ work) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  long long i0[3], i1[3];
+  double f[3];
+  for (int d = 0; d < 3; ++d) {
+    const double g = X[3 * i + d] / dx - 0.5;
+    const double fl = floor(g);
+    const long long c = (long long)fl;
+    f[d] = g - fl;
+    i0[d] = ((c % N) + N) % N;
+    i1[d] = (((c + 1) % N) + N) % N;
+  }
+  const double one = (double)PM_FIX_ONE;
+  const double Fx = f[0] * one, Gx = one - Fx, gy = 1.0 - f[1], gz = 1.0 - f[2];
+  const double pl[4] = {Gx * gy, Gx * f[1], Fx * gy, Fx * f[1]};
+  u64 w[8], sum = 0;
+  for (int c = 0; c < 7; ++c) {
+    w[c] = fix_round(pl[c >> 1], (c & 1) ? f[2] : gz);
+    sum += w[c];
+  }
+  w[7] = PM_FIX_ONE - sum;
+  for (int c = 0; c < 8; ++c) {
+    const int cx = c >> 2, cy = (c >> 1) & 1, cz = c & 1;
+    const long long o = ((cx ? i1[0] : i0[0]) * N + (cy ? i1[1] : i0[1])) * N + (cz ? i1[2] : i0[2]);
+    atomicAdd((unsigned long long*)&work[o], (unsigned long long)w[c]);
+  }
+}
+
+__global__ void k_fix_counts(const u64* __restrict__ work, long long n3, double* __restrict__ counts) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n3) counts[i] = (double)(long long)work[i] * (1.0 / (double)PM_FIX_ONE);
+}
+
 }  // namespace
 
 // Dynamic shared memory of the largest super-tile in use (the smaller ones fit inside).
@@ -1471,4 +1523,10 @@ void launch_get_particles(const StepArgs& A, int pk, const PeakDesc& P, double* 
 }
 void launch_interp64(const double* F, const double* X, long long n, int N, double dx, double* out, cudaStream_t s) {
   k_interp64<<<nb(n, PM_THREADS), PM_THREADS, 0, s>>>(F, X, n, N, dx, out);
+}
+void launch_deposit64(const double* X, long long n, int N, double dx, u64* work, double* counts, cudaStream_t s) {
+  const long long n3 = (long long)N * N * N;
+  cudaMemsetAsync(work, 0, sizeof(u64) * (size_t)n3, s);
+  if (n > 0) k_deposit64<<<nb(n, PM_THREADS), PM_THREADS, 0, s>>>(X, n, N, dx, work);
+  k_fix_counts<<<nb(n3, PM_THREADS), PM_THREADS, 0, s>>>(work, n3, counts);
 }

@@ -115,3 +115,4 @@ void launch_reload(const StepArgs& A, const PeakDesc& P, cudaStream_t s);  // st
 void launch_get_particles(const StepArgs& A, int pk, const PeakDesc& P, double* x, double* p, double* acc,
                           double a_acc, cudaStream_t s);
 void launch_interp64(const double* F, const double* X, long long n, int N, double dx, double* out, cudaStream_t s);
+void launch_deposit64(const double* X, long long n, int N, double dx, u64* work, double* counts, cudaStream_t s);

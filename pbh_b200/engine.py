@@ -167,6 +167,19 @@ def interp64(F, X, L: float):
     return out
 
 
+def deposit64(X, N: int, L: float):
+    """PM3D.deposit on the GPU (pm3d.py:81-89): float64 CIC counts of arbitrary positions, from
+    64-bit fixed-point integer sums (independent of the order of X)."""
+    torch = _lib.require_cuda()
+    lib = _lib.load()
+    Xt = torch.as_tensor(np.asarray(X, dtype=np.float64).reshape(-1, 3)).cuda().contiguous()
+    work = torch.empty(N ** 3, dtype=torch.int64, device="cuda")
+    out = torch.empty((N, N, N), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    check(lib.pm_deposit64(_ptr(Xt), Xt.shape[0], int(N), float(L), _ptr(work), _ptr(out)), "pm_deposit64")
+    return out
+
+
 def sort_u64(keys, lo: int = 0, hi: int = 64):
     """Stable radix sort of uint64 keys over bits [lo, hi) on the GPU: (sorted keys, permutation)."""
     torch = _lib.require_cuda()
