@@ -43,6 +43,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-errors", action="store_true", help="skip the per-output errors against the float64 oracle")
+    ap.add_argument("--no-late", action="store_true", help="skip the device-timed window late in the run")
     ap.add_argument("--full-sort", action="store_true", help="sort the whole cell key every step")
     ap.add_argument("--no-serve", action="store_true", help="skip the served-stream latency run")
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="arrival window of the served stream")
@@ -353,7 +354,7 @@ def run_ours(args):
     late = None
     run_len = min(sp.steps for sp in specs)
     done_steps = args.warmup + args.steps + 16
-    if run_len >= 140 and done_steps <= 120:
+    if run_len >= 140 and done_steps <= 120 and not args.no_late:
         ens.step(120 - done_steps)
         n_late = ens.active_particles()
         ens.engine.sync()

@@ -6,10 +6,11 @@
 
 #include "pm_kernels.cuh"
 
-// Segmented sums over same-cell runs in the deposit when a warp holds fewer than this many runs
-// (0: never; every particle then adds its own eight corners).
+// Segmented sums over same-cell runs in the deposit when a warp's 32 particles lie in fewer
+// than this many cells (runs of four or more on average, as in collapsed regions); otherwise
+// every particle adds its own eight corners (0: never scan).
 #ifndef PM_DEP_SCAN
-#define PM_DEP_SCAN 24
+#define PM_DEP_SCAN 8
 #endif
 
 namespace {
@@ -217,17 +218,15 @@ __device__ __forceinline__ void push_super(const StepArgs& A, const PeakDesc& P,
     // z0 = sz*T is a multiple of 4 and the grids are 256-byte aligned).
     const unsigned sbase = (unsigned)__cvta_generic_to_shared(s_f);
     const int z0 = sz * T, zl = (sz * T + T) & (N - 1);
-    // One patch row (T/4 copies of 16 bytes, then the wrapped last node) per thread and pass:
-    // the row's source and destination are found once, not per copy.
-    for (int row = threadIdx.x; row < 3 * T1 * T1; row += PUSH_THREADS) {
+    for (int i = threadIdx.x; i < 3 * T1 * T1 * CH; i += PUSH_THREADS) {
+      const int row = i / CH, part = i - row * CH;
       const int comp = row / (T1 * T1), r = row - comp * (T1 * T1);
       const int lx = r / T1, ly = r - lx * T1;
       const int gx = (sx * T + lx) & (N - 1), gy = (sy * T + ly) & (N - 1);
       const float* src = P.force + comp * N3 + ((long long)gx * N + gy) * N;
-      const unsigned dst = sbase + 4u * (unsigned)(comp * CS + lx * PS + ly * RS);
-#pragma unroll
-      for (int part = 0; part < CH - 1; ++part) cp_async16(dst + 16u * part, src + z0 + part * 4);
-      cp_async4(dst + 16u * (CH - 1), src + zl);
+      const unsigned dst = sbase + 4u * (unsigned)(comp * CS + lx * PS + ly * RS + part * 4);
+      if (part < T / 4) cp_async16(dst, src + z0 + part * 4);
+      else cp_async4(dst, src + zl);
     }
     cp_async_wait_all();
   }

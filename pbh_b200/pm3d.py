@@ -46,7 +46,10 @@ class StateArray(np.ndarray):
     has rebound is: writing into it changes nothing."""
 
     def __array_finalize__(self, obj):
-        self._owner = getattr(obj, "_owner", None)
+        # views share the state's memory and stay tied to it; a copy (own memory) is a plain
+        # snapshot, as a copy of the reference's array is
+        view = self.base is not None
+        self._owner = getattr(obj, "_owner", None) if view else None
         self._gen = getattr(obj, "_gen", -1)
 
     def _touch(self):
@@ -310,8 +313,8 @@ class PM3D:
             c = eng.clock(0)
             if callback and every > 0:
                 self._stale()
-            callback(self, c.a, c.nsteps)
-            self._flush()
+                callback(self, c.a, c.nsteps)
+                self._flush()
         if eng.clock(0).state == _lib.STATE_FINALIZE:
             eng.run(1)
         self._stale()

@@ -56,6 +56,7 @@ class Request:
     error: str = ""
     status: int = 0              # the peak's device status word when it ended (pm_stats_info.status)
     admit_step: int = -1         # index of the engine step that primed it
+    end_step: int = -1           # index of the engine step after which it was seen to have ended
 
     @property
     def latency(self) -> float:
@@ -246,6 +247,7 @@ class Server:
             if st.status:
                 req.status = int(st.status)
                 req.steps = c.nsteps
+                req.end_step = step_index
                 self._free_slot(slot)
                 self._finish(req, time.perf_counter() - self._t0, ok=False,
                              error=f"device status 0x{req.status:x}")
@@ -253,6 +255,7 @@ class Server:
             if c.state != _lib.STATE_IDLE:
                 continue
             req.steps = c.nsteps
+            req.end_step = step_index
             req.a_collapse_cfg = c.a_collapse / 100.0 if c.a_collapse > 0 else -1.0
             pinned = None
             if self.cfg.keep_delta:

@@ -181,3 +181,7 @@ def test_state_arrays_track_writes_like_the_references_plain_arrays():
     s = fresh(gen=2)                                 # stale copy from an earlier state
     s[0] = 5.0
     assert not owner._host_dirty
+    a = fresh()
+    c = a.copy()                                     # a copy is a snapshot, not the state
+    c[0] = 9.0
+    assert not owner._host_dirty and a[0, 0] == 0.0
