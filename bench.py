@@ -204,11 +204,11 @@ NATIVE_FFT_SIZES = (64, 128, 256, 512)   # meshes the native transform serves (t
 
 def launches_per_step(sizes, fft: str) -> int:
     """Our kernel launches in one steady (non-priming) step of an ensemble with these mesh sizes:
-    push, energy, advance, 3 re-bin, super-tile sort, deposit (faces completed inside) and Green
-    (9); the native transform adds 6 per mesh size it serves (3 passes each way) and drops the
-    Green launch when it serves every mesh.  The radix sort runs only in steps that prime a peak."""
+    push, energy, advance, 3 re-bin, super-tile sort, deposit, fix-up and Green (10); the native
+    transform adds 6 per mesh size it serves (3 passes each way) and drops the Green launch when
+    it serves every mesh.  The radix sort runs only in steps that prime a peak."""
     native = {n for n in sizes if fft == "native" and n in NATIVE_FFT_SIZES}
-    return 9 + 6 * len(native) - (1 if native and all(n in native for n in sizes) else 0)
+    return 10 + 6 * len(native) - (1 if native and all(n in native for n in sizes) else 0)
 
 # DRAM bytes (read + write) per launch from single-kernel ncu captures of a 128^3 run (the
 # summaries under profiles/ give the commands), per particle (per mode for Green), scaled to a

@@ -90,7 +90,6 @@ struct pm_engine {
   u32* sort_gate = nullptr;  // one word: any peak sorts this step
   u32* refresh_gate = nullptr;  // one word: any peak re-sorts its super-tiles this step
   u32* totals = nullptr;
-  u32* face_cnt = nullptr;
   long long* face = nullptr;
   long long* halo = nullptr;
   SortPlan sort{};       // Morton-key sort used by priming and every full_every steps
@@ -146,7 +145,6 @@ struct pm_engine {
     A.face = face;
     A.halo = halo;
     A.sort_err = sort.err;
-    A.face_cnt = face_cnt;
     return A;
   }
 
@@ -220,6 +218,7 @@ struct pm_engine {
     launch_tile_sort(A, nst, stream);
     CU(mark());
     launch_deposit(A, nst, smem_dep, nullptr, stream);
+    launch_fixup(A, nst, nullptr, stream);
     CU(mark());
     if ((r = fft_r2c())) return r;
     CU(mark());
@@ -305,7 +304,7 @@ struct pm_engine {
     void* bufs[] = {d_peaks, d_clocks, d_stats, d_st_base, d_p_base, d_mode_base, d_green_base, d_green_peak, epart,
                     wpart, eslice, ecount, pos, mom, tpos,
                     tmom, keys[0], keys[1], vals[0], vals[1], sstart[0], sstart[1], counts, lpre, far_count,
-                    far_fill, sort_gate, refresh_gate, totals, face_cnt, face, halo};
+                    far_fill, sort_gate, refresh_gate, totals, face, halo};
     for (void* b : bufs) cudaFree(b);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -535,7 +534,6 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   if ((r = E->alloc(&E->sort_gate, 1))) return r;
   if ((r = E->alloc(&E->refresh_gate, 1))) return r;
   if ((r = E->alloc(&E->totals, E->nst))) return r;
-  if ((r = E->alloc(&E->face_cnt, E->nst))) return r;
   if ((r = E->alloc(&E->face, E->nfc))) return r;
   if ((r = E->alloc(&E->halo, E->nhc))) return r;
   CU(cudaMemcpy(E->d_peaks, E->peaks.data(), sizeof(PeakDesc) * npeaks, cudaMemcpyHostToDevice));
@@ -556,7 +554,6 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   CU(cudaMemset(E->tmom, 0, sizeof(float4) * E->ntot));
   CU(cudaMemset(E->far_count, 0, sizeof(u32) * E->nst));
   CU(cudaMemset(E->far_fill, 0, sizeof(u32) * E->nst));
-  CU(cudaMemset(E->face_cnt, 0, sizeof(u32) * E->nst));
   CU(cudaMemset(E->epart, 0, sizeof(double2) * 4 * E->nst));
   CU(cudaMemset(E->wpart, 0, sizeof(double) * E->nmodeblk * (PM_THREADS / 32)));
   CU(cudaMemset(E->ecount, 0, sizeof(u32) * npeaks));
@@ -792,6 +789,7 @@ int pm_get_counts(pm_engine* e, int peak, double* counts) {
   CU(cudaMemcpy(e->d_stats + peak, &st, sizeof(PeakStats), cudaMemcpyHostToDevice));
   // Same kernels with the extra float64 output; delta is rewritten with identical values.
   launch_deposit(e->args(), e->nst, e->smem_dep, counts, e->stream);
+  launch_fixup(e->args(), e->nst, counts, e->stream);
   CU(cudaGetLastError());
   CU(cudaStreamSynchronize(e->stream));
   CU(cudaMemcpy(e->d_clocks, all.data(), sizeof(PeakClock) * e->npeaks, cudaMemcpyHostToDevice));

@@ -1,13 +1,14 @@
 // Step kernels of the pm3d engine: push (CIC gather + kicks + drift, re-binning class),
 // clock advance, regrouping (re-binning scatter, or radix-sort permutation), halo-exchange CIC
-// deposit (faces completed in the same kernel), Green's function + gradient, and particle I/O.
+// deposit with its face fix-up, Green's function + gradient, and particle I/O.
 #include <algorithm>
 #include <type_traits>
 
 #include "pm_kernels.cuh"
 
-#ifndef PM_DEP_F64
-#define PM_DEP_F64 0
+// Sweeps of particle positions a deposit thread keeps in flight (loads issued ahead of use).
+#ifndef PM_DEP_DEPTH
+#define PM_DEP_DEPTH 1
 #endif
 
 namespace {
@@ -220,28 +221,32 @@ __device__ __forceinline__ void push_super(const StepArgs& A, const PeakDesc& P,
   __syncthreads();
   bool bad = false;
   double4 acc_e = make_double4(0.0, 0.0, 0.0, 0.0);  // this thread's momentum and p^2 sums
-  // One particle per thread per sweep, the next two sweeps' particles in flight meanwhile.
-  long long j = b + threadIdx.x;
+  // One particle per thread per sweep, the next two sweeps' particles in flight meanwhile;
+  // 32-bit indices inside the super-tile's range.
+  const int4* __restrict__ pp = A.pos + b;
+  const float4* __restrict__ mp = A.mom + b;
+  const int n = (int)(e - b);
+  int k = threadIdx.x;
   int4 pa = make_int4(0, 0, 0, 0), pb = pa;
   float4 ma = make_float4(0.f, 0.f, 0.f, 0.f), mb = ma;
-  if (j < e) {
-    pa = A.pos[j];
-    ma = A.mom[j];
+  if (k < n) {
+    pa = pp[k];
+    ma = mp[k];
   }
-  if (j + PUSH_THREADS < e) {
-    pb = A.pos[j + PUSH_THREADS];
-    mb = A.mom[j + PUSH_THREADS];
+  if (k + PUSH_THREADS < n) {
+    pb = pp[k + PUSH_THREADS];
+    mb = mp[k + PUSH_THREADS];
   }
-  for (; j < e; j += PUSH_THREADS) {
+  for (; k < n; k += PUSH_THREADS) {
     const int4 p0 = pa;
     const float4 m0 = ma;
     pa = pb;
     ma = mb;
-    if (j + 2 * PUSH_THREADS < e) {
-      pb = A.pos[j + 2 * PUSH_THREADS];
-      mb = A.mom[j + 2 * PUSH_THREADS];
+    if (k + 2 * PUSH_THREADS < n) {
+      pb = pp[k + 2 * PUSH_THREADS];
+      mb = mp[k + 2 * PUSH_THREADS];
     }
-    push_one<T>(A, P, s_f, K, sx, sy, sz, p0, m0, j, s_cnt, bad, acc_e);
+    push_one<T>(A, P, s_f, K, sx, sy, sz, p0, m0, b + k, s_cnt, bad, acc_e);
   }
   if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&A.stats[pk].status, 1u);
   for (int c = threadIdx.x; c < P.NC; c += PUSH_THREADS) A.counts[(P.st_base + st) * BIN_CLASSES + c] = s_cnt[c];
@@ -751,8 +756,8 @@ __global__ void __launch_bounds__(TSORT_THREADS) k_tile_sort(StepArgs A, long lo
 // lower faces (which neighbours also reach) and on the upper halo (which belongs to the
 // neighbours) are written as 64-bit partials.
 //
-// The face nodes are completed in the same kernel (complete_faces): own partial plus the lower
-// neighbours' halo partials, by whichever of the 8 contributing CTAs finishes last.
+// The face fix-up (k_fixup, the next launch) completes the face nodes: own partial plus the
+// lower neighbours' halo partials.
 // Integer sums make the result independent of particle order, bit for bit; no float atomics.
 __device__ __forceinline__ int face_index(int lx, int ly, int lz, int T) {
   if (lx == 0) return ly * T + lz;
@@ -784,7 +789,7 @@ __device__ __forceinline__ void face_coords(int f, int& lx, int& ly, int& lz) {
   }
 }
 
-// Finish the face nodes of super-tile Y (a whole deposit CTA): each face node's own
+// Finish the face nodes of super-tile Y (whole CTA of FIX_THREADS): each face node's own
 // partial plus the halo partials of the lower neighbours Y - o, o = (ox, oy, oz) in {0,1}^3 \ 0,
 // that reach it (node (lx + TS ox, ...) of the neighbour, which lies on its upper halo, for a
 // face node with (lx, ly, lz) zero where o is one).  nb[o]: the neighbours' halo partials.
@@ -796,7 +801,7 @@ __device__ __forceinline__ void fixup_faces(const StepArgs& A, const PeakDesc& P
   const int N = P.N;
   const int sx = pm_compact3(Y >> 2), sy = pm_compact3(Y >> 1), sz = pm_compact3(Y);
   const long long* face = A.face + P.face_off + (long long)Y * FC;
-  for (int f = threadIdx.x; f < FC; f += DEP_THREADS) {
+  for (int f = threadIdx.x; f < FC; f += FIX_THREADS) {
     int lx, ly, lz;
     face_coords<TS>(f, lx, ly, lz);
     long long S = __ldcg(face + f);
@@ -810,48 +815,6 @@ __device__ __forceinline__ void fixup_faces(const StepArgs& A, const PeakDesc& P
     if (rho64) rho64[node] = (double)S * (1.0 / (double)PM_FIX_ONE);
     dsum += Dv;
     smax = S > smax ? S : smax;
-  }
-}
-
-// Completion of the lower faces inside the deposit kernel.  A super-tile's face nodes need its
-// own partials and the halo partials of its 7 lower neighbours, so every deposit CTA, once its
-// partials are written, counts itself in at the 8 super-tiles they reach (its own and its 7
-// upper neighbours); the CTA whose count is the 8th for a super-tile completes that super-tile's
-// faces and resets its counter for the next deposit.  Nobody waits: the last contributor is
-// the one that finds everything in place.  Writers fence before counting and the completer
-// fences after, so the completer's L2 reads see every contributor's partials.
-template <int TS>
-__device__ __forceinline__ void complete_faces(const StepArgs& A, const PeakDesc& P, u32 st, double* rho64,
-                                               long long& dsum, long long& smax) {
-  __shared__ u32 s_tgt[8];
-  __shared__ const long long* s_nb[8];
-  const int NS = P.NS;
-  const int sx = pm_compact3(st >> 2), sy = pm_compact3(st >> 1), sz = pm_compact3(st);
-  __threadfence();   // this thread's partial stores, before the count below
-  __syncthreads();
-  if (threadIdx.x < 8) {
-    const int o = threadIdx.x;
-    const u32 tgt = pm_morton3((sx + (o & 1)) & (NS - 1), (sy + ((o >> 1) & 1)) & (NS - 1),
-                               (sz + (o >> 2)) & (NS - 1));
-    const u32 prev = atomicAdd(&A.face_cnt[P.st_base + tgt], 1u);
-    s_tgt[o] = prev == 7u ? tgt : 0xFFFFFFFFu;
-  }
-  __syncthreads();
-#pragma unroll 1
-  for (int k = 0; k < 8; ++k) {
-    const u32 Y = s_tgt[k];
-    if (Y == 0xFFFFFFFFu) continue;  // uniform across the block
-    __threadfence();
-    if (threadIdx.x < 8) {
-      const int o = threadIdx.x, ox = o & 1, oy = (o >> 1) & 1, oz = (o >> 2) & 1;
-      const u32 sn = pm_morton3((pm_compact3(Y >> 2) - ox) & (NS - 1), (pm_compact3(Y >> 1) - oy) & (NS - 1),
-                                (pm_compact3(Y) - oz) & (NS - 1));
-      s_nb[o] = A.halo + P.halo_off + (long long)sn * P.hc;
-    }
-    if (threadIdx.x == 0) A.face_cnt[P.st_base + Y] = 0u;
-    __syncthreads();
-    fixup_faces<TS>(A, P, Y, s_nb, rho64, dsum, smax);
-    __syncthreads();  // s_nb is rewritten for the next completion
   }
 }
 
@@ -941,16 +904,24 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
   constexpr int CH_IT = 8191 / DEP_THREADS;  // sweeps of DEP_THREADS particles per chunk
   static_assert(CH_IT >= 1 && CH_IT * DEP_THREADS <= 8191, "chunk too large for the split accumulators");
   static_assert(PM_FIX_BITS == 38, "the split accumulators assume 38 fractional bits");
-  const long long nit = (total + DEP_THREADS - 1) / DEP_THREADS;
-  long long j = b + threadIdx.x;
-  int4 pn = j < e ? A.pos[j] : make_int4(-1, 0, 0, 0);  // the next sweep's particle, in flight
+  // 32-bit indices inside the super-tile's range (fewer integer instructions than 64-bit ones).
+  const int4* __restrict__ pp = A.pos + b;
+  const int n = (int)total;
+  const int nit = (n + DEP_THREADS - 1) / DEP_THREADS;
+  int k = threadIdx.x;
+  constexpr int DEPTH = PM_DEP_DEPTH;
+  int4 q[DEPTH];  // the particles of the next DEPTH sweeps, loads in flight
+#pragma unroll
+  for (int d = 0; d < DEPTH; ++d) q[d] = k + d * DEP_THREADS < n ? pp[k + d * DEP_THREADS] : make_int4(-1, 0, 0, 0);
   bool bad = false;
   int left = CH_IT;
-  for (long long it = 0; it < nit; ++it) {
-    const int4 ps = pn;
-    const bool valid = j < e;
-    if (j + DEP_THREADS < e) pn = A.pos[j + DEP_THREADS];
-    j += DEP_THREADS;
+  for (int it = 0; it < nit; ++it) {
+    const int4 ps = q[0];
+    const bool valid = k < n;
+#pragma unroll
+    for (int d = 0; d + 1 < DEPTH; ++d) q[d] = q[d + 1];
+    if (k + DEPTH * DEP_THREADS < n) q[DEPTH - 1] = pp[k + DEPTH * DEP_THREADS];
+    k += DEP_THREADS;
     {
       const int c = ps.x;
       const bool in = valid && (c & ~local) == tile_bits;
@@ -989,7 +960,7 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
   if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&A.stats[pk].status, 1u);
   // Write-out of the last chunk (plus the folded ones), four nodes of a patch row at a time:
   // interior nodes final as FP32 delta (16-byte stores; the first node of an interior row is a
-  // face node, stored here from this super-tile's own sum and completed by complete_faces), nodes on
+  // face node, stored here from this super-tile's own sum and completed by k_fixup), nodes on
   // the lower faces and on the upper halo as 64-bit partials.
   long long dsum = 0, smax = 0;
   const long long gbase = ((long long)sx * TS * N + (long long)sy * TS) * N + sz * TS;
@@ -1044,7 +1015,6 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
       }
     }
   }
-  complete_faces<TS>(A, P, st, rho64, dsum, smax);
   for (int d = 16; d > 0; d >>= 1) {
     dsum += __shfl_xor_sync(0xffffffffu, dsum, d);
     const long long om = __shfl_xor_sync(0xffffffffu, smax, d);
@@ -1068,176 +1038,6 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
   }
 }
 
-#if PM_DEP_F64
-// Deposit with FP64 shared-memory accumulators: every corner weight is an integer in units of
-// 2^-38 below 2^39 in magnitude, and a node's sum over a chunk of at most 8191 particles stays
-// below 2^51, so FP64 additions of them are exact and the sums do not depend on the order: the
-// same bits as the split 32-bit accumulators, with one atomic per corner instead of two.  Row
-// and plane strides of the patch put the 16 doubles of each half-warp of Morton-consecutive
-// cells into distinct bank pairs.
-__host__ __device__ constexpr int dep64_rs(int TS) { return TS == 4 ? 12 : TS == 8 ? 12 : 20; }
-__host__ __device__ constexpr int dep64_ps(int TS) { return TS == 4 ? 72 : TS == 8 ? 120 : 360; }
-
-template <int TS>
-__device__ __noinline__ void fold_chunk64(u64* acc64, double* acc, bool add) {
-  constexpr int T1 = TS + 1, NN = T1 * T1 * T1;
-  for (int node = threadIdx.x; node < NN; node += DEP_THREADS) {
-    const int lx = node / (T1 * T1), r = node - lx * (T1 * T1), ly = r / T1, lz = r - ly * T1;
-    const int ad = lx * dep64_ps(TS) + ly * dep64_rs(TS) + lz;
-    acc64[node] = (add ? acc64[node] : 0ull) + (u64)__double2ll_rn(acc[ad]);
-    acc[ad] = 0.0;
-  }
-}
-
-template <int TS>
-__device__ __forceinline__ void deposit_super64(const StepArgs& A, const PeakDesc& P, const PeakClock& C, int pk,
-                                                u32 st, u32* smem, double* rho64) {
-  constexpr int T1 = TS + 1, NN = T1 * T1 * T1;
-  constexpr int RS = dep64_rs(TS), PS = dep64_ps(TS), SZ = T1 * PS;
-  constexpr int NG = TS / 4 + 1;
-  constexpr int FC = TS * TS * TS - (TS - 1) * (TS - 1) * (TS - 1);
-  static_assert(RS % 4 == 0 && PS % 4 == 0 && RS >= 4 * NG, "patch rows are read 32 bytes at a time");
-  double* acc = reinterpret_cast<double*>(smem);
-  __shared__ long long s_red[DEP_THREADS / 32];
-  __shared__ long long s_max[DEP_THREADS / 32];
-  const int N = P.N, l2 = P.log2N;
-  const int sx = pm_compact3(st >> 2), sy = pm_compact3(st >> 1), sz = pm_compact3(st);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  static_assert(SZ % 2 == 0, "accumulators are cleared 16 bytes at a time");
-  for (int i = threadIdx.x; i < SZ / 2; i += DEP_THREADS) reinterpret_cast<uint4*>(smem)[i] = make_uint4(0u, 0u, 0u, 0u);
-  const u32* ss = sst(A, C.sbuf) + P.sst_off;
-  const long long b = ss[st], e = ss[st + 1];
-  const long long total = e - b;
-  const int local = ((TS - 1) << (2 * l2)) | ((TS - 1) << l2) | (TS - 1);
-  const int tile_bits = ((sx * TS) << (2 * l2)) | ((sy * TS) << l2) | (sz * TS);
-  __syncthreads();
-  static_assert((8191 / DEP_THREADS) * DEP_THREADS * sizeof(int4) >= NN * sizeof(u64), "fold scratch too small");
-  bool folded = false;
-  constexpr int CH_IT = 8191 / DEP_THREADS;
-  const long long nit = (total + DEP_THREADS - 1) / DEP_THREADS;
-  long long j = b + threadIdx.x;
-  int4 pn = j < e ? A.pos[j] : make_int4(-1, 0, 0, 0);
-  bool bad = false;
-  int left = CH_IT;
-  for (long long it = 0; it < nit; ++it) {
-    const int4 ps = pn;
-    const bool valid = j < e;
-    if (j + DEP_THREADS < e) pn = A.pos[j + DEP_THREADS];
-    j += DEP_THREADS;
-    {
-      const int c = ps.x;
-      const bool in = valid && (c & ~local) == tile_bits;
-      bad |= valid && !in;
-      const double one = (double)PM_FIX_ONE, big = 4503599627370496.0;
-      const double fx = __int_as_float(ps.y), fy = __int_as_float(ps.z), fz = __int_as_float(ps.w);
-      const double Fx = fx * one, Gx = one - Fx;
-      const double gy = 1.0 - fy, gz = 1.0 - fz;
-      const double w00 = Gx * gy, w01 = Gx * fy, w10 = Fx * gy, w11 = Fx * fy;
-      double w[8];
-      w[0] = fma(w00, gz, big) - big;
-      w[1] = fma(w00, fz, big) - big;
-      w[2] = fma(w01, gz, big) - big;
-      w[3] = fma(w01, fz, big) - big;
-      w[4] = fma(w10, gz, big) - big;
-      w[5] = fma(w10, fz, big) - big;
-      w[6] = fma(w11, gz, big) - big;
-      w[7] = one - (((w[0] + w[1]) + (w[2] + w[3])) + ((w[4] + w[5]) + w[6]));
-      if (in) {
-        const int nb = ((c >> (2 * l2)) & (TS - 1)) * PS + ((c >> l2) & (TS - 1)) * RS + (c & (TS - 1));
-        const int off[8] = {0, 1, RS, RS + 1, PS, PS + 1, PS + RS, PS + RS + 1};
-#pragma unroll
-        for (int q = 0; q < 8; ++q) atomicAdd(&acc[nb + off[q]], w[q]);
-      }
-    }
-    if (--left == 0 && it + 1 < nit) {
-      left = CH_IT;
-      __syncthreads();
-      fold_chunk64<TS>(reinterpret_cast<u64*>(A.tpos + b), acc, folded);
-      folded = true;
-      __syncthreads();
-    }
-  }
-  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&A.stats[pk].status, 1u);
-  long long dsum = 0, smax = 0;
-  const long long gbase = ((long long)sx * TS * N + (long long)sy * TS) * N + sz * TS;
-  long long* face = A.face + P.face_off + (long long)st * FC;
-  long long* halo = A.halo + P.halo_off + (long long)st * P.hc;
-  const u64* fold = reinterpret_cast<const u64*>(A.tpos + b);
-  const long long nmf = P.n_mean_fix;
-  const double inv = P.inv_fix_nmean;
-  for (int item = threadIdx.x; item < T1 * T1 * NG; item += DEP_THREADS) {
-    const int row = item / NG, g = item - row * NG;
-    const int lx = row / T1, ly = row - lx * T1;
-    const int ad = lx * PS + ly * RS + 4 * g;
-    const double2 h0 = *reinterpret_cast<const double2*>(acc + ad);
-    const double2 h1 = *reinterpret_cast<const double2*>(acc + ad + 2);
-    long long S[4] = {__double2ll_rn(h0.x), __double2ll_rn(h0.y), __double2ll_rn(h1.x), __double2ll_rn(h1.y)};
-    const int nbase = row * T1 + 4 * g;
-    if (folded) {
-#pragma unroll
-      for (int k = 0; k < 4; ++k)
-        if (4 * g + k <= TS) S[k] += (long long)fold[nbase + k];
-    }
-    if (lx == TS || ly == TS) {
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const int lz = 4 * g + k;
-        if (lz <= TS) halo[halo_index(lx, ly, lz, TS)] = S[k];
-      }
-    } else if (g == NG - 1) {
-      halo[halo_index(lx, ly, TS, TS)] = S[0];
-    } else if (lx == 0 || ly == 0) {
-#pragma unroll
-      for (int k = 0; k < 4; ++k) face[face_index(lx, ly, 4 * g + k, TS)] = S[k];
-    } else {
-      if (g == 0) face[face_index(lx, ly, 0, TS)] = S[0];
-      float4 d;
-      float* dv = &d.x;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const long long D = S[k] - nmf;
-        dv[k] = (float)((double)D * inv);
-        if (g > 0 || k > 0) {
-          dsum += D;
-          smax = S[k] > smax ? S[k] : smax;
-        }
-      }
-      const long long gi = gbase + ((long long)lx * N + ly) * N + 4 * g;
-      *reinterpret_cast<float4*>(P.delta + gi) = d;
-      if (rho64) {
-#pragma unroll
-        for (int k = 0; k < 4; ++k)
-          if (g > 0 || k > 0) rho64[gi + k] = (double)S[k] * (1.0 / (double)PM_FIX_ONE);
-      }
-    }
-  }
-  complete_faces<TS>(A, P, st, rho64, dsum, smax);
-  for (int d = 16; d > 0; d >>= 1) {
-    dsum += __shfl_xor_sync(0xffffffffu, dsum, d);
-    const long long om = __shfl_xor_sync(0xffffffffu, smax, d);
-    smax = om > smax ? om : smax;
-  }
-  if (lane == 0) {
-    s_red[warp] = dsum;
-    s_max[warp] = smax;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    long long ts = 0, tm = 0;
-    for (int w2 = 0; w2 < DEP_THREADS / 32; ++w2) {
-      ts += s_red[w2];
-      tm = s_max[w2] > tm ? s_max[w2] : tm;
-    }
-    atomicAdd((unsigned long long*)&A.stats[pk].mass_defect, (unsigned long long)ts);
-    atomicMax(&A.stats[pk].max_fix, (u64)tm);
-    A.far_count[P.st_base + st] = 0u;
-    A.far_fill[P.st_base + st] = 0u;
-  }
-}
-#define PM_DEPOSIT_SUPER deposit_super64
-#else
-#define PM_DEPOSIT_SUPER deposit_super
-#endif
 
 __global__ void __launch_bounds__(DEP_THREADS, 4) k_deposit(StepArgs A, double* rho64) {
   extern __shared__ __align__(16) u32 s_dep[];
@@ -1246,9 +1046,54 @@ __global__ void __launch_bounds__(DEP_THREADS, 4) k_deposit(StepArgs A, double* 
   if (!C.dep) return;
   const PeakDesc P = A.peaks[tr.pk];
   switch (P.TS) {
-    case 4: PM_DEPOSIT_SUPER<4>(A, P, C, tr.pk, (u32)tr.t, s_dep, rho64); break;
-    case 8: PM_DEPOSIT_SUPER<8>(A, P, C, tr.pk, (u32)tr.t, s_dep, rho64); break;
-    default: PM_DEPOSIT_SUPER<16>(A, P, C, tr.pk, (u32)tr.t, s_dep, rho64); break;
+    case 4: deposit_super<4>(A, P, C, tr.pk, (u32)tr.t, s_dep, rho64); break;
+    case 8: deposit_super<8>(A, P, C, tr.pk, (u32)tr.t, s_dep, rho64); break;
+    default: deposit_super<16>(A, P, C, tr.pk, (u32)tr.t, s_dep, rho64); break;
+  }
+}
+
+// Face fix-up: one CTA per super-tile whose peak deposited this step.  Small and
+// latency-bound, so many CTAs per SM.
+__global__ void __launch_bounds__(FIX_THREADS) k_fixup(StepArgs A, double* rho64) {
+  __shared__ long long s_red[FIX_THREADS / 32];
+  __shared__ long long s_max[FIX_THREADS / 32];
+  __shared__ const long long* s_nb[8];
+  const TileRef tr = find_tile(A.st_base, A.npeaks);
+  if (!A.clocks[tr.pk].dep) return;
+  const PeakDesc P = A.peaks[tr.pk];
+  const u32 Y = (u32)tr.t;
+  if (threadIdx.x < 8) {
+    const int o = threadIdx.x, NS = P.NS;
+    const u32 sn = pm_morton3((pm_compact3(Y >> 2) - (o & 1)) & (NS - 1), (pm_compact3(Y >> 1) - ((o >> 1) & 1)) & (NS - 1),
+                              (pm_compact3(Y) - (o >> 2)) & (NS - 1));
+    s_nb[o] = A.halo + P.halo_off + (long long)sn * P.hc;
+  }
+  __syncthreads();
+  long long dsum = 0, smax = 0;
+  switch (P.TS) {
+    case 4: fixup_faces<4>(A, P, Y, s_nb, rho64, dsum, smax); break;
+    case 8: fixup_faces<8>(A, P, Y, s_nb, rho64, dsum, smax); break;
+    default: fixup_faces<16>(A, P, Y, s_nb, rho64, dsum, smax); break;
+  }
+  for (int d = 16; d > 0; d >>= 1) {
+    dsum += __shfl_xor_sync(0xffffffffu, dsum, d);
+    const long long om = __shfl_xor_sync(0xffffffffu, smax, d);
+    smax = om > smax ? om : smax;
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    s_red[warp] = dsum;
+    s_max[warp] = smax;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long ts = 0, tm = 0;
+    for (int w = 0; w < FIX_THREADS / 32; ++w) {
+      ts += s_red[w];
+      tm = s_max[w] > tm ? s_max[w] : tm;
+    }
+    atomicAdd((unsigned long long*)&A.stats[tr.pk].mass_defect, (unsigned long long)ts);
+    atomicMax(&A.stats[tr.pk].max_fix, (u64)tm);
   }
 }
 
@@ -1555,13 +1400,7 @@ __global__ void k_fix_counts(const u64* __restrict__ work, long long n3, double*
 }  // namespace
 
 // Dynamic shared memory of the largest super-tile in use (the smaller ones fit inside).
-size_t pm_deposit_smem(int TSmax) {
-#if PM_DEP_F64
-  return sizeof(double) * (size_t)(TSmax + 1) * dep64_ps(TSmax);
-#else
-  return sizeof(u32) * 2 * (size_t)patch_size(TSmax);
-#endif
-}
+size_t pm_deposit_smem(int TSmax) { return sizeof(u32) * 2 * (size_t)patch_size(TSmax); }
 size_t pm_push_smem(int TSmax) { return sizeof(float) * 3 * (size_t)patch_size(TSmax); }
 
 size_t pm_tile_sort_smem() {
@@ -1613,6 +1452,9 @@ void launch_bin(const StepArgs& A, long long nst, cudaStream_t s) {
 }
 void launch_deposit(const StepArgs& A, long long nst, size_t smem, double* rho64, cudaStream_t s) {
   k_deposit<<<(unsigned)nst, DEP_THREADS, smem, s>>>(A, rho64);
+}
+void launch_fixup(const StepArgs& A, long long nst, double* rho64, cudaStream_t s) {
+  k_fixup<<<(unsigned)nst, FIX_THREADS, 0, s>>>(A, rho64);
 }
 void launch_green(const StepArgs& A, long long nblocks, cudaStream_t s) {
   k_green<<<(unsigned)nblocks, PM_THREADS, 0, s>>>(A);

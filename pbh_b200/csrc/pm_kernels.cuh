@@ -12,8 +12,8 @@
 //              (local counting sort); when particles are first loaded, a full Morton-key radix
 //              sort plus a permutation instead
 //   deposit    per super-tile: CIC density of its particles into (TS+1)^3 nodes; interior nodes
-//              final, face and upper-halo nodes as 64-bit partials; the last of the 8 CTAs whose
-//              partials reach a super-tile's faces completes them (own + lower neighbours' halos)
+//              final, face and upper-halo nodes as 64-bit partials
+//   fixup      per super-tile: face nodes = own partial + the lower neighbours' halo partials
 //   R2C, Green, C2R (x3)
 #pragma once
 #include "common.cuh"
@@ -24,6 +24,7 @@
 #define DEP_THREADS 256    // deposit CTA (4 per SM)
 #define GREEN_MODES 4      // modes per thread of the Green kernel (a block covers PM_THREADS * GREEN_MODES)
 #define ENERGY_SLICES 16   // CTAs per peak of the energy reduction
+#define FIX_THREADS 256    // face fix-up CTA
 #define TSORT_THREADS 1024 // super-tile sort (refresh) CTA
 #define TSORT_CAP 5120     // particles of a super-tile sorted in shared memory; denser ones via global
 #define BIN_CLASSES 128   // stride of the per-super-tile class arrays (>= 125)
@@ -65,7 +66,6 @@ struct StepArgs {
   double2* eslice;             // [peak][ENERGY_SLICES][5] slice partials of the energy kernel
   u32* ecount;                 // [peak] energy slices finished this step (0 between steps)
   int* sort_err;               // [peak] the priming sort's bounded look-back gave up (sort plan)
-  u32* face_cnt;               // [super-tile] deposit CTAs whose partials reached its faces (0 between deposits)
 };
 
 // Binary search: largest i in [0, n) with base[i] <= v.
@@ -90,6 +90,7 @@ void launch_st_starts(const StepArgs& A, long long ntot, cudaStream_t s);
 void launch_bin(const StepArgs& A, long long nst, cudaStream_t s);
 void launch_tile_sort(const StepArgs& A, long long nst, cudaStream_t s);
 void launch_deposit(const StepArgs& A, long long nst, size_t smem, double* rho64, cudaStream_t s);
+void launch_fixup(const StepArgs& A, long long nst, double* rho64, cudaStream_t s);
 void launch_green(const StepArgs& A, long long nblocks, cudaStream_t s);
 
 // Native real FFT of 256^3 and 512^3 meshes (native_fft.cu).  fft_native_init: once per device

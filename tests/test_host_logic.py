@@ -97,14 +97,14 @@ def test_served_slot_pool_fits_the_budget():
 
 def test_launch_accounting():
     import bench
-    assert bench.launches_per_step([32], "native") == 9               # cuFFT size only
-    assert bench.launches_per_step([32, 64], "native") == 15          # 64^3 native, Green for 32^3
-    assert bench.launches_per_step([32, 64, 128, 256], "native") == 27  # the batched ensemble
-    assert bench.launches_per_step([256], "cufft") == 9
-    assert bench.launches_per_step([256], "native") == 14             # + 6, no Green launch
-    assert bench.launches_per_step([512], "native") == 14
-    assert bench.launches_per_step([32, 256, 256], "native") == 15    # Green still runs for 32^3
-    assert bench.launches_per_step([256, 512], "native") == 20
+    assert bench.launches_per_step([32], "native") == 10              # cuFFT size only
+    assert bench.launches_per_step([32, 64], "native") == 16          # 64^3 native, Green for 32^3
+    assert bench.launches_per_step([32, 64, 128, 256], "native") == 28  # the batched ensemble
+    assert bench.launches_per_step([256], "cufft") == 10
+    assert bench.launches_per_step([256], "native") == 15             # + 6, no Green launch
+    assert bench.launches_per_step([512], "native") == 15
+    assert bench.launches_per_step([32, 256, 256], "native") == 16    # Green still runs for 32^3
+    assert bench.launches_per_step([256, 512], "native") == 21
 
 
 def test_algorithmic_bytes_per_phase():
