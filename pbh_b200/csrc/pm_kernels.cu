@@ -23,31 +23,6 @@ __host__ __device__ constexpr int patch_rs(int TS) { return TS == 4 ? 8 : TS == 
 __host__ __device__ constexpr int patch_ps(int TS) { return TS == 4 ? 44 : TS == 8 ? 112 : 368; }
 __host__ __device__ constexpr int patch_size(int TS) { return (TS + 1) * patch_ps(TS); }
 
-#ifndef PM_XU_FREE
-#define PM_XU_FREE 1
-#endif
-// Exact FP64 value of an FP32 without the conversion unit: a normal float's exponent is
-// re-biased (127 -> 1023) and its 23-bit mantissa moved to the top of the double's 52; zero,
-// subnormals, infinities and NaN (rare) take the conversion instruction.
-__device__ __forceinline__ double f32_to_f64(float f) {
-#if PM_XU_FREE
-  const u32 b = __float_as_uint(f), e = (b >> 23) & 0xFFu;
-  if (e - 1u >= 254u) return (double)f;
-  return __hiloint2double((int)((b & 0x80000000u) | ((e + 896u) << 20) | ((b >> 3) & 0xFFFFFu)), (int)(b << 29));
-#else
-  return (double)f;
-#endif
-}
-// Exact FP64 value of a 64-bit integer |D| < 2^51 without the conversion unit: added to 1.5 2^52
-// in the integer domain it is the mantissa of a double whose value is D + 1.5 2^52.
-__device__ __forceinline__ double fix_to_double(long long D) {
-#if PM_XU_FREE
-  return __longlong_as_double(D + 0x4338000000000000LL) - 6755399441055744.0;
-#else
-  return (double)D;
-#endif
-}
-
 __device__ __forceinline__ void cp_async16(unsigned dst, const void* src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
 }
@@ -157,7 +132,7 @@ __device__ __forceinline__ void push_one(const StepArgs& A, const PeakDesc& P, c
   // Momentum synchronised with the positions (after the closing kick): energy and momentum sums.
   {
     double4 t = acc_e;
-    const double dx = f32_to_f64(px), dy = f32_to_f64(py), dz = f32_to_f64(pz);
+    const double dx = px, dy = py, dz = pz;
     t.x += dx;
     t.y += dy;
     t.z += dz;
@@ -837,7 +812,7 @@ __device__ __forceinline__ void fixup_faces(const StepArgs& A, const PeakDesc& P
     }
     const long long Dv = S - P.n_mean_fix;
     const long long node = ((long long)(sx * TS + lx) * N + (sy * TS + ly)) * N + (sz * TS + lz);
-    P.delta[node] = (float)(fix_to_double(Dv) * P.inv_fix_nmean);
+    P.delta[node] = (float)((double)Dv * P.inv_fix_nmean);
     if (rho64) rho64[node] = (double)S * (1.0 / (double)PM_FIX_ONE);
     dsum += Dv;
     smax = S > smax ? S : smax;
@@ -953,8 +928,7 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
       const bool in = valid && (c & ~local) == tile_bits;
       bad |= valid && !in;
       const double one = (double)PM_FIX_ONE;
-      const double fx = f32_to_f64(__int_as_float(ps.y)), fy = f32_to_f64(__int_as_float(ps.z)),
-                   fz = f32_to_f64(__int_as_float(ps.w));
+      const double fx = __int_as_float(ps.y), fy = __int_as_float(ps.z), fz = __int_as_float(ps.w);
       const double Fx = fx * one, Gx = one - Fx;   // exact: fx has 24 significant bits
       const double gy = 1.0 - fy, gz = 1.0 - fz;
       const double w00 = Gx * gy, w01 = Gx * fy, w10 = Fx * gy, w11 = Fx * fy;
@@ -1027,7 +1001,7 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         const long long D = S[k] - nmf;
-        dv[k] = (float)(fix_to_double(D) * inv);
+        dv[k] = (float)((double)D * inv);
         if (g > 0 || k > 0) {
           dsum += D;
           smax = S[k] > smax ? S[k] : smax;
