@@ -95,7 +95,7 @@ struct PushCoef {
 template <int T>
 __device__ __forceinline__ void push_one(const StepArgs& A, const PeakDesc& P, const float* __restrict__ s_f,
                                          const PushCoef& K, int sx, int sy, int sz, int4 ps, float4 m, long long j,
-                                         u32* s_cnt, bool& bad, float4& acc_f) {
+                                         u32* s_cnt, bool& bad, double4& acc_e) {
   constexpr int RS = patch_rs(T), PS = patch_ps(T), CS = patch_size(T);
   const int N = P.N, l2 = P.log2N;
   const int ix = ps.x >> (2 * l2), iy = (ps.x >> l2) & (N - 1), iz = ps.x & (N - 1);
@@ -129,12 +129,16 @@ __device__ __forceinline__ void push_one(const StepArgs& A, const PeakDesc& P, c
   ay *= K.gscale;
   az *= K.gscale;
   float px = m.x + K.kA * ax, py = m.y + K.kA * ay, pz = m.z + K.kA * az;
-  // Momentum synchronised with the positions (after the closing kick): energy and momentum sums,
-  // FP32 over at most PUSH_FLUSH particles of this thread, then added to its FP64 sums.
-  acc_f.x += px;
-  acc_f.y += py;
-  acc_f.z += pz;
-  acc_f.w = fmaf(px, px, fmaf(py, py, fmaf(pz, pz, acc_f.w)));
+  // Momentum synchronised with the positions (after the closing kick): energy and momentum sums.
+  {
+    double4 t = acc_e;
+    const double dx = px, dy = py, dz = pz;
+    t.x += dx;
+    t.y += dy;
+    t.z += dz;
+    t.w += dx * dx + dy * dy + dz * dz;
+    acc_e = t;
+  }
   int nx = ix, ny = iy, nz = iz;
   int mx = 0, my = 0, mz = 0;  // cells moved along each axis
   const bool finite = isfinite(px) && isfinite(py) && isfinite(pz);
@@ -217,21 +221,7 @@ __device__ __forceinline__ void push_super(const StepArgs& A, const PeakDesc& P,
   }
   __syncthreads();
   bool bad = false;
-  // This thread's momentum and p^2 sums: FP32 over its last few particles, added into FP64 sums
-  // kept in shared memory (registers are the push's limit).
-  // after the patch in dynamic shared memory, rounded up to 32 bytes
-  double4* s_acc = reinterpret_cast<double4*>(s_f + ((3 * CS + 7) & ~7));
-  s_acc[threadIdx.x] = make_double4(0.0, 0.0, 0.0, 0.0);
-  float4 acc_f = make_float4(0.f, 0.f, 0.f, 0.f);
-  auto flush = [&]() {
-    double4 t = s_acc[threadIdx.x];
-    t.x += (double)acc_f.x;
-    t.y += (double)acc_f.y;
-    t.z += (double)acc_f.z;
-    t.w += (double)acc_f.w;
-    s_acc[threadIdx.x] = t;
-    acc_f = make_float4(0.f, 0.f, 0.f, 0.f);
-  };
+  double4 acc_e = make_double4(0.0, 0.0, 0.0, 0.0);  // this thread's momentum and p^2 sums
   // One particle per thread per sweep, the next two sweeps' particles in flight meanwhile;
   // 32-bit indices inside the super-tile's range.
   const int4* __restrict__ pp = A.pos + b;
@@ -257,17 +247,14 @@ __device__ __forceinline__ void push_super(const StepArgs& A, const PeakDesc& P,
       pb = pp[k + 2 * PUSH_THREADS];
       mb = mp[k + 2 * PUSH_THREADS];
     }
-    push_one<T>(A, P, s_f, K, sx, sy, sz, p0, m0, b + k, s_cnt, bad, acc_f);
-    static_assert((PUSH_FLUSH & (PUSH_FLUSH - 1)) == 0 && PUSH_THREADS == 512, "sweep index is k >> 9");
-    if (((k >> 9) & (PUSH_FLUSH - 1)) == PUSH_FLUSH - 1) flush();
+    push_one<T>(A, P, s_f, K, sx, sy, sz, p0, m0, b + k, s_cnt, bad, acc_e);
   }
-  flush();
   if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&A.stats[pk].status, 1u);
   for (int c = threadIdx.x; c < P.NC; c += PUSH_THREADS) A.counts[(P.st_base + st) * BIN_CLASSES + c] = s_cnt[c];
   // Super-tile partials of the momentum and p^2 sums (compensated, fixed order).
   __shared__ CSum s_e[PUSH_THREADS / 32][4];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const double4 ev = s_acc[threadIdx.x];
+  const double4 ev = acc_e;
   const double ea[4] = {ev.x, ev.y, ev.z, ev.w};
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
@@ -283,7 +270,7 @@ __device__ __forceinline__ void push_super(const StepArgs& A, const PeakDesc& P,
 }
 
 __global__ void __launch_bounds__(PUSH_THREADS, 2) k_push(StepArgs A) {
-  extern __shared__ __align__(32) float s_f[];
+  extern __shared__ __align__(16) float s_f[];
   __shared__ PushCoef s_k;
   __shared__ u32 s_cnt[BIN_CLASSES];
   const TileRef tr = find_tile(A.st_base, A.npeaks);
@@ -1415,11 +1402,7 @@ __global__ void k_fix_counts(const u64* __restrict__ work, long long n3, double*
 
 // Dynamic shared memory of the largest super-tile in use (the smaller ones fit inside).
 size_t pm_deposit_smem(int TSmax) { return sizeof(u32) * 2 * (size_t)patch_size(TSmax); }
-// The force patch, then (from the next 32-byte boundary) one double4 of FP64 energy sums per
-// thread; the largest super-tile in use covers the smaller ones.
-size_t pm_push_smem(int TSmax) {
-  return sizeof(float) * (size_t)((3 * patch_size(TSmax) + 7) & ~7) + sizeof(double4) * PUSH_THREADS;
-}
+size_t pm_push_smem(int TSmax) { return sizeof(float) * 3 * (size_t)patch_size(TSmax); }
 
 size_t pm_tile_sort_smem() {
   return sizeof(u32) * 16 * 16 * 16 + (size_t)TSORT_CAP * (sizeof(int4) + sizeof(float4) + sizeof(u32) + sizeof(unsigned short));

@@ -21,7 +21,6 @@
 
 #define PM_THREADS 256
 #define PUSH_THREADS 512
-#define PUSH_FLUSH 8       // particles a push thread sums in FP32 before adding to its FP64 energy sums
 #define DEP_THREADS 256    // deposit CTA (4 per SM)
 #define GREEN_MODES 4      // modes per thread of the Green kernel (a block covers PM_THREADS * GREEN_MODES)
 #define ENERGY_SLICES 16   // CTAs per peak of the energy reduction
