@@ -210,10 +210,10 @@ def launches_per_step(sizes, fft: str) -> int:
     native = {n for n in sizes if fft == "native" and n in NATIVE_FFT_SIZES}
     return 10 + 6 * len(native) - (1 if native and all(n in native for n in sizes) else 0)
 
-# DRAM bytes (read + write) per launch from single-kernel ncu captures of a 128^3 run (the
-# summaries under profiles/ give the commands), per particle (per mode for Green), scaled to a
-# launch by the particles (modes) it processes.
-NCU_TRAFFIC = {"push": 77.17, "bin": 61.18, "deposit": 28.62, "green_per_mode": 25.69}
+# DRAM bytes (read + write) per launch from single-kernel ncu captures of the plain 256^3 run
+# (the Green kernel's from the same run with cuFFT transforms), per particle (per mode for Green),
+# scaled to a launch by the particles (modes) it processes; deposit includes its face fix-up.
+NCU_TRAFFIC = {"push": 77.19, "bin": 61.25, "deposit": 26.94, "green_per_mode": 25.89}
 
 
 def replica_throughput(t_local: float, n_local: int, steps: int, dist=None, device="cpu"):
@@ -391,8 +391,8 @@ def run_ours(args):
         return NCU_TRAFFIC[name] * n_step if name in NCU_TRAFFIC else None
     roofline = {"bound": "hbm", "kernel": top, "achieved": kern[top]["gbs"], "peak": hbm, "unit": "GB/s",
                 "frac": kern[top]["gbs"] / hbm, "traffic": traffic(top),
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the plain 256^3 capture, "
-                                  "per particle, times this launch's particles",
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of single-kernel captures of the "
+                                  "plain 256^3 run, per particle, times this launch's particles",
                 "algorithmic_bytes": kern[top]["algorithmic_bytes"], "peak_source": hbm_src,
                 "per_kernel": {k: {"ms": round(v["ms"], 4), "gbs": None if v["gbs"] is None else round(v["gbs"], 1),
                                    "frac": None if v["gbs"] is None else round(v["gbs"] / hbm, 3)}
