@@ -44,7 +44,7 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-errors", action="store_true", help="skip the per-output errors against the float64 oracle")
     ap.add_argument("--no-late", action="store_true", help="skip the device-timed window late in the run")
-    ap.add_argument("--full-sort", action="store_true", help="sort the whole cell key every step")
+    ap.add_argument("--full-sort", action="store_true", help="re-sort every super-tile by cell every step (instead of every 16th)")
     ap.add_argument("--no-serve", action="store_true", help="skip the served-stream latency run")
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="arrival window of the served stream")
     ap.add_argument("--serve-rate", type=float, default=20.0, help="mean request arrivals per second")
@@ -187,9 +187,7 @@ def run_reference(args):
 def algorithmic_bytes(phase: str, n: int, cells: int, modes: int, npass: int) -> float:
     if phase == "push":        # read state 32, write state 32, force grids 12 per cell
         return n * (32 + 32) + cells * 12.0
-    if phase == "sort":        # super-tile re-sort in shared memory (every 16th step): read + write state
-        return n * 64.0
-    if phase == "bin":         # read state 32, write state 32
+    if phase == "refresh":     # super-tile re-sort (every 16th step): read + write state
         return n * 64.0
     if phase == "deposit":     # read positions 16, write delta 4 per cell (face/halo partials are overhead)
         return n * 16.0 + cells * 4.0
@@ -198,13 +196,14 @@ def algorithmic_bytes(phase: str, n: int, cells: int, modes: int, npass: int) ->
     return 0.0
 
 
-PHASES = ["push", "advance", "bin", "sort", "deposit", "r2c", "green", "c2r"]
+PHASES = ["push", "advance", "regroup", "refresh", "deposit", "r2c", "green", "c2r"]
 NATIVE_FFT_SIZES = (64, 128, 256, 512)   # meshes the native transform serves (the others use cuFFT)
 
 
 def launches_per_step(sizes, fft: str) -> int:
     """Our kernel launches in one steady (non-priming) step of an ensemble with these mesh sizes:
-    push, energy, advance, 3 re-bin, super-tile sort, deposit, fix-up and Green (10); the native
+    push, energy, advance, bin layout and 2 relayout copies (gated: they return at once unless a
+    push overflowed a bin), super-tile sort, deposit, fix-up and Green (10); the native
     transform adds 6 per mesh size it serves (3 passes each way) and drops the Green launch when
     it serves every mesh.  The radix sort runs only in steps that prime a peak."""
     native = {n for n in sizes if fft == "native" and n in NATIVE_FFT_SIZES}
@@ -213,7 +212,7 @@ def launches_per_step(sizes, fft: str) -> int:
 # DRAM bytes (read + write) per launch from single-kernel ncu captures of the plain 256^3 run
 # (the Green kernel's from the same run with cuFFT transforms), per particle (per mode for Green),
 # scaled to a launch by the particles (modes) it processes; deposit includes its face fix-up.
-NCU_TRAFFIC = {"push": 77.19, "bin": 61.25, "deposit": 26.94, "green_per_mode": 25.89}
+NCU_TRAFFIC = {"push": 77.19, "deposit": 26.94, "green_per_mode": 25.89}
 
 
 def replica_throughput(t_local: float, n_local: int, steps: int, dist=None, device="cpu"):
@@ -283,10 +282,11 @@ def oracle_errors(specs, tiles, device: int, nsteps: int = 50) -> dict:
                            and worst["positions_cells"] <= 1e-5)}
 
 
-# Ideal HBM bytes of a whole step: 176 per particle outside the transforms (push 64, regroup 64,
-# deposit 16 + 4 per cell ... per particle = cell) and 24 per cell for the transforms (R2C reads
-# delta and writes the half spectrum, C2R reads it and writes three force grids).
-IDEAL_BYTES_PER_PARTICLE = 176.0
+# Ideal HBM bytes of a whole step: 112 per particle outside the transforms (push 64 + 12 per cell
+# of force grids, deposit 16 + 4 per cell, Green 32 per mode = 16 per cell; particles = cells) and
+# 24 per cell for the transforms (R2C reads delta and writes the half spectrum, C2R reads it and
+# writes three force grids).
+IDEAL_BYTES_PER_PARTICLE = 112.0
 IDEAL_FFT_BYTES_PER_CELL = 24.0
 
 
@@ -331,6 +331,7 @@ def run_ours(args):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     ens.engine.sync()
+    relayouts0 = sum(s.relayouts for s in ens.stats())
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -347,9 +348,10 @@ def run_ours(args):
     t, value = replica_throughput(e0.elapsed_time(e1) / 1e3, n_step, args.steps, dist,
                                   device=f"cuda:{local}")
     ms_per_step = t / args.steps * 1e3
+    relayouts = sum(s.relayouts for s in ens.stats()) - relayouts0
 
     # Per-kernel device times: a few ungraphed steps with events between phases, same stream.
-    ph = ens.timed_phases(16)                     # one sort step and fifteen re-binning steps
+    ph = ens.timed_phases(16)                     # one refresh step and fifteen plain ones
     # A second device-timed window late in the run (past the collapse of the early peaks).
     late = None
     run_len = min(sp.steps for sp in specs)
@@ -358,6 +360,7 @@ def run_ours(args):
         ens.step(120 - done_steps)
         n_late = ens.active_particles()
         ens.engine.sync()
+        r_late0 = sum(s.relayouts for s in ens.stats())
         l0, l1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         l0.record(stream)
         ens.step(20)
@@ -365,7 +368,9 @@ def run_ours(args):
         l1.synchronize()
         t_late = l0.elapsed_time(l1) / 1e3
         a_cfg = ens.clocks()[0].a / 100.0
+        r_late = sum(s.relayouts for s in ens.stats()) - r_late0
         late = {"steps": [121, 140], "ms_per_step": t_late / 20 * 1e3, "value": n_late * 20 / t_late, "unit": UNIT,
+                "relayouts": r_late,
                 "a_cfg_end": a_cfg,
                 "peaks_past_design_collapse": int(sum(1 for sp in specs if sp.a_collapse_cfg <= a_cfg))}
     cells = sum(s.N ** 3 for s in specs)
@@ -374,7 +379,7 @@ def run_ours(args):
     kern = {}
     for k, name in enumerate(PHASES):
         b = algorithmic_bytes(name, n_step, cells, modes, npass)
-        if name == "sort":
+        if name == "refresh":
             b /= 16.0
         kern[name] = {"ms": ph[k], "algorithmic_bytes": b, "gbs": (b / (ph[k] / 1e3) / 1e9) if b and ph[k] > 0 else None}
     peaks_file = ROOT / "MEASURED_PEAKS.json"
@@ -383,7 +388,7 @@ def run_ours(args):
         hbm_src = "measured"
     else:
         hbm, hbm_src = 6650.0, "fallback"
-    ours = {k: v for k, v in kern.items() if k in ("push", "sort", "bin", "deposit", "green")}
+    ours = {k: v for k, v in kern.items() if k in ("push", "refresh", "deposit", "green")}
     top = max(ours, key=lambda k: ours[k]["ms"])
     def traffic(name):
         if name == "green":
@@ -404,10 +409,11 @@ def run_ours(args):
             "vs_baseline": None, "dtype": "f32 (fields, offsets, momenta; i32 cells; i64 fixed-point density sums)",
             "data": "synthetic (recipe peaks, seeded numpy noise)",
             "config": workload_config(desc, specs, world),
-            "engine": {"regroup": "Morton radix sort every step" if args.full_sort else
-                       "re-binning each step, super-tile re-sort every 16th", "timed_steps": [1 + args.warmup,
+            "engine": {"regroup": "push into bins, super-tile re-sort every step" if args.full_sort else
+                       "push into bins, super-tile re-sort every 16th", "timed_steps": [1 + args.warmup,
                                                                                        args.warmup + args.steps],
                        "super_tiles": {str(k): v for k, v in sorted(tiles.items())},
+                       "relayouts_timed": relayouts,
                        "fft_64_to_512": "native (Green fused into the inverse)" if args.fft == "native" else "cuFFT"},
             "clocks": clocks, "gpu_launches": args.steps * launches_per_step([sp.N for sp in specs], args.fft),
             "roofline": roofline}
@@ -427,7 +433,7 @@ def run_ours(args):
                                     "batched_ms_per_step": ms_per_step,
                                     "max_batched_over_plain": plain_ms / ideal_ms,
                                     "how": "sum of the plain per-peak step times / the ensemble step at the HBM "
-                                           "roofline (176 B per particle + 24 B per cell at the measured peak)"})
+                                           "roofline (112 B per particle + 24 B per cell at the measured peak)"})
         ps = pm3d_step_rate(specs, steps=5, warmup=2, device=local)
         line["plain_pm3d_step"] = dict(ps, batched_over_pm3d_step=value / world / ps["particle_steps_per_s"],
                                        how="each peak alone through PM3D.step (delta returned to the host "
@@ -481,13 +487,14 @@ def e2e_job(ens, specs, torch, device):
     finals = ens.deltas()                        # the job's result: every peak's final delta
     torch.cuda.synchronize()
     t = time.perf_counter() - t0
+    relayouts = sum(s.relayouts for s in ens.stats())
     del noises
     result_bytes = sum(int(f.nbytes) for f in finals)
     assert all(np.isfinite(f).all() for f in finals)
     ps = sum(s.n for s in specs) * steps
     return {"value": ps / t, "unit": UNIT, "h2d_bytes_per_step": h2d / steps,
             "d2h_bytes_per_step": (stats_bytes + result_bytes) / steps,
-            "job_steps": steps, "seconds": t, "result_bytes": result_bytes,
+            "job_steps": steps, "seconds": t, "result_bytes": result_bytes, "relayouts": relayouts,
             "how": "public Ensemble API: pinned host noise -> device IC -> all steps with per-step stats to the "
                    "host -> every peak's final delta to the host; wall clock"}
 

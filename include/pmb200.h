@@ -78,16 +78,19 @@ typedef struct {
   double potential;          /* W = (1/2) rho_b a^3 dx^3 sum_nodes delta Phi (the PM mesh potential) */
   double li_residual;
   double li_scale;
+  int relayouts;             /* steps since the load whose push overflowed a super-tile's bin (the
+                              * peak's bins were then re-sized and its particles moved) */
 } pm_stats_info;
 
 /* Create an engine holding npeaks independent peaks (a batched ensemble; npeaks = 1 is the
  * plain single run).  Allocates all device memory and cuFFT plans up front; no later call
  * allocates.  flags: bits 8..15 = re-sort every super-tile's particles by cell every that many
- * steps (16 if 0; re-binning keeps them grouped between); bit 1 = replay the step as a CUDA
+ * steps (16 if 0; the push keeps them binned by super-tile between); bit 1 = replay the step as a CUDA
  * graph; bit 2 = dynamic mode for served runs: no graph, and each step's FFTs cover only the
  * slots up to the highest one in use in each mesh size (slots are the peaks of one size, in
  * order); bit 3 = the native transform with the Green multiply fused (pm_rfft3_native) for
- * meshes 64^3-512^3 instead of cuFFT. */
+ * meshes 64^3-512^3 instead of cuFFT; bit 16 = bins without spare capacity (a test mode: almost
+ * every step overflows a bin and relayouts; results are the same bit for bit). */
 int pm_engine_create(const pm_peak_cfg* cfg, int npeaks, int device, int flags, pm_engine** out);
 int pm_engine_destroy(pm_engine* e);
 int pm_engine_sync(pm_engine* e);
@@ -105,9 +108,10 @@ int pm_set_particles(pm_engine* e, int peak, const double* x, const double* p, d
 int pm_run(pm_engine* e, int nsteps);
 
 /* pm_run without the graph, with a CUDA event between kernel phases on the engine's stream;
- * adds each phase's device time (ms) into phase_ms[8]: push, energy + clock advance,
- * re-binning, sorts (priming radix sort with its permutation; super-tile re-sort on refresh
- * steps), deposit (with the face fix-up), R2C, Green, C2R.  For per-kernel rooflines. */
+ * adds each phase's device time (ms) into phase_ms[8]: push, energy + clock advance, regroup
+ * (priming radix sort with its permutation, bin layouts, relayouts of peaks whose push
+ * overflowed a bin), super-tile re-sort (refresh steps), deposit (with the face fix-up), R2C,
+ * Green, C2R.  For per-kernel rooflines. */
 int pm_run_timed(pm_engine* e, int nsteps, double* phase_ms);
 /* The engine's CUDA stream (cudaStream_t), for events and stream ordering by callers. */
 void* pm_engine_stream(pm_engine* e);

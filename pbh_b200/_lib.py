@@ -16,6 +16,7 @@ FLAG_BUCKET_SORT = 1
 FLAG_GRAPH = 2
 FLAG_DYNAMIC = 4
 FLAG_NATIVE_FFT = 8
+FLAG_TIGHT_BINS = 1 << 16
 NOALLOC_MAX_KEYS = 1 << 18          # PM_NOALLOC_MAX_KEYS of include/pmb200.h
 
 
@@ -34,7 +35,7 @@ class StatsInfo(C.Structure):
     _fields_ = [("rho_max_over_mean", C.c_double), ("delta_max", C.c_double), ("mass_defect", C.c_double),
                 ("status", C.c_uint), ("energy_samples", C.c_int), ("a_energy", C.c_double),
                 ("momentum", C.c_double * 3), ("kinetic", C.c_double), ("potential", C.c_double),
-                ("li_residual", C.c_double), ("li_scale", C.c_double)]
+                ("li_residual", C.c_double), ("li_scale", C.c_double), ("relayouts", C.c_int)]
 
 
 class ICParams(C.Structure):

@@ -89,8 +89,9 @@ class Ensemble:
             steps += chunk
 
     def timed_phases(self, nsteps: int):
-        """Per-phase device ms (push, energy + advance, re-bin, sorts, deposit with its face fix-up,
-        R2C, Green, C2R) over nsteps ungraphed steps, from CUDA events on the engine's stream."""
+        """Per-phase device ms (push, energy + advance, regroup (priming sort, relayouts),
+        refresh (super-tile re-sort), deposit with its face fix-up, R2C, Green, C2R) over nsteps
+        ungraphed steps, from CUDA events on the engine's stream."""
         ms = (ctypes.c_double * 8)()
         _lib.check(_lib.load().pm_run_timed(self.engine._h, int(nsteps), ms), "pm_run_timed")
         return np.array(list(ms)) / max(nsteps, 1)

@@ -45,21 +45,22 @@ struct PeakDesc {
   int TS, log2TS;          // super-tile side: the unit of push, deposit and particle grouping
   int NS;                  // super-tiles per axis (N / TS)
   int nst;                 // super-tiles (NS^3)
-  int W;                   // re-binning classes per axis: min(NS, 5) (offsets 0, +1, +2, -1, -2)
-  int NC;                  // classes (W^3)
   int key_bits;            // 3*log2N: Morton key of the CIC cell
   int st_shift;            // 3*log2TS: key >> st_shift is the super-tile
   int fc, hc;              // face nodes (any local coordinate 0) and upper-halo nodes per super-tile
   int gradient;            // 0 spectral (reference), 1 two-point finite difference, 2 four-point
-  int full_every;          // a full Morton-key sort every this many steps (re-binning between)
+  int full_every;          // every super-tile's particles re-sorted by cell every this many steps
   int native_fft;          // 1: the native 256^3 transform carries the Green multiply (no k_green)
-  int pad_nf;
+  int bin_shift, bin_min;  // bin capacity: count + (count >> bin_shift) + bin_min, rounded up to BIN_ALIGN
+  int bin_grow;            // relayout: room for this many more steps of a bin's growth (region allowing)
+  int pad_bg;
   double L, dx, smooth, n_mean, m_part;
   long long n_mean_fix;    // round(n_mean * 2^38)
   double inv_fix_nmean;    // 2^-38 / n_mean
-  long long p_off, n;      // particle range in the arena
+  long long p_off, n;      // particle range in the loading/overflow area (and in the sort arrays)
+  long long r_off, r_size; // bin region of this peak in each of the two bin buffers
   long long st_base;       // first global super-tile index of this peak
-  long long sst_off;       // offset of this peak's super-tile start arrays (nst + 1 entries)
+  long long sst_off;       // offset of this peak's super-tile start array (nst + 1 entries)
   long long face_off;      // offset of this peak's face partials (nst * fc)
   long long halo_off;      // offset of this peak's halo partials (nst * hc)
   long long mode_base;     // first global mode-block of this peak (Green kernel)
@@ -83,10 +84,12 @@ struct PeakClock {
   int state;       // PeakState
   int nsteps;      // steps taken
   int max_steps;   // SCHED_RATIO length
-  int sbuf;        // which super-tile start array describes the current grouping
+  int sbuf;        // bin buffer holding the current particles (the push writes the other one)
+  int lgen;        // bin layout generation in use ({base, capacity} per super-tile)
   int dep;         // 1 when this step re-deposits (set by the advance kernel)
-  int sortstep;    // 1 when this step groups by a full Morton-key sort (priming; else re-binning)
-  int refresh;     // 1 when this step re-sorts every super-tile's particles by cell after re-binning
+  int sortstep;    // 1 when this step groups the loaded particles by a full Morton-key sort (priming)
+  int relayout;    // 1 when this step's push overflowed a bin: new bin capacities, particles moved
+  int refresh;     // 1 when this step re-sorts every super-tile's particles by cell
   int has_delta;   // delta/grids hold data
   int stop_on_collapse;  // end the run (finalize) on the step that detects collapse
   double delta_collapse;  // collapse threshold on max delta (<= 0: not tracked)
@@ -100,6 +103,8 @@ struct PeakStats {
   long long mass_defect;  // sum over nodes of (S - n_mean_fix): 0 when mass is exact
   u32 status;             // bit 0: non-finite force/momentum, bit 1: fixed-point overflow
   u32 nsamples;           // energy samples taken since the peak was loaded
+  u32 relayouts;          // steps since the peak was loaded whose push overflowed a bin
+  u32 pad;
   // Energy and momentum at a_e, from compensated FP64 sums in a fixed reduction order.  With
   // p = a^2 dx/dt, dp/dt = -grad Phi (pbhgr/pbhgr/pm3d.py:3-6) the Layzer-Irvine equation reads
   // d[a (K + W)]/da = -K, so a (K + W) + int_{a0}^{a} K da stays equal to a0 (K0 + W0).

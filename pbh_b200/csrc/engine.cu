@@ -72,24 +72,25 @@ struct pm_engine {
   int* d_green_peak = nullptr;
   int ngreen = 0;
   long long ngreenblk = 0;
-  int4* pos = nullptr;   // state, grouped by super-tile
-  float4* mom = nullptr;
-  int4* tpos = nullptr;  // push output / loading area
-  float4* tmom = nullptr;
+  long long rtot = 0;                          // slots of each bin buffer
+  int4* bpos[2] = {nullptr, nullptr};          // bin buffers (state, binned by super-tile)
+  float4* bmom[2] = {nullptr, nullptr};
+  int4* lpos = nullptr;                        // loading area / overflow area
+  float4* lmom = nullptr;
+  BinLayout* lay[2] = {nullptr, nullptr};      // bin layouts, two generations
+  BinFill* fill[2] = {nullptr, nullptr};       // bin fills of the two buffers
+  u32* ovf_n = nullptr;                        // [peak] overflow-area particles
+  u32* ovf_in = nullptr;                       // [super-tile] overflowed arrivals
   u32* keys[2] = {nullptr, nullptr};
   u32* vals[2] = {nullptr, nullptr};
-  u32* sstart[2] = {nullptr, nullptr};
-  u32* counts = nullptr;
-  u32* lpre = nullptr;
-  u32* far_count = nullptr;
-  u32* far_fill = nullptr;
+  u32* sstart = nullptr;
   double2* epart = nullptr;  // push partials of the energy sums
   double* wpart = nullptr;   // Green partials of the potential energy (per warp)
   double2* eslice = nullptr; // energy slice partials
   u32* ecount = nullptr;     // energy slices done per peak
-  u32* sort_gate = nullptr;  // one word: any peak sorts this step
+  u32* sort_gate = nullptr;  // one word: any peak primes by sort this step
+  u32* layout_gate = nullptr;   // one word: any peak primes or relayouts this step
   u32* refresh_gate = nullptr;  // one word: any peak re-sorts its super-tiles this step
-  u32* totals = nullptr;
   long long* face = nullptr;
   long long* halo = nullptr;
   SortPlan sort{};       // Morton-key sort used by priming and every full_every steps
@@ -126,22 +127,25 @@ struct pm_engine {
     A.eslice = eslice;
     A.ecount = ecount;
     A.npeaks = npeaks;
-    A.pos = pos;
-    A.mom = mom;
-    A.tpos = tpos;
-    A.tmom = tmom;
+    A.pos0 = bpos[0];
+    A.mom0 = bmom[0];
+    A.pos1 = bpos[1];
+    A.mom1 = bmom[1];
+    A.lpos = lpos;
+    A.lmom = lmom;
+    A.lay[0] = lay[0];
+    A.lay[1] = lay[1];
+    A.fill[0] = fill[0];
+    A.fill[1] = fill[1];
+    A.ovf_n = ovf_n;
+    A.ovf_in = ovf_in;
     A.keys_push = keys[0];
     A.keys_sorted = keys[sort_result];
     A.perm = vals[sort_result];
-    A.sstart[0] = sstart[0];
-    A.sstart[1] = sstart[1];
-    A.counts = counts;
-    A.lpre = lpre;
-    A.far_count = far_count;
-    A.far_fill = far_fill;
+    A.sstart = sstart;
     A.sort_gate = sort_gate;
+    A.layout_gate = layout_gate;
     A.refresh_gate = refresh_gate;
-    A.totals = totals;
     A.face = face;
     A.halo = halo;
     A.sort_err = sort.err;
@@ -195,8 +199,8 @@ struct pm_engine {
   }
 
   // One step for every peak.  With ev != nullptr an event is recorded after each phase and the
-  // phase times (push, energy + advance, re-bin, sorts, deposit with its face fix-up, R2C, Green,
-  // C2R) are accumulated.
+  // phase times (push, energy + advance, relayout, priming sort and refresh, deposit with its face
+  // fix-up, R2C, Green, C2R) are accumulated.
   int launch_step(bool with_sort, cudaEvent_t* ev = nullptr, double* phase_ms = nullptr) {
     const StepArgs A = args();
     int k = 0;
@@ -207,14 +211,14 @@ struct pm_engine {
     launch_energy(A, stream);
     launch_advance(A, stream);
     CU(mark());
-    launch_bin(A, nst, stream);
-    CU(mark());
     int r = 0;
-    if (with_sort) {  // only steps that prime a peak: no launches at all in the steady state
+    if (with_sort) {  // only steps that prime a peak: no sort launches at all in the steady state
       if ((r = sort_run<u32>(&sort, keys[0], vals[0], keys[1], vals[1], true, true, stream))) return r;
-      launch_permute(A, ntot, stream);
       launch_st_starts(A, ntot, stream);
     }
+    launch_layout(A, nst, ntot, stream);  // layouts of priming peaks; relayouts (gated, rare)
+    if (with_sort) launch_permute(A, ntot, stream);
+    CU(mark());
     launch_tile_sort(A, nst, stream);
     CU(mark());
     launch_deposit(A, nst, smem_dep, nullptr, stream);
@@ -302,9 +306,9 @@ struct pm_engine {
     }
     cudaFree(sort_dbg);
     void* bufs[] = {d_peaks, d_clocks, d_stats, d_st_base, d_p_base, d_mode_base, d_green_base, d_green_peak, epart,
-                    wpart, eslice, ecount, pos, mom, tpos,
-                    tmom, keys[0], keys[1], vals[0], vals[1], sstart[0], sstart[1], counts, lpre, far_count,
-                    far_fill, sort_gate, refresh_gate, totals, face, halo};
+                    wpart, eslice, ecount, bpos[0], bpos[1], bmom[0], bmom[1], lpos, lmom, lay[0], lay[1],
+                    fill[0], fill[1], ovf_n, ovf_in, keys[0], keys[1], vals[0], vals[1], sstart,
+                    sort_gate, layout_gate, refresh_gate, face, halo};
     for (void* b : bufs) cudaFree(b);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -329,6 +333,7 @@ void fill_stats(const PeakDesc& P, const PeakStats& s, int sort_err, pm_stats_in
   o->delta_max = o->rho_max_over_mean - 1.0;
   o->mass_defect = (double)s.mass_defect / (double)PM_FIX_ONE;
   o->status = s.status | (sort_err ? 2u : 0u);
+  o->relayouts = (int)s.relayouts;
   fill_energy(s, o);
 }
 
@@ -350,7 +355,7 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   E->peaks.resize(npeaks);
   E->occupied.assign(npeaks, 0);
   std::map<int, int> class_of;
-  long long poff = 0, stb = 0, mb = 0, sso = 0, fo = 0, ho = 0;
+  long long poff = 0, roff = 0, stb = 0, mb = 0, sso = 0, fo = 0, ho = 0;
   int TSmax = 1, max_bits = 0;
   const int full_every = std::max(1, (E->flags >> 8) & 0xFF ? (E->flags >> 8) & 0xFF : 16);
   std::vector<long long> st_base(npeaks + 1), p_base(npeaks + 1), mode_base(npeaks + 1);
@@ -372,14 +377,19 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
     P.log2TS = ilog2(TS);
     P.NS = c.N / TS;
     P.nst = P.NS * P.NS * P.NS;
-    P.W = std::min(P.NS, 5);
-    P.NC = P.W * P.W * P.W;
     P.key_bits = 3 * l2;
     P.st_shift = 3 * P.log2TS;
     P.fc = TS * TS * TS - (TS - 1) * (TS - 1) * (TS - 1);
     P.hc = (TS + 1) * (TS + 1) * (TS + 1) - TS * TS * TS;
     P.gradient = c.gradient;
     P.full_every = full_every;
+    // Spare bin capacity: count / 8 + BIN_SLACK_MIN, plus room for BIN_GROW_STEPS steps of growth
+    // after a relayout; none with flag bit 16 (a test mode in which almost every step overflows
+    // a bin and relayouts).
+    const bool tight = (E->flags & (1 << 16)) != 0;
+    P.bin_shift = tight ? 32 : BIN_SLACK_SHIFT;
+    P.bin_min = tight ? 0 : BIN_SLACK_MIN;
+    P.bin_grow = tight ? 0 : BIN_GROW_STEPS;
     P.L = c.L;
     P.dx = c.L / c.N;
     P.smooth = c.smooth;
@@ -390,6 +400,13 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
     P.inv_fix_nmean = 1.0 / ((double)PM_FIX_ONE * P.n_mean);
     P.p_off = poff;
     P.n = npart;
+    // Bin region: every base layout k_layout makes (count + count/8 + BIN_SLACK_MIN per bin,
+    // rounded up to BIN_ALIGN) fits in n + n/8 + (BIN_SLACK_MIN + BIN_ALIGN) per super-tile; a
+    // further n >> BIN_SPARE_SHIFT slots hold the allowance for arrivals and growth of relayouts.
+    P.r_off = roff;
+    P.r_size = (npart + (npart >> BIN_SLACK_SHIFT) + (npart >> BIN_SPARE_SHIFT) +
+                (long long)(BIN_SLACK_MIN + BIN_ALIGN) * P.nst + BIN_ALIGN - 1) / BIN_ALIGN * BIN_ALIGN;
+    roff += P.r_size;
     P.st_base = stb;
     P.sst_off = sso;
     P.face_off = fo;
@@ -418,8 +435,9 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   st_base[npeaks] = stb;
   p_base[npeaks] = poff;
   mode_base[npeaks] = mb;
-  if (poff >= (1LL << 32)) return -2005;
+  if (poff >= (1LL << 32) || roff >= (1LL << 32)) return -2005;
   E->ntot = poff;
+  E->rtot = roff;
   E->nst = stb;
   E->nmodeblk = mb;
   E->nsst = sso;
@@ -514,26 +532,26 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   CU(cudaMemcpy(E->d_green_base, green_base.data(), sizeof(long long) * green_base.size(), cudaMemcpyHostToDevice));
   if (E->ngreen)
     CU(cudaMemcpy(E->d_green_peak, green_peak.data(), sizeof(int) * green_peak.size(), cudaMemcpyHostToDevice));
-  if ((r = E->alloc(&E->pos, E->ntot))) return r;
-  if ((r = E->alloc(&E->mom, E->ntot))) return r;
-  if ((r = E->alloc(&E->tpos, E->ntot))) return r;
-  if ((r = E->alloc(&E->tmom, E->ntot))) return r;
   for (int b = 0; b < 2; ++b) {
+    if ((r = E->alloc(&E->bpos[b], E->rtot))) return r;
+    if ((r = E->alloc(&E->bmom[b], E->rtot))) return r;
+    if ((r = E->alloc(&E->lay[b], E->nst))) return r;
+    if ((r = E->alloc(&E->fill[b], E->nst))) return r;
     if ((r = E->alloc(&E->keys[b], E->ntot))) return r;
     if ((r = E->alloc(&E->vals[b], E->ntot))) return r;
-    if ((r = E->alloc(&E->sstart[b], E->nsst))) return r;
   }
-  if ((r = E->alloc(&E->counts, E->nst * BIN_CLASSES))) return r;
-  if ((r = E->alloc(&E->lpre, E->nst * BIN_CLASSES))) return r;
-  if ((r = E->alloc(&E->far_count, E->nst))) return r;
-  if ((r = E->alloc(&E->far_fill, E->nst))) return r;
+  if ((r = E->alloc(&E->lpos, E->ntot))) return r;
+  if ((r = E->alloc(&E->lmom, E->ntot))) return r;
+  if ((r = E->alloc(&E->sstart, E->nsst))) return r;
+  if ((r = E->alloc(&E->ovf_n, npeaks))) return r;
+  if ((r = E->alloc(&E->ovf_in, E->nst))) return r;
   if ((r = E->alloc(&E->epart, 4 * E->nst))) return r;
   if ((r = E->alloc(&E->wpart, E->nmodeblk * (PM_THREADS / 32)))) return r;
   if ((r = E->alloc(&E->eslice, (size_t)npeaks * ENERGY_SLICES * 5))) return r;
   if ((r = E->alloc(&E->ecount, npeaks))) return r;
   if ((r = E->alloc(&E->sort_gate, 1))) return r;
+  if ((r = E->alloc(&E->layout_gate, 1))) return r;
   if ((r = E->alloc(&E->refresh_gate, 1))) return r;
-  if ((r = E->alloc(&E->totals, E->nst))) return r;
   if ((r = E->alloc(&E->face, E->nfc))) return r;
   if ((r = E->alloc(&E->halo, E->nhc))) return r;
   CU(cudaMemcpy(E->d_peaks, E->peaks.data(), sizeof(PeakDesc) * npeaks, cudaMemcpyHostToDevice));
@@ -548,18 +566,23 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   }
   CU(cudaMemcpy(E->d_clocks, clocks.data(), sizeof(PeakClock) * npeaks, cudaMemcpyHostToDevice));
   CU(cudaMemset(E->d_stats, 0, sizeof(PeakStats) * npeaks));
-  CU(cudaMemset(E->pos, 0, sizeof(int4) * E->ntot));
-  CU(cudaMemset(E->mom, 0, sizeof(float4) * E->ntot));
-  CU(cudaMemset(E->tpos, 0, sizeof(int4) * E->ntot));
-  CU(cudaMemset(E->tmom, 0, sizeof(float4) * E->ntot));
-  CU(cudaMemset(E->far_count, 0, sizeof(u32) * E->nst));
-  CU(cudaMemset(E->far_fill, 0, sizeof(u32) * E->nst));
+  for (int b = 0; b < 2; ++b) {
+    CU(cudaMemset(E->bpos[b], 0, sizeof(int4) * E->rtot));
+    CU(cudaMemset(E->bmom[b], 0, sizeof(float4) * E->rtot));
+    CU(cudaMemset(E->lay[b], 0, sizeof(BinLayout) * E->nst));
+    CU(cudaMemset(E->fill[b], 0, sizeof(BinFill) * E->nst));
+  }
+  CU(cudaMemset(E->lpos, 0, sizeof(int4) * E->ntot));
+  CU(cudaMemset(E->lmom, 0, sizeof(float4) * E->ntot));
+  CU(cudaMemset(E->ovf_n, 0, sizeof(u32) * npeaks));
+  CU(cudaMemset(E->ovf_in, 0, sizeof(u32) * E->nst));
+  CU(cudaMemset(E->layout_gate, 0, sizeof(u32)));
   CU(cudaMemset(E->epart, 0, sizeof(double2) * 4 * E->nst));
   CU(cudaMemset(E->wpart, 0, sizeof(double) * E->nmodeblk * (PM_THREADS / 32)));
   CU(cudaMemset(E->ecount, 0, sizeof(u32) * npeaks));
   CU(cudaMemset(E->sort_gate, 0, sizeof(u32)));
   CU(cudaMemset(E->refresh_gate, 0, sizeof(u32)));
-  for (int b = 0; b < 2; ++b) CU(cudaMemset(E->sstart[b], 0, sizeof(u32) * E->nsst));
+  CU(cudaMemset(E->sstart, 0, sizeof(u32) * E->nsst));
 
   // Sort plan: one segment per peak over the whole Morton key (sorted at priming and every
   // full_every steps; the segment of a peak is active only on those steps).
@@ -725,7 +748,7 @@ int pm_step_explicit(pm_engine* e, int peak, double a, double da) {
   if (c.state == PS_IDLE || c.state == PS_PRIME || (c.state == PS_HOLD && !c.has_delta)) {
     // A loaded peak (PRIME) has its particles in the loading area already; any other state
     // holds them in the grouped state, from where they are reloaded for the priming sort.
-    if (c.state != PS_PRIME) launch_reload(e->args(), e->peaks[peak], e->stream);
+    if (c.state != PS_PRIME) launch_reload(e->args(), peak, e->peaks[peak], e->stream);
     c.a = a;
     c.a_grid = a;
     c.mode = SCHED_EXPLICIT;

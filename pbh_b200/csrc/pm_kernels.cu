@@ -38,9 +38,38 @@ __device__ __forceinline__ u32 lanemask_lt() {
 }
 
 
-// Super-tile start arrays without indexing the kernel-parameter array dynamically (which would
-// copy the parameter struct to local memory).
-__device__ __forceinline__ u32* sst(const StepArgs& A, int b) { return b ? A.sstart[1] : A.sstart[0]; }
+// Bin buffers, layouts and fills selected by a per-peak bit without indexing the
+// kernel-parameter arrays dynamically (which would copy the parameter struct to local memory).
+__device__ __forceinline__ int4* bpos(const StepArgs& A, int b) { return b ? A.pos1 : A.pos0; }
+__device__ __forceinline__ float4* bmom(const StepArgs& A, int b) { return b ? A.mom1 : A.mom0; }
+__device__ __forceinline__ BinLayout* blay(const StepArgs& A, int g) { return g ? A.lay[1] : A.lay[0]; }
+__device__ __forceinline__ BinFill* bfill(const StepArgs& A, int b) { return b ? A.fill[1] : A.fill[0]; }
+
+// The two runs of a filled bin: slots [b0, b0 + n0) (stayers) and [b1 + n0, b1 + n0 + n1)
+// (arrivals), i.e. particle k < n0 + n1 of the bin sits at slot (k < n0 ? b0 : b1) + k.  The
+// fill's counts are clamped into the bin, so a corrupted fill can never address outside it.
+struct BinRuns {
+  long long b0, b1;
+  int n0, n1;
+  __device__ __forceinline__ int total() const { return n0 + n1; }
+  __device__ __forceinline__ long long slot(int k) const { return (k < n0 ? b0 : b1) + k; }
+};
+__device__ __forceinline__ BinRuns bin_runs(const BinLayout& L, const BinFill& F) {
+  const u32 gap = min(F.gap, L.cap);
+  const u32 stay = min(F.stay, gap);
+  const u32 moved = min(F.moved, L.cap - gap);
+  BinRuns r;
+  r.b0 = L.base;
+  r.n0 = (int)stay;
+  r.b1 = (long long)L.base + gap - stay;
+  r.n1 = (int)moved;
+  return r;
+}
+// Particles in a bin: stayers plus the arrivals that found room.
+__device__ __forceinline__ u32 bin_count(const BinLayout& L, const BinFill& F) {
+  const u32 gap = min(F.gap, L.cap);
+  return min(F.stay, gap) + min(F.moved, L.cap - gap);
+}
 
 // Locate the peak and the peak-local index of this CTA (uniform across the block).
 struct TileRef {
@@ -58,56 +87,51 @@ __device__ __forceinline__ TileRef find_tile(const long long* base, int npeaks) 
   return r;
 }
 
-// Re-binning classes: per axis, the offset u = (destination - source) mod NS of the super-tile a
-// particle moved to is one of 0, +1, +2, -1, -2 (NS - 1, NS - 2), or any offset when NS <= 5.
-__device__ __forceinline__ int bin_digit(int u, int NS) {
-  if (NS <= 5 || u <= 2) return u;
-  if (u >= NS - 2) return 2 + (NS - u);
-  return -1;
-}
-__device__ __forceinline__ int bin_offset(int d, int NS) { return (NS <= 5 || d <= 2) ? d : NS - (d - 2); }
-
-// Re-binning class of a particle of super-tile (sx, sy, sz) whose cell is now `cell`: class 0 is
-// "stayed", BIN_FAR "moved more than two super-tiles" (its destination super-tile in *far_st).
-__device__ __forceinline__ int bin_class(int cell, int sx, int sy, int sz, const PeakDesc& P, u32* far_st) {
-  const int l2 = P.log2N, N = P.N, NS = P.NS;
-  const int tx = (cell >> (2 * l2)) >> P.log2TS, ty = ((cell >> l2) & (N - 1)) >> P.log2TS,
-            tz = (cell & (N - 1)) >> P.log2TS;
-  const int dxc = bin_digit((tx - sx) & (NS - 1), NS), dyc = bin_digit((ty - sy) & (NS - 1), NS),
-            dzc = bin_digit((tz - sz) & (NS - 1), NS);
-  if (dxc >= 0 && dyc >= 0 && dzc >= 0) return (dxc * P.W + dyc) * P.W + dzc;
-  *far_st = pm_morton3(tx, ty, tz);
-  return BIN_FAR;
-}
-
 // ------------------------------------------------------------------------------------------
 // Push: CIC gather of the three force grids (pm3d.py:91-99) fused with the pending closing
 // kick of the previous step, the opening kick and the drift of this one (pm3d.py:122-127).
 // One CTA per super-tile: the (TS+1)^3 node patch of all three grids is staged in shared
-// memory, and the super-tile's particles -- one contiguous range -- read their 8 corners from
-// there.  Each result is written to the same position of the temporary state with the class of
-// its new super-tile; per-class counts feed the re-binning.
+// memory, and the particles of the super-tile's bin read their 8 corners from there.  Each
+// result goes straight into the bin of the super-tile it is now in, in the other buffer:
+// stayers take ranks from a shared-memory counter (one add per warp), arrivals from an atomic on
+// the destination's `moved` count, placed after the destination's count before the step (which
+// no stayer rank reaches).  An arrival that finds no room, which the spare capacity makes rare,
+// goes to the peak's overflow area and the peak relayouts this step.
 struct PushCoef {
   float kA, kB, D, gscale;
   int run;
 };
 
+// Where one push CTA reads and writes.
+struct PushCtx {
+  int sx, sy, sz;        // this super-tile
+  long long gS;          // its global index
+  u32 base, cap;         // its bin
+  const BinLayout* lay;  // bin layouts (global super-tile index)
+  const BinFill* fcur;   // fills of the buffer read
+  BinFill* fnxt;         // fills of the buffer written
+  int4* opos;            // the buffer written
+  float4* omom;
+};
+
 template <int T>
-__device__ __forceinline__ void push_one(const StepArgs& A, const PeakDesc& P, const float* __restrict__ s_f,
-                                         const PushCoef& K, int sx, int sy, int sz, int4 ps, float4 m, long long j,
-                                         u32* s_cnt, bool& bad, double4& acc_e) {
+__device__ __forceinline__ void push_one(const StepArgs& A, const PeakDesc& P, int pk, const float* __restrict__ s_f,
+                                         const PushCoef& K, const PushCtx& X, int4 ps, float4 m, u32* s_stay,
+                                         bool& bad, bool& lost, double4& acc_e) {
   constexpr int RS = patch_rs(T), PS = patch_ps(T), CS = patch_size(T);
   const int N = P.N, l2 = P.log2N;
-  const int ix = ps.x >> (2 * l2), iy = (ps.x >> l2) & (N - 1), iz = ps.x & (N - 1);
-  const int lx = ix - sx * T, ly = iy - sy * T, lz = iz - sz * T;
-  if ((unsigned)lx >= (unsigned)T || (unsigned)ly >= (unsigned)T || (unsigned)lz >= (unsigned)T) {
-    bad = true;  // grouping and state disagree: flag it, never index outside the patch
-    return;
-  }
+  const int ix = (ps.x >> (2 * l2)) & (N - 1), iy = (ps.x >> l2) & (N - 1), iz = ps.x & (N - 1);
+  const int lx = ix - X.sx * T, ly = iy - X.sy * T, lz = iz - X.sz * T;
+  // A particle outside this super-tile (bins and state disagree) is flagged and moved on
+  // unchanged to the bin its cell names; nothing indexes outside the patch.
+  const bool inside = ps.x >= 0 && ps.x < N * N * N && (unsigned)lx < (unsigned)T && (unsigned)ly < (unsigned)T &&
+                      (unsigned)lz < (unsigned)T;
+  bad |= !inside;
   float fx = __int_as_float(ps.y), fy = __int_as_float(ps.z), fz = __int_as_float(ps.w);
-  const float gx = 1.0f - fx, gy = 1.0f - fy, gz = 1.0f - fz;
-  const int o = lx * PS + ly * RS + lz;
   float ax = 0.f, ay = 0.f, az = 0.f;
+  if (inside) {
+    const float gx = 1.0f - fx, gy = 1.0f - fy, gz = 1.0f - fz;
+    const int o = lx * PS + ly * RS + lz;
 #define PM_CORNER(w, d)                       \
   {                                           \
     const float w_ = (w);                     \
@@ -115,19 +139,20 @@ __device__ __forceinline__ void push_one(const StepArgs& A, const PeakDesc& P, c
     ay = fmaf(w_, s_f[CS + o + (d)], ay);     \
     az = fmaf(w_, s_f[2 * CS + o + (d)], az); \
   }
-  const float w00 = gx * gy, w01 = gx * fy, w10 = fx * gy, w11 = fx * fy;
-  PM_CORNER(w00 * gz, 0)
-  PM_CORNER(w00 * fz, 1)
-  PM_CORNER(w01 * gz, RS)
-  PM_CORNER(w01 * fz, RS + 1)
-  PM_CORNER(w10 * gz, PS)
-  PM_CORNER(w10 * fz, PS + 1)
-  PM_CORNER(w11 * gz, PS + RS)
-  PM_CORNER(w11 * fz, PS + RS + 1)
+    const float w00 = gx * gy, w01 = gx * fy, w10 = fx * gy, w11 = fx * fy;
+    PM_CORNER(w00 * gz, 0)
+    PM_CORNER(w00 * fz, 1)
+    PM_CORNER(w01 * gz, RS)
+    PM_CORNER(w01 * fz, RS + 1)
+    PM_CORNER(w10 * gz, PS)
+    PM_CORNER(w10 * fz, PS + 1)
+    PM_CORNER(w11 * gz, PS + RS)
+    PM_CORNER(w11 * fz, PS + RS + 1)
 #undef PM_CORNER
-  ax *= K.gscale;
-  ay *= K.gscale;
-  az *= K.gscale;
+    ax *= K.gscale;
+    ay *= K.gscale;
+    az *= K.gscale;
+  }
   float px = m.x + K.kA * ax, py = m.y + K.kA * ay, pz = m.z + K.kA * az;
   // Momentum synchronised with the positions (after the closing kick): energy and momentum sums.
   {
@@ -140,13 +165,12 @@ __device__ __forceinline__ void push_one(const StepArgs& A, const PeakDesc& P, c
     acc_e = t;
   }
   int nx = ix, ny = iy, nz = iz;
-  int mx = 0, my = 0, mz = 0;  // cells moved along each axis
   const bool finite = isfinite(px) && isfinite(py) && isfinite(pz);
-  if (K.run && finite) {  // a non-finite particle stays where it is (the peak is flagged below)
+  if (K.run && finite && inside) {  // a non-finite particle stays where it is (the peak is flagged below)
     px += K.kB * ax;
     py += K.kB * ay;
     pz += K.kB * az;
-#define PM_DRIFT(f, p, i, m)    \
+#define PM_DRIFT(f, p, i)       \
   {                             \
     float fn = f + K.D * p;     \
     float c = floorf(fn);       \
@@ -156,62 +180,82 @@ __device__ __forceinline__ void push_one(const StepArgs& A, const PeakDesc& P, c
       c += 1.0f;                \
     }                           \
     f = fn;                     \
-    m = (int)c;                 \
-    i = (i + m) & (N - 1);      \
+    i = (i + (int)c) & (N - 1); \
   }
-    PM_DRIFT(fx, px, nx, mx)
-    PM_DRIFT(fy, py, ny, my)
-    PM_DRIFT(fz, pz, nz, mz)
+    PM_DRIFT(fx, px, nx)
+    PM_DRIFT(fy, py, ny)
+    PM_DRIFT(fz, pz, nz)
 #undef PM_DRIFT
   }
   bad |= !(finite && isfinite(px) && isfinite(py) && isfinite(pz));
   const int cell = (nx << (2 * l2)) | (ny << l2) | nz;
-  A.tpos[j] = make_int4(cell, __float_as_int(fx), __float_as_int(fy), __float_as_int(fz));
-  A.tmom[j] = make_float4(px, py, pz, m.w);
-  // Class of the destination super-tile (re-derived from the cell by the scatter), counted:
-  // most particles stay (one warp-aggregated add), the few movers add one each.  With more than
-  // five super-tiles per axis the class follows from the local cell and the cells moved
-  // (super-tile offsets -2..2 per axis, the same class bin_class gives); anything else, and
-  // smaller meshes, go through bin_class.  The sums are formed modulo 2^32: a saturated move of
-  // a runaway particle stays far outside -2..2.
-  u32 far_st = 0;
-  int c;
-  const int ox = (int)((u32)lx + (u32)mx) >> P.log2TS, oy = (int)((u32)ly + (u32)my) >> P.log2TS,
-            oz = (int)((u32)lz + (u32)mz) >> P.log2TS;
-  if (P.NS > 5 && (unsigned)(ox + 2) <= 4u && (unsigned)(oy + 2) <= 4u && (unsigned)(oz + 2) <= 4u)
-    c = ((ox >= 0 ? ox : 2 - ox) * 5 + (oy >= 0 ? oy : 2 - oy)) * 5 + (oz >= 0 ? oz : 2 - oz);
-  else
-    c = bin_class(cell, sx, sy, sz, P, &far_st);
-  const u32 stay = __ballot_sync(__activemask(), c == 0);
-  if (c == 0) {
-    if ((stay & lanemask_lt()) == 0) atomicAdd(&s_cnt[0], (u32)__popc(stay));
-  } else if (c == BIN_FAR) {
-    atomicAdd(&A.far_count[P.st_base + far_st], 1u);  // counted at its own destination
+  const int4 np = make_int4(cell, __float_as_int(fx), __float_as_int(fy), __float_as_int(fz));
+  const float4 nm = make_float4(px, py, pz, m.w);
+  const int tx = nx >> P.log2TS, ty = ny >> P.log2TS, tz = nz >> P.log2TS;
+  const bool stay = tx == X.sx && ty == X.sy && tz == X.sz;
+  const u32 sm = __ballot_sync(__activemask(), stay);
+  long long dst = -1, gD = X.gS;
+  if (stay) {
+    const int leader = __ffs(sm) - 1;
+    u32 r0 = 0;
+    if ((int)(threadIdx.x & 31) == leader) r0 = atomicAdd(s_stay, (u32)__popc(sm));
+    r0 = __shfl_sync(sm, r0, leader);
+    const u32 r = r0 + (u32)__popc(sm & lanemask_lt());
+    if (r < X.cap) dst = (long long)X.base + r;  // always: the stayers are at most the bin's count
   } else {
-    atomicAdd(&s_cnt[c], 1u);
+    gD = P.st_base + pm_morton3(tx, ty, tz);
+    const BinLayout L = X.lay[gD];
+    const u32 cnt = bin_count(L, X.fcur[gD]);
+    const u32 r = atomicAdd(&X.fnxt[gD].moved, 1u);
+    if (r < L.cap - cnt) dst = (long long)L.base + cnt + r;
+  }
+  if (dst >= 0) {
+    X.opos[dst] = np;
+    X.omom[dst] = nm;
+  } else {
+    const u32 o = atomicAdd(&A.ovf_n[pk], 1u);
+    if (o < (u32)P.n) {
+      A.lpos[P.p_off + o] = np;
+      A.lmom[P.p_off + o] = nm;
+      atomicAdd(&A.ovf_in[gD], 1u);
+    } else {
+      lost = true;  // more overflows than particles: the bins were corrupted
+    }
   }
 }
 
 template <int T>
 __device__ __forceinline__ void push_super(const StepArgs& A, const PeakDesc& P, const PeakClock& C, int pk, u32 st,
-                                           float* s_f, u32* s_cnt, const PushCoef& K) {
+                                           float* s_f, u32* s_stay, const PushCoef& K) {
   constexpr int T1 = T + 1, RS = patch_rs(T), PS = patch_ps(T), CS = patch_size(T);
   constexpr int CH = T / 4 + 1;  // per patch row: T/4 copies of 16 bytes, then the (wrapped) last node
   const int N = P.N;
-  const int sx = pm_compact3(st >> 2), sy = pm_compact3(st >> 1), sz = pm_compact3(st);
+  PushCtx X;
+  X.sx = pm_compact3(st >> 2);
+  X.sy = pm_compact3(st >> 1);
+  X.sz = pm_compact3(st);
+  X.gS = P.st_base + st;
+  X.lay = blay(A, C.lgen);
+  X.fcur = bfill(A, C.sbuf);
+  X.fnxt = bfill(A, C.sbuf ^ 1);
+  X.opos = bpos(A, C.sbuf ^ 1);
+  X.omom = bmom(A, C.sbuf ^ 1);
+  const BinLayout L = X.lay[X.gS];
+  X.base = L.base;
+  X.cap = L.cap;
+  const BinRuns R = bin_runs(L, X.fcur[X.gS]);
+  const int n = R.total();
   const long long N3 = (long long)N * N * N;
-  const u32* ss = sst(A, C.sbuf) + P.sst_off;
-  const long long b = ss[st], e = ss[st + 1];
-  if (b < e) {
+  if (n > 0) {
     // Asynchronous copies of the patch rows (every row start is 16-byte aligned on both sides:
     // z0 = sz*T is a multiple of 4 and the grids are 256-byte aligned).
     const unsigned sbase = (unsigned)__cvta_generic_to_shared(s_f);
-    const int z0 = sz * T, zl = (sz * T + T) & (N - 1);
+    const int z0 = X.sz * T, zl = (X.sz * T + T) & (N - 1);
     for (int i = threadIdx.x; i < 3 * T1 * T1 * CH; i += PUSH_THREADS) {
       const int row = i / CH, part = i - row * CH;
       const int comp = row / (T1 * T1), r = row - comp * (T1 * T1);
       const int lx = r / T1, ly = r - lx * T1;
-      const int gx = (sx * T + lx) & (N - 1), gy = (sy * T + ly) & (N - 1);
+      const int gx = (X.sx * T + lx) & (N - 1), gy = (X.sy * T + ly) & (N - 1);
       const float* src = P.force + comp * N3 + ((long long)gx * N + gy) * N;
       const unsigned dst = sbase + 4u * (unsigned)(comp * CS + lx * PS + ly * RS + part * 4);
       if (part < T / 4) cp_async16(dst, src + z0 + part * 4);
@@ -220,37 +264,48 @@ __device__ __forceinline__ void push_super(const StepArgs& A, const PeakDesc& P,
     cp_async_wait_all();
   }
   __syncthreads();
-  bool bad = false;
+  bool bad = false, lost = false;
   double4 acc_e = make_double4(0.0, 0.0, 0.0, 0.0);  // this thread's momentum and p^2 sums
   // One particle per thread per sweep, the next two sweeps' particles in flight meanwhile;
-  // 32-bit indices inside the super-tile's range.
-  const int4* __restrict__ pp = A.pos + b;
-  const float4* __restrict__ mp = A.mom + b;
-  const int n = (int)(e - b);
+  // 32-bit indices inside the bin's two runs: particle k sits at [k] in the first run, at
+  // [k + d1] in the second.
+  const int4* __restrict__ pp = bpos(A, C.sbuf) + R.b0;
+  const float4* __restrict__ mp = bmom(A, C.sbuf) + R.b0;
+  const int n0 = R.n0, d1 = (int)(R.b1 - R.b0);
   int k = threadIdx.x;
   int4 pa = make_int4(0, 0, 0, 0), pb = pa;
   float4 ma = make_float4(0.f, 0.f, 0.f, 0.f), mb = ma;
   if (k < n) {
-    pa = pp[k];
-    ma = mp[k];
+    const int j = k < n0 ? k : k + d1;
+    pa = pp[j];
+    ma = mp[j];
   }
   if (k + PUSH_THREADS < n) {
-    pb = pp[k + PUSH_THREADS];
-    mb = mp[k + PUSH_THREADS];
+    const int j = k + PUSH_THREADS < n0 ? k + PUSH_THREADS : k + PUSH_THREADS + d1;
+    pb = pp[j];
+    mb = mp[j];
   }
   for (; k < n; k += PUSH_THREADS) {
     const int4 p0 = pa;
     const float4 m0 = ma;
     pa = pb;
     ma = mb;
-    if (k + 2 * PUSH_THREADS < n) {
-      pb = pp[k + 2 * PUSH_THREADS];
-      mb = mp[k + 2 * PUSH_THREADS];
+    const int k2 = k + 2 * PUSH_THREADS;
+    if (k2 < n) {
+      const int j = k2 < n0 ? k2 : k2 + d1;
+      pb = pp[j];
+      mb = mp[j];
     }
-    push_one<T>(A, P, s_f, K, sx, sy, sz, p0, m0, b + k, s_cnt, bad, acc_e);
+    push_one<T>(A, P, pk, s_f, K, X, p0, m0, s_stay, bad, lost, acc_e);
   }
-  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&A.stats[pk].status, 1u);
-  for (int c = threadIdx.x; c < P.NC; c += PUSH_THREADS) A.counts[(P.st_base + st) * BIN_CLASSES + c] = s_cnt[c];
+  const bool any_bad = __syncthreads_or(bad), any_lost = __syncthreads_or(lost);
+  if (threadIdx.x == 0) {
+    if (any_bad) atomicOr(&A.stats[pk].status, 1u);
+    if (any_lost) atomicOr(&A.stats[pk].status, 4u);
+    // This bin's fill in the buffer written: its stayers, and where its arrivals start.
+    X.fnxt[X.gS].stay = *s_stay;
+    X.fnxt[X.gS].gap = (u32)n;
+  }
   // Super-tile partials of the momentum and p^2 sums (compensated, fixed order).
   __shared__ CSum s_e[PUSH_THREADS / 32][4];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -272,12 +327,11 @@ __device__ __forceinline__ void push_super(const StepArgs& A, const PeakDesc& P,
 __global__ void __launch_bounds__(PUSH_THREADS, 2) k_push(StepArgs A) {
   extern __shared__ __align__(16) float s_f[];
   __shared__ PushCoef s_k;
-  __shared__ u32 s_cnt[BIN_CLASSES];
+  __shared__ u32 s_stay;
   const TileRef tr = find_tile(A.st_base, A.npeaks);
   const PeakClock C = A.clocks[tr.pk];
   if (C.state != PS_RUN && C.state != PS_FINALIZE) return;
   const PeakDesc P = A.peaks[tr.pk];
-  if (threadIdx.x < BIN_CLASSES) s_cnt[threadIdx.x] = 0u;
   if (threadIdx.x == 0) {
     const double a = C.a, da = C.da;
     const bool run = C.state == PS_RUN;
@@ -287,21 +341,25 @@ __global__ void __launch_bounds__(PUSH_THREADS, 2) k_push(StepArgs A) {
     s_k.D = run ? (float)(da / (amid * amid * amid * pm_hubble(amid)) / P.dx) : 0.f;
     s_k.gscale = (float)(C.a_grid / a);
     s_k.run = run ? 1 : 0;
+    s_stay = 0u;
   }
   __syncthreads();
   const PushCoef K = s_k;
   const u32 st = (u32)tr.t;
   switch (P.TS) {
-    case 4: push_super<4>(A, P, C, tr.pk, st, s_f, s_cnt, K); break;
-    case 8: push_super<8>(A, P, C, tr.pk, st, s_f, s_cnt, K); break;
-    default: push_super<16>(A, P, C, tr.pk, st, s_f, s_cnt, K); break;
+    case 4: push_super<4>(A, P, C, tr.pk, st, s_f, &s_stay, K); break;
+    case 8: push_super<8>(A, P, C, tr.pk, st, s_f, &s_stay, K); break;
+    default: push_super<16>(A, P, C, tr.pk, st, s_f, &s_stay, K); break;
   }
 }
 
 // Clock advance (one thread per peak): applies the step that the push kernel just made,
-// selects the next step size, whether this step regroups by sort, and which peaks re-deposit.
+// selects the next step size, whether this step primes by sort, relayouts (the push overflowed
+// a bin) or re-sorts the super-tiles by cell, and which peaks re-deposit.  A running peak's
+// particles are now in the other bin buffer, unless it relayouts: the relayout copies them back
+// into the buffer the push read, under a new layout generation.
 __global__ void k_advance(StepArgs A) {
-  int any_sort = 0, any_refresh = 0;
+  int any_sort = 0, any_layout = 0, any_refresh = 0;
   for (int pk = threadIdx.x; pk < A.npeaks; pk += blockDim.x) {
     PeakClock c = A.clocks[pk];
     const PeakDesc P = A.peaks[pk];
@@ -317,12 +375,15 @@ __global__ void k_advance(StepArgs A) {
         stop_now = c.stop_on_collapse && c.state == PS_RUN;
       }
     }
+    const bool pushed = c.state == PS_RUN || c.state == PS_FINALIZE;
+    const int ovf = pushed && A.ovf_n[pk] != 0u ? 1 : 0;
     switch (c.state) {
       case PS_PRIME:
         dep = 1;
         c.sortstep = 1;
+        c.relayout = 0;
         c.refresh = 0;
-        c.sbuf ^= 1;
+        c.lgen ^= 1;
         c.kpend = 0.0;
         c.a_grid = c.a;
         c.has_delta = 1;
@@ -336,7 +397,6 @@ __global__ void k_advance(StepArgs A) {
         c.nsteps += 1;
         c.sortstep = 0;
         c.refresh = (c.nsteps % P.full_every) == 0 ? 1 : 0;
-        c.sbuf ^= 1;
         dep = 1;
         if (c.mode == SCHED_RATIO) {
           if (c.nsteps >= c.max_steps) c.state = PS_FINALIZE;
@@ -354,17 +414,23 @@ __global__ void k_advance(StepArgs A) {
         c.kpend = 0.0;
         c.sortstep = 0;
         c.refresh = 0;
-        c.sbuf ^= 1;
         dep = 1;
         c.state = PS_IDLE;
         break;
       default:
         break;
     }
+    if (pushed) {
+      if (ovf) A.stats[pk].relayouts += 1u;
+      c.relayout = ovf;
+      if (ovf) c.lgen ^= 1;
+      else c.sbuf ^= 1;
+    }
     c.dep = dep;
     A.clocks[pk] = c;
     A.sortseg[pk].active = dep && c.sortstep;
     any_sort |= dep && c.sortstep;
+    any_layout |= dep && (c.sortstep || c.relayout);
     any_refresh |= dep && c.refresh;
     if (dep) {
       A.stats[pk].max_fix = 0;
@@ -372,9 +438,11 @@ __global__ void k_advance(StepArgs A) {
     }
   }
   any_sort = __syncthreads_or(any_sort);
+  any_layout = __syncthreads_or(any_layout);
   any_refresh = __syncthreads_or(any_refresh);
   if (threadIdx.x == 0) {
     *A.sort_gate = any_sort ? 1u : 0u;
+    *A.layout_gate = any_layout ? 1u : 0u;
     *A.refresh_gate = any_refresh ? 1u : 0u;
   }
 }
@@ -461,27 +529,10 @@ __global__ void __launch_bounds__(PM_THREADS) k_energy(StepArgs A) {
 }
 
 // ------------------------------------------------------------------------------------------
-// Regrouping by sort (priming and every full_every steps): gather the temporary state in
-// sorted order and find the super-tile starts in the sorted keys.
-// Both are grid-stride loops over a grid of a few CTAs per SM and return at once on the steps
-// where no peak sorts.
-__global__ void k_permute(StepArgs A, long long ntot) {
-  if (*A.sort_gate == 0u) return;
-  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < ntot; j += (long long)gridDim.x * blockDim.x) {
-    const int pk = pm_find(A.p_base, A.npeaks, j);
-    const PeakClock C = A.clocks[pk];
-    if (!(C.dep && C.sortstep)) continue;
-    const u32 q = A.perm[j];
-    const PeakDesc& P = A.peaks[pk];
-    if ((long long)q < P.p_off || (long long)q >= P.p_off + P.n) {  // a failed sort: never read outside
-      atomicOr(&A.stats[pk].status, 2u);
-      continue;
-    }
-    A.pos[j] = A.tpos[q];
-    A.mom[j] = A.tmom[q];
-  }
-}
-
+// Priming (particles loaded into the loading area): the Morton-key radix sort, the super-tile
+// starts in the sorted keys, the bin layout from the counts (k_layout), then the gather of the
+// loading area into the bins of the current buffer in sorted order.  Grid-stride loops over a
+// grid of a few CTAs per SM that return at once on the steps where no peak primes.
 __global__ void k_st_starts(StepArgs A, long long ntot) {
   if (*A.sort_gate == 0u) return;
   for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < ntot; j += (long long)gridDim.x * blockDim.x) {
@@ -489,7 +540,7 @@ __global__ void k_st_starts(StepArgs A, long long ntot) {
     const PeakClock C = A.clocks[pk];
     if (!(C.dep && C.sortstep)) continue;
     const PeakDesc P = A.peaks[pk];
-    u32* ss = sst(A, C.sbuf) + P.sst_off;
+    u32* ss = A.sstart + P.sst_off;
     // Super-tile of each sorted key; a key outside the peak's key range (a failed sort) is
     // clamped, so no start is ever written outside the peak's table.
     const u32 kb = A.keys_sorted[j] >> P.st_shift;
@@ -502,55 +553,117 @@ __global__ void k_st_starts(StepArgs A, long long ntot) {
   }
 }
 
-// ------------------------------------------------------------------------------------------
-// Regrouping by re-binning (the other steps).  Destination super-tile D takes, in class order,
-// the run of each source D - u(c) whose particles moved by u(c), then its far movers.
-// scan1: per destination, offsets of its incoming runs and its total.
-__global__ void __launch_bounds__(BIN_CLASSES) k_bin_scan1(StepArgs A) {
-  __shared__ u32 s_w[BIN_CLASSES / 32];
-  const TileRef tr = find_tile(A.st_base, A.npeaks);
-  const PeakClock C = A.clocks[tr.pk];
-  if (!(C.dep && !C.sortstep)) return;
-  const PeakDesc P = A.peaks[tr.pk];
-  const u32 D = (u32)tr.t;
-  const int dx = pm_compact3(D >> 2), dy = pm_compact3(D >> 1), dz = pm_compact3(D);
-  const int c = threadIdx.x, lane = c & 31, warp = c >> 5;
-  u32 v = 0, src = 0;
-  if (c < P.NC) {
-    const int W = P.W, NS = P.NS;
-    const int ux = bin_offset(c / (W * W), NS), uy = bin_offset((c / W) % W, NS), uz = bin_offset(c % W, NS);
-    src = pm_morton3((dx - ux) & (NS - 1), (dy - uy) & (NS - 1), (dz - uz) & (NS - 1));
-    v = A.counts[(P.st_base + src) * BIN_CLASSES + c];
+__global__ void k_permute(StepArgs A, long long ntot) {
+  if (*A.sort_gate == 0u) return;
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < ntot; j += (long long)gridDim.x * blockDim.x) {
+    const int pk = pm_find(A.p_base, A.npeaks, j);
+    const PeakClock C = A.clocks[pk];
+    if (!(C.dep && C.sortstep)) continue;
+    const PeakDesc& P = A.peaks[pk];
+    const u32 q = A.perm[j];
+    const u32 S = min(A.keys_sorted[j] >> P.st_shift, (u32)(P.nst - 1));
+    const BinLayout L = blay(A, C.lgen)[P.st_base + S];
+    const long long r = j - (long long)A.sstart[P.sst_off + S];
+    // A failed sort (a value outside the peak, a rank outside the bin): never read or write outside.
+    if ((long long)q < P.p_off || (long long)q >= P.p_off + P.n || r < 0 || r >= (long long)L.cap) {
+      atomicOr(&A.stats[pk].status, 2u);
+      continue;
+    }
+    bpos(A, C.sbuf)[L.base + r] = A.lpos[q];
+    bmom(A, C.sbuf)[L.base + r] = A.lmom[q];
   }
-  u32 incl = v;
-  for (int d = 1; d < 32; d <<= 1) {
-    const u32 t = __shfl_up_sync(0xffffffffu, incl, d);
-    if (lane >= d) incl += t;
-  }
-  if (lane == 31) s_w[warp] = incl;
-  __syncthreads();
-  u32 off = 0;
-  for (int w = 0; w < warp; ++w) off += s_w[w];
-  if (c < P.NC) A.lpre[(P.st_base + src) * BIN_CLASSES + c] = off + incl - v;
-  if (c == BIN_CLASSES - 1) A.totals[P.st_base + D] = off + incl + A.far_count[P.st_base + D];
 }
 
-// scan2: per peak, super-tile starts from the totals.
-__global__ void __launch_bounds__(1024) k_bin_scan2(StepArgs A) {
-  __shared__ u32 s_w[32];
+// Bin layout of every peak that primes or relayouts this step (one CTA per peak).  The new count
+// of each super-tile comes from the sorted keys when priming; else it is the bin the push filled
+// plus its arrivals in the overflow area.  Each bin gets capacity count + count/8 +
+// BIN_SLACK_MIN (the peak's bin_shift and bin_min), rounded up to BIN_ALIGN.  On a relayout a bin
+// also asks for room for the arrivals of one more step like this one plus bin_grow more steps of
+// its net growth in this step (a bin that particles stream through needs room for its arrivals
+// even when its count stays put), beyond that base spare; the region's spare beyond the base
+// capacities is shared out in proportion to these wants, so that collapsing and infalling regions
+// do not relayout every step.  The region, n + n/4 + (BIN_SLACK_MIN + BIN_ALIGN) nst slots,
+// covers every base layout.  The
+// bases follow as a prefix sum.  The layout goes into generation clock.lgen (the advance kernel
+// switched to it); the fill of the current buffer is set to the new counts, which the
+// permutation or the relayout copies then provide.
+__global__ void __launch_bounds__(LAYOUT_THREADS) k_layout(StepArgs A) {
+  __shared__ u32 s_w[LAYOUT_THREADS / 32];
+  __shared__ unsigned long long s_r[2][LAYOUT_THREADS / 32];
   __shared__ long long s_carry;
+  if (*A.layout_gate == 0u) return;
   const int pk = blockIdx.x;
   const PeakClock C = A.clocks[pk];
-  if (!(C.dep && !C.sortstep)) return;
+  if (!(C.dep && (C.sortstep || C.relayout))) return;
   const PeakDesc P = A.peaks[pk];
-  u32* ss = sst(A, C.sbuf) + P.sst_off;
+  const BinLayout* old = blay(A, C.lgen ^ 1) + P.st_base;
+  BinLayout* lay = blay(A, C.lgen) + P.st_base;
+  const BinFill* pushed = bfill(A, C.sbuf ^ 1) + P.st_base;  // relayout: the buffer the push filled
+  BinFill* cur = bfill(A, C.sbuf) + P.st_base;
+  BinFill* nxt = bfill(A, C.sbuf ^ 1) + P.st_base;
+  const u32* ss = A.sstart + P.sst_off;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (threadIdx.x == 0) s_carry = P.p_off;
+  // Count, base capacity and wanted extra capacity of bin i.
+  auto bin = [&](int i, u32& cnt, u32& cap, u32& want) {
+    want = 0u;
+    u32 need = 0u;
+    if (C.sortstep) {
+      cnt = ss[i + 1] >= ss[i] ? ss[i + 1] - ss[i] : 0u;
+    } else {
+      const u32 prev = min(pushed[i].gap, old[i].cap);  // the bin's count before the push
+      cnt = bin_count(old[i], pushed[i]) + A.ovf_in[P.st_base + i];
+      const u32 grow = cnt > prev ? cnt - prev : 0u;
+      const unsigned long long nd =
+          (unsigned long long)pushed[i].moved * BIN_ARRIVALS + (unsigned long long)grow * (unsigned)P.bin_grow;
+      need = (u32)min(nd, (unsigned long long)P.n);
+    }
+    cnt = min(cnt, (u32)P.n);
+    cap = (cnt + (P.bin_shift < 32 ? cnt >> P.bin_shift : 0u) + (u32)P.bin_min + BIN_ALIGN - 1) & ~(u32)(BIN_ALIGN - 1);
+    if (P.bin_grow > 0 && need > cap - cnt) want = need - (cap - cnt);
+  };
+  // Relayout: the base capacities' total and the total wanted extra, for the allowance.
+  unsigned long long spare = 0, want_tot = 0;
+  if (C.relayout && P.bin_grow > 0) {
+    unsigned long long sc = 0, sg = 0;
+    for (int i = threadIdx.x; i < P.nst; i += LAYOUT_THREADS) {
+      u32 cnt, cap, want;
+      bin(i, cnt, cap, want);
+      sc += cap;
+      sg += want;
+    }
+    for (int d = 16; d > 0; d >>= 1) {
+      sc += __shfl_xor_sync(0xffffffffu, sc, d);
+      sg += __shfl_xor_sync(0xffffffffu, sg, d);
+    }
+    if (lane == 0) {
+      s_r[0][warp] = sc;
+      s_r[1][warp] = sg;
+    }
+    __syncthreads();
+    sc = 0;
+    sg = 0;
+    for (int w = 0; w < LAYOUT_THREADS / 32; ++w) {
+      sc += s_r[0][w];
+      sg += s_r[1][w];
+    }
+    spare = (long long)sc < P.r_size ? (unsigned long long)(P.r_size - (long long)sc) : 0ull;
+    want_tot = sg;
+  }
+  if (threadIdx.x == 0) s_carry = 0;
   __syncthreads();
-  for (int base = 0; base < P.nst; base += 1024) {
+  bool bad = false;
+  for (int base = 0; base < P.nst; base += LAYOUT_THREADS) {
     const int i = base + threadIdx.x;
-    const u32 v = i < P.nst ? A.totals[P.st_base + i] : 0u;
-    u32 incl = v;
+    u32 cnt = 0, cap = 0;
+    if (i < P.nst) {
+      u32 want;
+      bin(i, cnt, cap, want);
+      if (want && want_tot) {  // the wanted extra, or its share of the spare
+        const unsigned long long share = (unsigned long long)want * spare / want_tot;
+        cap += (u32)(min(share, (unsigned long long)want) & ~(unsigned long long)(BIN_ALIGN - 1));
+      }
+    }
+    u32 incl = cap;
     for (int d = 1; d < 32; d <<= 1) {
       const u32 t = __shfl_up_sync(0xffffffffu, incl, d);
       if (lane >= d) incl += t;
@@ -560,75 +673,87 @@ __global__ void __launch_bounds__(1024) k_bin_scan2(StepArgs A) {
     u32 off = 0;
     for (int w = 0; w < warp; ++w) off += s_w[w];
     const long long carry = s_carry;
-    if (i < P.nst) ss[i] = (u32)(carry + off + incl - v);
+    if (i < P.nst) {
+      long long b = carry + off + incl - cap;  // bin start inside the peak's region
+      if (b + cap > P.r_size) {                // counts above the particle total: never past the region
+        bad = true;
+        b = min(b, P.r_size);
+        cap = (u32)(P.r_size - b);
+        cnt = min(cnt, cap);
+      }
+      lay[i] = BinLayout{(u32)(P.r_off + b), cap};
+      cur[i] = BinFill{cnt, cnt, 0u, 0u};
+      if (C.sortstep) {
+        nxt[i] = BinFill{0u, 0u, 0u, 0u};
+        A.ovf_in[P.st_base + i] = 0u;
+      }
+    }
     __syncthreads();
-    if (threadIdx.x == 1023) s_carry = carry + off + incl;
+    if (threadIdx.x == LAYOUT_THREADS - 1) s_carry = carry + off + incl;
     __syncthreads();
   }
-  if (threadIdx.x == 0) {
-    ss[P.nst] = (u32)(P.p_off + P.n);
-    if (s_carry != P.p_off + P.n) atomicOr(&A.stats[pk].status, 4u);  // counts lost a particle
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&A.stats[pk].status, 4u);
+  if (C.sortstep && threadIdx.x == 0) A.ovf_n[pk] = 0u;
+}
+
+// Relayout, per super-tile: the bin the push filled (old layout, other buffer) copied in order
+// to the start of the new bin in the current buffer.
+__global__ void __launch_bounds__(PM_THREADS) k_relayout_copy(StepArgs A) {
+  if (*A.layout_gate == 0u) return;
+  const TileRef tr = find_tile(A.st_base, A.npeaks);
+  const PeakClock C = A.clocks[tr.pk];
+  if (!(C.dep && C.relayout)) return;
+  const long long g = A.st_base[tr.pk] + tr.t;
+  const BinRuns R = bin_runs(blay(A, C.lgen ^ 1)[g], bfill(A, C.sbuf ^ 1)[g]);
+  const BinLayout L = blay(A, C.lgen)[g];
+  const int4* ip = bpos(A, C.sbuf ^ 1);
+  const float4* im = bmom(A, C.sbuf ^ 1);
+  int4* op = bpos(A, C.sbuf) + L.base;
+  float4* om = bmom(A, C.sbuf) + L.base;
+  const int n = min(R.total(), (int)L.cap);
+  for (int k = threadIdx.x; k < n; k += PM_THREADS) {
+    const long long j = R.slot(k);
+    op[k] = ip[j];
+    om[k] = im[j];
   }
 }
 
-// scatter: per source super-tile, every particle to its place in the new grouping.
-__global__ void __launch_bounds__(PUSH_THREADS) k_bin_scatter(StepArgs A) {
-  __shared__ u32 s_rank[BIN_CLASSES];
-  const TileRef tr = find_tile(A.st_base, A.npeaks);
-  const PeakClock C = A.clocks[tr.pk];
-  if (!(C.dep && !C.sortstep)) return;
-  const PeakDesc P = A.peaks[tr.pk];
-  const u32 S = (u32)tr.t;
-  const u32* old = sst(A, C.sbuf ^ 1) + P.sst_off;
-  const u32* ss = sst(A, C.sbuf) + P.sst_off;
-  if (threadIdx.x < BIN_CLASSES) s_rank[threadIdx.x] = 0u;
-  __syncthreads();
-  const int sx = pm_compact3(S >> 2), sy = pm_compact3(S >> 1), sz = pm_compact3(S);
-  const int NS = P.NS, W = P.W;
-  const long long b = old[S], e = old[S + 1];
-  // Run of the stayers (class 0) in this super-tile's own new range.
-  const long long stay0 = (long long)ss[S] + A.lpre[(P.st_base + S) * BIN_CLASSES];
-  for (long long j = b + threadIdx.x; j < e; j += PUSH_THREADS) {
-    const int4 ps = A.tpos[j];
-    const float4 m = A.tmom[j];
-    u32 D = 0;
-    const int c = bin_class(ps.x, sx, sy, sz, P, &D);
-    long long dest;
-    // Ranks inside a class run: one warp-aggregated add for the stayers, one add per mover.
-    // The order inside a run is arbitrary; nothing downstream depends on it.
-    const u32 stay = __ballot_sync(__activemask(), c == 0);
-    if (c == 0) {
-      const int leader = __ffs(stay) - 1;
-      u32 base = 0;
-      if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(&s_rank[0], (u32)__popc(stay));
-      base = __shfl_sync(stay, base, leader);
-      dest = stay0 + base + __popc(stay & lanemask_lt());
-    } else if (c != BIN_FAR) {
-      const int ux = bin_offset(c / (W * W), NS), uy = bin_offset((c / W) % W, NS), uz = bin_offset(c % W, NS);
-      D = pm_morton3((sx + ux) & (NS - 1), (sy + uy) & (NS - 1), (sz + uz) & (NS - 1));
-      dest = (long long)ss[D] + A.lpre[(P.st_base + S) * BIN_CLASSES + c] + atomicAdd(&s_rank[c], 1u);
-    } else {
-      dest = (long long)ss[D + 1] - A.far_count[P.st_base + D] + atomicAdd(&A.far_fill[P.st_base + D], 1u);
-    }
-    if (dest < P.p_off || dest >= P.p_off + P.n) {  // counts and classes disagree: never write outside
-      atomicOr(&A.stats[tr.pk].status, 4u);
+// Relayout: each particle of the overflow area to the end of its new bin (ovf_in counts down to
+// zero, one rank per particle).
+__global__ void k_relayout_ovf(StepArgs A, long long ntot) {
+  if (*A.layout_gate == 0u) return;
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < ntot; j += (long long)gridDim.x * blockDim.x) {
+    const int pk = pm_find(A.p_base, A.npeaks, j);
+    const PeakClock C = A.clocks[pk];
+    if (!(C.dep && C.relayout)) continue;
+    const PeakDesc& P = A.peaks[pk];
+    if (j - P.p_off >= (long long)min(A.ovf_n[pk], (u32)P.n)) continue;
+    const int4 ps = A.lpos[j];
+    const int N = P.N, l2 = P.log2N, s = P.log2TS;
+    const u32 S = pm_morton3(((ps.x >> (2 * l2)) & (N - 1)) >> s, ((ps.x >> l2) & (N - 1)) >> s, (ps.x & (N - 1)) >> s);
+    const long long g = P.st_base + S;
+    const BinLayout L = blay(A, C.lgen)[g];
+    const u32 cnt = bfill(A, C.sbuf)[g].stay;  // the new count, arrivals from the overflow area included
+    const u32 v = atomicSub(&A.ovf_in[g], 1u);
+    if (v == 0u || v > cnt || cnt > L.cap) {  // counts that disagree: never write outside the bin
+      atomicOr(&A.stats[pk].status, 4u);
       continue;
     }
-    A.pos[dest] = ps;
-    A.mom[dest] = m;
+    bpos(A, C.sbuf)[L.base + cnt - v] = ps;
+    bmom(A, C.sbuf)[L.base + cnt - v] = A.lmom[j];
   }
 }
 
 // ------------------------------------------------------------------------------------------
-// Refresh: every full_every steps, after re-binning, each super-tile's particles are re-sorted
-// by cell (local Morton code of the cell inside the super-tile), so the deposit's and the
-// push's warps see neighbouring cells and same-cell runs again.  A counting sort per
-// super-tile: the order inside one cell is not kept (nothing downstream depends on it; the
-// deposit sums integers).  Up to TSORT_CAP particles the super-tile is staged in shared memory
-// and written back in place, coalesced (64 bytes of traffic per particle); denser super-tiles
-// go through the temporary state (push output, free after re-binning) and back.  Persistent
-// grid (one CTA per SM) over the super-tiles; every launch returns at once when no peak
-// refreshes this step.
+// Refresh: every full_every steps each super-tile's particles are re-sorted by cell (local
+// Morton code of the cell inside the super-tile), so the deposit's and the push's warps see
+// neighbouring cells and same-cell runs again, and the bin's two runs become one.  A counting
+// sort per super-tile: the order inside one cell is not kept (nothing downstream depends on it;
+// the deposit sums integers).  Up to TSORT_CAP particles the super-tile is staged in shared
+// memory and written back to the start of its bin, coalesced (64 bytes of traffic per particle);
+// denser super-tiles are copied to the same bin of the other buffer (free until the next push)
+// and placed back from there.  Persistent grid (one CTA per SM) over the super-tiles; every
+// launch returns at once when no peak refreshes this step.
 template <int TS>
 __device__ __forceinline__ void tile_sort(const StepArgs& A, const PeakDesc& P, const PeakClock& C, u32 st,
                                           unsigned char* smem) {
@@ -639,10 +764,19 @@ __device__ __forceinline__ void tile_sort(const StepArgs& A, const PeakDesc& P, 
   u32* cr = (u32*)(smom + TSORT_CAP);                               // [TSORT_CAP] cell << 16 | rank
   unsigned short* inv = (unsigned short*)(cr + TSORT_CAP);          // [TSORT_CAP] slot -> particle
   __shared__ u32 s_wsum[TSORT_THREADS / 32];
-  const u32* ss = sst(A, C.sbuf) + P.sst_off;
-  const long long b = ss[st], e = ss[st + 1];
-  const int n = (int)(e - b);
-  if (n < 2) return;  // uniform
+  const long long g = P.st_base + st;
+  const BinLayout L = blay(A, C.lgen)[g];
+  BinFill* F = bfill(A, C.sbuf) + g;
+  const BinRuns R = bin_runs(L, *F);
+  const int n = R.total();
+  int4* pos = bpos(A, C.sbuf);
+  float4* mom = bmom(A, C.sbuf);
+  int4* tpos = bpos(A, C.sbuf ^ 1);
+  float4* tmom = bmom(A, C.sbuf ^ 1);
+  const long long b = L.base;
+  __syncthreads();  // every thread has read the fill before it is rewritten
+  if (threadIdx.x == 0) *F = BinFill{(u32)n, (u32)n, 0u, 0u};  // one run from here on
+  if (n < 2 && R.n0 == n) return;  // uniform: nothing to move
   const int N = P.N, l2 = P.log2N;
   const int sx = pm_compact3(st >> 2), sy = pm_compact3(st >> 1), sz = pm_compact3(st);
   // Local cell code; masked into the super-tile so a corrupted grouping cannot index outside.
@@ -655,16 +789,20 @@ __device__ __forceinline__ void tile_sort(const StepArgs& A, const PeakDesc& P, 
   const bool staged = n <= TSORT_CAP;
   if (staged) {
     for (int i = threadIdx.x; i < n; i += TSORT_THREADS) {
-      const int4 p = A.pos[b + i];
+      const long long j = R.slot(i);
+      const int4 p = pos[j];
       spos[i] = p;
-      smom[i] = A.mom[b + i];
+      smom[i] = mom[j];
       const u32 c = cell_of(p.x);
       cr[i] = (c << 16) | atomicAdd(&hist[c], 1u);
     }
   } else {
     for (int i = threadIdx.x; i < n; i += TSORT_THREADS) {
-      const u32 c = cell_of(A.pos[b + i].x);
-      A.keys_push[b + i] = atomicAdd(&hist[c], 1u);
+      const long long j = R.slot(i);
+      const int4 p = pos[j];
+      tpos[b + i] = p;
+      tmom[b + i] = mom[j];
+      atomicAdd(&hist[cell_of(p.x)], 1u);
     }
   }
   __syncthreads();
@@ -706,20 +844,19 @@ __device__ __forceinline__ void tile_sort(const StepArgs& A, const PeakDesc& P, 
     __syncthreads();
     for (int o = threadIdx.x; o < n; o += TSORT_THREADS) {
       const int i = inv[o];
-      A.pos[b + o] = spos[i];
-      A.mom[b + o] = smom[i];
+      pos[b + o] = spos[i];
+      mom[b + o] = smom[i];
     }
   } else {
+    // The copies in the other buffer are visible to the block after the barrier above; each
+    // particle takes the next rank of its cell (order inside a cell arbitrary).
     for (int i = threadIdx.x; i < n; i += TSORT_THREADS) {
-      const int4 p = A.pos[b + i];
-      const long long d = b + hist[cell_of(p.x)] + A.keys_push[b + i];
-      A.tpos[d] = p;
-      A.tmom[d] = A.mom[b + i];
-    }
-    __syncthreads();  // the block's global writes are visible to the block after the barrier
-    for (int o = threadIdx.x; o < n; o += TSORT_THREADS) {
-      A.pos[b + o] = A.tpos[b + o];
-      A.mom[b + o] = A.tmom[b + o];
+      const int4 p = tpos[b + i];
+      const u32 o = atomicAdd(&hist[cell_of(p.x)], 1u);
+      if (o < (u32)n) {
+        pos[b + o] = p;
+        mom[b + o] = tmom[b + i];
+      }
     }
   }
   __syncthreads();  // shared arrays are reused by the next super-tile
@@ -866,7 +1003,7 @@ __device__ __forceinline__ Split fix_split(double a, double b) {
   return Split{__funnelshift_r(wl, wh, 19), wl & 0x7FFFFu};
 }
 
-template <int TS>
+template <int TS, int SB>
 __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc& P, const PeakClock& C, int pk,
                                               u32 st, u32* smem, double* rho64) {
   constexpr int T1 = TS + 1, NN = T1 * T1 * T1;
@@ -883,17 +1020,17 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   static_assert((2 * SZ) % 4 == 0, "accumulators are cleared 16 bytes at a time");
   for (int i = threadIdx.x; i < 2 * SZ / 4; i += DEP_THREADS) reinterpret_cast<uint4*>(smem)[i] = make_uint4(0u, 0u, 0u, 0u);
-  const u32* ss = sst(A, C.sbuf) + P.sst_off;
-  const long long b = ss[st], e = ss[st + 1];
-  const long long total = e - b;
+  const long long gst = P.st_base + st;
+  const BinLayout L = blay(A, C.lgen)[gst];
+  const BinRuns R = bin_runs(L, bfill(A, SB)[gst]);
   // A cell index belongs to this super-tile iff its bits outside the local ones equal the
   // super-tile's: one mask and one compare (negative or out-of-mesh values never match).
   const int local = ((TS - 1) << (2 * l2)) | ((TS - 1) << l2) | (TS - 1);
   const int tile_bits = ((sx * TS) << (2 * l2)) | ((sy * TS) << l2) | (sz * TS);
   __syncthreads();
   // Nodes' sums of the chunks folded so far, only for a super-tile of more than one chunk: kept
-  // in the temporary particle state of its own range (free during the deposit; a range of more
-  // than one chunk of 16-byte entries holds the NN 8-byte sums several times over).
+  // in the same bin of the other buffer (free until the next push; a bin of more than one chunk
+  // of 16-byte entries holds the NN 8-byte sums several times over).
   static_assert((8191 / DEP_THREADS) * DEP_THREADS * sizeof(int4) >= NN * sizeof(u64), "fold scratch too small");
   bool folded = false;
   // Split accumulators.  A weight W (at most 2^38, at least -3 for the remainder corner) goes in
@@ -905,15 +1042,20 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
   constexpr int CH_IT = 8191 / DEP_THREADS;  // sweeps of DEP_THREADS particles per chunk
   static_assert(CH_IT >= 1 && CH_IT * DEP_THREADS <= 8191, "chunk too large for the split accumulators");
   static_assert(PM_FIX_BITS == 38, "the split accumulators assume 38 fractional bits");
-  // 32-bit indices inside the super-tile's range (fewer integer instructions than 64-bit ones).
-  const int4* __restrict__ pp = A.pos + b;
-  const int n = (int)total;
+  // 32-bit indices inside the bin's two runs (fewer integer instructions and live registers than
+  // 64-bit pointers): particle k sits at pp[k] in the first run, at pp[k + d1] in the second.
+  const int4* __restrict__ pp = (SB ? A.pos1 : A.pos0) + R.b0;
+  const int n = R.total(), n0 = R.n0, d1 = (int)(R.b1 - R.b0);
+  u64* const fold = reinterpret_cast<u64*>((SB ? A.pos0 : A.pos1) + L.base);
   const int nit = (n + DEP_THREADS - 1) / DEP_THREADS;
   int k = threadIdx.x;
   constexpr int DEPTH = PM_DEP_DEPTH;
   int4 q[DEPTH];  // the particles of the next DEPTH sweeps, loads in flight
 #pragma unroll
-  for (int d = 0; d < DEPTH; ++d) q[d] = k + d * DEP_THREADS < n ? pp[k + d * DEP_THREADS] : make_int4(-1, 0, 0, 0);
+  for (int d = 0; d < DEPTH; ++d) {
+    const int kk = k + d * DEP_THREADS;
+    q[d] = kk < n ? pp[kk < n0 ? kk : kk + d1] : make_int4(-1, 0, 0, 0);
+  }
   bool bad = false;
   int left = CH_IT;
   for (int it = 0; it < nit; ++it) {
@@ -921,7 +1063,8 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
     const bool valid = k < n;
 #pragma unroll
     for (int d = 0; d + 1 < DEPTH; ++d) q[d] = q[d + 1];
-    if (k + DEPTH * DEP_THREADS < n) q[DEPTH - 1] = pp[k + DEPTH * DEP_THREADS];
+    const int kn = k + DEPTH * DEP_THREADS;
+    if (kn < n) q[DEPTH - 1] = pp[kn < n0 ? kn : kn + d1];
     k += DEP_THREADS;
     {
       const int c = ps.x;
@@ -953,7 +1096,7 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
     if (--left == 0 && it + 1 < nit) {  // chunk full and more to come: fold it into acc64
       left = CH_IT;
       __syncthreads();
-      fold_chunk<TS>(reinterpret_cast<u64*>(A.tpos + b), acc_hi, acc_lo, folded);
+      fold_chunk<TS>(fold, acc_hi, acc_lo, folded);
       folded = true;
       __syncthreads();
     }
@@ -967,7 +1110,6 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
   const long long gbase = ((long long)sx * TS * N + (long long)sy * TS) * N + sz * TS;
   long long* face = A.face + P.face_off + (long long)st * FC;
   long long* halo = A.halo + P.halo_off + (long long)st * P.hc;
-  const u64* fold = reinterpret_cast<const u64*>(A.tpos + b);
   const long long nmf = P.n_mean_fix;
   const double inv = P.inv_fix_nmean;
   for (int item = threadIdx.x; item < T1 * T1 * NG; item += DEP_THREADS) {
@@ -1034,8 +1176,6 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
     }
     atomicAdd((unsigned long long*)&A.stats[pk].mass_defect, (unsigned long long)ts);
     atomicMax(&A.stats[pk].max_fix, (u64)tm);
-    A.far_count[P.st_base + st] = 0u;  // consumed by this step's regrouping
-    A.far_fill[P.st_base + st] = 0u;
   }
 }
 
@@ -1047,9 +1187,20 @@ __global__ void __launch_bounds__(DEP_THREADS, 4) k_deposit(StepArgs A, double* 
   if (!C.dep) return;
   const PeakDesc P = A.peaks[tr.pk];
   switch (P.TS) {
-    case 4: deposit_super<4>(A, P, C, tr.pk, (u32)tr.t, s_dep, rho64); break;
-    case 8: deposit_super<8>(A, P, C, tr.pk, (u32)tr.t, s_dep, rho64); break;
-    default: deposit_super<16>(A, P, C, tr.pk, (u32)tr.t, s_dep, rho64); break;
+    // The bin buffer as a template argument: its pointers are then kernel parameters, not a
+    // per-thread select (the particle loop is register-bound).
+    case 4:
+      if (C.sbuf) deposit_super<4, 1>(A, P, C, tr.pk, (u32)tr.t, s_dep, rho64);
+      else deposit_super<4, 0>(A, P, C, tr.pk, (u32)tr.t, s_dep, rho64);
+      break;
+    case 8:
+      if (C.sbuf) deposit_super<8, 1>(A, P, C, tr.pk, (u32)tr.t, s_dep, rho64);
+      else deposit_super<8, 0>(A, P, C, tr.pk, (u32)tr.t, s_dep, rho64);
+      break;
+    default:
+      if (C.sbuf) deposit_super<16, 1>(A, P, C, tr.pk, (u32)tr.t, s_dep, rho64);
+      else deposit_super<16, 0>(A, P, C, tr.pk, (u32)tr.t, s_dep, rho64);
+      break;
   }
 }
 
@@ -1060,9 +1211,16 @@ __global__ void __launch_bounds__(FIX_THREADS) k_fixup(StepArgs A, double* rho64
   __shared__ long long s_max[FIX_THREADS / 32];
   __shared__ const long long* s_nb[8];
   const TileRef tr = find_tile(A.st_base, A.npeaks);
-  if (!A.clocks[tr.pk].dep) return;
+  const PeakClock C = A.clocks[tr.pk];
+  if (!C.dep) return;
   const PeakDesc P = A.peaks[tr.pk];
   const u32 Y = (u32)tr.t;
+  if (threadIdx.x == 0) {
+    // Ready for the next push, which fills the other buffer: no arrivals yet, overflow area
+    // empty.  (Here rather than in the deposit, whose particle loop is register-bound.)
+    bfill(A, C.sbuf ^ 1)[P.st_base + Y].moved = 0u;
+    if (Y == 0) A.ovf_n[tr.pk] = 0u;
+  }
   if (threadIdx.x < 8) {
     const int o = threadIdx.x, NS = P.NS;
     const u32 sn = pm_morton3((pm_compact3(Y >> 2) - (o & 1)) & (NS - 1), (pm_compact3(Y >> 1) - ((o >> 1) & 1)) & (NS - 1),
@@ -1241,6 +1399,7 @@ __global__ void k_reset_peak(StepArgs A, int pk, double a0, int mode, double par
   A.clocks[pk] = c;
   A.stats[pk].status = 0;
   A.stats[pk].nsamples = 0;
+  A.stats[pk].relayouts = 0;
   A.sort_err[pk] = 0;
 }
 
@@ -1274,37 +1433,53 @@ __global__ void k_set_particles(StepArgs A, int pk, PeakDesc P, const double* __
   }
   const int cell = (ii[0] << (2 * P.log2N)) | (ii[1] << P.log2N) | ii[2];
   const long long g = P.p_off + i;
-  // Loaded into the temporary state in lattice order; the priming step sorts it into place.
-  A.tpos[g] = make_int4(cell, __float_as_int(ff[0]), __float_as_int(ff[1]), __float_as_int(ff[2]));
-  A.tmom[g] = make_float4((float)p[3 * i], (float)p[3 * i + 1], (float)p[3 * i + 2], __int_as_float((int)i));
+  // Loaded into the loading area in lattice order; the priming step sorts it into bins.
+  A.lpos[g] = make_int4(cell, __float_as_int(ff[0]), __float_as_int(ff[1]), __float_as_int(ff[2]));
+  A.lmom[g] = make_float4((float)p[3 * i], (float)p[3 * i + 1], (float)p[3 * i + 2], __int_as_float((int)i));
   A.keys_push[g] = pm_cell_key(ii[0], ii[1], ii[2]);
 }
 
-// Re-priming an existing state: copy it back to the loading area with its sort keys.
-__global__ void k_reload(StepArgs A, PeakDesc P) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= P.n) return;
-  const long long g = P.p_off + i;
-  const int4 ps = A.pos[g];
-  A.tpos[g] = ps;
-  A.tmom[g] = A.mom[g];
+// Re-priming an existing state: copy it back to the loading area with its sort keys.  One CTA
+// per super-tile of the peak; places in the loading area from a per-peak counter (ovf_n, zeroed
+// by the host before the launch; the priming step zeroes it again), one add per warp.
+__global__ void __launch_bounds__(PM_THREADS) k_reload(StepArgs A, int pk, PeakDesc P) {
+  const PeakClock C = A.clocks[pk];
+  const long long g = P.st_base + blockIdx.x;
+  const BinRuns R = bin_runs(blay(A, C.lgen)[g], bfill(A, C.sbuf)[g]);
+  const int4* ip = bpos(A, C.sbuf);
+  const float4* im = bmom(A, C.sbuf);
   const int N = P.N, l2 = P.log2N;
-  A.keys_push[g] = pm_cell_key(ps.x >> (2 * l2), (ps.x >> l2) & (N - 1), ps.x & (N - 1));
+  const int n = R.total();
+  for (int base = 0; base < n; base += PM_THREADS) {  // uniform trip count: the ballot sees whole warps
+    const int k = base + threadIdx.x;
+    const bool v = k < n;
+    const u32 vm = __ballot_sync(0xffffffffu, v);
+    u32 o0 = 0;
+    if ((threadIdx.x & 31) == 0 && vm) o0 = atomicAdd(&A.ovf_n[pk], (u32)__popc(vm));
+    o0 = __shfl_sync(0xffffffffu, o0, 0);
+    if (!v) continue;
+    const u32 o = o0 + (u32)__popc(vm & lanemask_lt());
+    if (o >= (u32)P.n) {
+      atomicOr(&A.stats[pk].status, 4u);
+      continue;
+    }
+    const long long j = R.slot(k);
+    const int4 ps = ip[j];
+    A.lpos[P.p_off + o] = ps;
+    A.lmom[P.p_off + o] = im[j];
+    A.keys_push[P.p_off + o] = pm_cell_key((ps.x >> (2 * l2)) & (N - 1), (ps.x >> l2) & (N - 1), ps.x & (N - 1));
+  }
 }
 
 // Current state -> float64 x, p (lattice order).  p includes the pending closing kick; acc
-// (optional) receives -grad Phi at the particles evaluated for expansion factor a_acc.
-__global__ void k_get_particles(StepArgs A, int pk, PeakDesc P, double* __restrict__ x, double* __restrict__ p,
-                                double* __restrict__ acc, double a_acc) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= P.n) return;
-  const PeakClock C = A.clocks[pk];
-  // A peak loaded but not yet primed still has its particles in the loading area.
-  const bool loaded_only = C.state == PS_PRIME;
-  const int4 ps = loaded_only ? A.tpos[P.p_off + i] : A.pos[P.p_off + i];
-  const float4 m = loaded_only ? A.tmom[P.p_off + i] : A.mom[P.p_off + i];
+// (optional) receives -grad Phi at the particles evaluated for expansion factor a_acc.  One CTA
+// per super-tile of the peak walks its bin; a peak loaded but not yet primed has its particles in
+// the loading area instead, where CTA t takes the t-th slice.
+__device__ __forceinline__ void get_one(const StepArgs& A, int pk, const PeakDesc& P, const PeakClock& C, int4 ps,
+                                        float4 m, double* __restrict__ x, double* __restrict__ p,
+                                        double* __restrict__ acc, double a_acc) {
   const int N = P.N;
-  const int ii[3] = {ps.x >> (2 * P.log2N), (ps.x >> P.log2N) & (N - 1), ps.x & (N - 1)};
+  const int ii[3] = {(ps.x >> (2 * P.log2N)) & (N - 1), (ps.x >> P.log2N) & (N - 1), ps.x & (N - 1)};
   const float f[3] = {__int_as_float(ps.y), __int_as_float(ps.z), __int_as_float(ps.w)};
   const long long id = (long long)__float_as_int(m.w);
   if (id < 0 || id >= P.n) {  // never write through an id that is not a lattice index
@@ -1333,6 +1508,27 @@ __global__ void k_get_particles(StepArgs A, int pk, PeakDesc P, double* __restri
     }
     if (p) p[3 * id + d] = mv[d] + C.kpend * (C.a_grid / C.a) * g[d];
     if (acc) acc[3 * id + d] = g[d] * (C.a_grid / a_acc);
+  }
+}
+
+__global__ void __launch_bounds__(PM_THREADS) k_get_particles(StepArgs A, int pk, PeakDesc P, double* __restrict__ x,
+                                                              double* __restrict__ p, double* __restrict__ acc,
+                                                              double a_acc) {
+  const PeakClock C = A.clocks[pk];
+  if (C.state == PS_PRIME) {
+    const long long per = (P.n + P.nst - 1) / P.nst;
+    const long long i0 = per * blockIdx.x, i1 = min(P.n, i0 + per);
+    for (long long i = i0 + threadIdx.x; i < i1; i += PM_THREADS)
+      get_one(A, pk, P, C, A.lpos[P.p_off + i], A.lmom[P.p_off + i], x, p, acc, a_acc);
+    return;
+  }
+  const long long g = P.st_base + blockIdx.x;
+  const BinRuns R = bin_runs(blay(A, C.lgen)[g], bfill(A, C.sbuf)[g]);
+  const int4* ip = bpos(A, C.sbuf);
+  const float4* im = bmom(A, C.sbuf);
+  for (int k = threadIdx.x; k < R.total(); k += PM_THREADS) {
+    const long long j = R.slot(k);
+    get_one(A, pk, P, C, ip[j], im[j], x, p, acc, a_acc);
   }
 }
 
@@ -1446,10 +1642,10 @@ void launch_st_starts(const StepArgs& A, long long ntot, cudaStream_t s) {
 void launch_tile_sort(const StepArgs& A, long long nst, cudaStream_t s) {
   k_tile_sort<<<stride_grid(nst, 1, 1), TSORT_THREADS, pm_tile_sort_smem(), s>>>(A, nst);
 }
-void launch_bin(const StepArgs& A, long long nst, cudaStream_t s) {
-  k_bin_scan1<<<(unsigned)nst, BIN_CLASSES, 0, s>>>(A);
-  k_bin_scan2<<<(unsigned)A.npeaks, 1024, 0, s>>>(A);
-  k_bin_scatter<<<(unsigned)nst, PUSH_THREADS, 0, s>>>(A);
+void launch_layout(const StepArgs& A, long long nst, long long ntot, cudaStream_t s) {
+  k_layout<<<(unsigned)A.npeaks, LAYOUT_THREADS, 0, s>>>(A);
+  k_relayout_copy<<<(unsigned)nst, PM_THREADS, 0, s>>>(A);
+  k_relayout_ovf<<<stride_grid(ntot, PM_THREADS, 8), PM_THREADS, 0, s>>>(A, ntot);
 }
 void launch_deposit(const StepArgs& A, long long nst, size_t smem, double* rho64, cudaStream_t s) {
   k_deposit<<<(unsigned)nst, DEP_THREADS, smem, s>>>(A, rho64);
@@ -1469,12 +1665,13 @@ void launch_set_particles(const StepArgs& A, int pk, const PeakDesc& P, const do
                           cudaStream_t s) {
   k_set_particles<<<nb(P.n, PM_THREADS), PM_THREADS, 0, s>>>(A, pk, P, x, p);
 }
-void launch_reload(const StepArgs& A, const PeakDesc& P, cudaStream_t s) {
-  k_reload<<<nb(P.n, PM_THREADS), PM_THREADS, 0, s>>>(A, P);
+void launch_reload(const StepArgs& A, int pk, const PeakDesc& P, cudaStream_t s) {
+  cudaMemsetAsync(A.ovf_n + pk, 0, sizeof(u32), s);
+  k_reload<<<(unsigned)P.nst, PM_THREADS, 0, s>>>(A, pk, P);
 }
 void launch_get_particles(const StepArgs& A, int pk, const PeakDesc& P, double* x, double* p, double* acc,
                           double a_acc, cudaStream_t s) {
-  k_get_particles<<<nb(P.n, PM_THREADS), PM_THREADS, 0, s>>>(A, pk, P, x, p, acc, a_acc);
+  k_get_particles<<<(unsigned)P.nst, PM_THREADS, 0, s>>>(A, pk, P, x, p, acc, a_acc);
 }
 void launch_interp64(const double* F, const double* X, long long n, int N, double dx, double* out, cudaStream_t s) {
   k_interp64<<<nb(n, PM_THREADS), PM_THREADS, 0, s>>>(F, X, n, N, dx, out);

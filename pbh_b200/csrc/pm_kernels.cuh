@@ -1,16 +1,21 @@
 // Kernels of one PM step (pbhgr/pbhgr/pm3d.py:101-129) over a batch of peaks.
 //
-// Particles live grouped by super-tile (TS^3 cells): super-tile S of a peak owns the contiguous
-// range [sstart[S], sstart[S+1]) of the state arrays.  One step:
-//   push       per super-tile: CIC gather of the forces, kicks, drift; output in place into the
-//              temporary state, tagged with the class of the super-tile the particle moved to
-//              (one of <= 125 neighbours) and counted per class
+// Particles live in bins, one per super-tile (TS^3 cells), in two bin buffers that alternate
+// every step.  Both buffers share a bin layout: super-tile S of a peak owns slots
+// [base[S], base[S] + cap[S]) of each buffer, with spare capacity (an eighth of its count plus
+// 32, and room for further growth after a relayout, set whenever the layout is made).  A filled bin holds two runs: the particles that stayed
+// in S, from base[S] up, and the particles that arrived from other super-tiles, from
+// base[S] + (the bin's count before the step) up (BinFill).  One step:
+//   push       per super-tile: CIC gather of the forces, kicks, drift; each particle appended
+//              to the bin of the super-tile it is now in, in the other buffer (stayers ranked in
+//              shared memory, arrivals by an atomic on the destination's count); a particle
+//              for which the destination bin has no room goes to the peak's overflow area
 //   energy     per peak: momentum, kinetic and potential energy, Layzer-Irvine integral
-//   advance    per peak clock (and which peaks regroup by sort this step)
-//   regroup    re-binning (scan of the class counts, then a scatter into the new grouping);
-//              every full_every steps each super-tile's particles are then re-sorted by cell
-//              (local counting sort); when particles are first loaded, a full Morton-key radix
-//              sort plus a permutation instead
+//   advance    per peak clock; a peak whose push overflowed relayouts this step
+//   regroup    relayout (new capacities from the counts, bins and overflow area copied into the
+//              buffer the push read); every full_every steps each super-tile's particles are
+//              re-sorted by cell (local counting sort); when particles are first loaded, a full
+//              Morton-key radix sort of the loading area and a permutation into fresh bins
 //   deposit    per super-tile: CIC density of its particles into (TS+1)^3 nodes; interior nodes
 //              final, face and upper-halo nodes as 64-bit partials
 //   fixup      per super-tile: face nodes = own partial + the lower neighbours' halo partials
@@ -27,8 +32,35 @@
 #define FIX_THREADS 256    // face fix-up CTA
 #define TSORT_THREADS 1024 // super-tile sort (refresh) CTA
 #define TSORT_CAP 5120     // particles of a super-tile sorted in shared memory; denser ones via global
-#define BIN_CLASSES 128   // stride of the per-super-tile class arrays (>= 125)
-#define BIN_FAR 255       // class of a particle that moved more than 2 super-tiles
+// Bin capacities: count + (count >> BIN_SLACK_SHIFT) + BIN_SLACK_MIN, rounded up to BIN_ALIGN;
+// a relayout adds room for BIN_ARRIVALS times the arrivals of the step plus BIN_GROW_STEPS times
+// its net growth, out of a further (n >> BIN_SPARE_SHIFT) slots of the peak's bin region.
+#ifndef BIN_SLACK_SHIFT
+#define BIN_SLACK_SHIFT 3
+#endif
+#ifndef BIN_SPARE_SHIFT
+#define BIN_SPARE_SHIFT 3
+#endif
+#ifndef BIN_ARRIVALS
+#define BIN_ARRIVALS 1
+#endif
+#ifndef BIN_GROW_STEPS
+#define BIN_GROW_STEPS 4
+#endif
+#define BIN_SLACK_MIN 32
+#define BIN_ALIGN 8        // bin bases and capacities are multiples of 8 slots (128 bytes)
+#define LAYOUT_THREADS 1024
+
+// Fill of one bin in one buffer: the stayers occupy [base, base + stay), the arrivals
+// [base + gap, base + gap + min(moved, cap - gap)); gap is the bin's count before the push
+// that filled it (no stayer rank reaches it).  `moved` is incremented atomically by the pushes
+// of all source super-tiles and may exceed the room; the excess went to the overflow area.
+struct BinFill {
+  u32 stay, gap, moved, pad;
+};
+struct BinLayout {
+  u32 base, cap;  // slot offset in a bin buffer, capacity
+};
 
 // Views of the engine's device arrays handed to every kernel.
 struct StepArgs {
@@ -36,7 +68,8 @@ struct StepArgs {
   PeakClock* clocks;
   PeakStats* stats;
   SortSeg* sortseg;            // sort activity flags, written by the advance kernel
-  u32* sort_gate;              // 1 when any peak regroups by sort this step (advance kernel)
+  u32* sort_gate;              // 1 when any peak primes by sort this step (advance kernel)
+  u32* layout_gate;            // 1 when any peak primes or relayouts this step (advance kernel)
   u32* refresh_gate;           // 1 when any peak re-sorts its super-tiles this step (advance kernel)
   const long long* st_base;    // [npeaks + 1] prefix of super-tiles
   const long long* p_base;     // [npeaks + 1] prefix of particles
@@ -45,20 +78,20 @@ struct StepArgs {
   const int* green_peak;       // [ngreen] those peaks (the others use the native transform)
   int npeaks;
   int ngreen;
-  int4* pos;                   // state, grouped by super-tile
-  float4* mom;
-  int4* tpos;                  // push output (same order as the input), regrouped into pos/mom
-  float4* tmom;
-  u32* keys_push;              // Morton keys written by set_particles / reload (priming sort input);
-                               // per-particle scratch of the super-tile sort on refresh steps
+  int4* pos0;                  // bin buffers 0 and 1 (clock.sbuf: the current one)
+  float4* mom0;
+  int4* pos1;
+  float4* mom1;
+  int4* lpos;                  // loading area (set_particles, reload) and overflow area of the push,
+  float4* lmom;                // [p_off, p_off + n) per peak
+  BinLayout* lay[2];           // [super-tile] bin layouts, two generations (clock.lgen selects)
+  BinFill* fill[2];            // [super-tile] bin fills of buffers 0 and 1
+  u32* ovf_n;                  // [peak] particles in the overflow area (push), reset by the deposit
+  u32* ovf_in;                 // [super-tile] overflowed particles whose destination it is
+  u32* keys_push;              // Morton keys written by set_particles / reload (priming sort input)
   const u32* keys_sorted;      // sort output keys
   const u32* perm;             // sort output permutation
-  u32* sstart[2];              // super-tile starts, two generations (clock.sbuf selects)
-  u32* counts;                 // [super-tile][BIN_CLASSES] class counts of the source
-  u32* lpre;                   // [super-tile][BIN_CLASSES] offset of a run in its destination
-  u32* far_count;              // [super-tile] far movers arriving (destination)
-  u32* far_fill;               // [super-tile] far movers placed so far
-  u32* totals;                 // [super-tile] particles arriving
+  u32* sstart;                 // [peak][nst + 1] starts of the super-tiles in the sorted keys
   long long* face;             // face partials
   long long* halo;             // upper-halo partials
   double2* epart;              // [super-tile][4] push partials (sum, compensation): p_x, p_y, p_z, p^2
@@ -87,7 +120,8 @@ void launch_advance(const StepArgs& A, cudaStream_t s);
 void launch_energy(const StepArgs& A, cudaStream_t s);
 void launch_permute(const StepArgs& A, long long ntot, cudaStream_t s);
 void launch_st_starts(const StepArgs& A, long long ntot, cudaStream_t s);
-void launch_bin(const StepArgs& A, long long nst, cudaStream_t s);
+// Bin layouts of the priming and relayout peaks, then the relayout's copies (gated launches).
+void launch_layout(const StepArgs& A, long long nst, long long ntot, cudaStream_t s);
 void launch_tile_sort(const StepArgs& A, long long nst, cudaStream_t s);
 void launch_deposit(const StepArgs& A, long long nst, size_t smem, double* rho64, cudaStream_t s);
 void launch_fixup(const StepArgs& A, long long nst, double* rho64, cudaStream_t s);
@@ -110,7 +144,7 @@ void launch_reset_peak(const StepArgs& A, int pk, double a0, int mode, double pa
 void launch_release_peak(const StepArgs& A, int pk, cudaStream_t s);
 void launch_set_particles(const StepArgs& A, int pk, const PeakDesc& P, const double* x, const double* p,
                           cudaStream_t s);
-void launch_reload(const StepArgs& A, const PeakDesc& P, cudaStream_t s);  // state -> loading area + keys
+void launch_reload(const StepArgs& A, int pk, const PeakDesc& P, cudaStream_t s);  // bins -> loading area + keys
 void launch_get_particles(const StepArgs& A, int pk, const PeakDesc& P, double* x, double* p, double* acc,
                           double a_acc, cudaStream_t s);
 void launch_interp64(const double* F, const double* X, long long n, int N, double dx, double* out, cudaStream_t s);

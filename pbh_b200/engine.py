@@ -43,7 +43,7 @@ def _ptr(t) -> int:
 
 class Engine:
     def __init__(self, peaks, device: int = 0, graph: bool = True, full_every: int = 16, dynamic: bool = False,
-                 bucket_sort: bool = True, native_fft: bool = True):
+                 bucket_sort: bool = True, native_fft: bool = True, tight_bins: bool = False):
         torch = _lib.require_cuda()
         self._torch = torch
         lib = _lib.load()
@@ -52,15 +52,18 @@ class Engine:
         arr = (_lib.PeakCfg * len(self.cfgs))(*[c.cstruct() for c in self.cfgs])
         h = C.c_void_p()
         self.device = int(device)
-        # Particles are regrouped each step by re-binning into neighbouring super-tiles, and every
-        # `full_every` steps each super-tile is re-sorted by cell (bucket_sort=False: every step).
-        # Results do not depend on the choice: the deposit is order-independent bit for bit.
+        # The push appends every particle to the bin of its new super-tile, and every `full_every`
+        # steps each super-tile is re-sorted by cell (bucket_sort=False: every step).  Results do
+        # not depend on the choice: the deposit is order-independent bit for bit.  tight_bins:
+        # bins without spare capacity, so that almost every step overflows and relayouts (a test
+        # of that path; same results).
         # dynamic: served runs; no graph, and each step's FFTs cover only the slots in use.
         # native_fft: 64^3-512^3 meshes use the native transform with the Green multiply fused
         # (False: cuFFT and the separate Green kernel, as for every other mesh size).
         every = int(full_every) if bucket_sort else 1
         flags = ((max(1, min(every, 255)) & 0xFF) << 8) | (_lib.FLAG_GRAPH if graph else 0) | \
-                (_lib.FLAG_DYNAMIC if dynamic else 0) | (_lib.FLAG_NATIVE_FFT if native_fft else 0)
+                (_lib.FLAG_DYNAMIC if dynamic else 0) | (_lib.FLAG_NATIVE_FFT if native_fft else 0) | \
+                (_lib.FLAG_TIGHT_BINS if tight_bins else 0)
         self.npeaks = len(self.cfgs)
         torch.cuda.set_device(self.device)
         check(lib.pm_engine_create(arr, len(self.cfgs), self.device, flags, C.byref(h)), "pm_engine_create")

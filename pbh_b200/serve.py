@@ -69,7 +69,8 @@ NATIVE_FFT_SIZES = (64, 128, 256, 512)   # meshes the engine transforms natively
 def slot_bytes(N: int, native_fft: bool = True) -> int:
     """Device bytes one slot of mesh N holds in the engine (particles = cells)."""
     n = N ** 3
-    per_particle = 2 * 16 + 2 * 16 + 2 * 4 + 2 * 4 + 4      # state x2, keys x2, values x2, bucket starts
+    # two bin buffers with a quarter spare, the loading/overflow area, keys x2, values x2, tables
+    per_particle = 2 * 32 * 5 / 4 + 32 + 2 * 4 + 2 * 4 + 4
     per_cell = 4 + 8 * (N // 2 + 1) / N * 4 + 12            # delta, 4 spectra, 3 force grids
     native = native_fft and N in NATIVE_FFT_SIZES
     fft_work = 0 if native else 16 * n                      # cuFFT's shared work area (~13-14 B per cell measured)

@@ -174,11 +174,11 @@ def test_batched_peaks_equal_alone():
 
 
 @pytest.mark.parametrize("Np,tile", [(32, 8), (48, 16)])
-def test_regroup_by_rebinning_equals_sorting_every_step(Np, tile):
-    """Re-binning with the per-super-tile re-sort every step or every 16th step give the same
-    run, bit for bit (the order inside a super-tile never changes a result).  Np = 48 on a 32^3
-    mesh with 16^3 super-tiles puts ~13.8k particles in each super-tile, beyond the shared-memory
-    capacity of the re-sort (5120), so its global-memory path runs too."""
+def test_refresh_every_step_equals_every_16th(Np, tile):
+    """Bins kept by the push with the per-super-tile re-sort every step or every 16th step give
+    the same run, bit for bit (the order inside a super-tile never changes a result).  Np = 48 on
+    a 32^3 mesh with 16^3 super-tiles puts ~13.8k particles in each super-tile, beyond the
+    shared-memory capacity of the re-sort (5120), so its global-memory path runs too."""
     from pbh_b200._lib import SCHED_RATIO
     N = 32
     mesh, ic = recipe(N, Np, delta0=0.05, seed=8)
@@ -195,8 +195,36 @@ def test_regroup_by_rebinning_equals_sorting_every_step(Np, tile):
         assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("N,Np,tile,pscale", [(32, 32, 8, 3.0), (32, 48, 16, 3.0), (64, 32, 4, 6.0)])
+def test_overflowing_bins_relayout_without_changing_results(N, Np, tile, pscale):
+    """Bins without spare capacity overflow on almost every step once particles cross super-tile
+    faces (random positions, momenta drifting about a cell per step); each overflow sends the
+    peak through the relayout (new bin capacities, the bins and the overflow area copied into the
+    buffer the push read).  Positions, momenta and delta stay the same bit for bit as with the
+    normal spare capacity, and the mass stays exact.  Np = 48 with 16^3 super-tiles also takes
+    the global-memory paths of the super-tile re-sort and of the deposit (more than one chunk)."""
+    from pbh_b200._lib import SCHED_RATIO
+    rng = np.random.default_rng(31)
+    x = rng.uniform(0.0, 1.0, size=(Np ** 3, 3))
+    p = rng.normal(0.0, pscale, size=(Np ** 3, 3))
+    runs, relayouts = [], []
+    for tight in (False, True):
+        eng = engine([dict(N=N, Np=Np, L=1.0, tile=tile)], tight_bins=tight)
+        eng.set_particles(0, x, p, 1.0, mode=SCHED_RATIO, param=RATIO_100, max_steps=20)
+        eng.run(22)
+        xg, pg = [t.cpu().numpy() for t in eng.particles(0)]
+        runs.append((xg, pg, eng.delta(0).cpu().numpy()))
+        s = eng.stats(0)
+        assert s.mass_defect == 0.0 and s.status == 0, (tight, s.status)
+        relayouts.append(s.relayouts)
+        eng.close()
+    assert relayouts[1] >= 15, relayouts          # tight bins: most steps relayout
+    for a, b in zip(runs[0], runs[1]):
+        assert np.array_equal(a, b)
+
+
 def test_fast_particles_cross_several_super_tiles():
-    """Particles that move more than two super-tiles in one step take the far-mover path."""
+    """Particles that move more than two super-tiles in one step land in their new bins."""
     N, Np = 64, 16
     mesh = O.Mesh(N, 1.0, Np)
     rng = np.random.default_rng(21)

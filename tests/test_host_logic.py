@@ -111,7 +111,8 @@ def test_algorithmic_bytes_per_phase():
     import bench
     n, cells, modes = 1000, 1000, 600
     assert bench.algorithmic_bytes("push", n, cells, modes, 3) == n * 64 + cells * 12
-    assert bench.algorithmic_bytes("bin", n, cells, modes, 3) == n * 64
+    assert bench.algorithmic_bytes("refresh", n, cells, modes, 3) == n * 64
+    assert bench.algorithmic_bytes("regroup", n, cells, modes, 3) == 0.0   # relayouts only on overflow
     assert bench.algorithmic_bytes("deposit", n, cells, modes, 3) == n * 16 + cells * 4
     assert bench.algorithmic_bytes("green", n, cells, modes, 3) == modes * 32
     assert bench.algorithmic_bytes("r2c", n, cells, modes, 3) == 0.0
