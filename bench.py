@@ -373,6 +373,9 @@ def run_ours(args):
                 "relayouts": r_late,
                 "a_cfg_end": a_cfg,
                 "peaks_past_design_collapse": int(sum(1 for sp in specs if sp.a_collapse_cfg <= a_cfg))}
+        # Where the late steps spend their time: per-phase device ms over the next 4 (ungraphed) steps.
+        ph_late = ens.timed_phases(4)
+        late["phase_ms"] = {name: round(float(v), 4) for name, v in zip(PHASES, ph_late)}
     cells = sum(s.N ** 3 for s in specs)
     # modes the Green kernel handles (the native 256^3 transform applies its own multiply)
     modes = sum(s.N * s.N * (s.N // 2 + 1) for s in specs if not (args.fft == "native" and s.N in NATIVE_FFT_SIZES))
