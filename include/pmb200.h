@@ -79,7 +79,9 @@ typedef struct {
   double li_residual;
   double li_scale;
   int relayouts;             /* steps since the load whose push overflowed a super-tile's bin (the
-                              * peak's bins were then re-sized and its particles moved) */
+                              * overflowed bins were then moved to free space with more capacity) */
+  int relayouts_full;        /* of those, the steps with no such space left: every bin of the peak
+                              * was re-laid out and all of its particles moved */
 } pm_stats_info;
 
 /* Create an engine holding npeaks independent peaks (a batched ensemble; npeaks = 1 is the

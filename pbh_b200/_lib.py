@@ -35,7 +35,8 @@ class StatsInfo(C.Structure):
     _fields_ = [("rho_max_over_mean", C.c_double), ("delta_max", C.c_double), ("mass_defect", C.c_double),
                 ("status", C.c_uint), ("energy_samples", C.c_int), ("a_energy", C.c_double),
                 ("momentum", C.c_double * 3), ("kinetic", C.c_double), ("potential", C.c_double),
-                ("li_residual", C.c_double), ("li_scale", C.c_double), ("relayouts", C.c_int)]
+                ("li_residual", C.c_double), ("li_scale", C.c_double), ("relayouts", C.c_int),
+                ("relayouts_full", C.c_int)]
 
 
 class ICParams(C.Structure):

@@ -88,7 +88,9 @@ struct PeakClock {
   int lgen;        // bin layout generation in use ({base, capacity} per super-tile)
   int dep;         // 1 when this step re-deposits (set by the advance kernel)
   int sortstep;    // 1 when this step groups the loaded particles by a full Morton-key sort (priming)
-  int relayout;    // 1 when this step's push overflowed a bin: new bin capacities, particles moved
+  int relayout;    // this step's push overflowed a bin: 1 until the layout kernel decides, then 1 for a
+                   // partial relayout (the overflowed bins move to free space at the end of the peak's
+                   // region) or 2 for a full one (every bin re-laid out, into the other buffer)
   int refresh;     // 1 when this step re-sorts every super-tile's particles by cell
   int has_delta;   // delta/grids hold data
   int stop_on_collapse;  // end the run (finalize) on the step that detects collapse
@@ -104,7 +106,7 @@ struct PeakStats {
   u32 status;             // bit 0: non-finite force/momentum, bit 1: fixed-point overflow
   u32 nsamples;           // energy samples taken since the peak was loaded
   u32 relayouts;          // steps since the peak was loaded whose push overflowed a bin
-  u32 pad;
+  u32 relayouts_full;     // of those, the steps that re-laid out every bin of the peak
   // Energy and momentum at a_e, from compensated FP64 sums in a fixed reduction order.  With
   // p = a^2 dx/dt, dp/dt = -grad Phi (pbhgr/pbhgr/pm3d.py:3-6) the Layzer-Irvine equation reads
   // d[a (K + W)]/da = -K, so a (K + W) + int_{a0}^{a} K da stays equal to a0 (K0 + W0).

@@ -334,6 +334,7 @@ void fill_stats(const PeakDesc& P, const PeakStats& s, int sort_err, pm_stats_in
   o->mass_defect = (double)s.mass_defect / (double)PM_FIX_ONE;
   o->status = s.status | (sort_err ? 2u : 0u);
   o->relayouts = (int)s.relayouts;
+  o->relayouts_full = (int)s.relayouts_full;
   fill_energy(s, o);
 }
 

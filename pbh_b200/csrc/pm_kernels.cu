@@ -356,8 +356,8 @@ __global__ void __launch_bounds__(PUSH_THREADS, 2) k_push(StepArgs A) {
 // Clock advance (one thread per peak): applies the step that the push kernel just made,
 // selects the next step size, whether this step primes by sort, relayouts (the push overflowed
 // a bin) or re-sorts the super-tiles by cell, and which peaks re-deposit.  A running peak's
-// particles are now in the other bin buffer, unless it relayouts: the relayout copies them back
-// into the buffer the push read, under a new layout generation.
+// particles are now in the other bin buffer; one that relayouts switches to a new layout
+// generation, which the layout kernel fills in.
 __global__ void k_advance(StepArgs A) {
   int any_sort = 0, any_layout = 0, any_refresh = 0;
   for (int pk = threadIdx.x; pk < A.npeaks; pk += blockDim.x) {
@@ -420,11 +420,11 @@ __global__ void k_advance(StepArgs A) {
       default:
         break;
     }
-    if (pushed) {
+    if (pushed) {  // the particles are now in the buffer the push wrote
       if (ovf) A.stats[pk].relayouts += 1u;
       c.relayout = ovf;
+      c.sbuf ^= 1;
       if (ovf) c.lgen ^= 1;
-      else c.sbuf ^= 1;
     }
     c.dep = dep;
     A.clocks[pk] = c;
@@ -576,20 +576,27 @@ __global__ void k_permute(StepArgs A, long long ntot) {
 
 // Bin layout of every peak that primes or relayouts this step (one CTA per peak).  The new count
 // of each super-tile comes from the sorted keys when priming; else it is the bin the push filled
-// plus its arrivals in the overflow area.  Each bin gets capacity count + count/8 +
-// BIN_SLACK_MIN (the peak's bin_shift and bin_min), rounded up to BIN_ALIGN.  On a relayout a bin
-// also asks for room for the arrivals of one more step like this one plus bin_grow more steps of
-// its net growth in this step (a bin that particles stream through needs room for its arrivals
-// even when its count stays put), beyond that base spare; the region's spare beyond the base
-// capacities is shared out in proportion to these wants, so that collapsing and infalling regions
-// do not relayout every step.  The region, n + n/4 + (BIN_SLACK_MIN + BIN_ALIGN) nst slots,
-// covers every base layout.  The
-// bases follow as a prefix sum.  The layout goes into generation clock.lgen (the advance kernel
-// switched to it); the fill of the current buffer is set to the new counts, which the
-// permutation or the relayout copies then provide.
+// plus its arrivals in the overflow area.  A bin's base capacity is count + count/8 +
+// BIN_SLACK_MIN (the peak's bin_shift and bin_min), rounded up to BIN_ALIGN.  On a relayout a
+// bin also asks for room for BIN_ARRIVALS times the arrivals of this step plus bin_grow steps
+// of its net growth in this step (a bin that particles stream through needs room for its
+// arrivals even when its count stays put), so that collapsing and infalling regions do not
+// relayout every step.
+//   Partial relayout (clock.relayout = 1): when the free space after the last bin of the peak's
+// region holds every overflowed bin with its base capacity and wanted room, only those bins
+// move there (to the buffer the push filled, which stays current); the others keep their place
+// and their two runs.  Their old places stay unused until the next full relayout.
+//   Full relayout (clock.relayout = 2): every bin is laid out again from the start of the
+// region, the wanted room shared out of the region's spare beyond the base capacities in
+// proportion to the wants, and every particle is copied into the other buffer, which becomes
+// current.  The region, n + n/8 + n/8 + (BIN_SLACK_MIN + BIN_ALIGN) nst slots, covers every base
+// layout.
+// The layout goes into generation clock.lgen (the advance kernel switched to it).  The relayout
+// copies set the new fills; when priming, this kernel sets them to the counts, which the
+// permutation then provides.
 __global__ void __launch_bounds__(LAYOUT_THREADS) k_layout(StepArgs A) {
   __shared__ u32 s_w[LAYOUT_THREADS / 32];
-  __shared__ unsigned long long s_r[2][LAYOUT_THREADS / 32];
+  __shared__ unsigned long long s_r[4][LAYOUT_THREADS / 32];
   __shared__ long long s_carry;
   if (*A.layout_gate == 0u) return;
   const int pk = blockIdx.x;
@@ -598,10 +605,11 @@ __global__ void __launch_bounds__(LAYOUT_THREADS) k_layout(StepArgs A) {
   const PeakDesc P = A.peaks[pk];
   const BinLayout* old = blay(A, C.lgen ^ 1) + P.st_base;
   BinLayout* lay = blay(A, C.lgen) + P.st_base;
-  const BinFill* pushed = bfill(A, C.sbuf ^ 1) + P.st_base;  // relayout: the buffer the push filled
+  const BinFill* pushed = bfill(A, C.sbuf) + P.st_base;  // relayout: the buffer the push filled
   BinFill* cur = bfill(A, C.sbuf) + P.st_base;
   BinFill* nxt = bfill(A, C.sbuf ^ 1) + P.st_base;
   const u32* ss = A.sstart + P.sst_off;
+  const u32* ovf_in = A.ovf_in + P.st_base;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   // Count, base capacity and wanted extra capacity of bin i.
   auto bin = [&](int i, u32& cnt, u32& cap, u32& want) {
@@ -611,7 +619,7 @@ __global__ void __launch_bounds__(LAYOUT_THREADS) k_layout(StepArgs A) {
       cnt = ss[i + 1] >= ss[i] ? ss[i + 1] - ss[i] : 0u;
     } else {
       const u32 prev = min(pushed[i].gap, old[i].cap);  // the bin's count before the push
-      cnt = bin_count(old[i], pushed[i]) + A.ovf_in[P.st_base + i];
+      cnt = bin_count(old[i], pushed[i]) + ovf_in[i];
       const u32 grow = cnt > prev ? cnt - prev : 0u;
       const unsigned long long nd =
           (unsigned long long)pushed[i].moved * BIN_ARRIVALS + (unsigned long long)grow * (unsigned)P.bin_grow;
@@ -621,35 +629,55 @@ __global__ void __launch_bounds__(LAYOUT_THREADS) k_layout(StepArgs A) {
     cap = (cnt + (P.bin_shift < 32 ? cnt >> P.bin_shift : 0u) + (u32)P.bin_min + BIN_ALIGN - 1) & ~(u32)(BIN_ALIGN - 1);
     if (P.bin_grow > 0 && need > cap - cnt) want = need - (cap - cnt);
   };
-  // Relayout: the base capacities' total and the total wanted extra, for the allowance.
-  unsigned long long spare = 0, want_tot = 0;
-  if (C.relayout && P.bin_grow > 0) {
-    unsigned long long sc = 0, sg = 0;
+  // Capacity of an overflowed bin moved by a partial relayout: base capacity plus its want.
+  auto moved_cap = [&](u32 cap, u32 want) -> u32 {
+    return (u32)min((unsigned long long)cap + want + BIN_ALIGN - 1, (unsigned long long)P.r_size) &
+           ~(u32)(BIN_ALIGN - 1);
+  };
+  // Relayout: the base capacities' total, the total want, the space the overflowed bins need when
+  // moved, and the end of the last bin of the current layout; then partial or full.
+  bool partial = false;
+  unsigned long long spare = 0, want_tot = 0, tail = 0;
+  if (C.relayout) {
+    unsigned long long sc = 0, sg = 0, sp = 0, mt = 0;
     for (int i = threadIdx.x; i < P.nst; i += LAYOUT_THREADS) {
       u32 cnt, cap, want;
       bin(i, cnt, cap, want);
       sc += cap;
       sg += want;
+      if (ovf_in[i]) sp += moved_cap(cap, want);
+      const unsigned long long e = (unsigned long long)old[i].base + old[i].cap - (unsigned long long)P.r_off;
+      mt = e > mt ? e : mt;
     }
     for (int d = 16; d > 0; d >>= 1) {
       sc += __shfl_xor_sync(0xffffffffu, sc, d);
       sg += __shfl_xor_sync(0xffffffffu, sg, d);
+      sp += __shfl_xor_sync(0xffffffffu, sp, d);
+      const unsigned long long o = __shfl_xor_sync(0xffffffffu, mt, d);
+      mt = o > mt ? o : mt;
     }
     if (lane == 0) {
       s_r[0][warp] = sc;
       s_r[1][warp] = sg;
+      s_r[2][warp] = sp;
+      s_r[3][warp] = mt;
     }
     __syncthreads();
-    sc = 0;
-    sg = 0;
+    sc = sg = sp = mt = 0;
     for (int w = 0; w < LAYOUT_THREADS / 32; ++w) {
       sc += s_r[0][w];
       sg += s_r[1][w];
+      sp += s_r[2][w];
+      mt = s_r[3][w] > mt ? s_r[3][w] : mt;
     }
-    spare = (long long)sc < P.r_size ? (unsigned long long)(P.r_size - (long long)sc) : 0ull;
-    want_tot = sg;
+    tail = mt;
+    partial = tail + sp <= (unsigned long long)P.r_size;
+    if (!partial && P.bin_grow > 0) {
+      spare = (long long)sc < P.r_size ? (unsigned long long)(P.r_size - (long long)sc) : 0ull;
+      want_tot = sg;
+    }
   }
-  if (threadIdx.x == 0) s_carry = 0;
+  if (threadIdx.x == 0) s_carry = partial ? (long long)tail : 0;
   __syncthreads();
   bool bad = false;
   for (int base = 0; base < P.nst; base += LAYOUT_THREADS) {
@@ -658,7 +686,9 @@ __global__ void __launch_bounds__(LAYOUT_THREADS) k_layout(StepArgs A) {
     if (i < P.nst) {
       u32 want;
       bin(i, cnt, cap, want);
-      if (want && want_tot) {  // the wanted extra, or its share of the spare
+      if (partial) {
+        cap = ovf_in[i] ? moved_cap(cap, want) : 0u;  // only the overflowed bins take new space
+      } else if (want && want_tot) {  // the wanted extra, or its share of the spare
         const unsigned long long share = (unsigned long long)want * spare / want_tot;
         cap += (u32)(min(share, (unsigned long long)want) & ~(unsigned long long)(BIN_ALIGN - 1));
       }
@@ -674,16 +704,20 @@ __global__ void __launch_bounds__(LAYOUT_THREADS) k_layout(StepArgs A) {
     for (int w = 0; w < warp; ++w) off += s_w[w];
     const long long carry = s_carry;
     if (i < P.nst) {
-      long long b = carry + off + incl - cap;  // bin start inside the peak's region
-      if (b + cap > P.r_size) {                // counts above the particle total: never past the region
-        bad = true;
-        b = min(b, P.r_size);
-        cap = (u32)(P.r_size - b);
-        cnt = min(cnt, cap);
+      if (partial && cap == 0u) {
+        lay[i] = old[i];  // not overflowed: stays where it is
+      } else {
+        long long b = carry + off + incl - cap;  // bin start inside the peak's region
+        if (b + cap > P.r_size) {                // counts above the particle total: never past the region
+          bad = true;
+          b = min(b, P.r_size);
+          cap = (u32)(P.r_size - b);
+          cnt = min(cnt, cap);
+        }
+        lay[i] = BinLayout{(u32)(P.r_off + b), cap};
       }
-      lay[i] = BinLayout{(u32)(P.r_off + b), cap};
-      cur[i] = BinFill{cnt, cnt, 0u, 0u};
       if (C.sortstep) {
+        cur[i] = BinFill{cnt, cnt, 0u, 0u};
         nxt[i] = BinFill{0u, 0u, 0u, 0u};
         A.ovf_in[P.st_base + i] = 0u;
       }
@@ -693,41 +727,67 @@ __global__ void __launch_bounds__(LAYOUT_THREADS) k_layout(StepArgs A) {
     __syncthreads();
   }
   if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&A.stats[pk].status, 4u);
-  if (C.sortstep && threadIdx.x == 0) A.ovf_n[pk] = 0u;
-}
-
-// Relayout, per super-tile: the bin the push filled (old layout, other buffer) copied in order
-// to the start of the new bin in the current buffer.
-__global__ void __launch_bounds__(PM_THREADS) k_relayout_copy(StepArgs A) {
-  if (*A.layout_gate == 0u) return;
-  const TileRef tr = find_tile(A.st_base, A.npeaks);
-  const PeakClock C = A.clocks[tr.pk];
-  if (!(C.dep && C.relayout)) return;
-  const long long g = A.st_base[tr.pk] + tr.t;
-  const BinRuns R = bin_runs(blay(A, C.lgen ^ 1)[g], bfill(A, C.sbuf ^ 1)[g]);
-  const BinLayout L = blay(A, C.lgen)[g];
-  const int4* ip = bpos(A, C.sbuf ^ 1);
-  const float4* im = bmom(A, C.sbuf ^ 1);
-  int4* op = bpos(A, C.sbuf) + L.base;
-  float4* om = bmom(A, C.sbuf) + L.base;
-  const int n = min(R.total(), (int)L.cap);
-  for (int k = threadIdx.x; k < n; k += PM_THREADS) {
-    const long long j = R.slot(k);
-    op[k] = ip[j];
-    om[k] = im[j];
+  if (threadIdx.x == 0) {
+    if (C.sortstep) A.ovf_n[pk] = 0u;
+    if (C.relayout) {
+      A.clocks[pk].relayout = partial ? 1 : 2;
+      if (!partial) {  // the full relayout fills the other buffer, which becomes current
+        A.clocks[pk].sbuf = C.sbuf ^ 1;
+        A.stats[pk].relayouts_full += 1u;
+      }
+    }
   }
 }
 
-// Relayout: each particle of the overflow area to the end of its new bin (ovf_in counts down to
-// zero, one rank per particle).
-__global__ void k_relayout_ovf(StepArgs A, long long ntot) {
+// Relayout, per super-tile.  Full (clock.relayout = 2): every bin the push filled (old layout,
+// other buffer) is copied in order to the start of its new bin in the current buffer.  Partial
+// (1): only the bins with arrivals in the overflow area move, inside the current buffer, to
+// their new place after the last bin.  Either way the bin's fill is then set to its new count,
+// which includes the arrivals k_relayout_ovf places next.
+__global__ void __launch_bounds__(PM_THREADS) k_relayout_copy(StepArgs A) {
   if (*A.layout_gate == 0u) return;
-  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < ntot; j += (long long)gridDim.x * blockDim.x) {
-    const int pk = pm_find(A.p_base, A.npeaks, j);
-    const PeakClock C = A.clocks[pk];
-    if (!(C.dep && C.relayout)) continue;
-    const PeakDesc& P = A.peaks[pk];
-    if (j - P.p_off >= (long long)min(A.ovf_n[pk], (u32)P.n)) continue;
+  const int pk = blockIdx.y;  // RELAYOUT_COPY_BLOCKS CTAs per peak, each looping over its bins
+  const PeakClock C = A.clocks[pk];
+  if (!(C.dep && C.relayout)) return;
+  const bool full = C.relayout == 2;
+  const int src = full ? (C.sbuf ^ 1) : C.sbuf;
+  const long long st0 = A.st_base[pk], nst = A.st_base[pk + 1] - st0;
+  for (long long t = blockIdx.x; t < nst; t += gridDim.x) {
+    const long long g = st0 + t;
+    const u32 arrivals = A.ovf_in[g];
+    if (!full && arrivals == 0u) continue;  // partial relayout: this bin stays as it is (uniform)
+    const BinRuns R = bin_runs(blay(A, C.lgen ^ 1)[g], bfill(A, src)[g]);
+    const BinLayout L = blay(A, C.lgen)[g];
+    const int4* ip = bpos(A, src);
+    const float4* im = bmom(A, src);
+    int4* op = bpos(A, C.sbuf) + L.base;
+    float4* om = bmom(A, C.sbuf) + L.base;
+    const int n = min(R.total(), (int)L.cap);
+    for (int k = threadIdx.x; k < n; k += PM_THREADS) {  // old and new places never overlap
+      const long long j = R.slot(k);
+      op[k] = ip[j];
+      om[k] = im[j];
+    }
+    __syncthreads();  // every thread has read the old fill (a partial relayout rewrites that entry)
+    if (threadIdx.x == 0) {
+      const u32 cnt = min((u32)R.total() + arrivals, L.cap);
+      bfill(A, C.sbuf)[g] = BinFill{cnt, cnt, 0u, 0u};
+    }
+  }
+}
+
+// Relayout: each particle of a relayouting peak's overflow area to the end of its new bin
+// (ovf_in counts down to zero, one rank per particle).  RELAYOUT_OVF_BLOCKS CTAs per peak walk
+// only that peak's overflow entries.
+__global__ void __launch_bounds__(PM_THREADS) k_relayout_ovf(StepArgs A) {
+  if (*A.layout_gate == 0u) return;
+  const int pk = blockIdx.y;
+  const PeakClock C = A.clocks[pk];
+  if (!(C.dep && C.relayout)) return;
+  const PeakDesc& P = A.peaks[pk];
+  const long long novf = (long long)min(A.ovf_n[pk], (u32)P.n);
+  for (long long o = (long long)blockIdx.x * blockDim.x + threadIdx.x; o < novf; o += (long long)gridDim.x * blockDim.x) {
+    const long long j = P.p_off + o;
     const int4 ps = A.lpos[j];
     const int N = P.N, l2 = P.log2N, s = P.log2TS;
     const u32 S = pm_morton3(((ps.x >> (2 * l2)) & (N - 1)) >> s, ((ps.x >> l2) & (N - 1)) >> s, (ps.x & (N - 1)) >> s);
@@ -1400,6 +1460,7 @@ __global__ void k_reset_peak(StepArgs A, int pk, double a0, int mode, double par
   A.stats[pk].status = 0;
   A.stats[pk].nsamples = 0;
   A.stats[pk].relayouts = 0;
+  A.stats[pk].relayouts_full = 0;
   A.sort_err[pk] = 0;
 }
 
@@ -1644,8 +1705,8 @@ void launch_tile_sort(const StepArgs& A, long long nst, cudaStream_t s) {
 }
 void launch_layout(const StepArgs& A, long long nst, long long ntot, cudaStream_t s) {
   k_layout<<<(unsigned)A.npeaks, LAYOUT_THREADS, 0, s>>>(A);
-  k_relayout_copy<<<(unsigned)nst, PM_THREADS, 0, s>>>(A);
-  k_relayout_ovf<<<stride_grid(ntot, PM_THREADS, 8), PM_THREADS, 0, s>>>(A, ntot);
+  k_relayout_copy<<<dim3(RELAYOUT_COPY_BLOCKS, (unsigned)A.npeaks), PM_THREADS, 0, s>>>(A);
+  k_relayout_ovf<<<dim3(RELAYOUT_OVF_BLOCKS, (unsigned)A.npeaks), PM_THREADS, 0, s>>>(A);
 }
 void launch_deposit(const StepArgs& A, long long nst, size_t smem, double* rho64, cudaStream_t s) {
   k_deposit<<<(unsigned)nst, DEP_THREADS, smem, s>>>(A, rho64);

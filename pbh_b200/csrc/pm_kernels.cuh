@@ -50,6 +50,8 @@
 #define BIN_SLACK_MIN 32
 #define BIN_ALIGN 8        // bin bases and capacities are multiples of 8 slots (128 bytes)
 #define LAYOUT_THREADS 1024
+#define RELAYOUT_OVF_BLOCKS 32  // CTAs per peak placing a relayout's overflow area
+#define RELAYOUT_COPY_BLOCKS 256  // CTAs per peak moving a relayout's bins
 
 // Fill of one bin in one buffer: the stayers occupy [base, base + stay), the arrivals
 // [base + gap, base + gap + min(moved, cap - gap)); gap is the bin's count before the push

@@ -195,19 +195,24 @@ def test_refresh_every_step_equals_every_16th(Np, tile):
         assert np.array_equal(a, b)
 
 
-@pytest.mark.parametrize("N,Np,tile,pscale", [(32, 32, 8, 3.0), (32, 48, 16, 3.0), (64, 32, 4, 6.0)])
-def test_overflowing_bins_relayout_without_changing_results(N, Np, tile, pscale):
+@pytest.mark.parametrize("N,Np,tile,pscale,fast", [(32, 32, 8, 3.0, 1.0), (32, 48, 16, 3.0, 1.0), (64, 32, 4, 6.0, 1.0),
+                                                    (32, 32, 8, 3.0, 0.002), (64, 64, 16, 3.0, 0.0005)])
+def test_overflowing_bins_relayout_without_changing_results(N, Np, tile, pscale, fast):
     """Bins without spare capacity overflow on almost every step once particles cross super-tile
-    faces (random positions, momenta drifting about a cell per step); each overflow sends the
-    peak through the relayout (new bin capacities, the bins and the overflow area copied into the
-    buffer the push read).  Positions, momenta and delta stay the same bit for bit as with the
-    normal spare capacity, and the mass stays exact.  Np = 48 with 16^3 super-tiles also takes
-    the global-memory paths of the super-tile re-sort and of the deposit (more than one chunk)."""
+    faces (random positions; a fraction `fast` of them with momenta drifting about a cell per
+    step, the rest at rest).  Each overflow sends the peak through a relayout: the overflowed
+    bins move to free space after the last bin when it holds them (partial), else every bin is
+    laid out again and copied to the other buffer (full).  With every particle fast the bins all
+    overflow and the relayouts are full; with a few fast ones most are partial.  Positions,
+    momenta and delta stay the same bit for bit as with the normal spare capacity, and the mass
+    stays exact.  Np = 48 with 16^3 super-tiles also takes the global-memory paths of the
+    super-tile re-sort and of the deposit (more than one chunk)."""
     from pbh_b200._lib import SCHED_RATIO
     rng = np.random.default_rng(31)
     x = rng.uniform(0.0, 1.0, size=(Np ** 3, 3))
     p = rng.normal(0.0, pscale, size=(Np ** 3, 3))
-    runs, relayouts = [], []
+    p[rng.uniform(size=Np ** 3) >= fast] = 0.0
+    runs, counts = [], []
     for tight in (False, True):
         eng = engine([dict(N=N, Np=Np, L=1.0, tile=tile)], tight_bins=tight)
         eng.set_particles(0, x, p, 1.0, mode=SCHED_RATIO, param=RATIO_100, max_steps=20)
@@ -216,9 +221,14 @@ def test_overflowing_bins_relayout_without_changing_results(N, Np, tile, pscale)
         runs.append((xg, pg, eng.delta(0).cpu().numpy()))
         s = eng.stats(0)
         assert s.mass_defect == 0.0 and s.status == 0, (tight, s.status)
-        relayouts.append(s.relayouts)
+        counts.append((s.relayouts, s.relayouts_full))
         eng.close()
-    assert relayouts[1] >= 15, relayouts          # tight bins: most steps relayout
+    relayouts, full = counts[1]
+    assert relayouts >= 10, counts                # tight bins: most steps relayout
+    if fast == 1.0:
+        assert full >= 1, counts                  # every bin overflows: no room for a partial move
+    else:
+        assert relayouts - full >= 1, counts      # a few bins overflow: moved after the last bin
     for a, b in zip(runs[0], runs[1]):
         assert np.array_equal(a, b)
 
