@@ -44,7 +44,7 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-errors", action="store_true", help="skip the per-output errors against the float64 oracle")
     ap.add_argument("--no-late", action="store_true", help="skip the device-timed window late in the run")
-    ap.add_argument("--full-sort", action="store_true", help="re-sort every super-tile by cell every step (instead of every 16th)")
+    ap.add_argument("--full-sort", action="store_true", help="re-sort every super-tile by cell every step (by default never)")
     ap.add_argument("--no-serve", action="store_true", help="skip the served-stream latency run")
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="arrival window of the served stream")
     ap.add_argument("--serve-rate", type=float, default=20.0, help="mean request arrivals per second")
@@ -187,7 +187,7 @@ def run_reference(args):
 def algorithmic_bytes(phase: str, n: int, cells: int, modes: int, npass: int) -> float:
     if phase == "push":        # read state 32, write state 32, force grids 12 per cell
         return n * (32 + 32) + cells * 12.0
-    if phase == "refresh":     # super-tile re-sort (every 16th step): read + write state
+    if phase == "refresh":     # super-tile re-sort (only with --full-sort): read + write state
         return n * 64.0
     if phase == "deposit":     # read positions 16, write delta 4 per cell (face/halo partials are overhead)
         return n * 16.0 + cells * 4.0
@@ -351,7 +351,7 @@ def run_ours(args):
     relayouts = sum(s.relayouts for s in ens.stats()) - relayouts0
 
     # Per-kernel device times: a few ungraphed steps with events between phases, same stream.
-    ph = ens.timed_phases(16)                     # one refresh step and fifteen plain ones
+    ph = ens.timed_phases(16)                     # sixteen steady steps
     # A second device-timed window late in the run (past the collapse of the early peaks).
     late = None
     run_len = min(sp.steps for sp in specs)
@@ -382,8 +382,8 @@ def run_ours(args):
     kern = {}
     for k, name in enumerate(PHASES):
         b = algorithmic_bytes(name, n_step, cells, modes, npass)
-        if name == "refresh":
-            b /= 16.0
+        if name == "refresh" and not args.full_sort:
+            b = 0.0                                # no re-sort in these steps
         kern[name] = {"ms": ph[k], "algorithmic_bytes": b, "gbs": (b / (ph[k] / 1e3) / 1e9) if b and ph[k] > 0 else None}
     peaks_file = ROOT / "MEASURED_PEAKS.json"
     if peaks_file.exists():
@@ -413,7 +413,7 @@ def run_ours(args):
             "data": "synthetic (recipe peaks, seeded numpy noise)",
             "config": workload_config(desc, specs, world),
             "engine": {"regroup": "push into bins, super-tile re-sort every step" if args.full_sort else
-                       "push into bins, super-tile re-sort every 16th", "timed_steps": [1 + args.warmup,
+                       "push into bins, no super-tile re-sort", "timed_steps": [1 + args.warmup,
                                                                                        args.warmup + args.steps],
                        "super_tiles": {str(k): v for k, v in sorted(tiles.items())},
                        "relayouts_timed": relayouts,

@@ -87,7 +87,8 @@ typedef struct {
 /* Create an engine holding npeaks independent peaks (a batched ensemble; npeaks = 1 is the
  * plain single run).  Allocates all device memory and cuFFT plans up front; no later call
  * allocates.  flags: bits 8..15 = re-sort every super-tile's particles by cell every that many
- * steps (16 if 0; the push keeps them binned by super-tile between); bit 1 = replay the step as a CUDA
+ * steps (never if 0, the default: the push keeps them binned by super-tile, and the order inside
+ * a bin was measured not to matter); bit 1 = replay the step as a CUDA
  * graph; bit 2 = dynamic mode for served runs: no graph, and each step's FFTs cover only the
  * slots up to the highest one in use in each mesh size (slots are the peaks of one size, in
  * order); bit 3 = the native transform with the Green multiply fused (pm_rfft3_native) for

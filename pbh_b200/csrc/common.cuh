@@ -49,7 +49,7 @@ struct PeakDesc {
   int st_shift;            // 3*log2TS: key >> st_shift is the super-tile
   int fc, hc;              // face nodes (any local coordinate 0) and upper-halo nodes per super-tile
   int gradient;            // 0 spectral (reference), 1 two-point finite difference, 2 four-point
-  int full_every;          // every super-tile's particles re-sorted by cell every this many steps
+  int full_every;          // every super-tile's particles re-sorted by cell every this many steps (0: never)
   int native_fft;          // 1: the native 256^3 transform carries the Green multiply (no k_green)
   int bin_shift, bin_min;  // bin capacity: count + (count >> bin_shift) + bin_min, rounded up to BIN_ALIGN
   int bin_grow;            // relayout: room for this many more steps of a bin's growth (region allowing)

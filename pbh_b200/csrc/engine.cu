@@ -93,7 +93,7 @@ struct pm_engine {
   u32* refresh_gate = nullptr;  // one word: any peak re-sorts its super-tiles this step
   long long* face = nullptr;
   long long* halo = nullptr;
-  SortPlan sort{};       // Morton-key sort used by priming and every full_every steps
+  SortPlan sort{};       // Morton-key sort used by priming
   int sort_result = 0;   // which (keys, vals) pair holds the sorted output
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // replayed step without / with the priming sort
   bool prime_pending = false;  // a peak was (re)loaded: the next step must include the priming sort
@@ -358,7 +358,7 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   std::map<int, int> class_of;
   long long poff = 0, roff = 0, stb = 0, mb = 0, sso = 0, fo = 0, ho = 0;
   int TSmax = 1, max_bits = 0;
-  const int full_every = std::max(1, (E->flags >> 8) & 0xFF ? (E->flags >> 8) & 0xFF : 16);
+  const int full_every = (E->flags >> 8) & 0xFF;  // 0: never (the default; measured not to pay)
   std::vector<long long> st_base(npeaks + 1), p_base(npeaks + 1), mode_base(npeaks + 1);
   for (int i = 0; i < npeaks; ++i) {
     const pm_peak_cfg& c = cfg[i];

@@ -396,7 +396,7 @@ __global__ void k_advance(StepArgs A) {
         c.a_grid = an;
         c.nsteps += 1;
         c.sortstep = 0;
-        c.refresh = (c.nsteps % P.full_every) == 0 ? 1 : 0;
+        c.refresh = P.full_every > 0 && (c.nsteps % P.full_every) == 0 ? 1 : 0;
         dep = 1;
         if (c.mode == SCHED_RATIO) {
           if (c.nsteps >= c.max_steps) c.state = PS_FINALIZE;
@@ -805,7 +805,8 @@ __global__ void __launch_bounds__(PM_THREADS) k_relayout_ovf(StepArgs A) {
 }
 
 // ------------------------------------------------------------------------------------------
-// Refresh: every full_every steps each super-tile's particles are re-sorted by cell (local
+// Refresh (optional, off by default): every full_every steps each super-tile's particles are
+// re-sorted by cell (local
 // Morton code of the cell inside the super-tile), so the deposit's and the push's warps see
 // neighbouring cells and same-cell runs again, and the bin's two runs become one.  A counting
 // sort per super-tile: the order inside one cell is not kept (nothing downstream depends on it;

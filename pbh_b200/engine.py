@@ -42,7 +42,7 @@ def _ptr(t) -> int:
 
 
 class Engine:
-    def __init__(self, peaks, device: int = 0, graph: bool = True, full_every: int = 16, dynamic: bool = False,
+    def __init__(self, peaks, device: int = 0, graph: bool = True, full_every: int = 0, dynamic: bool = False,
                  bucket_sort: bool = True, native_fft: bool = True, tight_bins: bool = False):
         torch = _lib.require_cuda()
         self._torch = torch
@@ -52,8 +52,9 @@ class Engine:
         arr = (_lib.PeakCfg * len(self.cfgs))(*[c.cstruct() for c in self.cfgs])
         h = C.c_void_p()
         self.device = int(device)
-        # The push appends every particle to the bin of its new super-tile, and every `full_every`
-        # steps each super-tile is re-sorted by cell (bucket_sort=False: every step).  Results do
+        # The push appends every particle to the bin of its new super-tile; every `full_every`
+        # steps (0: never, the default) each super-tile is re-sorted by cell (bucket_sort=False:
+        # every step).  Results do
         # not depend on the choice: the deposit is order-independent bit for bit.  tight_bins:
         # bins without spare capacity, so that almost every step overflows and relayouts (a test
         # of that path; same results).

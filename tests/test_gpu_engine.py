@@ -214,7 +214,7 @@ def test_overflowing_bins_relayout_without_changing_results(N, Np, tile, pscale,
     p[rng.uniform(size=Np ** 3) >= fast] = 0.0
     runs, counts = [], []
     for tight in (False, True):
-        eng = engine([dict(N=N, Np=Np, L=1.0, tile=tile)], tight_bins=tight)
+        eng = engine([dict(N=N, Np=Np, L=1.0, tile=tile)], tight_bins=tight, full_every=16)
         eng.set_particles(0, x, p, 1.0, mode=SCHED_RATIO, param=RATIO_100, max_steps=20)
         eng.run(22)
         xg, pg = [t.cpu().numpy() for t in eng.particles(0)]
