@@ -61,15 +61,24 @@ class Ensemble:
         _lib.check(rc, "pm_get_stats_all")
         return list(arr)
 
-    def deltas(self):
+    def result_buffers(self):
+        """Page-locked host buffers for deltas(), one N^3 float32 array per peak (allocate once
+        and reuse: page-locking memory is slow)."""
+        torch = _lib.require_cuda()
+        return [torch.empty((s.N,) * 3, dtype=torch.float32, pin_memory=True) for s in self.specs]
+
+    def deltas(self, out=None):
         """Every peak's density contrast of its last deposit (N^3 float32) on the host: one
         asynchronous copy per peak into page-locked memory behind the engine's work, then one
-        wait.  Returns a list of numpy arrays (views of the page-locked buffers)."""
-        torch = _lib.require_cuda()
+        wait.  `out`: buffers from result_buffers() (allocated here if None).  Returns a list of
+        numpy arrays (views of the page-locked buffers)."""
         lib = _lib.load()
+        bufs = out if out is not None else self.result_buffers()
         outs = []
         for i, s in enumerate(self.specs):
-            buf = torch.empty((s.N,) * 3, dtype=torch.float32, pin_memory=True)
+            buf = bufs[i]
+            if tuple(buf.shape) != (s.N,) * 3 or not buf.is_pinned():
+                raise ValueError(f"result buffer {i} must be a page-locked {s.N}^3 float32 tensor")
             _lib.check(lib.pm_get_delta_async(self.engine._h, i, buf.data_ptr()), "pm_get_delta_async")
             outs.append(buf)
         self.engine.sync()

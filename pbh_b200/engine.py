@@ -41,6 +41,17 @@ def _ptr(t) -> int:
     return 0 if t is None else int(t.data_ptr())
 
 
+def engine_flags(graph: bool = True, full_every: int = 0, dynamic: bool = False, bucket_sort: bool = True,
+                 native_fft: bool = True, tight_bins: bool = False) -> int:
+    """The `flags` word of pm_engine_create: bits 8..15 the super-tile re-sort period (0: never;
+    bucket_sort=False: every step; periods above 255 become 255), bit 1 graph replay, bit 2
+    served (dynamic) mode, bit 3 the native transforms, bit 16 bins without spare capacity."""
+    every = int(full_every) if bucket_sort else 1
+    return ((max(0, min(every, 255)) & 0xFF) << 8) | (_lib.FLAG_GRAPH if graph else 0) | \
+        (_lib.FLAG_DYNAMIC if dynamic else 0) | (_lib.FLAG_NATIVE_FFT if native_fft else 0) | \
+        (_lib.FLAG_TIGHT_BINS if tight_bins else 0)
+
+
 class Engine:
     def __init__(self, peaks, device: int = 0, graph: bool = True, full_every: int = 0, dynamic: bool = False,
                  bucket_sort: bool = True, native_fft: bool = True, tight_bins: bool = False):
@@ -54,17 +65,14 @@ class Engine:
         self.device = int(device)
         # The push appends every particle to the bin of its new super-tile; every `full_every`
         # steps (0: never, the default) each super-tile is re-sorted by cell (bucket_sort=False:
-        # every step).  Results do
-        # not depend on the choice: the deposit is order-independent bit for bit.  tight_bins:
+        # every step).  Results do not depend on the choice: the deposit is order-independent bit
+        # for bit.  tight_bins:
         # bins without spare capacity, so that almost every step overflows and relayouts (a test
         # of that path; same results).
         # dynamic: served runs; no graph, and each step's FFTs cover only the slots in use.
         # native_fft: 64^3-512^3 meshes use the native transform with the Green multiply fused
         # (False: cuFFT and the separate Green kernel, as for every other mesh size).
-        every = int(full_every) if bucket_sort else 1
-        flags = ((max(1, min(every, 255)) & 0xFF) << 8) | (_lib.FLAG_GRAPH if graph else 0) | \
-                (_lib.FLAG_DYNAMIC if dynamic else 0) | (_lib.FLAG_NATIVE_FFT if native_fft else 0) | \
-                (_lib.FLAG_TIGHT_BINS if tight_bins else 0)
+        flags = engine_flags(graph, full_every, dynamic, bucket_sort, native_fft, tight_bins)
         self.npeaks = len(self.cfgs)
         torch.cuda.set_device(self.device)
         check(lib.pm_engine_create(arr, len(self.cfgs), self.device, flags, C.byref(h)), "pm_engine_create")

@@ -95,6 +95,22 @@ def test_served_slot_pool_fits_the_budget():
     assert pool <= 150e9
 
 
+def test_engine_flags():
+    """The engine flags word: no super-tile re-sort by default, a period when asked for, every
+    step without bucketed regrouping; the feature bits."""
+    from pbh_b200 import _lib
+    from pbh_b200.engine import engine_flags
+    period = lambda f: (f >> 8) & 0xFF
+    assert period(engine_flags()) == 0
+    assert period(engine_flags(full_every=16)) == 16
+    assert period(engine_flags(full_every=1000)) == 255
+    assert period(engine_flags(full_every=16, bucket_sort=False)) == 1
+    f = engine_flags(graph=False, dynamic=True, native_fft=False, tight_bins=True)
+    assert not f & _lib.FLAG_GRAPH and f & _lib.FLAG_DYNAMIC and not f & _lib.FLAG_NATIVE_FFT
+    assert f & _lib.FLAG_TIGHT_BINS
+    assert engine_flags() & _lib.FLAG_GRAPH and engine_flags() & _lib.FLAG_NATIVE_FFT
+
+
 def test_launch_accounting():
     import bench
     assert bench.launches_per_step([32], "native") == 10              # cuFFT size only
