@@ -1,5 +1,6 @@
-// Step kernels of the pm3d engine: push (CIC gather + kicks + drift, re-binning class),
-// clock advance, regrouping (re-binning scatter, or radix-sort permutation), halo-exchange CIC
+// Step kernels of the pm3d engine: push (CIC gather + kicks + drift, each particle written into
+// the bin of its new super-tile), clock advance, regrouping (bin layouts and relayouts, the
+// priming radix-sort permutation, the optional per-super-tile re-sort), halo-exchange CIC
 // deposit with its face fix-up, Green's function + gradient, and particle I/O.
 #include <algorithm>
 #include <type_traits>
