@@ -233,6 +233,35 @@ def test_overflowing_bins_relayout_without_changing_results(N, Np, tile, pscale,
         assert np.array_equal(a, b)
 
 
+def test_converging_flow_piles_particles_into_few_super_tiles():
+    """Momenta pointing at the box centre move most particles into the few central super-tiles
+    within five steps: their bins grow ten times over and more (relayouts with large
+    capacities).  Positions after each step against the float64 oracle, exact mass,
+    and the pile-up itself."""
+    N, Np = 32, 32
+    mesh = O.Mesh(N, 1.0, Np)
+    rng = np.random.default_rng(41)
+    x = rng.uniform(0.0, 1.0, size=(Np ** 3, 3))
+    p = -(x - 0.5) * 26.0                                 # about a fifth of the way in per step
+    eng = engine([dict(N=N, Np=Np, L=1.0, tile=8)])        # 4 super-tiles per axis, 512 particles each
+    eng.set_particles(0, x, p, 1.0)
+    x0, p0 = [t.cpu().numpy() for t in eng.particles(0)]
+    tr = O.Trajectory(mesh, x0, p0)
+    a = 1.0
+    for _ in range(5):
+        eng.step_explicit(0, a, 0.05)
+        a, delta = tr.step(a, 0.05)
+        xg = eng.particles(0)[0].cpu().numpy()
+        assert np.max(np.abs(wrap(xg - tr.x, 1.0))) / mesh.dx < TOL_POS_CELLS
+    s = eng.stats(0)
+    assert s.mass_defect == 0.0 and s.status == 0
+    assert s.relayouts >= 1
+    tiles = np.floor(((xg / mesh.dx - 0.5) % N) / 8).astype(int)
+    counts = np.bincount((tiles[:, 0] * 4 + tiles[:, 1]) * 4 + tiles[:, 2], minlength=64)
+    assert counts.max() >= 8 * Np ** 3 // 64               # the central bins hold many times their share
+    assert rel(eng.delta(0).cpu().numpy(), O.density_contrast(mesh, xg)) < TOL_DENSITY
+
+
 def test_fast_particles_cross_several_super_tiles():
     """Particles that move more than two super-tiles in one step land in their new bins."""
     N, Np = 64, 16
