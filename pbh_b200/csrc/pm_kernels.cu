@@ -584,9 +584,10 @@ __global__ void k_permute(StepArgs A, long long ntot) {
 // arrivals even when its count stays put), so that collapsing and infalling regions do not
 // relayout every step.
 //   Partial relayout (clock.relayout = 1): when the free space after the last bin of the peak's
-// region holds every overflowed bin with its base capacity and wanted room, only those bins
-// move there (to the buffer the push filled, which stays current); the others keep their place
-// and their two runs.  Their old places stay unused until the next full relayout.
+// region holds, with their base capacity and wanted room, every overflowed bin and every bin
+// whose remaining room is below another step of its arrivals, only those bins move there (in
+// the buffer the push filled, which stays current); the others keep their place and their two
+// runs.  The old places stay unused until the next full relayout.
 //   Full relayout (clock.relayout = 2): every bin is laid out again from the start of the
 // region, the wanted room shared out of the region's spare beyond the base capacities in
 // proportion to the wants, and every particle is copied into the other buffer, which becomes
@@ -630,7 +631,16 @@ __global__ void __launch_bounds__(LAYOUT_THREADS) k_layout(StepArgs A) {
     cap = (cnt + (P.bin_shift < 32 ? cnt >> P.bin_shift : 0u) + (u32)P.bin_min + BIN_ALIGN - 1) & ~(u32)(BIN_ALIGN - 1);
     if (P.bin_grow > 0 && need > cap - cnt) want = need - (cap - cnt);
   };
-  // Capacity of an overflowed bin moved by a partial relayout: base capacity plus its want.
+  // Whether a partial relayout moves bin i (new count cnt): it overflowed, or (with spare capacity
+  // in use) its remaining room is below another step of its arrivals, so that its neighbours'
+  // overflows do not relayout the peak again in the next steps.
+  auto moves = [&](int i, u32 cnt) -> bool {
+    if (ovf_in[i]) return true;
+    if (P.bin_grow == 0) return false;
+    const u32 room = old[i].cap > cnt ? old[i].cap - cnt : 0u;
+    return (unsigned long long)room < (unsigned long long)pushed[i].moved * BIN_ARRIVALS;
+  };
+  // Capacity of a bin moved by a partial relayout: base capacity plus its want.
   auto moved_cap = [&](u32 cap, u32 want) -> u32 {
     return (u32)min((unsigned long long)cap + want + BIN_ALIGN - 1, (unsigned long long)P.r_size) &
            ~(u32)(BIN_ALIGN - 1);
@@ -646,7 +656,7 @@ __global__ void __launch_bounds__(LAYOUT_THREADS) k_layout(StepArgs A) {
       bin(i, cnt, cap, want);
       sc += cap;
       sg += want;
-      if (ovf_in[i]) sp += moved_cap(cap, want);
+      if (moves(i, cnt)) sp += moved_cap(cap, want);
       const unsigned long long e = (unsigned long long)old[i].base + old[i].cap - (unsigned long long)P.r_off;
       mt = e > mt ? e : mt;
     }
@@ -688,7 +698,7 @@ __global__ void __launch_bounds__(LAYOUT_THREADS) k_layout(StepArgs A) {
       u32 want;
       bin(i, cnt, cap, want);
       if (partial) {
-        cap = ovf_in[i] ? moved_cap(cap, want) : 0u;  // only the overflowed bins take new space
+        cap = moves(i, cnt) ? moved_cap(cap, want) : 0u;  // only the moved bins take new space
       } else if (want && want_tot) {  // the wanted extra, or its share of the spare
         const unsigned long long share = (unsigned long long)want * spare / want_tot;
         cap += (u32)(min(share, (unsigned long long)want) & ~(unsigned long long)(BIN_ALIGN - 1));
@@ -742,8 +752,8 @@ __global__ void __launch_bounds__(LAYOUT_THREADS) k_layout(StepArgs A) {
 
 // Relayout, per super-tile.  Full (clock.relayout = 2): every bin the push filled (old layout,
 // other buffer) is copied in order to the start of its new bin in the current buffer.  Partial
-// (1): only the bins with arrivals in the overflow area move, inside the current buffer, to
-// their new place after the last bin.  Either way the bin's fill is then set to its new count,
+// (1): only the bins that got a new place after the last bin move there, inside the current
+// buffer.  Either way the bin's fill is then set to its new count,
 // which includes the arrivals k_relayout_ovf places next.
 __global__ void __launch_bounds__(PM_THREADS) k_relayout_copy(StepArgs A) {
   if (*A.layout_gate == 0u) return;
@@ -756,9 +766,9 @@ __global__ void __launch_bounds__(PM_THREADS) k_relayout_copy(StepArgs A) {
   for (long long t = blockIdx.x; t < nst; t += gridDim.x) {
     const long long g = st0 + t;
     const u32 arrivals = A.ovf_in[g];
-    if (!full && arrivals == 0u) continue;  // partial relayout: this bin stays as it is (uniform)
-    const BinRuns R = bin_runs(blay(A, C.lgen ^ 1)[g], bfill(A, src)[g]);
-    const BinLayout L = blay(A, C.lgen)[g];
+    const BinLayout L0 = blay(A, C.lgen ^ 1)[g], L = blay(A, C.lgen)[g];
+    if (!full && L.base == L0.base) continue;  // partial relayout: this bin stays as it is (uniform)
+    const BinRuns R = bin_runs(L0, bfill(A, src)[g]);
     const int4* ip = bpos(A, src);
     const float4* im = bmom(A, src);
     int4* op = bpos(A, C.sbuf) + L.base;
