@@ -252,15 +252,29 @@ __device__ __forceinline__ void push_super(const StepArgs& A, const PeakDesc& P,
     // z0 = sz*T is a multiple of 4 and the grids are 256-byte aligned).
     const unsigned sbase = (unsigned)__cvta_generic_to_shared(s_f);
     const int z0 = X.sz * T, zl = (X.sz * T + T) & (N - 1);
-    for (int i = threadIdx.x; i < 3 * T1 * T1 * CH; i += PUSH_THREADS) {
-      const int row = i / CH, part = i - row * CH;
-      const int comp = row / (T1 * T1), r = row - comp * (T1 * T1);
-      const int lx = r / T1, ly = r - lx * T1;
-      const int gx = (X.sx * T + lx) & (N - 1), gy = (X.sy * T + ly) & (N - 1);
-      const float* src = P.force + comp * N3 + ((long long)gx * N + gy) * N;
-      const unsigned dst = sbase + 4u * (unsigned)(comp * CS + lx * PS + ly * RS + part * 4);
-      if (part < T / 4) cp_async16(dst, src + z0 + part * 4);
-      else cp_async4(dst, src + zl);
+    // Thread t copies piece t % CH of patch rows t / CH, t / CH + RSTEP, ... (the row number
+    // advanced incrementally: RSTEP rows are DX planes and DY rows further on).
+    constexpr int NTH = PUSH_THREADS - PUSH_THREADS % CH, RSTEP = NTH / CH, DX = RSTEP / T1, DY = RSTEP % T1;
+    if (threadIdx.x < NTH) {
+      const int part = threadIdx.x % CH, r0 = threadIdx.x / CH;
+      int comp = r0 / (T1 * T1), lx = (r0 / T1) % T1, ly = r0 % T1;
+      for (int row = r0; row < 3 * T1 * T1; row += RSTEP) {
+        const int gx = (X.sx * T + lx) & (N - 1), gy = (X.sy * T + ly) & (N - 1);
+        const float* src = P.force + comp * N3 + ((long long)gx * N + gy) * N;
+        const unsigned dst = sbase + 4u * (unsigned)(comp * CS + lx * PS + ly * RS + part * 4);
+        if (part < T / 4) cp_async16(dst, src + z0 + part * 4);
+        else cp_async4(dst, src + zl);
+        ly += DY;
+        if (ly >= T1) {
+          ly -= T1;
+          ++lx;
+        }
+        lx += DX;
+        while (lx >= T1) {
+          lx -= T1;
+          ++comp;
+        }
+      }
     }
     cp_async_wait_all();
   }
