@@ -212,7 +212,7 @@ def launches_per_step(sizes, fft: str) -> int:
 # DRAM bytes (read + write) per launch from single-kernel ncu captures of the plain 256^3 run
 # (the Green kernel's from the same run with cuFFT transforms), per particle (per mode for Green),
 # scaled to a launch by the particles (modes) it processes; deposit includes its face fix-up.
-NCU_TRAFFIC = {"push": 77.12, "deposit": 26.94, "green_per_mode": 25.89}
+NCU_TRAFFIC = {"push": 77.10, "deposit": 26.94, "green_per_mode": 25.89}
 
 
 def replica_throughput(t_local: float, n_local: int, steps: int, dist=None, device="cpu"):
