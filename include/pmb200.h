@@ -84,8 +84,8 @@ typedef struct {
                               * was re-laid out and all of its particles moved */
 } pm_stats_info;
 
-/* Create an engine holding npeaks independent peaks (a batched ensemble; npeaks = 1 is the
- * plain single run).  Allocates all device memory and cuFFT plans up front; no later call
+/* Create an engine holding npeaks independent peaks (1 <= npeaks <= 65535; a batched ensemble;
+ * npeaks = 1 is the plain single run).  Allocates all device memory and cuFFT plans up front; no later call
  * allocates.  flags: bits 8..15 = re-sort every super-tile's particles by cell every that many
  * steps (never if 0, the default: the push keeps them binned by super-tile, and the order inside
  * a bin was measured not to matter); bit 1 = replay the step as a CUDA

@@ -66,6 +66,7 @@ struct pm_engine {
   PeakClock* d_clocks = nullptr;
   PeakStats* d_stats = nullptr;
   long long* d_st_base = nullptr;
+  unsigned short* d_st_peak = nullptr;  // [super-tile] its peak
   long long* d_p_base = nullptr;
   long long* d_mode_base = nullptr;
   long long* d_green_base = nullptr;  // Green blocks of the peaks that k_green serves
@@ -117,6 +118,7 @@ struct pm_engine {
     A.stats = d_stats;
     A.sortseg = sort.seg;
     A.st_base = d_st_base;
+    A.st_peak = d_st_peak;
     A.p_base = d_p_base;
     A.mode_base = d_mode_base;
     A.green_base = d_green_base;
@@ -305,7 +307,7 @@ struct pm_engine {
       if (sn.done) cudaEventDestroy(sn.done);
     }
     cudaFree(sort_dbg);
-    void* bufs[] = {d_peaks, d_clocks, d_stats, d_st_base, d_p_base, d_mode_base, d_green_base, d_green_peak, epart,
+    void* bufs[] = {d_peaks, d_clocks, d_stats, d_st_base, d_st_peak, d_p_base, d_mode_base, d_green_base, d_green_peak, epart,
                     wpart, eslice, ecount, bpos[0], bpos[1], bmom[0], bmom[1], lpos, lmom, lay[0], lay[1],
                     fill[0], fill[1], ovf_n, ovf_in, keys[0], keys[1], vals[0], vals[1], sstart,
                     sort_gate, layout_gate, refresh_gate, face, halo};
@@ -557,6 +559,13 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
   if ((r = E->alloc(&E->halo, E->nhc))) return r;
   CU(cudaMemcpy(E->d_peaks, E->peaks.data(), sizeof(PeakDesc) * npeaks, cudaMemcpyHostToDevice));
   CU(cudaMemcpy(E->d_st_base, st_base.data(), sizeof(long long) * (npeaks + 1), cudaMemcpyHostToDevice));
+  {
+    std::vector<unsigned short> stp((size_t)E->nst);
+    for (int i = 0; i < npeaks; ++i)
+      for (long long t = st_base[i]; t < st_base[i + 1]; ++t) stp[(size_t)t] = (unsigned short)i;
+    if ((r = E->alloc(&E->d_st_peak, E->nst))) return r;
+    CU(cudaMemcpy(E->d_st_peak, stp.data(), sizeof(unsigned short) * E->nst, cudaMemcpyHostToDevice));
+  }
   CU(cudaMemcpy(E->d_p_base, p_base.data(), sizeof(long long) * (npeaks + 1), cudaMemcpyHostToDevice));
   CU(cudaMemcpy(E->d_mode_base, mode_base.data(), sizeof(long long) * (npeaks + 1), cudaMemcpyHostToDevice));
   std::vector<PeakClock> clocks(npeaks);
@@ -622,7 +631,7 @@ int engine_init(pm_engine* E, const pm_peak_cfg* cfg, int npeaks) {
 extern "C" {
 
 int pm_engine_create(const pm_peak_cfg* cfg, int npeaks, int device, int flags, pm_engine** out) {
-  if (!cfg || npeaks < 1 || !out) return -2000;
+  if (!cfg || npeaks < 1 || npeaks > 65535 || !out) return -2000;  // peaks indexed by 16 bits
   *out = nullptr;
   CU(cudaSetDevice(device));
   pm_engine* E = new (std::nothrow) pm_engine();

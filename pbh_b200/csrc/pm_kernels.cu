@@ -78,12 +78,9 @@ struct TileRef {
   long long t;
 };
 
-__device__ __forceinline__ TileRef find_tile(const long long* base, int npeaks) {
-  __shared__ int s_pk;
-  if (threadIdx.x == 0) s_pk = pm_find(base, npeaks, (long long)blockIdx.x);
-  __syncthreads();
+__device__ __forceinline__ TileRef find_tile(const long long* base, const unsigned short* st_peak) {
   TileRef r;
-  r.pk = s_pk;
+  r.pk = st_peak[blockIdx.x];  // the same for every thread of the CTA
   r.t = (long long)blockIdx.x - base[r.pk];
   return r;
 }
@@ -346,7 +343,7 @@ __global__ void __launch_bounds__(PUSH_THREADS, 2) k_push(StepArgs A) {
   extern __shared__ __align__(16) float s_f[];
   __shared__ PushCoef s_k;
   __shared__ u32 s_stay;
-  const TileRef tr = find_tile(A.st_base, A.npeaks);
+  const TileRef tr = find_tile(A.st_base, A.st_peak);
   const PeakClock C = A.clocks[tr.pk];
   if (C.state != PS_RUN && C.state != PS_FINALIZE) return;
   const PeakDesc P = A.peaks[tr.pk];
@@ -1299,7 +1296,7 @@ __device__ __forceinline__ void deposit_super(const StepArgs& A, const PeakDesc&
 
 __global__ void __launch_bounds__(DEP_THREADS, 4) k_deposit(StepArgs A, double* rho64) {
   extern __shared__ __align__(16) u32 s_dep[];
-  const TileRef tr = find_tile(A.st_base, A.npeaks);
+  const TileRef tr = find_tile(A.st_base, A.st_peak);
   const PeakClock C = A.clocks[tr.pk];
   if (!C.dep) return;
   const PeakDesc P = A.peaks[tr.pk];
@@ -1327,7 +1324,7 @@ __global__ void __launch_bounds__(FIX_THREADS) k_fixup(StepArgs A, double* rho64
   __shared__ long long s_red[FIX_THREADS / 32];
   __shared__ long long s_max[FIX_THREADS / 32];
   __shared__ const long long* s_nb[8];
-  const TileRef tr = find_tile(A.st_base, A.npeaks);
+  const TileRef tr = find_tile(A.st_base, A.st_peak);
   const PeakClock C = A.clocks[tr.pk];
   if (!C.dep) return;
   const PeakDesc P = A.peaks[tr.pk];

@@ -74,6 +74,7 @@ struct StepArgs {
   u32* layout_gate;            // 1 when any peak primes or relayouts this step (advance kernel)
   u32* refresh_gate;           // 1 when any peak re-sorts its super-tiles this step (advance kernel)
   const long long* st_base;    // [npeaks + 1] prefix of super-tiles
+  const unsigned short* st_peak;  // [super-tile] its peak (one load instead of a search)
   const long long* p_base;     // [npeaks + 1] prefix of particles
   const long long* mode_base;  // [npeaks + 1] prefix of Green blocks
   const long long* green_base; // [ngreen + 1] prefix of Green blocks over the peaks k_green serves
