@@ -15,10 +15,12 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import queue
 import statistics
 import subprocess
 import sys
 import tempfile
+import threading
 import time
 from pathlib import Path
 
@@ -118,50 +120,154 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------------------ CPU side
+CPU_BYTES_PER_PARTICLE = 400      # resident set of one float64 oracle peak (6.1 GB measured at 256^3)
+CPU_BYTES_PER_WORKER = 300 << 20   # interpreter, numpy and the oracle module
+
+
 def _cpu_worker(args):
-    """One peak of the recipe on the CPU oracle (float64 numpy restatement of pm3d):
-    IC, `warmup` untimed steps, then `steps` timed steps.  Returns (n, seconds)."""
-    N, R, delta0, seed, ratio, steps, warmup = args
+    """One peak of the recipe on the CPU oracle (float64 numpy restatement of pm3d): IC, the
+    initial forces and `warmup` steps untimed; then, once every worker is ready (`barrier`),
+    timed KDK steps until `budget` seconds have passed (at least `min_steps`).  Puts (index, N,
+    particles * steps, seconds) on `out`, or (index, N, 0, error text)."""
+    idx, N, R, delta0, seed, ratio, warmup, budget, min_steps, barrier, out = args
     os.environ.setdefault("OMP_NUM_THREADS", "1")
-    import warnings
-    warnings.filterwarnings("ignore")
-    from oracle import pm3d_oracle as O
-    from oracle.recipe_oracle import recipe_ic
-    mesh = O.Mesh(N, 1.0, N)
-    ic = recipe_ic(mesh, R, delta0, 0.01, seed)
-    tr = O.Trajectory(mesh, ic["x"], ic["p"])
-    a = 1.0
-    for _ in range(warmup):
-        a, _d = tr.step(a, a * ratio)
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        a, _d = tr.step(a, a * ratio)
-    return N ** 3, time.perf_counter() - t0
+    try:
+        import warnings
+        warnings.filterwarnings("ignore")
+        from oracle import pm3d_oracle as O
+        from oracle.recipe_oracle import recipe_ic
+        mesh = O.Mesh(N, 1.0, N)
+        ic = recipe_ic(mesh, R, delta0, 0.01, seed)
+        tr = O.Trajectory(mesh, ic["x"], ic["p"])
+        a = 1.0
+        tr.acc, _d = O.accelerations(mesh, tr.x, a)   # what the first step would compute twice
+        tr.acc_a = a
+        for _ in range(warmup):
+            a, _d = tr.step(a, a * ratio)
+        try:
+            barrier.wait(timeout=900)
+        except threading.BrokenBarrierError:   # a worker failed: time this one all the same
+            pass
+        t0 = time.perf_counter()
+        steps = 0
+        while steps < min_steps or time.perf_counter() - t0 < budget:
+            a, _d = tr.step(a, a * ratio)
+            steps += 1
+        out.put((idx, N, N ** 3 * steps, time.perf_counter() - t0))
+    except Exception as exc:  # reported by the parent; the other workers carry on
+        try:
+            barrier.abort()
+        except Exception:
+            pass
+        out.put((idx, N, 0, f"{type(exc).__name__}: {exc}"))
 
 
-def cpu_rate(specs, steps: int, warmup: int, max_mesh: int, workers: int | None = None) -> dict:
+def allocate_cpu_workers(particles_by_mesh: dict, cores: int, mem_bytes: float) -> dict:
+    """Workers per mesh size for the CPU sample of a mix: one per mesh size (largest meshes first
+    when there are fewer cores than sizes), the rest in proportion to each size's particles (its
+    share of the mix's work, so the cores are loaded roughly as a run of the whole mix would load
+    them), within `mem_bytes` of host memory.  A size whose one worker does not fit is left out."""
+    need = {N: CPU_BYTES_PER_PARTICLE * N ** 3 + CPU_BYTES_PER_WORKER for N in particles_by_mesh}
+    alloc, used = {}, 0.0
+    for N in sorted(particles_by_mesh, reverse=True):
+        if len(alloc) < cores and used + need[N] <= mem_bytes:
+            alloc[N] = 1
+            used += need[N]
+    total = sum(particles_by_mesh[N] for N in alloc)
+    while sum(alloc.values()) < cores and alloc:
+        # the size furthest below its share of the workers that still fits
+        cands = [N for N in alloc if used + need[N] <= mem_bytes]
+        if not cands:
+            break
+        N = max(cands, key=lambda m: particles_by_mesh[m] / total * cores - alloc[m])
+        alloc[N] += 1
+        used += need[N]
+    return alloc
+
+
+def mix_rate(particles_by_mesh: dict, rate_by_mesh: dict, cores: int) -> float:
+    """Particle-steps/s of a whole mix of peaks on `cores` cores, each core running one peak at a
+    time and none idle: one step of every peak costs sum_N P_N / r_N core-seconds (P_N the mix's
+    particles on N^3 meshes, r_N one core's particle-steps/s on such a peak)."""
+    return cores * sum(particles_by_mesh.values()) / sum(p / rate_by_mesh[N] for N, p in particles_by_mesh.items())
+
+
+def cpu_rate(specs, budget: float, warmup: int, workers: int | None = None) -> dict:
     """The oracle port of the reference path on the host cores, one peak per worker process
-    (spawned), the reference's own pattern for many runs (pbhgr/pbhgr/scan.py:223-232)."""
+    (spawned), the reference's own pattern for many runs (pbhgr/pbhgr/scan.py:223-232).  Every
+    mesh size of the workload is sampled, all workers step at once over the same timed window,
+    and the whole mix's rate follows from the per-size rates (`mix_rate`)."""
     import multiprocessing as mp
+    import platform
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
     workers = workers or cores
-    sample = [s for s in specs if s.N <= max_mesh] or specs
-    tasks = [(s.N, tuple(s.R), s.delta0, s.seed, s.ratio(), steps, warmup) for s in
-             (sample * (workers // len(sample) + 1))[:workers]]
+    pmesh = {}
+    for s in specs:
+        pmesh[s.N] = pmesh.get(s.N, 0) + s.n
+    try:
+        import psutil
+        mem = 0.6 * psutil.virtual_memory().available
+    except Exception:
+        mem = 0.6 * os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_AVPHYS_PAGES")
+    alloc = allocate_cpu_workers(pmesh, workers, mem)
+    by_mesh = {}
+    for s in specs:
+        by_mesh.setdefault(s.N, []).append(s)
+    picks = [by_mesh[N][i % len(by_mesh[N])] for N in sorted(alloc) for i in range(alloc[N])]
     ctx = mp.get_context("spawn")
+    barrier, out = ctx.Barrier(len(picks)), ctx.Queue()
+    procs = []
+    for i, s in enumerate(picks):
+        w = min(warmup, 1) if s.N <= 128 else 0   # numpy needs no warm-up beyond the initial forces
+        task = (i, s.N, tuple(s.R), s.delta0, s.seed, s.ratio(), w, budget, 1, barrier, out)
+        procs.append(ctx.Process(target=_cpu_worker, args=(task,), daemon=True))
     t0 = time.perf_counter()
-    with ctx.Pool(len(tasks)) as pool:
-        res = pool.map(_cpu_worker, tasks)
+    for p in procs:
+        p.start()
+    res, errors = [], []
+    pending = set(range(len(procs)))
+    while pending and time.perf_counter() - t0 < 1800:
+        try:
+            idx, N, ps, t = out.get(timeout=1.0)
+        except queue.Empty:
+            for i in sorted(pending):
+                if procs[i].exitcode not in (None, 0):   # ended without reporting (killed)
+                    pending.discard(i)
+                    errors.append(f"{picks[i].N}^3: worker exit code {procs[i].exitcode}")
+                    barrier.abort()
+            continue
+        pending.discard(idx)
+        if ps:
+            res.append((N, ps, t))
+        else:
+            errors.append(f"{N}^3: {t}")
+    errors += [f"{picks[i].N}^3: no report" for i in sorted(pending)]
+    for p in procs:
+        p.join(timeout=30)
+        if p.is_alive():
+            p.terminate()
     wall = time.perf_counter() - t0
-    ps = sum(n * steps for n, _ in res)
-    tmax = max(t for _, t in res)
-    import platform
-    return {"value": ps / tmax, "unit": UNIT, "cores": len(tasks), "kind": "port",
-            "sample": f"{len(tasks)} peaks of the workload (one per core) with meshes "
-                      f"{sorted({t[0] for t in tasks})}^3, {steps} timed KDK steps each after {warmup} untimed, "
-                      f"float64 numpy restatement of pm3d; meshes above {max_mesh}^3 are left out of the sample "
-                      f"(one float64 step of a 256^3 peak takes ~12 s on one core), and the per-core rate falls "
-                      f"slowly with mesh size, so the sample's rate is, if anything, above the full mix's",
+    rates = {}
+    for N, ps, t in res:
+        rates.setdefault(N, []).append(ps / t)
+    rate_by_mesh = {N: statistics.mean(v) for N, v in rates.items()}
+    if not rate_by_mesh:
+        raise RuntimeError("CPU sample failed: " + "; ".join(errors))
+    # A mesh size without a measurement (it did not fit the host's memory) takes the rate of
+    # the nearest measured size.
+    full = {N: rate_by_mesh.get(N) or rate_by_mesh[min(rate_by_mesh, key=lambda m: abs(m - N))] for N in pmesh}
+    value = mix_rate(pmesh, full, len(res))
+    missing = sorted(set(pmesh) - set(rate_by_mesh))
+    return {"value": value, "unit": UNIT, "cores": len(res), "kind": "port",
+            "sample": f"{len(res)} peaks of the workload at once (one per core: "
+                      + ", ".join(f"{alloc[N]} of {N}^3" for N in sorted(alloc))
+                      + f"), float64 numpy restatement of pm3d, timed KDK steps over a common window of "
+                      f"at least {budget:g} s after the IC and initial forces; the value is the whole "
+                      f"{len(specs)}-peak mix on {len(res)} cores with no core idle, from the per-size "
+                      f"per-core rates"
+                      + (f"; meshes {missing}^3 took the nearest measured size's rate (host memory)" if missing else ""),
+            "per_core_rate_by_mesh": {str(N): rate_by_mesh[N] for N in sorted(rate_by_mesh)},
+            "errors": errors or None,
             "host_cpus": cores, "cpu": platform.processor() or platform.machine(), "wall_s": wall}
 
 
@@ -170,13 +276,12 @@ def run_reference(args):
     if rank != 0:
         return
     specs, desc = workload_specs(args.workload, args.npeaks, args.seed, 0)
-    max_mesh = 128 if args.workload == "batched" else 64
-    cb = cpu_rate(specs, args.steps, args.warmup, max_mesh)
+    cb = cpu_rate(specs, budget=30.0, warmup=args.warmup)
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (recipe peaks, seeded numpy noise)",
             "config": workload_config(desc, specs, args.gpus),
-            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample", "per_core_rate_by_mesh")},
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -451,8 +556,8 @@ def run_ours(args):
     if rank == 0 and not args.no_serve:
         line["served"] = served_stream(args, local, tiles)
     if rank == 0 and world == 1 and not args.no_cpu:
-        cb = cpu_rate(specs, steps=4, warmup=1, max_mesh=128 if args.workload == "batched" else 64)
-        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        cb = cpu_rate(specs, budget=10.0, warmup=1)
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample", "per_core_rate_by_mesh")}
     if dist:
         dist.barrier()
         dist.destroy_process_group()

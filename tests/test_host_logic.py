@@ -134,6 +134,33 @@ def test_algorithmic_bytes_per_phase():
     assert bench.algorithmic_bytes("r2c", n, cells, modes, 3) == 0.0
 
 
+def test_cpu_sample_covers_every_mesh_size_of_the_mix():
+    """The CPU baseline samples every mesh size of the workload, loads the cores roughly in
+    proportion to each size's particles, stays inside the host memory it is given, and turns
+    per-size per-core rates into the rate of the whole mix."""
+    import bench
+    specs, _ = bench.workload_specs("batched", 64, 1234, 0)
+    pm = {}
+    for s in specs:
+        pm[s.N] = pm.get(s.N, 0) + s.n
+    assert sorted(pm) == [32, 64, 128, 256]
+    alloc = bench.allocate_cpu_workers(pm, 16, 1e12)
+    assert sorted(alloc) == [32, 64, 128, 256] and sum(alloc.values()) == 16
+    assert alloc[256] == max(alloc.values())                     # most of the mix's particles
+    need = lambda a: sum(k * (bench.CPU_BYTES_PER_PARTICLE * N ** 3 + bench.CPU_BYTES_PER_WORKER)
+                         for N, k in a.items())
+    tight = bench.allocate_cpu_workers(pm, 16, 20e9)
+    assert need(tight) <= 20e9 and tight[256] >= 1 and sum(tight.values()) <= 16
+    assert bench.allocate_cpu_workers(pm, 2, 1e12) == {256: 1, 128: 1}   # fewer cores than sizes
+    assert 256 not in bench.allocate_cpu_workers(pm, 16, 5e9)    # one 256^3 peak does not fit
+    # Equal per-core rates: the mix runs at cores x that rate; a slower size weighs by its particles.
+    assert bench.mix_rate(pm, {N: 1e6 for N in pm}, 16) == pytest.approx(16e6)
+    r = {32: 2e6, 64: 2e6, 128: 2e6, 256: 1e6}
+    p_tot = sum(pm.values())
+    expect = 16 * p_tot / (pm[256] / 1e6 + (p_tot - pm[256]) / 2e6)
+    assert bench.mix_rate(pm, r, 16) == pytest.approx(expect)
+
+
 def test_return_code_mapping():
     from pbh_b200 import _lib
     assert _lib.check(0, "x") == 0 and _lib.check(3, "x") == 3        # >0: flagged items
