@@ -256,10 +256,10 @@ int pm_irfft3_256(const void* spec, void* work, float* x, int nfields, void* str
  * same input and outputs but keeps all of its scratch in one static device array of
  * PM_NOALLOC_SCRATCH_BYTES inside this library, which every GPU that loads the library holds
  * until the process exits; it calls no allocating routine.  n must not exceed
- * PM_NOALLOC_MAX_KEYS (larger n returns -2003 and touches nothing).  The first call on a device
- * looks up the array's device address for that device (cudaGetSymbolAddress, with that device
- * current) and keeps it for the life of the process, so make that first call before any stream
- * capture, and do not reset the device (cudaDeviceReset) after it.  Every call shares the
+ * PM_NOALLOC_MAX_KEYS (larger n returns -2003 and touches nothing).  Each call looks up the
+ * array's device address on the current device (cudaGetSymbolAddress, which allocates nothing);
+ * the first call on a device also loads this library's kernels there, so make that first call
+ * before any stream capture.  Every call shares the
  * array: calls that overlap on the GPU (from several streams or threads) race, and must be
  * serialized by the caller.  Runs on `stream` (a cudaStream_t, NULL for the default stream);
  * each call copies the sort's error word back to the host and waits for `stream` before it

@@ -3,8 +3,6 @@
 // the ping-pong key/value buffers, digit histograms, look-back words, tile tables and the
 // error word -- lives in one file-scope static device array of PM_NOALLOC_SCRATCH_BYTES
 // (about 3.3 MB), which every GPU that loads this library holds until the process exits.
-#include <mutex>
-
 #include "../../include/pmb200.h"
 #include "sort.cuh"
 
@@ -31,21 +29,15 @@ static_assert(kBytes <= PM_NOALLOC_SCRATCH_BYTES, "scratch layout exceeds the de
 
 static __device__ __align__(256) unsigned char g_sort_scratch[PM_NOALLOC_SCRATCH_BYTES];
 
-// Per-device address of g_sort_scratch, looked up once per device with that device current.
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-unsigned char* g_dev_ptr[kMaxDevices] = {};
-
-int scratch_address(int device, unsigned char** out) {
-  if (device < 0 || device >= kMaxDevices) return -2004;
-  std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_dev_ptr[device]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_sort_scratch);
-    if (e != cudaSuccess) return -(int)e;
-    g_dev_ptr[device] = (unsigned char*)p;
-  }
-  *out = g_dev_ptr[device];
+// Device address of g_sort_scratch on the current device.  In host code the array's name
+// stands for a host-side shadow, not device memory, so the kernels get this address instead.
+// Looked up on every call (it allocates nothing): a cached address would go stale if the
+// device were reset and the module loaded again.
+int scratch_address(unsigned char** out) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_sort_scratch);
+  if (e != cudaSuccess) return -(int)e;
+  *out = (unsigned char*)p;
   return 0;
 }
 
@@ -79,12 +71,10 @@ extern "C" int pm_sort_u64_noalloc(const unsigned long long* keys, unsigned long
   if (lo < 0 || hi > 64 || hi <= lo) return -2001;
   if (n > kMaxKeys) return -2003;  // beyond the static scratch: PM_NOALLOC_MAX_KEYS
   if (n == 0) return 0;
-  int device = 0;
-  cudaError_t ce = cudaGetDevice(&device);
-  if (ce != cudaSuccess) return -(int)ce;
   unsigned char* base = nullptr;
-  int r = scratch_address(device, &base);
+  int r = scratch_address(&base);
   if (r) return r;
+  cudaError_t ce = cudaSuccess;
   cudaStream_t s = (cudaStream_t)stream;
   const int ntiles = (int)((n + SORT_TILE - 1) / SORT_TILE);
   const int npass = (hi - lo + 7) / 8;
