@@ -185,6 +185,26 @@ def allocate_cpu_workers(particles_by_mesh: dict, cores: int, mem_bytes: float) 
     return alloc
 
 
+def host_memory_available() -> float:
+    """Bytes this process can still use: the host's available memory, or less when a control
+    group limits the container (its limit minus its current use)."""
+    try:
+        import psutil
+        avail = float(psutil.virtual_memory().available)
+    except Exception:
+        avail = float(os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_AVPHYS_PAGES"))
+    for lim, cur in (("/sys/fs/cgroup/memory.max", "/sys/fs/cgroup/memory.current"),
+                     ("/sys/fs/cgroup/memory/memory.limit_in_bytes", "/sys/fs/cgroup/memory/memory.usage_in_bytes")):
+        try:
+            text = Path(lim).read_text().strip()
+            if text != "max":
+                avail = min(avail, float(text) - float(Path(cur).read_text().strip()))
+            break
+        except (OSError, ValueError):
+            continue
+    return max(avail, 0.0)
+
+
 def mix_rate(particles_by_mesh: dict, rate_by_mesh: dict, cores: int) -> float:
     """Particle-steps/s of a whole mix of peaks on `cores` cores, each core running one peak at a
     time and none idle: one step of every peak costs sum_N P_N / r_N core-seconds (P_N the mix's
@@ -204,12 +224,7 @@ def cpu_rate(specs, budget: float, warmup: int, workers: int | None = None) -> d
     pmesh = {}
     for s in specs:
         pmesh[s.N] = pmesh.get(s.N, 0) + s.n
-    try:
-        import psutil
-        mem = 0.6 * psutil.virtual_memory().available
-    except Exception:
-        mem = 0.6 * os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_AVPHYS_PAGES")
-    alloc = allocate_cpu_workers(pmesh, workers, mem)
+    alloc = allocate_cpu_workers(pmesh, workers, 0.6 * host_memory_available())
     by_mesh = {}
     for s in specs:
         by_mesh.setdefault(s.N, []).append(s)
