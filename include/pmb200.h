@@ -145,7 +145,7 @@ int pm_set_collapse_threshold(pm_engine* e, int peak, double delta_collapse, int
 int pm_release(pm_engine* e, int peak);
 
 /* Entry points of a request loop that never waits on the device between steps (the served form
- * of north_star; no counterpart in pm3d.py, whose driver runs one peak at a time,
+ * with continuous batching; no counterpart in pm3d.py, whose driver runs one peak at a time,
  * pbhgr/scripts/pm3d_peak.py:24-33).  Each is ordered on the engine's stream and returns without
  * waiting.
  *
