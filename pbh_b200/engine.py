@@ -174,6 +174,8 @@ def interp64(F, X, L: float):
     Ft = torch.as_tensor(np.asarray(F, dtype=np.float64)).cuda().contiguous()
     Xt = torch.as_tensor(np.asarray(X, dtype=np.float64)).cuda().contiguous()
     out = torch.empty(Xt.shape[0], dtype=torch.float64, device="cuda")
+    if Xt.shape[0] == 0:        # no positions: an empty gather, as the reference's indexing gives
+        return out
     torch.cuda.synchronize()
     check(lib.pm_interp64(_ptr(Ft), _ptr(Xt), Xt.shape[0], Ft.shape[0], float(L), _ptr(out)), "pm_interp64")
     return out
@@ -185,6 +187,8 @@ def deposit64(X, N: int, L: float):
     torch = _lib.require_cuda()
     lib = _lib.load()
     Xt = torch.as_tensor(np.asarray(X, dtype=np.float64).reshape(-1, 3)).cuda().contiguous()
+    if Xt.shape[0] == 0:        # no particles: zero counts, as the reference's bincount gives
+        return torch.zeros((N, N, N), dtype=torch.float64, device="cuda")
     work = torch.empty(N ** 3, dtype=torch.int64, device="cuda")
     out = torch.empty((N, N, N), dtype=torch.float64, device="cuda")
     torch.cuda.synchronize()

@@ -104,6 +104,11 @@ def test_recipe_peak_and_deposit_interp(golden):
     perm = np.random.default_rng(1).permutation(len(gm["X"]))
     assert np.array_equal(pm8.deposit(gm["X"][perm]), rho)
     assert rel(pm8.interp(gm["F"], gm["X"]), gm["Fi"]) < 1e-14
+    # no particles: zero counts and an empty gather, as the reference's bincount and indexing give
+    empty = np.empty((0, 3))
+    rho0 = pm8.deposit(empty)
+    assert rho0.shape == (8, 8, 8) and not rho0.any()
+    assert pm8.interp(gm["F"], empty).shape == (0,)
 
 
 def test_run_loop_matches_explicit_steps():
