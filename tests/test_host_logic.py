@@ -161,6 +161,25 @@ def test_cpu_sample_covers_every_mesh_size_of_the_mix():
     assert bench.mix_rate(pm, r, 16) == pytest.approx(expect)
 
 
+def test_cpu_sample_runs_and_survives_a_failing_worker():
+    """The CPU sample end to end on small meshes (spawned workers, a common timed window), and a
+    worker that fails before the window (a negative seed, which numpy's generator rejects): it is
+    reported, and the others are still timed and give the mix's rate."""
+    import dataclasses
+
+    import bench
+    from pbh_b200 import recipe
+    specs = recipe.ensemble(npeaks=6, sizes=(8, 16), steps=100, seed=5)
+    cb = bench.cpu_rate(specs, budget=0.3, warmup=1, workers=3)
+    assert cb["cores"] == 3 and cb["errors"] is None and cb["value"] > 0
+    assert sorted(cb["per_core_rate_by_mesh"]) == sorted(str(N) for N in {s.N for s in specs})
+    bad = [dataclasses.replace(s, seed=-1) if s.N == 16 else s for s in specs]
+    cb = bench.cpu_rate(bad, budget=0.3, warmup=1, workers=3)
+    assert cb["errors"] and all("16^3" in e for e in cb["errors"])
+    assert cb["cores"] == 3 - len(cb["errors"]) and cb["value"] > 0
+    assert list(cb["per_core_rate_by_mesh"]) == ["8"]        # 16^3 takes the measured size's rate
+
+
 def test_return_code_mapping():
     from pbh_b200 import _lib
     assert _lib.check(0, "x") == 0 and _lib.check(3, "x") == 3        # >0: flagged items
