@@ -75,3 +75,54 @@ def test_native_fft_rejects_other_sizes_before_touching_the_device():
     assert lib.pm_rfft3_native(32, 16, 16, 1, None) == -2000
     assert lib.pm_irfft3_native(1024, 16, 16, 16, 1, None) == -2000
     assert lib.pm_rfft3_native(300, 16, 16, 1, None) == -2000
+
+
+def test_ctypes_structures_match_the_header_layout(tmp_path):
+    """Every structure the bindings pass through the C ABI has the header's size and field
+    offsets (a mismatch would silently corrupt the engine's configuration or results)."""
+    import ctypes as C
+    import shutil
+    import subprocess
+
+    import pytest
+    from pbh_b200 import _lib
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    structs = {"pm_peak_cfg": _lib.PeakCfg, "pm_clock_info": _lib.ClockInfo, "pm_stats_info": _lib.StatsInfo,
+               "pm_ic_params": _lib.ICParams}
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "pmb200.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'  printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c11", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    got = {}
+    for row in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines():
+        cname, key, val = row.split()
+        got[(cname, key)] = int(val)
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
+
+
+def test_bindings_pass_as_many_arguments_as_the_header_declares():
+    """The ctypes signatures of every entry point have the header prototype's parameter count and
+    a return type of the same width."""
+    import ctypes as C
+
+    from pbh_b200 import _lib
+    text = re.sub(r"/\*.*?\*/", "", (ROOT / "include" / "pmb200.h").read_text(), flags=re.S)
+    protos = re.findall(r"^\s*(int|long long|void\*)\s+(pm_\w+)\s*\(([^)]*)\)\s*;", text, re.M | re.S)
+    assert sorted(name for _, name, _ in protos) == header_symbols()
+    width = {"int": C.sizeof(C.c_int), "long long": C.sizeof(C.c_longlong), "void*": C.sizeof(C.c_void_p)}
+    for ret, name, args in protos:
+        restype, argtypes = _lib._SIGS[name]
+        nargs = 0 if args.strip() in ("", "void") else len(args.split(","))
+        assert len(argtypes) == nargs, name
+        assert C.sizeof(restype) == width[ret], name
