@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--no-serve", action="store_true", help="skip the served-stream latency run")
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="arrival window of the served stream")
     ap.add_argument("--serve-rate", type=float, default=20.0, help="mean request arrivals per second")
+    ap.add_argument("--cpu-seconds", type=float, default=None,
+                    help="timed window of the CPU sample (default 30 s for --impl reference, 10 s for cpu_baseline)")
     ap.add_argument("--tiles", default="auto", help="super-tile side: 'auto' (autotuned per mesh size) or 4/8/16")
     ap.add_argument("--fft", choices=["cufft", "native"], default="native",
                     help="64^3-512^3 transforms: cuFFT, or the native kernels with the Green multiply fused")
@@ -291,7 +293,7 @@ def run_reference(args):
     if rank != 0:
         return
     specs, desc = workload_specs(args.workload, args.npeaks, args.seed, 0)
-    cb = cpu_rate(specs, budget=30.0, warmup=args.warmup)
+    cb = cpu_rate(specs, budget=30.0 if args.cpu_seconds is None else args.cpu_seconds, warmup=args.warmup)
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (recipe peaks, seeded numpy noise)",
@@ -571,7 +573,7 @@ def run_ours(args):
     if rank == 0 and not args.no_serve:
         line["served"] = served_stream(args, local, tiles)
     if rank == 0 and world == 1 and not args.no_cpu:
-        cb = cpu_rate(specs, budget=10.0, warmup=1)
+        cb = cpu_rate(specs, budget=10.0 if args.cpu_seconds is None else args.cpu_seconds, warmup=1)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample", "per_core_rate_by_mesh")}
     if dist:
         dist.barrier()

@@ -1,6 +1,6 @@
 """Host-side logic that needs no GPU: the benchmark recipes, the served stream's arrivals,
-latency summary and slot budget, the benchmark's launch and byte accounting, and the error
-mapping of the C ABI's return codes."""
+latency summary and slot budget, the benchmark's launch and byte accounting, its CPU sample and
+reference-arm line, and the error mapping of the C ABI's return codes."""
 import sys
 from pathlib import Path
 
@@ -248,3 +248,30 @@ def test_state_arrays_track_writes_like_the_references_plain_arrays():
     c = a.copy()                                     # a copy is a snapshot, not the state
     c[0] = 9.0
     assert not owner._host_dirty and a[0, 0] == 0.0
+
+
+def test_reference_arm_prints_one_contract_line(monkeypatch, capsys):
+    """`bench.py --impl reference` prints one JSON line with the contract's keys, the workload's
+    own config and a cpu_baseline describing the sample (small meshes stand in for the mix)."""
+    import argparse
+    import json
+
+    import bench
+    from pbh_b200 import recipe
+    small = recipe.ensemble(npeaks=4, sizes=(8, 16), steps=100, seed=3)
+    monkeypatch.setattr(bench, "workload_specs", lambda name, npeaks, seed, rank: (small, {"workload": "small mix"}))
+    monkeypatch.delenv("RANK", raising=False)
+    args = argparse.Namespace(workload="batched", npeaks=4, seed=1, gpus=1, steps=20, warmup=5, cpu_seconds=0.2)
+    bench.run_reference(args)
+    lines = [ln for ln in capsys.readouterr().out.splitlines() if ln.strip()]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["metric"] == bench.METRIC and d["unit"] == bench.UNIT
+    assert d["higher_is_better"] is True and d["value"] > 0 and (d["steps"], d["warmup"]) == (20, 5)
+    assert d["config"]["workload"] == "small mix" and d["config"]["peaks"] == 4
+    cb = d["cpu_baseline"]
+    assert cb["value"] == d["value"] and cb["kind"] == "port" and cb["cores"] >= 1 and cb["sample"]
+    assert d["e2e"] == {"value": d["value"], "unit": bench.UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    monkeypatch.setenv("RANK", "1")                      # other ranks of a multi-GPU launch print nothing
+    bench.run_reference(args)
+    assert capsys.readouterr().out.strip() == ""
