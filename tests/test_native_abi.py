@@ -126,3 +126,27 @@ def test_bindings_pass_as_many_arguments_as_the_header_declares():
         nargs = 0 if args.strip() in ("", "void") else len(args.split(","))
         assert len(argtypes) == nargs, name
         assert C.sizeof(restype) == width[ret], name
+
+
+def test_no_kernel_spills_registers(tmp_path):
+    """Every kernel compiles for sm_100a without register spills (the push and the deposit run
+    at the register limit of their launch bounds, where a spill would add local-memory traffic
+    to an HBM-bound loop).  Compiles each source to an object in a scratch folder."""
+    import shutil
+    import subprocess
+
+    import pytest
+    from pbh_b200 import build
+    try:
+        nvcc = build.nvcc()
+    except RuntimeError:
+        pytest.skip("nvcc not found")
+    if not shutil.which(nvcc) and not Path(nvcc).exists():
+        pytest.skip("nvcc not found")
+    for src in build.sources():
+        res = subprocess.run([nvcc, *build.ARCH, "-O3", "-std=c++17", "-Xptxas", "-v", "-c", str(src),
+                              "-o", str(tmp_path / (src.stem + ".o"))], capture_output=True, text=True)
+        assert res.returncode == 0, res.stderr[-2000:]
+        counts = re.findall(r"(\d+) bytes spill stores, (\d+) bytes spill loads", res.stderr)
+        assert counts, src.name
+        assert all(st == "0" and ld == "0" for st, ld in counts), (src.name, res.stderr[-2000:])
