@@ -148,5 +148,5 @@ def test_no_kernel_spills_registers(tmp_path):
                               "-o", str(tmp_path / (src.stem + ".o"))], capture_output=True, text=True)
         assert res.returncode == 0, res.stderr[-2000:]
         counts = re.findall(r"(\d+) bytes spill stores, (\d+) bytes spill loads", res.stderr)
-        assert counts, src.name
+        assert counts or "__global__" not in src.read_text(), src.name
         assert all(st == "0" and ld == "0" for st, ld in counts), (src.name, res.stderr[-2000:])
