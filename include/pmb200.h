@@ -93,11 +93,15 @@ typedef struct {
  * slots up to the highest one in use in each mesh size (slots are the peaks of one size, in
  * order); bit 3 = the native transform with the Green multiply fused (pm_rfft3_native) for
  * meshes 64^3-512^3 instead of cuFFT; bit 16 = bins without spare capacity (a test mode: almost
- * every step overflows a bin and relayouts; results are the same bit for bit). */
+ * every step overflows a bin and relayouts; results are the same bit for bit).
+ * Replaces: PM3D(N, L, Np, seed, smooth) (pm3d.py:27-37), once per peak. */
 int pm_engine_create(const pm_peak_cfg* cfg, int npeaks, int device, int flags, pm_engine** out);
+/* Free the engine's device memory, plans and graphs (no counterpart: the reference's arrays are
+ * garbage-collected). */
 int pm_engine_destroy(pm_engine* e);
+/* Wait for the engine's stream (no counterpart: the reference is synchronous). */
 int pm_engine_sync(pm_engine* e);
-/* Bytes of device memory the engine holds. */
+/* Bytes of device memory the engine holds (no counterpart; the served loop's HBM accounting). */
 long long pm_engine_device_bytes(const pm_engine* e);
 
 /* Load particles (lattice order) for one peak at expansion factor a0 and choose its schedule.
@@ -114,23 +118,28 @@ int pm_run(pm_engine* e, int nsteps);
  * adds each phase's device time (ms) into phase_ms[8]: push, energy + clock advance, regroup
  * (priming radix sort with its permutation, bin layouts, relayouts of peaks whose push
  * overflowed a bin), super-tile re-sort (refresh steps), deposit (with the face fix-up), R2C,
- * Green, C2R.  For per-kernel rooflines. */
+ * Green, C2R.  For per-kernel rooflines (no counterpart; the reference times nothing finer than
+ * the driver's wall clock, pbhgr/scripts/pm3d_peak.py:24,32,35). */
 int pm_run_timed(pm_engine* e, int nsteps, double* phase_ms);
-/* The engine's CUDA stream (cudaStream_t), for events and stream ordering by callers. */
+/* The engine's CUDA stream (cudaStream_t), for events and stream ordering by callers (no
+ * counterpart). */
 void* pm_engine_stream(pm_engine* e);
-/* info[6]: npeaks, particles, super-tiles, sort passes, mesh classes, device bytes. */
+/* info[6]: npeaks, particles, super-tiles, sort passes, mesh classes, device bytes (no
+ * counterpart). */
 int pm_engine_info(const pm_engine* e, long long* info);
 
 /* PM3D.step(a, da) for one peak (pm3d.py:117-129): a KDK step from a to a + da.  Forces at
  * a are reused when the peak's current state is at a (pm3d.py:119), else recomputed. */
 int pm_step_explicit(pm_engine* e, int peak, double a, double da);
 
-/* Current particles, float64, lattice order; p includes the closing kick. (PM3D.x, PM3D.p) */
+/* Current particles, float64, lattice order; p includes the closing kick.  Replaces: reading
+ * PM3D.x, PM3D.p (pm3d.py:67-68, 122-128). */
 int pm_get_particles(pm_engine* e, int peak, double* x, double* p);
 /* -grad Phi at the particles for expansion factor a, lattice order: the acc of
  * PM3D.forces(a) (pm3d.py:101-114) at the current positions. */
 int pm_get_acc(pm_engine* e, int peak, double a, double* acc);
-/* delta of the last deposit (N^3 float32): the delta returned by PM3D.step/forces. */
+/* delta of the last deposit (N^3 float32): the delta returned by PM3D.step/forces
+ * (pm3d.py:103-104, 129). */
 int pm_get_delta(pm_engine* e, int peak, float* delta);
 /* Float64 CIC counts of the current positions (N^3): PM3D.deposit(PM3D.x) (pm3d.py:81-89). */
 int pm_get_counts(pm_engine* e, int peak, double* counts);
@@ -138,10 +147,13 @@ int pm_get_counts(pm_engine* e, int peak, double* counts);
  * delta_collapse is recorded on the device (pm_clock_info.a_collapse); <= 0 disables.  With
  * stop != 0 the run ends there: the step on which the crossing is detected (the one after the
  * deposit that crossed) completes, the next applies its closing kick, and the peak goes idle at
- * the a that step reached. */
+ * the a that step reached.  No counterpart in pm3d.py, which defines no collapse time; the
+ * criterion reads the max delta that PM3D.step returns (pm3d.py:129), as the driver's rows do
+ * (pbhgr/scripts/pm3d_peak.py:30). */
 int pm_set_collapse_threshold(pm_engine* e, int peak, double delta_collapse, int stop);
 /* Free a peak's slot: it goes idle, its mesh is no longer transformed (dynamic mode).  Ordered
- * on the engine's stream after the work queued so far; returns without waiting. */
+ * on the engine's stream after the work queued so far; returns without waiting.  No counterpart
+ * (the reference's driver ends with its process, pbhgr/scripts/pm3d_peak.py:34-35). */
 int pm_release(pm_engine* e, int peak);
 
 /* Entry points of a request loop that never waits on the device between steps (the served form
@@ -171,10 +183,15 @@ int pm_get_delta_async(pm_engine* e, int peak, void* dst);
  * tile after it runs out after spin_limit polls; the sort then proceeds with that tile counted
  * as empty (every write stays inside the peak's range, the peak's result is wrong) and the
  * peak's status gets bit 1.  peak < 0 or spin_limit <= 0 restores the normal sort.  The peak
- * needs more than one sort tile (2048 particles); synchronizes the engine's stream. */
+ * needs more than one sort tile (2048 particles); synchronizes the engine's stream.  No
+ * counterpart (the reference has no device waits). */
 int pm_debug_sort_stall(pm_engine* e, int peak, int spin_limit);
-int pm_get_clock(pm_engine* e, int peak, pm_clock_info* out);   /* host struct */
-int pm_get_stats(pm_engine* e, int peak, pm_stats_info* out);   /* host struct */
+/* One peak's clock and statistics (host structs): the a and da of the driver loop
+ * (pbhgr/scripts/pm3d_peak.py:24-27), rho_max_over_mean of analyse (pm3d.py:158), max delta of
+ * the driver's rows (pm3d_peak.py:30), and the status word in the reference's convention for
+ * native code (a count of flagged items, pbhgr/csrc/kernels.c:36,73). */
+int pm_get_clock(pm_engine* e, int peak, pm_clock_info* out);
+int pm_get_stats(pm_engine* e, int peak, pm_stats_info* out);
 /* All peaks at once (host arrays of npeaks); the return value counts flagged peaks. */
 int pm_get_stats_all(pm_engine* e, pm_stats_info* out);
 int pm_get_clocks_all(pm_engine* e, pm_clock_info* out);
@@ -211,7 +228,8 @@ int pm_make_ic(const pm_ic_params* prm, double* x_out, double* p_out, double* de
  * issue them on one stream.  kind 0 returns -2003. */
 int pm_make_ic_async(const pm_ic_params* prm, double* x_out, double* p_out, void* stream);
 /* pm_make_ic and pm_make_ic_async keep their float64 work buffers and cuFFT plans per (device,
- * N) after the first call; this frees them. */
+ * N) after the first call; this frees them (no counterpart: the reference's make_ic keeps no
+ * state between calls, pm3d.py:40-73). */
 int pm_ic_release_cache(void);
 
 /* Stateless helpers. */
@@ -223,7 +241,8 @@ int pm_interp64(const double* F, const double* X, long long n, int N, double L, 
  * of N^3 unsigned 64-bit words.  Synchronizes the device. */
 int pm_deposit64(const double* X, long long n, int N, double L, unsigned long long* work, double* counts);
 /* Stable sort of n 64-bit keys over bits [lo, hi): keys_out, perm_out (original indices).
- * tmp_keys/tmp_vals are caller scratch of n entries each. */
+ * tmp_keys/tmp_vals are caller scratch of n entries each.  Replaces the argsorts of analyse
+ * (pm3d.py:137, 145) and the sort of cell keys that deposit and interp need for unsorted X. */
 int pm_sort_u64(const unsigned long long* keys, unsigned long long* keys_out, unsigned int* perm_out,
                 unsigned long long* tmp_keys, unsigned int* tmp_vals, long long n, int lo, int hi);
 /* Diagnostics of analyse (pm3d.py:132-159).  pm_rell_keys: the Lagrangian ellipsoidal radius
@@ -268,7 +287,8 @@ int pm_irfft3_256(const void* spec, void* work, float* x, int nfields, void* str
 #define PM_NOALLOC_SCRATCH_BYTES (3670016)
 int pm_sort_u64_noalloc(const unsigned long long* keys, unsigned long long* keys_out, unsigned int* perm_out,
                         long long n, int lo, int hi, void* stream);
-/* Sort keys (Morton code of the CIC cell) of split positions, host pointers; for tests. */
+/* Sort keys (Morton code of the CIC cell) of split positions, host pointers; for tests (no
+ * counterpart: the reference indexes cells directly, pm3d.py:76-79). */
 int pm_cell_keys(const int* cells, long long n, int N, int tile, unsigned int* keys_out);
 
 #ifdef __cplusplus
