@@ -1,6 +1,7 @@
 """Host-side logic that needs no GPU: the benchmark recipes, the served stream's arrivals,
-latency summary and slot budget, the benchmark's launch and byte accounting, its CPU sample and
-reference-arm line, and the error mapping of the C ABI's return codes."""
+latency summary, slot budget and retire/fail/cancel decisions (the device replaced by a script),
+the benchmark's launch and byte accounting, its CPU sample and reference-arm line, and the error
+mapping of the C ABI's return codes."""
 import sys
 from pathlib import Path
 
@@ -275,3 +276,105 @@ def test_reference_arm_prints_one_contract_line(monkeypatch, capsys):
     monkeypatch.setenv("RANK", "1")                      # other ranks of a multi-GPU launch print nothing
     bench.run_reference(args)
     assert capsys.readouterr().out.strip() == ""
+
+
+class _FakeEvent:
+    def record(self, stream=None):
+        pass
+
+    def query(self):
+        return True
+
+    def synchronize(self):
+        pass
+
+
+class _FakeTorch:
+    """The few torch calls the served loop's retire path makes, on the CPU."""
+    float32 = None
+
+    class cuda:
+        Event = _FakeEvent
+
+    @staticmethod
+    def empty(n, dtype=None, pin_memory=False):
+        import torch
+        return torch.zeros(n, dtype=torch.float32)
+
+
+class _FakeServedLib:
+    """Stands in for libpmb200's served-loop entry points: pm_snapshot_read fills the clocks and
+    statistics from a script, pm_release and pm_get_delta_async record their calls."""
+
+    def __init__(self, script):
+        self.script, self.released, self.delta_copies = script, [], []
+
+    def pm_snapshot_read(self, h, slot, wait, clocks, stats):
+        for peak, (state, nsteps, a_collapse, status) in self.script.items():
+            clocks[peak].state, clocks[peak].nsteps, clocks[peak].a_collapse = state, nsteps, a_collapse
+            stats[peak].status = status
+        return 0
+
+    def pm_release(self, h, peak):
+        self.released.append(peak)
+        return 0
+
+    def pm_get_delta_async(self, h, peak, dst):
+        self.delta_copies.append(peak)
+        return 0
+
+
+def _server_on_fakes(script, nslots=3, N=8):
+    """A Server whose engine is replaced by `_FakeServedLib` (its host-side bookkeeping only)."""
+    import collections
+    import time
+
+    from pbh_b200 import _lib
+    from pbh_b200.serve import Server, ServerConfig
+    srv = Server.__new__(Server)
+    srv.cfg = ServerConfig(slots={N: nslots}, keep_delta=True)
+    srv._lib, srv._h, srv._torch, srv._estream = _FakeServedLib(script), None, _FakeTorch, None
+    srv.slot_N = [N] * nslots
+    srv.free = {N: collections.deque()}          # every slot busy
+    srv.active, srv.queue, srv.done = {}, collections.deque(), []
+    srv._finishing, srv._pending, srv._pinned = [], collections.deque(), {N: []}
+    srv._clocks = (_lib.ClockInfo * nslots)()
+    srv._stats = (_lib.StatsInfo * nslots)()
+    srv.bytes_in_use, srv.engine_steps, srv._t0 = 0, 5, time.perf_counter()
+    return srv
+
+
+def test_served_loop_retires_fails_and_cancels_runs_on_the_host():
+    """The served loop's decisions from a step's snapshot, with the device replaced by a script:
+    a peak whose clock went idle completes (collapse a in the config's units, its delta copied
+    out behind the running work), a peak whose status word is nonzero fails while the others go
+    on, a run loaded after the snapshot was taken is not judged by it, and cancelling frees a
+    running slot or drops a queued request.  Every freed slot returns to the pool."""
+    from pbh_b200 import _lib, recipe
+    from pbh_b200.serve import Request, slot_bytes
+    N = 8
+    script = {0: (_lib.STATE_IDLE, 40, 55.0, 0),      # collapsed at a_pm = 55 -> a_cfg = 0.55
+              1: (_lib.STATE_RUN, 12, -1.0, 0x1),     # non-finite momentum
+              2: (_lib.STATE_IDLE, 0, -1.0, 0)}       # loaded after the snapshot: not judged yet
+    srv = _server_on_fakes(script, N=N)
+    spec = recipe.ensemble(npeaks=1, sizes=(N,), seed=2)[0]
+    reqs = [Request(rid=i, spec=spec, t_arrival=0.0) for i in range(4)]
+    for slot, admit in ((0, 3), (1, 3), (2, 6)):
+        reqs[slot].slot, reqs[slot].admit_step = slot, admit
+        srv.active[slot] = reqs[slot]
+        srv.bytes_in_use += slot_bytes(N)
+    srv.queue.append(reqs[3])
+    srv._read_snapshot(4)
+    assert srv._lib.released == [0, 1] and srv._lib.delta_copies == [0]
+    failed = [r for r in srv.done if not r.ok]
+    assert [r.rid for r in failed] == [1] and failed[0].status == 1 and "0x1" in failed[0].error
+    assert list(srv.active) == [2] and [r.rid for r, _, _ in srv._finishing] == [0]
+    srv._collect(lambda: 1.0)
+    done0 = next(r for r in srv.done if r.rid == 0)
+    assert done0.ok and done0.steps == 40 and done0.a_collapse_cfg == pytest.approx(0.55)
+    assert done0.delta.shape == (N, N, N) and done0.t_done == 1.0
+    assert srv.cancel(2, now=2.0) and srv.cancel(3, now=2.0) and not srv.cancel(99, now=2.0)
+    assert srv._lib.released == [0, 1, 2] and not srv.active and not srv.queue
+    assert {r.rid: r.error for r in srv.done if not r.ok} == {1: "device status 0x1", 2: "cancelled",
+                                                            3: "cancelled"}
+    assert sorted(srv.free[N]) == [0, 1, 2] and srv.bytes_in_use == 0
