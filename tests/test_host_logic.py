@@ -378,3 +378,64 @@ def test_served_loop_retires_fails_and_cancels_runs_on_the_host():
     assert {r.rid: r.error for r in srv.done if not r.ok} == {1: "device status 0x1", 2: "cancelled",
                                                             3: "cancelled"}
     assert sorted(srv.free[N]) == [0, 1, 2] and srv.bytes_in_use == 0
+
+
+def test_served_admission_waits_for_a_slot_an_ic_buffer_and_budget():
+    """Admission on the host, the device replaced by recorders: a queued request starts only when
+    its mesh size has a free slot, an initial-condition buffer whose last load has finished, and
+    room under the HBM budget; the others keep their order in the queue."""
+    import collections
+
+    from pbh_b200 import recipe
+    from pbh_b200.serve import Request, slot_bytes
+    N = 8
+
+    class Ev(_FakeEvent):
+        done = False                                   # the engine's stream has passed every load
+        cuda_event = None
+
+        def query(self):
+            return Ev.done
+
+    class Buf:                                         # serve._ICBuffer with host stand-ins
+        def __init__(self, loaded):
+            self.loaded = loaded
+            self.x = self.p = type("T", (), {"data_ptr": lambda self: 0})()
+
+        def ready(self):
+            return self.loaded is None or self.loaded.query()
+
+    calls = []
+
+    class Lib(_FakeServedLib):
+        def pm_make_ic_async(self, prm, x, p, stream):
+            prm = prm._obj                              # ctypes.byref(ICParams)
+            calls.append(("ic", prm.N, prm.noise_seed))
+            return 0
+
+        def pm_load_peak(self, h, slot, *args):
+            calls.append(("load", slot))
+            return 0
+
+    srv = _server_on_fakes({}, nslots=3, N=N)
+    srv._lib = Lib({})
+    srv._torch = type("FT", (), {"cuda": type("C", (), {"Event": Ev})})
+    srv._icstream = type("S", (), {"cuda_stream": None})()
+    srv.free = {N: collections.deque([0, 1, 2])}
+    srv._icbuf = {N: [Buf(None), Buf(Ev())]}           # one buffer free, one still loading
+    spec = recipe.ensemble(npeaks=1, sizes=(N,), seed=2)[0]
+    for i in range(3):
+        srv.queue.append(Request(rid=i, spec=spec, t_arrival=0.0))
+    srv._admit(0.0)
+    assert list(srv.active) == [0] and [r.rid for r in srv.queue] == [1, 2]
+    assert calls == [("ic", N, spec.seed + 1), ("load", 0)] and srv.bytes_in_use == slot_bytes(N)
+    # the loads have finished, so both buffers are free again, but the budget holds one more slot
+    Ev.done = True
+    srv.cfg.budget_bytes = 2 * slot_bytes(N)
+    srv._admit(1.0)
+    assert sorted(srv.active) == [0, 1] and [r.rid for r in srv.queue] == [2]
+    srv._admit(2.0)                                    # buffers free, slot free, budget full
+    assert sorted(srv.active) == [0, 1] and [r.rid for r in srv.queue] == [2]
+    srv.cfg.budget_bytes = 150e9
+    srv._admit(3.0)
+    assert sorted(srv.active) == [0, 1, 2] and not srv.queue and srv.active[2].admit_step == srv.engine_steps
